@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the complex-coordinate FMM on B200: targets/sec at eps=1e-9.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+One step = one FMM solve (tree, lists, all eight passes, unsort) of the
+workload's synthetic inputs.  `value` is measured through the device-pointer C
+entry point with the inputs resident in HBM; `e2e` through the host-array C
+entry point (the drop-in call) with the inputs in pinned host memory, so each
+step includes the host->device copy of the inputs and the device->host copy of
+pot/grad.  Between timed steps L2 is flushed by writing a 256 MiB buffer
+(outside the timed events).  Multi-GPU: one process per GPU, each solving an
+independent replica (a single FMM is not sharded), value = all ranks' targets
+/ max-over-ranks time; scaling "weak".
+
+--impl reference times the reference algorithm on the host cores: the
+reference Fortran cannot be built on this image (no Fortran compiler), so it
+runs the C restatement in oracle/ with all host threads (OpenMP), on a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # zlfmm2d plain single solve, 20,000 points (sources = targets), charges +
+    # dipoles, pot + grad, isep=1, eps=1e-9
+    "zlfmm2d_uniform_20k": dict(kind="lap2d", n=20000, eps=1e-9, ifpgh=2, isep=1),
+}
+DEFAULT_WORKLOAD = "zlfmm2d_uniform_20k"
+
+# Algorithmic work per interaction (real flops; complex add 2, mul 6, div 11;
+# transcendental functions are not counted), per the frozen convention of the
+# project's measurement plan.  P = 2p+1 coefficients.
+#   P2P 2D Laplace pair (pot+grad, charge+dipole): 70 flops
+#   M2T / L2T (target, expansion) with gradient: 3 complex MACs per coefficient = 24 P
+#   M2L / M2M / L2L 2D: one dense P x P complex operator = 8 P^2
+#   P2M / P2L per source: 2 complex MACs per coefficient = 16 P
+def flop_model(kind, counts, p):
+    P = 2 * p + 1
+    if kind == "lap2d":
+        per = dict(p2p_pairs=70, m2t=24 * P, l2t=24 * P, m2l_pairs=8 * P * P, p2l=16 * P,
+                   m2m_pairs=8 * P * P, l2l_pairs=8 * P * P, p2m=16 * P)
+    else:
+        raise ValueError(kind)
+    steps = {
+        "p2m": counts["p2m"] * per["p2m"],
+        "m2m": counts["m2m_pairs"] * per["m2m_pairs"],
+        "m2l_p2l": counts["m2l_pairs"] * per["m2l_pairs"] + counts["p2l"] * per["p2l"],
+        "l2l": counts["l2l_pairs"] * per["l2l_pairs"],
+        "eval": counts["p2p_pairs"] * per["p2p_pairs"] + counts["m2t"] * per["m2t"]
+        + counts["l2t"] * per["l2t"],
+    }
+    return steps, per
+
+
+def make_inputs(wl, seed):
+    from zfmm_b200 import workloads as W
+    if wl["kind"] == "lap2d":
+        return W.lap2d_uniform(wl["n"], seed=seed)
+    raise ValueError(wl["kind"])
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_time_oracle(wl, inp, reps_min=1, budget_s=15.0):
+    """Oracle (C restatement, OpenMP) on the host cores; returns (sec per solve, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    cores = os.cpu_count() or 1
+    z = inp["zsrc"].T
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < reps_min or (time.perf_counter() < t_end and len(times) < 50):
+        t0 = time.perf_counter()
+        if wl["kind"] == "lap2d":
+            O.zlfmm2d(wl["eps"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
+                      ifpgh=wl["ifpgh"], isep=wl["isep"])
+        times.append(time.perf_counter() - t0)
+        if len(times) == 1 and times[0] > budget_s:
+            break
+    return statistics.median(times), cores, len(times)
+
+
+def run_reference(args, wl, ws, rank):
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    inp = make_inputs(wl, seed=0)
+    nt = wl["n"]
+    for _ in range(args.warmup):
+        cpu_time_oracle(wl, inp, reps_min=1, budget_s=0.0)
+    per = []
+    for _ in range(args.steps):
+        t, cores, _n = cpu_time_oracle(wl, inp, reps_min=1, budget_s=0.0)
+        per.append(t)
+    tot = sum(per)
+    value = nt * args.steps / tot
+    line = {
+        "impl": "reference", "metric": "targets/sec at eps=1e-9", "value": value,
+        "unit": "targets/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, "n": nt, "eps": wl["eps"], "ifpgh": wl["ifpgh"],
+                   "isep": wl["isep"], "l2": "n/a (host)"},
+        "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "port",
+                         "sample": f"full workload, {args.steps} solves"},
+        "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, wl, ws, rank, local):
+    import ctypes
+
+    import torch
+
+    import zfmm_b200
+    from zfmm_b200 import _capi
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _capi.lib()
+    inp = make_inputs(wl, seed=rank)
+    n = wl["n"]
+    ifpgh, isep, eps = wl["ifpgh"], wl["isep"], wl["eps"]
+    # device-resident inputs (Fortran layout = (n, 2) row-major complex128)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    zs = t(inp["zsrc"].T)
+    q, ds, dv = t(inp["charge"]), t(inp["dipstr"]), t(inp["dipvec"].T)
+    pot = torch.empty(n, dtype=torch.complex128, device=dev)
+    grad = torch.empty((n, 2), dtype=torch.complex128, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+
+    def solve():
+        _capi.check(L.zfmm_zlfmm2d_dev(eps, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot), P(grad),
+                                       n, P(zs), ifpgh, isep, sp))
+
+    for _ in range(max(args.warmup, 3)):
+        solve()
+    torch.cuda.synchronize()
+    # counts and per-step structure from one instrumented call (not timed)
+    L.zfmm_set_step_timing(2)
+    solve()
+    counts, _ = zfmm_b200.last_counts()
+    _, info = zfmm_b200.last_step_times()
+    L.zfmm_set_step_timing(1)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    step_ms = {k: 0.0 for k in ["setup", "p2m", "m2m", "m2l_p2l", "l2l", "eval", "unsort"]}
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.zfmm_launch_count()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            ev0[k].record(stream)
+            solve()
+            ev1[k].record(stream)
+            st, _ = zfmm_b200.last_step_times()
+            for kk in step_ms:
+                step_ms[kk] += st[kk]
+        torch.cuda.synchronize()
+    launches = L.zfmm_launch_count() - launches0
+    L.zfmm_set_step_timing(0)
+    tot_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    value = ws * n * args.steps / (tot_ms * 1e-3)
+
+    # end to end through the host-array entry point, pinned host inputs
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hz, hq, hds, hdv = pin(inp["zsrc"].T), pin(inp["charge"]), pin(inp["dipstr"]), pin(inp["dipvec"].T)
+    hpot = torch.empty(n, dtype=torch.complex128).pin_memory().numpy()
+    hgrad = torch.empty((n, 2), dtype=torch.complex128).pin_memory().numpy()
+    hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def solve_host():
+        _capi.check(L.zfmm_zlfmm2d(eps, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv), hp(hpot),
+                                   hp(hgrad), n, hp(hz), ifpgh, isep, 0))
+
+    solve_host()
+    if ws > 1:
+        dist.barrier()
+    e2e_t = []
+    for k in range(args.steps):
+        flush.fill_(k & 255)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solve_host()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_tot = sum(e2e_t)
+    if ws > 1:
+        tt = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_tot = float(tt.item())
+    h2d = hz.nbytes * 1 + hq.nbytes + hds.nbytes + hdv.nbytes + hz.nbytes  # zsrc, ztarg
+    d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
+    # accuracy against the direct sum on a seeded subset of targets (device direct sum)
+    pg = pot.cpu().numpy()
+    rng = np.random.default_rng(1234)
+    sub = np.sort(rng.choice(n, size=min(n, 4096), replace=False))
+    pd, _ = zfmm_b200.zl2devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                     inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
+    relerr = float(np.linalg.norm(pg[sub] * 2 * np.pi - pd) / np.linalg.norm(pd))
+
+    # roofline of the dominant kernel (FP64 pipe bound)
+    p = info["nterms"]
+    flops, per = flop_model(wl["kind"], counts, p)
+    avg = {k: v / args.steps for k, v in step_ms.items()}
+    top = max(flops, key=lambda k: avg[k])
+    achieved = flops[top] / (avg[top] * 1e-3) / 1e12
+    peak = float(L.zfmm_probe_fp64_tflops(20000))
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"{args.workload}_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(top)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        t_cpu, cores, nrep = cpu_time_oracle(wl, inp, reps_min=1, budget_s=12.0)
+        cpu = {"value": n / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
+               "sample": f"full workload (n={n}), median of {nrep} solves"}
+    if rank != 0:
+        return
+    line = {
+        "metric": "targets/sec at eps=1e-9", "value": value, "unit": "targets/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "eps": eps, "ifpgh": ifpgh, "isep": isep,
+                   "charges": True, "dipoles": True, "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": f"replicas x{ws}", "nboxes": info["nboxes"],
+                   "nlevels": info["nlevels"], "nterms": p},
+        "e2e": {"value": ws * n * args.steps / e2e_tot, "unit": "targets/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "rel_l2_err_vs_direct": relerr,
+        "step_ms": {k: round(v, 4) for k, v in avg.items()},
+        "roofline": {"bound": "fp64", "kernel": top, "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None,
+                     "peak_source": "measured FP64 FMA probe (zfmm_probe_fp64_tflops)",
+                     "traffic": traffic, "flops_per_step": flops[top],
+                     "flop_model": per},
+        "interactions": counts,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, wl, ws, rank)
+        else:
+            run_ours(args, wl, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

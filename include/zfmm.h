@@ -1,0 +1,110 @@
+/*
+ * zfmm_b200 C ABI: B200 (sm_100a) complex-coordinate fast multipole methods.
+ *
+ * Complex arrays are interleaved (re, im) doubles in Fortran column-major
+ * order, exactly the memory of the reference's `complex *16` arrays:
+ *   zsrc(d, ns)  -> double[2*d*ns]   (point i, coordinate k at 2*(d*i+k))
+ *   charge(ns), dipstr(ns) -> double[2*ns]
+ *   dipvec(d, ns) -> double[2*d*ns], pot(nt) -> double[2*nt],
+ *   grad(d, nt) -> double[2*d*nt]
+ * Integers are 32-bit (the reference's default INTEGER).
+ *
+ * Two families of entry points:
+ *   zlfmm2d_ ...            Fortran-callable (every argument by reference, host
+ *                           arrays, trailing underscore); drop-in replacements
+ *                           for the reference subroutines.  Like the reference
+ *                           they sanitise ifcharge/ifdipole/ifpgh in place and
+ *                           report no status (a failure leaves pot/grad zero
+ *                           and is readable through zfmm_last_error()).
+ *   zfmm_zlfmm2d ...        C entry points returning a status (0 = success),
+ *                           host arrays; the *_dev variants take device
+ *                           pointers and a cudaStream_t (as void*).
+ *
+ * Status codes: 0 ok, 1 bad argument, 2 CUDA error, 3 out of device memory,
+ * 4 internal error, 5 the CUDA library is unavailable (no GPU).
+ */
+#ifndef ZFMM_B200_H
+#define ZFMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces zlfmm2d (zfmm2d/src/laplace/zlfmm2d.f:14-15; MATLAB spec
+ * zfmm2d/matlab_linux/zlfmm2d.mw:7).  pot = sum q log(R)/2pi - ..., see the
+ * reference header comment (zlfmm2d.f:1-12). */
+void zlfmm2d_(const double *eps, const int *ns, const double *zsrc, int *ifcharge,
+              const double *charge, int *ifdipole, const double *dipstr, const double *dipvec,
+              double *pot, double *grad, const int *nt, const double *ztarg, int *ifpgh,
+              const int *isep, const int *ifprint);
+
+/* Replaces zl2devaldirect (zfmm2d/src/laplace/zlfmm2d.f:600-601; MATLAB spec
+ * zfmm2d/matlab_linux/zl2devaldirect.mw:6).  Adds the UNSCALED sums
+ * (no 1/2pi) into pot/grad, as the reference routine does. */
+void zl2devaldirect_(const int *nt, const double *ztarg, const int *ns, const double *zsrc,
+                     const double *charge, const double *dipstr, const double *dipvec,
+                     const int *ifcharge, double *pot, double *grad, const int *ifdipole,
+                     const int *ifpgh);
+
+/* C forms of the above (host arrays).  Flags are not modified; out-of-range
+ * flags are clamped the same way as the reference (zlfmm2d.f:58-68). */
+int zfmm_zlfmm2d(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
+                 int ifdipole, const double *dipstr, const double *dipvec, double *pot,
+                 double *grad, int nt, const double *ztarg, int ifpgh, int isep, int ifprint);
+int zfmm_zl2devaldirect(int nt, const double *ztarg, int ns, const double *zsrc,
+                        const double *charge, const double *dipstr, const double *dipvec,
+                        int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
+
+/* Device-pointer forms: every array is device memory, work is queued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream).  The FMM returns
+ * after its results are complete on that stream. */
+int zfmm_zlfmm2d_dev(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
+                     int ifdipole, const double *dipstr, const double *dipvec, double *pot,
+                     double *grad, int nt, const double *ztarg, int ifpgh, int isep,
+                     void *stream);
+int zfmm_zl2devaldirect_dev(int nt, const double *ztarg, int ns, const double *zsrc,
+                            const double *charge, const double *dipstr, const double *dipvec,
+                            int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh,
+                            void *stream);
+
+/* Per-step device times (ms) of the last FMM call on this host thread:
+ * [set-up, P2M, M2M, M2L+P2L, L2L, P2P+M2T+L2T, unsort], plus nboxes, nlevels
+ * and the expansion order.  Recording adds CUDA events; enable with
+ * zfmm_set_step_timing(1); level 2 also counts the interactions (one more
+ * kernel and a stream synchronisation after the solve). */
+void zfmm_set_step_timing(int on);
+int zfmm_last_step_times(double *ms7, int *nboxes, int *nlevels, int *nterms);
+/* Interaction counts of the last timed FMM call: [P2P pairs, M2T (target,
+ * box), L2T targets, M2L box pairs, P2L (box, source), M2M pairs, L2L pairs,
+ * P2M sources], and the number of kernels the call launched. */
+int zfmm_last_counts(long long *counts8, long *launches);
+/* Kernels launched by this library on the calling host thread so far. */
+long zfmm_launch_count(void);
+
+/* Tree inspection (tests and tools): builds the device tree for real parts of
+ * zsrc/ztarg (host arrays, dimension D = 2 or 3) exactly as the D-dimensional
+ * driver does for leaf size `ndiv`, and copies it back.  Box numbers are
+ * 0-based, -1 = none.  Call once with box_cap = 0 to learn nboxes/nlevels.
+ * Arrays: laddr[2*(nlevels+1)], ilevel/iparent/nchild[nboxes],
+ * ichild[2^D*nboxes], centers[D*nboxes], isrc[ns], isrcse[2*nboxes],
+ * itarg[nt], itargse[2*nboxes], nlist[4*nboxes], lists (the lists of every
+ * box concatenated, list k = 0..3 outermost), mnlist[4]. */
+int zfmm_tree_dump(int D, int ndiv, int isep, int ns, const double *zsrc, int nt,
+                   const double *ztarg, int box_cap, int list_cap, int *nboxes, int *nlevels,
+                   int *laddr, int *ilevel, int *iparent, int *nchild, int *ichild,
+                   double *centers, int *isrc, int *isrcse, int *itarg, int *itargse, int *nlist,
+                   int *lists, int *nlists_total, int *mnlist);
+
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (roofline
+ * denominator for the FP64-bound kernels); -1 on error. */
+double zfmm_probe_fp64_tflops(int iters);
+
+/* Last error message of this host thread ("" when none). */
+const char *zfmm_last_error(void);
+/* Library version string. */
+const char *zfmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -60,7 +60,7 @@ void o_zl2devaldirect(int nt, const double *ztarg, int ns, const double *zsrc,
       cplx x1my1 = -y1mx1, x2my2 = -y2mx2;
       cplx rsq = y1mx1 * y1mx1 + y2mx2 * y2mx2;
       cplx rz = csqrt(rsq);
-      if (cabs(rz) > 1e-16) {
+      if (cabs(rz) > (double)1e-16f) {  /* REAL*4 literal 1E-16 */
         if (ifcharge == 1) pi += q[j] * clog(rz);
         if (ifdipole == 1) pi -= ds[j] * (dv[2 * j] * y1mx1 + dv[2 * j + 1] * y2mx2) / rsq;
         if (ifpgh > 1) {

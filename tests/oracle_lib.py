@@ -120,7 +120,7 @@ def tree_dump(D, ndiv, zsrc, ztarg=None, isep=1):
     flat = np.zeros(cap, np.int32)
     f = lib().o_tree_dump
     f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
-                  ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 12 + [ctypes.c_int]
+                  ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 11 + [ctypes.c_int]
     n = f(D, ndiv, _p(zsrc), ns, _p(ztarg), nt, isep, _p(out["ilevel"]), _p(out["iparent"]),
           _p(out["nchild"]), _p(out["ichild"]), _p(out["centers"]), _p(out["isrc"]),
           _p(out["isrcse"]), _p(out["itarg"]), _p(out["itargse"]), _p(out["nlist"]), _p(flat),
@@ -129,3 +129,86 @@ def tree_dump(D, ndiv, zsrc, ztarg=None, isep=1):
     out["lists_flat"] = flat[:n]
     out.update(info)
     return out
+
+
+def hank103(z):
+    f = lib().o_hank103
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    a = np.zeros(2)
+    b = np.zeros(2)
+    f(float(np.real(z)), float(np.imag(z)), _p(a), _p(b))
+    return a[0] + 1j * a[1], b[0] + 1j * b[1]
+
+
+def h2dterms(bsize, zk, eps, isep=1):
+    f = lib().o_h2dterms
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    f.restype = ctypes.c_int
+    return f(bsize, zk.real, zk.imag, eps, isep)
+
+
+def jbessel2d(nterms, z, rscale, ifder=0):
+    f = lib().o_jbessel2d
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_void_p]
+    a = np.zeros(nterms + 2, np.complex128)
+    d = np.zeros(nterms + 2, np.complex128)
+    f(nterms, z.real, z.imag, rscale, _p(a), ifder, _p(d))
+    return a[:nterms + 1], d[:nterms + 1]
+
+
+def h2dall(nterms, z, rscale, ifder=0):
+    f = lib().o_h2dall
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_void_p]
+    a = np.zeros(nterms + 2, np.complex128)
+    d = np.zeros(nterms + 2, np.complex128)
+    f(nterms, z.real, z.imag, rscale, _p(a), ifder, _p(d))
+    return a[:nterms + 1], d[:nterms + 1]
+
+
+def zhfmm2d(eps, zk, zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1, isep=1):
+    """Oracle zhfmm2d (scaled by i/4 like the reference); arrays (n,2) complex."""
+    zsrc = c128(zsrc)
+    ns = zsrc.shape[0]
+    ztarg = zsrc if ztarg is None else c128(ztarg)
+    nt = ztarg.shape[0]
+    ifc = 0 if charge is None else 1
+    ifd = 0 if dipstr is None else 1
+    q = c128(charge) if ifc else np.zeros(1, np.complex128)
+    ds = c128(dipstr) if ifd else np.zeros(1, np.complex128)
+    dv = c128(dipvec) if ifd else np.zeros((1, 2), np.complex128)
+    zkv = np.array([complex(zk).real, complex(zk).imag])
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((nt, 2), np.complex128)
+    f = lib().o_zhfmm2d
+    f.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_int, ctypes.c_int]
+    rc = f(eps, _p(zkv), ns, _p(zsrc), ifc, _p(q), ifd, _p(ds), _p(dv), _p(pot), _p(grad), nt,
+           _p(ztarg), ifpgh, isep, 0)
+    assert rc == 0
+    return pot, grad
+
+
+def zh2ddirect(zk, zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1):
+    """Unscaled zh2devaldirect (no i/4), as in the reference."""
+    zsrc = c128(zsrc)
+    ztarg = zsrc if ztarg is None else c128(ztarg)
+    ns, nt = zsrc.shape[0], ztarg.shape[0]
+    ifc = 0 if charge is None else 1
+    ifd = 0 if dipstr is None else 1
+    q = c128(charge) if ifc else np.zeros(1, np.complex128)
+    ds = c128(dipstr) if ifd else np.zeros(1, np.complex128)
+    dv = c128(dipvec) if ifd else np.zeros((1, 2), np.complex128)
+    zkv = np.array([complex(zk).real, complex(zk).imag])
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((nt, 2), np.complex128)
+    f = lib().o_zh2devaldirect
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    f(_p(zkv), nt, _p(ztarg), ns, _p(zsrc), _p(q), _p(ds), _p(dv), ifc, _p(pot), _p(grad), ifd,
+      ifpgh)
+    return pot, grad

@@ -1,0 +1,66 @@
+"""CPU-side checks of the product library: it is built, loads without a GPU,
+exports every entry point declared in include/zfmm.h, and fails loudly (a
+status, no crash, no silent CPU fallback) when no GPU is present."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "zfmm.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?(?:void|int|double|char)\s*\*?\s*(\w+)\s*\(", src,
+                       flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ["zlfmm2d_", "zl2devaldirect_", "zfmm_zlfmm2d", "zfmm_zlfmm2d_dev",
+              "zfmm_zl2devaldirect", "zfmm_last_error"]:
+        assert n in names
+
+
+def test_library_loads_and_exports_all_symbols():
+    from zfmm_b200 import _capi
+    if not os.path.exists(_capi.LIB_PATH):
+        import zfmm_b200.build as b
+        b.build(verbose=False)
+    L = ctypes.CDLL(_capi.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    # the Python binding declares a signature for every exported C function
+    assert set(declared_functions()) <= set(_capi.SIGNATURES)
+
+
+def test_version_string():
+    import zfmm_b200
+    assert "sm_100a" in zfmm_b200.version()
+
+
+def test_no_gpu_is_an_error_not_a_fallback():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    import zfmm_b200
+    z = np.zeros((2, 4), np.complex128)
+    z[0] = np.arange(4)
+    with pytest.raises(zfmm_b200.ZfmmError, match="status 5"):
+        zfmm_b200.zlfmm2d(1e-6, 4, z, 1, np.ones(4), 0, None, None, 4, z, 1, 1)
+
+
+def test_argument_errors_are_reported():
+    import zfmm_b200
+    z = np.zeros((2, 4), np.complex128)
+    with pytest.raises(ValueError):
+        zfmm_b200.zlfmm2d(1e-6, 4, z[:, :3], 1, np.ones(4), 0, None, None, 4, z, 1, 1)
+    L = zfmm_b200.lib()
+    rc = L.zfmm_zlfmm2d(1e-6, -1, None, 1, None, 0, None, None, None, None, 1, None, 1, 1, 0)
+    assert rc == 1
+    assert b"ns and nt" in L.zfmm_last_error()

@@ -1,0 +1,180 @@
+"""zfmm_b200: complex-coordinate fast multipole methods on NVIDIA B200 (sm_100a).
+
+Python mirror of the reference's MATLAB/mwrap interface
+(zfmm2d/matlab_linux/zlfmm2d.mw:1, zl2devaldirect.mw:1): same names, same
+argument order and meaning, arrays in the reference's shapes:
+
+    pot, grad = zlfmm2d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr,
+                        dipvec, nt, ztarg, ifpgh, isep)
+
+zsrc/ztarg/dipvec are (2, n) complex arrays (MATLAB column layout), charge and
+dipstr (n,) complex, pot (nt,), grad (2, nt).  numpy inputs run through the
+host-array C entry point; torch CUDA tensors (complex128, shaped (n, 2) or
+(2, n) in Fortran order) run through the device entry point on the current
+stream.  Everything executes on the GPU; there is no CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from ._capi import ZfmmError, check, lib
+
+__all__ = ["zlfmm2d", "zl2devaldirect", "tree_dump", "ZfmmError", "set_step_timing",
+           "last_step_times", "version"]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _pts(z, d, n, name):
+    """(d, n) complex -> Fortran-ordered complex128 array (memory of zsrc(d,n))."""
+    a = np.asarray(z, dtype=np.complex128)
+    if a.shape == (n, d) and d != n:
+        a = a.T
+    if a.shape != (d, n):
+        raise ValueError(f"{name} must have shape ({d}, {n}), got {a.shape}")
+    return np.asfortranarray(a)
+
+
+def _vec(v, n, name):
+    a = np.ascontiguousarray(np.asarray(v, dtype=np.complex128).reshape(-1))
+    if a.size != n:
+        raise ValueError(f"{name} must have {n} entries, got {a.size}")
+    return a
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _torch_pts(x, d, n, name):
+    import torch
+    if x.dtype != torch.complex128 or not x.is_cuda:
+        raise ValueError(f"{name} must be a complex128 CUDA tensor")
+    if tuple(x.shape) == (n, d):
+        x = x.contiguous()
+    elif tuple(x.shape) == (d, n):
+        x = x.t().contiguous()
+    else:
+        raise ValueError(f"{name} must have shape ({n}, {d}) or ({d}, {n})")
+    return x
+
+
+def zlfmm2d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
+            isep=1):
+    """2D Laplace FMM with complex coordinates (reference zlfmm2d.f:14-234).
+
+    pot(i) = sum_j charge_j log(R_ij)/(2 pi) - dipstr_j <dipvec_j, grad_y log R_ij>/(2 pi),
+    R = sqrt((x1-y1)^2 + (x2-y2)^2) on the principal branch.  Returns (pot, grad).
+    """
+    if _is_torch(zsrc):
+        return _zlfmm2d_torch(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt,
+                              ztarg, ifpgh, isep)
+    ns, nt = int(ns), int(nt)
+    zs = _pts(zsrc, 2, ns, "zsrc")
+    zt = _pts(ztarg, 2, nt, "ztarg")
+    q = _vec(charge, ns, "charge") if ifcharge == 1 else None
+    ds = _vec(dipstr, ns, "dipstr") if ifdipole == 1 else None
+    dv = _pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((2, nt), np.complex128, order="F")
+    check(lib().zfmm_zlfmm2d(float(eps), ns, _ptr(zs), int(ifcharge), _ptr(q), int(ifdipole),
+                             _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt, _ptr(zt), int(ifpgh),
+                             int(isep), 0))
+    return pot, grad
+
+
+def _zlfmm2d_torch(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh,
+                   isep):
+    import torch
+    zs = _torch_pts(zsrc, 2, ns, "zsrc")
+    zt = _torch_pts(ztarg, 2, nt, "ztarg")
+    dev = zs.device
+    q = charge.contiguous() if ifcharge == 1 else None
+    ds = dipstr.contiguous() if ifdipole == 1 else None
+    dv = _torch_pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
+    pot = torch.empty(nt, dtype=torch.complex128, device=dev)
+    grad = torch.empty((nt, 2), dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+    check(lib().zfmm_zlfmm2d_dev(float(eps), int(ns), p(zs), int(ifcharge), p(q), int(ifdipole),
+                                 p(ds), p(dv), p(pot), p(grad), int(nt), p(zt), int(ifpgh),
+                                 int(isep), ctypes.c_void_p(stream)))
+    return pot, grad.t()
+
+
+def zl2devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
+    """Unscaled 2D Laplace direct sum (reference zlfmm2d.f:600-654; no 1/(2 pi))."""
+    ns, nt = int(ns), int(nt)
+    zs = _pts(zsrc, 2, ns, "zsrc")
+    zt = _pts(ztarg, 2, nt, "ztarg")
+    q = _vec(charge, ns, "charge") if ifcharge == 1 else None
+    ds = _vec(dipstr, ns, "dipstr") if ifdipole == 1 else None
+    dv = _pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((2, nt), np.complex128, order="F")
+    check(lib().zfmm_zl2devaldirect(nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds), _ptr(dv),
+                                    int(ifcharge), _ptr(pot), _ptr(grad), int(ifdipole),
+                                    int(ifpgh)))
+    return pot, grad
+
+
+def tree_dump(D, ndiv, zsrc, ztarg=None, isep=1):
+    """Device tree, sort and lists for the real parts of zsrc/ztarg ((n, D) complex)."""
+    zs = np.ascontiguousarray(np.asarray(zsrc, np.complex128))
+    zt = zs if ztarg is None else np.ascontiguousarray(np.asarray(ztarg, np.complex128))
+    ns, nt = zs.shape[0], zt.shape[0]
+    nb, nl, tot = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    mnl = np.zeros(4, np.int32)
+    L = lib()
+    z = [None] * 12
+    check(L.zfmm_tree_dump(D, ndiv, isep, ns, _ptr(zs), nt, _ptr(zt), 0, 0, ctypes.byref(nb),
+                           ctypes.byref(nl), *z, ctypes.byref(tot), _ptr(mnl)))
+    n, NC = nb.value, 1 << D
+    o = dict(laddr=np.zeros(2 * (nl.value + 1), np.int32), ilevel=np.zeros(n, np.int32),
+             iparent=np.zeros(n, np.int32), nchild=np.zeros(n, np.int32),
+             ichild=np.zeros((n, NC), np.int32), centers=np.zeros((n, D)),
+             isrc=np.zeros(ns, np.int32), isrcse=np.zeros((n, 2), np.int32),
+             itarg=np.zeros(nt, np.int32), itargse=np.zeros((n, 2), np.int32),
+             nlist=np.zeros((4, n), np.int32))
+    cap = 400 * n + 1000
+    flat = np.zeros(cap, np.int32)
+    check(L.zfmm_tree_dump(D, ndiv, isep, ns, _ptr(zs), nt, _ptr(zt), n, cap, ctypes.byref(nb),
+                           ctypes.byref(nl), _ptr(o["laddr"]), _ptr(o["ilevel"]),
+                           _ptr(o["iparent"]), _ptr(o["nchild"]), _ptr(o["ichild"]),
+                           _ptr(o["centers"]), _ptr(o["isrc"]), _ptr(o["isrcse"]),
+                           _ptr(o["itarg"]), _ptr(o["itargse"]), _ptr(o["nlist"]), _ptr(flat),
+                           ctypes.byref(tot), _ptr(mnl)))
+    o["lists_flat"] = flat[:tot.value]
+    o["nboxes"] = n
+    o["nlevels"] = nl.value
+    o["laddr"] = o["laddr"].reshape(-1, 2)
+    o["mnlist"] = mnl.tolist()
+    return o
+
+
+def set_step_timing(on=True):
+    lib().zfmm_set_step_timing(1 if on else 0)
+
+
+def last_step_times():
+    ms = np.zeros(7)
+    nb, nl, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().zfmm_last_step_times(_ptr(ms), ctypes.byref(nb), ctypes.byref(nl), ctypes.byref(nt))
+    names = ["setup", "p2m", "m2m", "m2l_p2l", "l2l", "eval", "unsort"]
+    return dict(zip(names, ms.tolist())), dict(nboxes=nb.value, nlevels=nl.value,
+                                                 nterms=nt.value)
+
+
+def last_counts():
+    """Interaction counts and kernel launches of the last timed FMM call."""
+    c = np.zeros(8, np.int64)
+    nl = ctypes.c_long()
+    lib().zfmm_last_counts(_ptr(c), ctypes.byref(nl))
+    names = ["p2p_pairs", "m2t", "l2t", "m2l_pairs", "p2l", "m2m_pairs", "l2l_pairs", "p2m"]
+    return dict(zip(names, c.tolist())), nl.value
+
+
+def version():
+    return lib().zfmm_version().decode()

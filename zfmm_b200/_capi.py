@@ -1,0 +1,68 @@
+"""ctypes binding of libzfmm_b200.so (include/zfmm.h).
+
+The library is built in-tree (python -m zfmm_b200.build).  Loading fails
+loudly when the library is missing: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libzfmm_b200.so")
+
+_lib = None
+
+c_int = ctypes.c_int
+c_double = ctypes.c_double
+c_void_p = ctypes.c_void_p
+c_int_p = ctypes.POINTER(ctypes.c_int)
+
+# name -> (restype, argtypes), in include/zfmm.h order
+SIGNATURES = {
+    "zlfmm2d_": (None, [c_void_p] * 15),
+    "zl2devaldirect_": (None, [c_void_p] * 12),
+    "zfmm_zlfmm2d": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                             c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int]),
+    "zfmm_zl2devaldirect": (c_int, [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_int, c_void_p, c_void_p, c_int, c_int]),
+    "zfmm_zlfmm2d_dev": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                                 c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
+                                 c_void_p]),
+    "zfmm_zl2devaldirect_dev": (c_int, [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_int, c_void_p, c_void_p, c_int, c_int,
+                                        c_void_p]),
+    "zfmm_set_step_timing": (None, [c_int]),
+    "zfmm_last_step_times": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p]),
+    "zfmm_last_counts": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_long)]),
+    "zfmm_launch_count": (ctypes.c_long, []),
+    "zfmm_tree_dump": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int,
+                               c_int_p, c_int_p] + [c_void_p] * 12 + [c_int_p, c_void_p]),
+    "zfmm_probe_fp64_tflops": (c_double, [c_int]),
+    "zfmm_last_error": (ctypes.c_char_p, []),
+    "zfmm_version": (ctypes.c_char_p, []),
+}
+
+
+class ZfmmError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ZfmmError(
+                f"{LIB_PATH} is missing: build it with `python -m zfmm_b200.build` "
+                "(zfmm_b200 has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        msg = lib().zfmm_last_error().decode()
+        raise ZfmmError(f"zfmm status {rc}: {msg}")

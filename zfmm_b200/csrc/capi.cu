@@ -1,0 +1,335 @@
+// extern "C" entry points (include/zfmm.h).
+//
+// Host-array entry points copy the caller's arrays to the device on the
+// per-thread default stream, run the device path and copy pot/grad back, so
+// they are synchronous and reentrant across host threads.  Exceptions never
+// cross the ABI: they become status codes plus a thread-local message.
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../../include/zfmm.h"
+#include "lfmm2d.cuh"
+
+using namespace zf;
+
+namespace zf {
+long& launch_counter() {
+  static thread_local long n = 0;
+  return n;
+}
+}  // namespace zf
+
+namespace {
+
+thread_local std::string g_err;
+thread_local int g_timing = 0;
+thread_local StepTimes g_times;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  g_err.clear();
+  try {
+    f();
+    return ZF_OK;
+  } catch (const zf_error& e) {
+    return fail(e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(ZF_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(ZF_ERR_INTERNAL, e.what());
+  }
+}
+
+void clamp_flags(int& ifcharge, int& ifdipole, int& ifpgh) {
+  // zlfmm2d.f:58-68
+  if (ifcharge < 0 || ifcharge > 1) ifcharge = 1;
+  if (ifdipole < 0 || ifdipole > 1) ifdipole = 0;
+  if (ifpgh < 0 || ifpgh > 2) ifpgh = 1;
+}
+
+void check_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) throw zf_error(5, "no CUDA device available");
+}
+
+struct HostIn {
+  DevBuf<zdc> zsrc, charge, dipstr, dipvec, ztarg;
+};
+
+void upload(DevBuf<zdc>& b, const double* h, size_t nz, cudaStream_t s) {
+  b.alloc(nz, s);
+  if (nz) ZF_CUDA(cudaMemcpyAsync(b.get(), h, nz * sizeof(zdc), cudaMemcpyHostToDevice, s));
+}
+
+Inputs2D make_inputs(int ns, const double* zsrc, int ifcharge, const double* charge,
+                     int ifdipole, const double* dipstr, const double* dipvec, int nt,
+                     const double* ztarg, int ifpgh) {
+  Inputs2D in;
+  in.ns = ns;
+  in.nt = nt;
+  in.zsrc = reinterpret_cast<const zdc*>(zsrc);
+  in.charge = reinterpret_cast<const zdc*>(charge);
+  in.dipstr = reinterpret_cast<const zdc*>(dipstr);
+  in.dipvec = reinterpret_cast<const zdc*>(dipvec);
+  in.ztarg = reinterpret_cast<const zdc*>(ztarg);
+  in.ifcharge = ifcharge;
+  in.ifdipole = ifdipole;
+  in.ifpgh = ifpgh;
+  return in;
+}
+
+void check_args2d(int ns, int nt, const double* zsrc, const double* ztarg, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr,
+                  const double* dipvec, double* pot, double* grad, int ifpgh) {
+  if (ns < 0 || nt < 0) throw zf_error(ZF_ERR_ARG, "ns and nt must be >= 0");
+  if ((ns > 0 && !zsrc) || (nt > 0 && (!ztarg || !pot)))
+    throw zf_error(ZF_ERR_ARG, "null coordinate or output array");
+  if (ns > 0 && ifcharge == 1 && !charge) throw zf_error(ZF_ERR_ARG, "ifcharge=1 needs charge");
+  if (ns > 0 && ifdipole == 1 && (!dipstr || !dipvec))
+    throw zf_error(ZF_ERR_ARG, "ifdipole=1 needs dipstr and dipvec");
+  if (nt > 0 && ifpgh > 1 && !grad) throw zf_error(ZF_ERR_ARG, "ifpgh=2 needs grad");
+}
+
+// device path shared by host and device entry points
+void run_zlfmm2d(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* grad, cudaStream_t s) {
+  if (in.nt > 0) {
+    ZF_CUDA(cudaMemsetAsync(pot, 0, sizeof(zdc) * in.nt, s));
+    if (grad) ZF_CUDA(cudaMemsetAsync(grad, 0, sizeof(zdc) * 2 * in.nt, s));
+  }
+  if (in.ns == 0 || in.nt == 0) return;
+  if (isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
+  StepTimes t;
+  t.want_counts = g_timing >= 2;
+  zlfmm2d_device(eps, in, isep, pot, grad, s, g_timing ? &t : nullptr);
+  if (g_timing) g_times = t;
+}
+
+int zlfmm2d_host(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
+                 int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+                 double* grad, int nt, const double* ztarg, int ifpgh, int isep) {
+  return guarded([&] {
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    check_device();
+    cudaStream_t s = cudaStreamPerThread;
+    HostIn h;
+    upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
+    upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
+    if (ifcharge == 1) upload(h.charge, charge, ns, s);
+    if (ifdipole == 1) {
+      upload(h.dipstr, dipstr, ns, s);
+      upload(h.dipvec, dipvec, 2 * (size_t)ns, s);
+    }
+    DevBuf<zdc> dpot(nt, s), dgrad(ifpgh > 1 ? 2 * (size_t)nt : 0, s);
+    Inputs2D in = make_inputs(ns, (const double*)h.zsrc.get(), ifcharge,
+                              (const double*)h.charge.get(), ifdipole,
+                              (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
+                              (const double*)h.ztarg.get(), ifpgh);
+    run_zlfmm2d(eps, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
+    if (nt > 0) {
+      ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
+      if (grad) {
+        if (ifpgh > 1)
+          ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 2 * nt, cudaMemcpyDeviceToHost, s));
+        else
+          memset(grad, 0, sizeof(zdc) * 2 * nt);
+      }
+    }
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* zfmm_last_error(void) { return g_err.c_str(); }
+const char* zfmm_version(void) { return "zfmm_b200 0.1 (sm_100a)"; }
+void zfmm_set_step_timing(int on) { g_timing = on; }
+
+int zfmm_last_step_times(double* ms7, int* nboxes, int* nlevels, int* nterms) {
+  for (int i = 0; i < 7; i++) ms7[i] = g_times.ms[i];
+  if (nboxes) *nboxes = g_times.nboxes;
+  if (nlevels) *nlevels = g_times.nlevels;
+  if (nterms) *nterms = g_times.nterms;
+  return 0;
+}
+
+int zfmm_last_counts(long long* counts8, long* launches) {
+  for (int i = 0; i < 8; i++) counts8[i] = (long long)g_times.counts[i];
+  if (launches) *launches = g_times.launches;
+  return 0;
+}
+
+long zfmm_launch_count(void) { return launch_counter(); }
+
+int zfmm_zlfmm2d(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
+                 int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+                 double* grad, int nt, const double* ztarg, int ifpgh, int isep, int ifprint) {
+  (void)ifprint;
+  return zlfmm2d_host(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, nt,
+                      ztarg, ifpgh, isep);
+}
+
+void zlfmm2d_(const double* eps, const int* ns, const double* zsrc, int* ifcharge,
+              const double* charge, int* ifdipole, const double* dipstr, const double* dipvec,
+              double* pot, double* grad, const int* nt, const double* ztarg, int* ifpgh,
+              const int* isep, const int* ifprint) {
+  clamp_flags(*ifcharge, *ifdipole, *ifpgh);  // written back, as the reference does
+  int rc = zlfmm2d_host(*eps, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec, pot, grad,
+                        *nt, ztarg, *ifpgh, *isep);
+  if (rc != 0 && *nt > 0) {
+    memset(pot, 0, sizeof(double) * 2 * *nt);
+    if (grad) memset(grad, 0, sizeof(double) * 4 * *nt);
+  }
+  (void)ifprint;
+}
+
+int zfmm_zlfmm2d_dev(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
+                     int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+                     double* grad, int nt, const double* ztarg, int ifpgh, int isep,
+                     void* stream) {
+  return guarded([&] {
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs2D in = make_inputs(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                              ifpgh);
+    run_zlfmm2d(eps, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_zl2devaldirect(int nt, const double* ztarg, int ns, const double* zsrc,
+                        const double* charge, const double* dipstr, const double* dipvec,
+                        int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
+  return guarded([&] {
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = cudaStreamPerThread;
+    HostIn h;
+    upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
+    upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
+    if (ifcharge == 1) upload(h.charge, charge, ns, s);
+    if (ifdipole == 1) {
+      upload(h.dipstr, dipstr, ns, s);
+      upload(h.dipvec, dipvec, 2 * (size_t)ns, s);
+    }
+    DevBuf<zdc> dpot, dgrad;
+    upload(dpot, pot, nt, s);
+    if (ifpgh > 1) upload(dgrad, grad, 2 * (size_t)nt, s);
+    Inputs2D in = make_inputs(ns, (const double*)h.zsrc.get(), ifcharge == 1,
+                              (const double*)h.charge.get(), ifdipole == 1,
+                              (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
+                              (const double*)h.ztarg.get(), ifpgh);
+    zl2ddirect_device(in, dpot.get(), dgrad.get(), nullptr, s);
+    ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
+    if (ifpgh > 1)
+      ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 2 * nt, cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+void zl2devaldirect_(const int* nt, const double* ztarg, const int* ns, const double* zsrc,
+                     const double* charge, const double* dipstr, const double* dipvec,
+                     const int* ifcharge, double* pot, double* grad, const int* ifdipole,
+                     const int* ifpgh) {
+  zfmm_zl2devaldirect(*nt, ztarg, *ns, zsrc, charge, dipstr, dipvec, *ifcharge, pot, grad,
+                      *ifdipole, *ifpgh);
+}
+
+int zfmm_zl2devaldirect_dev(int nt, const double* ztarg, int ns, const double* zsrc,
+                            const double* charge, const double* dipstr, const double* dipvec,
+                            int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh,
+                            void* stream) {
+  return guarded([&] {
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs2D in = make_inputs(ns, zsrc, ifcharge == 1, charge, ifdipole == 1, dipstr, dipvec, nt,
+                              ztarg, ifpgh);
+    zl2ddirect_device(in, (zdc*)pot, (zdc*)grad, nullptr, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_tree_dump(int D, int ndiv, int isep, int ns, const double* zsrc, int nt,
+                   const double* ztarg, int box_cap, int list_cap, int* nboxes, int* nlevels,
+                   int* laddr, int* ilevel, int* iparent, int* nchild, int* ichild,
+                   double* centers, int* isrc, int* isrcse, int* itarg, int* itargse, int* nlist,
+                   int* lists, int* nlists_total, int* mnlist) {
+  return guarded([&] {
+    if ((D != 2 && D != 3) || ns < 1 || nt < 1 || !zsrc || !ztarg)
+      throw zf_error(ZF_ERR_ARG, "bad tree_dump arguments");
+    check_device();
+    cudaStream_t s = cudaStreamPerThread;
+    std::vector<double> sr((size_t)D * ns), tr((size_t)D * nt);
+    for (size_t i = 0; i < sr.size(); i++) sr[i] = zsrc[2 * i];
+    for (size_t i = 0; i < tr.size(); i++) tr[i] = ztarg[2 * i];
+    DevBuf<double> dsr(sr.size(), s), dtr(tr.size(), s);
+    ZF_CUDA(cudaMemcpyAsync(dsr.get(), sr.data(), sr.size() * 8, cudaMemcpyHostToDevice, s));
+    ZF_CUDA(cudaMemcpyAsync(dtr.get(), tr.data(), tr.size() * 8, cudaMemcpyHostToDevice, s));
+    TreeParams tp;
+    tp.D = D;
+    tp.ndiv = ndiv;
+    tp.isep = isep;
+    tp.lr_isep_quirk = D == 3;
+    DevTree t;
+    build_tree(dsr.get(), ns, dtr.get(), nt, tp, t, s);
+    *nboxes = t.nboxes;
+    *nlevels = t.nlevels;
+    if (box_cap < t.nboxes) return;
+    int nb = t.nboxes, NC = 1 << D;
+    for (size_t i = 0; i < t.laddr.size(); i++) laddr[i] = t.laddr[i];
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+      ZF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    };
+    d2h(ilevel, t.ilevel.get(), nb * 4);
+    d2h(iparent, t.iparent.get(), nb * 4);
+    d2h(nchild, t.nchild.get(), nb * 4);
+    d2h(ichild, t.ichild.get(), (size_t)nb * NC * 4);
+    d2h(centers, t.centers.get(), (size_t)nb * D * 8);
+    DevBuf<int> pi, se;
+    sort_points(t, dsr.get(), ns, pi, se, s);
+    d2h(isrc, pi.get(), (size_t)ns * 4);
+    d2h(isrcse, se.get(), (size_t)nb * 8);
+    sort_points(t, dtr.get(), nt, pi, se, s);
+    d2h(itarg, pi.get(), (size_t)nt * 4);
+    d2h(itargse, se.get(), (size_t)nb * 8);
+    DevLists L;
+    build_lists(t, L, s);
+    std::vector<int> cnt(nb), buf;
+    size_t pos = 0;
+    for (int k = 0; k < 4; k++) {
+      mnlist[k] = L.mn[k];
+      d2h(cnt.data(), L.n[k].get(), nb * 4);
+      buf.resize((size_t)(L.mn[k] > 0 ? L.mn[k] : 1) * nb);
+      d2h(buf.data(), L.list[k].get(), buf.size() * 4);
+      ZF_CUDA(cudaStreamSynchronize(s));
+      for (int b = 0; b < nb; b++) {
+        nlist[k * nb + b] = cnt[b];
+        for (int i = 0; i < cnt[b]; i++) {
+          if ((long)pos < list_cap) lists[pos] = buf[(size_t)b * L.mn[k] + i];
+          pos++;
+        }
+      }
+    }
+    *nlists_total = (int)pos;
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// 2D driver set-up on the device (see fmm2d_common.cuh).
+#include "fmm2d_common.cuh"
+
+namespace zf {
+namespace {
+
+constexpr int TB = 256;
+
+__global__ void k_real_parts(const zdc* __restrict__ z, long n2, double* __restrict__ r) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n2) r[i] = z[i].re;
+}
+
+// gather sources/strengths (zreorderf, toolbox.f:2-21)
+__global__ void k_gather_src(int ns, const int* __restrict__ perm, const zdc* __restrict__ zsrc,
+                             const zdc* __restrict__ q, const zdc* __restrict__ ds,
+                             const zdc* __restrict__ dv, zdc* zs, zdc* qs, zdc* dss, zdc* dvs) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  int j = perm[i];
+  zs[2 * i] = zsrc[2 * j];
+  zs[2 * i + 1] = zsrc[2 * j + 1];
+  qs[i] = q ? q[j] : mkz(0.0);
+  dss[i] = ds ? ds[j] : mkz(0.0);
+  dvs[2 * i] = dv ? dv[2 * j] : mkz(0.0);
+  dvs[2 * i + 1] = dv ? dv[2 * j + 1] : mkz(0.0);
+}
+
+__global__ void k_gather_targ(int nt, const int* __restrict__ perm, const zdc* __restrict__ zt,
+                              zdc* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt) return;
+  int j = perm[i];
+  out[2 * i] = zt[2 * j];
+  out[2 * i + 1] = zt[2 * j + 1];
+}
+
+// sums of imaginary parts over each leaf's range: one warp per leaf
+__global__ void k_leaf_imag_sum(int nb, const int* __restrict__ nchild,
+                                const int* __restrict__ se, const zdc* __restrict__ pts,
+                                double* __restrict__ sums) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nb || nchild[w] > 0) return;
+  int s0 = se[2 * w], s1 = se[2 * w + 1];
+  double a = 0, b = 0;
+  for (int i = s0 + lane; i <= s1; i += 32) {
+    a += pts[2 * i].im;
+    b += pts[2 * i + 1].im;
+  }
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) { sums[2 * w] = a; sums[2 * w + 1] = b; }
+}
+
+__global__ void k_parent_imag_sum(int lo, int hi, const int* nchild, const int* ichild,
+                                  double* sums) {
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi || nchild[b] == 0) return;
+  double a = 0, c = 0;
+  for (int k = 0; k < 4; k++) {
+    int ch = ichild[4 * b + k];
+    a += sums[2 * ch];
+    c += sums[2 * ch + 1];
+  }
+  sums[2 * b] = a;
+  sums[2 * b + 1] = c;
+}
+
+__global__ void k_centres(int nb, const double* __restrict__ centers, const int* __restrict__ se,
+                          const double* __restrict__ sums, zdc* __restrict__ zc) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int n = se[2 * b + 1] - se[2 * b] + 1;
+  if (n > 0) {
+    zc[2 * b] = mkz(centers[2 * b], sums[2 * b] / n);
+    zc[2 * b + 1] = mkz(centers[2 * b + 1], sums[2 * b + 1] / n);
+  } else {
+    zc[2 * b] = mkz(0.0);
+    zc[2 * b + 1] = mkz(0.0);
+  }
+}
+
+void complex_centres(const DevTree& t, const DevBuf<int>& se, const DevBuf<zdc>& pts,
+                     DevBuf<zdc>& zc, cudaStream_t s) {
+  int nb = t.nboxes;
+  DevBuf<double> sums(2 * (size_t)nb, s);
+  klaunch(k_leaf_imag_sum, div_up((long)nb * 32, TB), TB, 0, s, nb, t.nchild.get(), se.get(),
+                                                          pts.get(), sums.get());
+  for (int l = t.nlevels - 1; l >= 0; l--) {
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    klaunch(k_parent_imag_sum, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, t.nchild.get(),
+                                                             t.ichild.get(), sums.get());
+  }
+  zc.alloc(2 * (size_t)nb, s);
+  klaunch(k_centres, div_up(nb, TB), TB, 0, s, nb, t.centers.get(), se.get(), sums.get(), zc.get());
+  ZF_LAUNCH_CHECK();
+}
+
+__global__ void k_unsort(int nt, const int* __restrict__ perm, const zdc* __restrict__ ps,
+                         const zdc* __restrict__ gs, zdc scale, int ifpgh, zdc* pot, zdc* grad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt) return;
+  int j = perm[i];
+  pot[j] = ps[i] * scale;
+  if (ifpgh > 1) {
+    grad[2 * j] = gs[2 * i] * scale;
+    grad[2 * j + 1] = gs[2 * i + 1] * scale;
+  }
+}
+
+}  // namespace
+
+void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t s) {
+  int ns = in.ns, nt = in.nt;
+  DevBuf<double> srcR(2 * (size_t)ns, s), targR(2 * (size_t)nt, s);
+  klaunch(k_real_parts, div_up(2L * ns, TB), TB, 0, s, in.zsrc, 2L * ns, srcR.get());
+  klaunch(k_real_parts, div_up(2L * nt, TB), TB, 0, s, in.ztarg, 2L * nt, targR.get());
+  ZF_LAUNCH_CHECK();
+  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
+  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  S.zsrcsort.alloc(2 * (size_t)ns, s);
+  S.chargesort.alloc(ns, s);
+  S.dipstrsort.alloc(ns, s);
+  S.dipvecsort.alloc(2 * (size_t)ns, s);
+  S.ztargsort.alloc(2 * (size_t)nt, s);
+  klaunch(k_gather_src, div_up(ns, TB), TB, 0, s, 
+      ns, S.isrc.get(), in.zsrc, in.ifcharge ? in.charge : nullptr,
+      in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr, S.zsrcsort.get(),
+      S.chargesort.get(), S.dipstrsort.get(), S.dipvecsort.get());
+  klaunch(k_gather_targ, div_up(nt, TB), TB, 0, s, nt, S.itarg.get(), in.ztarg, S.ztargsort.get());
+  ZF_LAUNCH_CHECK();
+  complex_centres(S.tree, S.isrcse, S.zsrcsort, S.zcsrc, s);
+  complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
+  build_lists(S.tree, S.lists, s);
+}
+
+void unsort2d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc scale,
+              int ifpgh, zdc* pot, zdc* grad, cudaStream_t s) {
+  klaunch(k_unsort, div_up(nt, TB), TB, 0, s, nt, itarg, potsort, gradsort, scale, ifpgh, pot, grad);
+  ZF_LAUNCH_CHECK();
+}
+
+}  // namespace zf

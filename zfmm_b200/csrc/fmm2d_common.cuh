@@ -1,0 +1,42 @@
+// Shared set-up of the 2D complex-coordinate FMMs (zlfmm2d / zhfmm2d):
+// real parts -> device tree -> sort -> reorder -> complex box centres.
+//
+// Reference: zfmm2d/src/laplace/zlfmm2d.f:70-200 (identical steps in
+// zfmm2d/src/helmholtz/zhfmm2d.f:73-195).  The complex centre of a box is its
+// real geometric centre plus i times the mean of the imaginary parts of the
+// box's sources (resp. targets), computed for every box.
+#pragma once
+#include <vector>
+#include "tree.cuh"
+#include "zcomplex.cuh"
+
+namespace zf {
+
+// Inputs as given by the caller, on the device, Fortran layout:
+// zsrc(2,ns), charge(ns), dipstr(ns), dipvec(2,ns), ztarg(2,nt).
+struct Inputs2D {
+  int ns = 0, nt = 0;
+  const zdc* zsrc = nullptr;
+  const zdc* charge = nullptr;
+  const zdc* dipstr = nullptr;
+  const zdc* dipvec = nullptr;
+  const zdc* ztarg = nullptr;
+  int ifcharge = 0, ifdipole = 0, ifpgh = 1;
+};
+
+struct Setup2D {
+  DevTree tree;
+  DevLists lists;
+  DevBuf<int> isrc, isrcse, itarg, itargse;
+  DevBuf<zdc> zsrcsort, ztargsort, chargesort, dipstrsort, dipvecsort;
+  DevBuf<zdc> zcsrc, zctarg;  // [2*nboxes]
+};
+
+// builds everything above for the given tree parameters (ndiv, idivflag, isep)
+void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t s);
+
+// potsort/gradsort (sorted order) -> pot/grad (user order), times `scale`
+void unsort2d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc scale,
+              int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);
+
+}  // namespace zf

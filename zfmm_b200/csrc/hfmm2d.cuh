@@ -1,0 +1,18 @@
+// 2D Helmholtz FMM entry points (device pointers).
+#pragma once
+#include "fmm2d_common.cuh"
+#include "lfmm2d.cuh"
+
+namespace zf {
+
+// h2dterms (zfmm2d/src/helmholtz/h2dterms.f:35-97) on the host
+int h2dterms_host(double bsize, zdc zk, double eps, int isep);
+
+// pot(nt), grad(2,nt) are overwritten; results carry the reference's i/4 factor
+void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
+                    cudaStream_t s, StepTimes* times);
+
+// zh2devaldirect over all pairs: ADDS the unscaled sums (no i/4) into pot/grad
+void zh2ddirect_device(zdc zk, const Inputs2D& in, zdc* pot, zdc* grad, cudaStream_t s);
+
+}  // namespace zf

@@ -1,0 +1,838 @@
+// Device tree builder: refinement, level restriction, renumbering, colleagues,
+// point sort and U/V/W/X lists, reproducing the reference's integer results.
+//
+// Reference algorithm (file:line in the reference tree):
+//   bounding box + refinement loop   zfmm2d/src/common/pts_tree2d.f:108-331, 455-611
+//   child creation (cumsum order)    zfmm2d/src/common/tree_routs2d.f:9-56
+//   stable partition into children   pts_tree2d.f:669-764 (3D: pts_tree3d.f:913-1102)
+//   colleagues                       tree_routs2d.f:100-212
+//   level restriction                pts_tree2d.f:768-1078, updateflags tree_routs2d.f:218-329
+//   renumbering after restriction    pts_tree2d.f:1083-1232
+//   final point sort                 pts_tree2d.f:1239-1264
+//   lists 1-4                        tree_routs2d.f:463-746 (3D: tree_routs3d.f:414-712)
+//
+// GPU formulation:
+//   * one thread per box of a level (or per point), one launch per level, as the
+//     reference's level loops are sequential but its box loops are independent;
+//   * new boxes are numbered by an exclusive scan of the refine flags of the
+//     level, i.e. children of the r-th refined box get ids nbctr + r*NC + c,
+//     which is the reference's cumsum numbering;
+//   * the final point order of pts_tree_sort (a stable recursive partition) is
+//     the order of a stable sort of the points by the start offset of their
+//     leaf, with leaf offsets from a bottom-up count and a top-down prefix in
+//     child order.  cub's radix sort is stable.
+// This file is compiled with --fmad=false so that the distance tests see the
+// same roundings as the reference (no contracted multiply-adds).
+#include <cub/cub.cuh>
+#include <vector>
+#include "tree.cuh"
+
+namespace zf {
+
+namespace {
+
+constexpr int TB = 256;
+
+template <int D>
+__device__ __forceinline__ bool within_tol(const double* a, const double* b, double tol) {
+#pragma unroll
+  for (int d = 0; d < D; d++)
+    if (!(fabs(a[d] - b[d]) <= tol)) return false;
+  return true;
+}
+
+template <int D>
+__device__ __forceinline__ int child_index(const double* p, const double* c) {
+  int k = 0;
+#pragma unroll
+  for (int d = 0; d < D; d++)
+    if (!(p[d] - c[d] < 0)) k |= 1 << d;
+  return k;
+}
+
+// ---- bounding box ------------------------------------------------------------
+template <int D>
+__global__ void k_bbox_partial(const double* __restrict__ a, int na, const double* __restrict__ b,
+                               int nb, double* __restrict__ part) {
+  double mn[D], mx[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) { mn[d] = INFINITY; mx[d] = -INFINITY; }
+  long tot = (long)na + nb;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+    const double* p = i < na ? a + i * D : b + (i - na) * D;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      double v = p[d];
+      mn[d] = fmin(mn[d], v);
+      mx[d] = fmax(mx[d], v);
+    }
+  }
+  __shared__ double smn[D][TB], smx[D][TB];
+#pragma unroll
+  for (int d = 0; d < D; d++) { smn[d][threadIdx.x] = mn[d]; smx[d][threadIdx.x] = mx[d]; }
+  __syncthreads();
+  for (int o = TB / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        smn[d][threadIdx.x] = fmin(smn[d][threadIdx.x], smn[d][threadIdx.x + o]);
+        smx[d][threadIdx.x] = fmax(smx[d][threadIdx.x], smx[d][threadIdx.x + o]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      part[blockIdx.x * 2 * D + d] = smn[d][0];
+      part[blockIdx.x * 2 * D + D + d] = smx[d][0];
+    }
+}
+
+// root box from the partial extrema (single thread)
+template <int D>
+__global__ void k_root(const double* part, int nparts, double* centers, double* bs0, int* ilevel,
+                       int* iparent, int* nchild, int* ichild, int* nsrc, int* ntarg, int ns,
+                       int nt) {
+  double mn[D], mx[D];
+  for (int d = 0; d < D; d++) { mn[d] = INFINITY; mx[d] = -INFINITY; }
+  for (int i = 0; i < nparts; i++)
+    for (int d = 0; d < D; d++) {
+      mn[d] = fmin(mn[d], part[i * 2 * D + d]);
+      mx[d] = fmax(mx[d], part[i * 2 * D + D + d]);
+    }
+  double b = mx[0] - mn[0];
+  for (int d = 1; d < D; d++)
+    if (mx[d] - mn[d] > b) b = mx[d] - mn[d];
+  *bs0 = b;
+  for (int d = 0; d < D; d++) centers[d] = (mn[d] + mx[d]) / 2;
+  ilevel[0] = 0;
+  iparent[0] = -1;
+  nchild[0] = 0;
+  for (int c = 0; c < (1 << D); c++) ichild[c] = -1;
+  nsrc[0] = ns;
+  ntarg[0] = nt;
+}
+
+// ---- refinement --------------------------------------------------------------
+__global__ void k_level_flags(int lo, int nb, const int* nsrc, const int* ntarg, int idivflag,
+                              int ndiv, int force, int* flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  int b = lo + i;
+  int r = 1;
+  if (!force) {
+    int nss = nsrc[b], ntt = ntarg[b];
+    int nn = idivflag == 0 ? nss : (idivflag == 1 ? ntt : max(nss, ntt));
+    r = nn > ndiv;
+  }
+  flag[b] = r;
+}
+
+__global__ void k_scan_total(const int* flag, const int* rank, int n, int* out) {
+  *out = n > 0 ? rank[n - 1] + (flag[n - 1] > 0 ? 1 : 0) : 0;
+}
+
+__global__ void k_gt0(const int* in, int n, int* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i] > 0 ? 1 : 0;
+}
+
+// children of every flagged box of [lo, lo+nb): ids first + rank*NC + c.
+// flagmode: children of iflag==1 parents become flag++ (3), of iflag==2 become 0
+// (tree_refine_boxes_flag); otherwise plain refinement.
+template <int D>
+__global__ void k_make_children(int lo, int nb, const int* flag01, const int* rank, int first,
+                                double bs, int lev, int flagmode, double* centers, int* ilevel,
+                                int* iparent, int* nchild, int* ichild, int* iflag, int* nsrc,
+                                int* ntarg) {
+  constexpr int NC = 1 << D;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb || !flag01[i]) return;
+  int b = lo + i;
+  int base = first + rank[i] * NC;
+  nchild[b] = NC;
+  double cb[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) cb[d] = centers[b * D + d];
+  int pf = iflag[b];
+  for (int c = 0; c < NC; c++) {
+    int j = base + c;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      double sgn = ((c >> d) & 1) ? 1.0 : -1.0;
+      centers[j * D + d] = cb[d] + (sgn * bs) / 2;
+    }
+    iparent[j] = b;
+    nchild[j] = 0;
+    for (int l = 0; l < NC; l++) ichild[j * NC + l] = -1;
+    ichild[b * NC + c] = j;
+    ilevel[j] = lev;
+    iflag[j] = flagmode ? (pf == 1 ? 3 : 0) : 0;
+    if (nsrc) { nsrc[j] = 0; ntarg[j] = 0; }
+  }
+}
+
+template <int D>
+__global__ void k_assign(const double* __restrict__ pts, int n, int* __restrict__ pbox,
+                         const int* __restrict__ ilevel, const int* __restrict__ nchild,
+                         const int* __restrict__ ichild, const double* __restrict__ centers,
+                         int lev, int* __restrict__ cnt) {
+  constexpr int NC = 1 << D;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int b = pbox[i];
+  if (ilevel[b] != lev || nchild[b] == 0) return;
+  double p[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) p[d] = pts[(long)i * D + d];
+  int c = child_index<D>(p, centers + b * D);
+  int j = ichild[b * NC + c];
+  pbox[i] = j;
+  atomicAdd(&cnt[j], 1);
+}
+
+// ---- colleagues --------------------------------------------------------------
+template <int D>
+__global__ void k_coll(int lo, int hi, double tol, const int* __restrict__ iparent,
+                       const int* __restrict__ ichild, const double* __restrict__ centers,
+                       int mnbors, int* ncoll, int* coll) {
+  constexpr int NC = 1 << D;
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi) return;
+  int dad = iparent[b];
+  int cnt = 0;
+  int nd = ncoll[dad];
+  for (int i = 0; i < nd; i++) {
+    int jb = coll[(long)dad * mnbors + i];
+    for (int c = 0; c < NC; c++) {
+      int kb = ichild[jb * NC + c];
+      if (kb >= 0 && within_tol<D>(centers + kb * D, centers + b * D, tol)) {
+        coll[(long)b * mnbors + cnt] = kb;
+        cnt++;
+      }
+    }
+  }
+  for (int k = cnt; k < mnbors; k++) coll[(long)b * mnbors + k] = -1;
+  ncoll[b] = cnt;
+}
+
+__global__ void k_coll_root(int* ncoll, int* coll, int mnbors) {
+  ncoll[0] = 1;
+  coll[0] = 0;
+  for (int k = 1; k < mnbors; k++) coll[k] = -1;
+}
+
+// ---- level restriction -------------------------------------------------------
+template <int D>
+__global__ void k_lr_flag1(int lo, int hi, double distest, const int* iparent, const int* nchild,
+                           const double* centers, const int* ncoll, const int* coll, int mnbors,
+                           int* iflag) {
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi) return;
+  int idad = iparent[b], igd = iparent[idad];
+  for (int i = 0; i < ncoll[igd]; i++) {
+    int jb = coll[(long)igd * mnbors + i];
+    if (nchild[jb] == 0 && iflag[jb] == 0 &&
+        within_tol<D>(centers + jb * D, centers + idad * D, distest))
+      iflag[jb] = 1;
+  }
+}
+
+template <int D>
+__global__ void k_lr_flag2(int lo, int hi, double distest, const int* iparent, const int* nchild,
+                           const double* centers, const int* ncoll, const int* coll, int mnbors,
+                           int* iflag) {
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi) return;
+  int f = iflag[b];
+  if (f != 1 && f != 2) return;
+  int idad = iparent[b];
+  for (int i = 0; i < ncoll[idad]; i++) {
+    int jb = coll[(long)idad * mnbors + i];
+    if (nchild[jb] == 0 && iflag[jb] == 0 &&
+        within_tol<D>(centers + jb * D, centers + b * D, distest))
+      iflag[jb] = 2;
+  }
+}
+
+template <int D>
+__global__ void k_updateflags(int lo, int hi, double distest, const int* nchild, const int* ichild,
+                              const double* centers, const int* ncoll, const int* coll,
+                              int mnbors, int* iflag) {
+  constexpr int NC = 1 << D;
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi || iflag[b] != 3) return;
+  int f = 0;
+  for (int i = 0; i < ncoll[b] && !f; i++) {
+    int jb = coll[(long)b * mnbors + i];
+    for (int c = 0; c < NC; c++) {
+      int kb = ichild[jb * NC + c];
+      if (kb >= 0 && nchild[kb] > 0 && within_tol<D>(centers + kb * D, centers + b * D, distest)) {
+        f = 1;
+        break;
+      }
+    }
+  }
+  iflag[b] = f;
+}
+
+__global__ void k_reset_flags(int n, int* iflag) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n && iflag[b] != 3) iflag[b] = 0;
+}
+
+// renumbering: lev_info[l] = {lo, hi, tlo, thi, base}
+__global__ void k_reorg_map(int n, const int* ilevel, const int* lev_info, int* map) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int l = ilevel[b];
+  const int* li = lev_info + 5 * l;
+  int m;
+  if (l <= 1) m = b;
+  else if (b >= li[0] && b <= li[1]) m = li[4] + (b - li[0]);
+  else m = li[4] + (li[1] - li[0] + 1) + (b - li[2]);
+  map[b] = m;
+}
+
+template <int D>
+__global__ void k_reorg_scatter(int n, const int* map, const int* ilevel, const int* iparent,
+                                const int* nchild, const int* ichild, const int* iflag,
+                                const double* centers, int* nilevel, int* niparent, int* nnchild,
+                                int* nichild, int* niflag, double* ncenters) {
+  constexpr int NC = 1 << D;
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int m = map[b];
+  nilevel[m] = ilevel[b];
+  nnchild[m] = nchild[b];
+  niflag[m] = iflag[b];
+  int p = iparent[b];
+  niparent[m] = p < 0 ? -1 : map[p];
+  for (int c = 0; c < NC; c++) {
+    int ch = ichild[b * NC + c];
+    nichild[m * NC + c] = ch < 0 ? -1 : map[ch];
+  }
+#pragma unroll
+  for (int d = 0; d < D; d++) ncenters[m * D + d] = centers[b * D + d];
+}
+
+// ---- point sort --------------------------------------------------------------
+template <int D>
+__global__ void k_descend(const double* __restrict__ pts, int n, const int* __restrict__ nchild,
+                          const int* __restrict__ ichild, const double* __restrict__ centers,
+                          int* __restrict__ leaf, int* __restrict__ cnt) {
+  constexpr int NC = 1 << D;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) p[d] = pts[(long)i * D + d];
+  int b = 0;
+  while (nchild[b] > 0) b = ichild[b * NC + child_index<D>(p, centers + b * D)];
+  leaf[i] = b;
+  atomicAdd(&cnt[b], 1);
+}
+
+template <int D>
+__global__ void k_sum_children(int lo, int hi, const int* nchild, const int* ichild, int* cnt) {
+  constexpr int NC = 1 << D;
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi || nchild[b] == 0) return;
+  int s = 0;
+  for (int c = 0; c < NC; c++) s += cnt[ichild[b * NC + c]];
+  cnt[b] = s;
+}
+
+template <int D>
+__global__ void k_child_starts(int lo, int hi, const int* nchild, const int* ichild,
+                               const int* cnt, int* start) {
+  constexpr int NC = 1 << D;
+  int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > hi || nchild[b] == 0) return;
+  int s = start[b];
+  for (int c = 0; c < NC; c++) {
+    int ch = ichild[b * NC + c];
+    start[ch] = s;
+    s += cnt[ch];
+  }
+}
+
+__global__ void k_sort_keys(int n, const int* leaf, const int* start, int* key, int* idx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  key[i] = start[leaf[i]];
+  idx[i] = i;
+}
+
+__global__ void k_ranges(int nb, const int* start, const int* cnt, int* se) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  se[2 * b] = start[b];
+  se[2 * b + 1] = start[b] + cnt[b] - 1;
+}
+
+// ---- lists 1..4 ----------------------------------------------------------------
+template <int D>
+__global__ void k_lists(int nb, int fill, const int* __restrict__ ilevel,
+                        const int* __restrict__ iparent, const int* __restrict__ nchild,
+                        const int* __restrict__ ichild, const double* __restrict__ C,
+                        const int* __restrict__ ncoll, const int* __restrict__ coll, int mnbors,
+                        const double* __restrict__ bsz, int isep, int* n1, int* n2, int* n3,
+                        int* n4, int* l1, int* l2, int* l3, int* l4, int m1, int m2, int m3,
+                        int m4) {
+  constexpr int NC = 1 << D;
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+#define PUSH(k, v)                                     \
+  do {                                                 \
+    if (fill) l##k[(long)b * m##k + c##k] = (v);      \
+    c##k++;                                            \
+  } while (0)
+  if (b == 0) {
+    if (nchild[0] == 0) PUSH(1, 0);
+  } else {
+    int ilev = ilevel[b];
+    int dad = iparent[b];
+    double sep = 1.05 * isep * bsz[ilev];
+    for (int i = 0; i < ncoll[dad]; i++) {
+      int jb = coll[(long)dad * mnbors + i];
+      for (int c = 0; c < NC; c++) {
+        int kb = ichild[jb * NC + c];
+        if (kb < 0) continue;
+        bool far = false;
+#pragma unroll
+        for (int d = 0; d < D; d++)
+          if (fabs(C[kb * D + d] - C[b * D + d]) >= sep) far = true;
+        if (far) PUSH(2, kb);
+      }
+    }
+    double dup = 1.05 * (bsz[ilev] + bsz[ilev + 1]) / 2.0 * isep;
+    double ddn = 1.05 * (bsz[ilev] + bsz[ilev - 1]) / 2.0 * isep;
+    if (nchild[b] == 0) {
+      for (int i = 0; i < ncoll[b]; i++) {
+        int jb = coll[(long)b * mnbors + i];
+        if (nchild[jb] == 0) {
+          PUSH(1, jb);
+        } else {
+          for (int c = 0; c < NC; c++) {
+            int kb = ichild[jb * NC + c];
+            if (kb < 0) continue;
+            bool near = true;
+#pragma unroll
+            for (int d = 0; d < D; d++)
+              if (!(fabs(C[kb * D + d] - C[b * D + d]) < dup)) near = false;
+            if (near) PUSH(1, kb);
+            else PUSH(3, kb);
+          }
+        }
+      }
+      for (int i = 0; i < ncoll[dad]; i++) {
+        int jb = coll[(long)dad * mnbors + i];
+        if (nchild[jb] == 0) {
+          bool near = true;
+#pragma unroll
+          for (int d = 0; d < D; d++)
+            if (!(fabs(C[jb * D + d] - C[b * D + d]) < ddn)) near = false;
+          if (near) PUSH(1, jb);
+        }
+      }
+    }
+    for (int i = 0; i < ncoll[dad]; i++) {
+      int jb = coll[(long)dad * mnbors + i];
+      if (nchild[jb] == 0) {
+        bool far = false;
+#pragma unroll
+        for (int d = 0; d < D; d++)
+          if (fabs(C[jb * D + d] - C[b * D + d]) > ddn) far = true;
+        if (far) PUSH(4, jb);
+      }
+    }
+  }
+#undef PUSH
+  n1[b] = c1;
+  n2[b] = c2;
+  n3[b] = c3;
+  n4[b] = c4;
+}
+
+__global__ void k_max4(int nb, const int* a, const int* b, const int* c, const int* d, int* out) {
+  __shared__ int s[4][TB];
+  int m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    m0 = max(m0, a[i]); m1 = max(m1, b[i]); m2 = max(m2, c[i]); m3 = max(m3, d[i]);
+  }
+  s[0][threadIdx.x] = m0; s[1][threadIdx.x] = m1; s[2][threadIdx.x] = m2; s[3][threadIdx.x] = m3;
+  __syncthreads();
+  for (int o = TB / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; k++) s[k][threadIdx.x] = max(s[k][threadIdx.x], s[k][threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+// ---- host helpers -----------------------------------------------------------
+struct Scanner {
+  DevBuf<char> tmp;
+  DevBuf<int> total;
+  DevBuf<int> flag01, rank;
+  int* h_total = nullptr;
+  cudaStream_t s;
+  explicit Scanner(cudaStream_t st) : s(st) {
+    total.alloc(1, s);
+    ZF_CUDA(cudaMallocHost((void**)&h_total, sizeof(int)));
+  }
+  ~Scanner() {
+    if (h_total) cudaFreeHost(h_total);
+  }
+  // flags01/rank over `src` (values > 0 count as set) of length n; returns total
+  int scan(const int* src, int n) {
+    if (n <= 0) return 0;
+    if ((int)flag01.size() < n) { flag01.alloc(n, s); rank.alloc(n, s); }
+    klaunch(k_gt0, div_up(n, TB), TB, 0, s, src, n, flag01.get());
+    size_t bytes = 0;
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag01.get(), rank.get(), n, s));
+    if (tmp.size() < bytes) tmp.alloc(bytes, s);
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, flag01.get(), rank.get(), n, s));
+    klaunch(k_scan_total, 1, 1, 0, s, flag01.get(), rank.get(), n, total.get());
+    ZF_CUDA(cudaMemcpyAsync(h_total, total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaStreamSynchronize(s));
+    return *h_total;
+  }
+};
+
+struct BoxArrays {
+  int D, NC;
+  size_t cap = 0;
+  cudaStream_t s;
+  DevBuf<int> ilevel, iparent, nchild, ichild, iflag, nsrc, ntarg;
+  DevBuf<double> centers;
+  void reserve(size_t need, size_t n_used) {
+    if (need <= cap) return;
+    size_t nc = cap ? cap : 1024;
+    while (nc < need) nc *= 2;
+    ilevel.grow(nc, n_used);
+    iparent.grow(nc, n_used);
+    nchild.grow(nc, n_used);
+    ichild.grow(nc * NC, n_used * NC);
+    iflag.grow(nc, n_used);
+    nsrc.grow(nc, n_used);
+    ntarg.grow(nc, n_used);
+    centers.grow(nc * D, n_used * D);
+    cap = nc;
+  }
+};
+
+template <int D>
+void colleagues_all(BoxArrays& B, int nlevels, const std::vector<int>& laddr,
+                    const std::vector<double>& bsz, int isep, int mnbors, DevBuf<int>& ncoll,
+                    DevBuf<int>& coll, cudaStream_t s) {
+  klaunch(k_coll_root, 1, 1, 0, s, ncoll.get(), coll.get(), mnbors);
+  for (int l = 1; l <= nlevels; l++) {
+    int lo = laddr[2 * l], hi = laddr[2 * l + 1];
+    if (hi < lo) continue;
+    double tol = (double)1.05f * bsz[l] * (double)isep;
+    klaunch(k_coll<D>, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, tol, B.iparent.get(), B.ichild.get(),
+                                                   B.centers.get(), mnbors, ncoll.get(), coll.get());
+  }
+  ZF_LAUNCH_CHECK();
+}
+
+// subdivide the flagged boxes (iflag>0) of [lo,hi]; returns number of new boxes
+template <int D>
+int refine_flag_range(BoxArrays& B, Scanner& S, int& n, int lo, int hi, double bs, int ilev,
+                      DevBuf<int>& ncoll, DevBuf<int>& coll, int mnbors, cudaStream_t s) {
+  constexpr int NC = 1 << D;
+  if (hi < lo) return 0;
+  int nb = hi - lo + 1;
+  int nref = S.scan(B.iflag.get() + lo, nb);
+  if (nref == 0) return 0;
+  B.reserve((size_t)n + (size_t)nref * NC, n);
+  ncoll.grow(B.cap, n);
+  coll.grow(B.cap * mnbors, (size_t)n * mnbors);
+  klaunch(k_make_children<D>, div_up(nb, TB), TB, 0, s, 
+      lo, nb, S.flag01.get(), S.rank.get(), n, bs, ilev + 1, 1, B.centers.get(), B.ilevel.get(),
+      B.iparent.get(), B.nchild.get(), B.ichild.get(), B.iflag.get(), nullptr, nullptr);
+  ZF_LAUNCH_CHECK();
+  n += nref * NC;
+  return nref * NC;
+}
+
+template <int D>
+void reorg(BoxArrays& B, int n, int nlevels, std::vector<int>& laddr, const std::vector<int>& tail,
+           cudaStream_t s) {
+  constexpr int NC = 1 << D;
+  std::vector<int> info(5 * (nlevels + 1), 0);
+  int cur = nlevels >= 2 ? laddr[4] : n;
+  for (int l = 0; l <= nlevels; l++) {
+    info[5 * l + 0] = laddr[2 * l];
+    info[5 * l + 1] = laddr[2 * l + 1];
+    info[5 * l + 2] = tail[2 * l];
+    info[5 * l + 3] = tail[2 * l + 1];
+  }
+  for (int l = 2; l <= nlevels; l++) {
+    int cnt = (laddr[2 * l + 1] - laddr[2 * l] + 1) + (tail[2 * l + 1] - tail[2 * l] + 1);
+    info[5 * l + 4] = cur;
+    laddr[2 * l] = cur;
+    cur += cnt;
+    laddr[2 * l + 1] = cur - 1;
+  }
+  DevBuf<int> d_info(info.size(), s), map(n, s);
+  ZF_CUDA(cudaMemcpyAsync(d_info.get(), info.data(), info.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, s));
+  klaunch(k_reorg_map, div_up(n, TB), TB, 0, s, n, B.ilevel.get(), d_info.get(), map.get());
+  DevBuf<int> il(B.cap, s), ip(B.cap, s), nc(B.cap, s), ic(B.cap * NC, s), fl(B.cap, s);
+  DevBuf<double> ce(B.cap * D, s);
+  klaunch(k_reorg_scatter<D>, div_up(n, TB), TB, 0, s, 
+      n, map.get(), B.ilevel.get(), B.iparent.get(), B.nchild.get(), B.ichild.get(),
+      B.iflag.get(), B.centers.get(), il.get(), ip.get(), nc.get(), ic.get(), fl.get(), ce.get());
+  ZF_LAUNCH_CHECK();
+  B.ilevel.swap(il);
+  B.iparent.swap(ip);
+  B.nchild.swap(nc);
+  B.ichild.swap(ic);
+  B.iflag.swap(fl);
+  B.centers.swap(ce);
+  ZF_CUDA(cudaStreamSynchronize(s));  // d_info host vector lifetime
+}
+
+template <int D>
+void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, const TreeParams& p,
+                  DevTree& t, cudaStream_t s) {
+  constexpr int NC = 1 << D;
+  if (ns < 1 || nt < 1) throw zf_error(ZF_ERR_ARG, "tree needs ns>=1 and nt>=1");
+  int mnbors = 1;
+  for (int d = 0; d < D; d++) mnbors *= (2 * p.isep + 1);
+  BoxArrays B;
+  B.D = D;
+  B.NC = NC;
+  B.s = s;
+  B.ilevel.alloc(0, s); B.iparent.alloc(0, s); B.nchild.alloc(0, s); B.ichild.alloc(0, s);
+  B.iflag.alloc(0, s); B.nsrc.alloc(0, s); B.ntarg.alloc(0, s); B.centers.alloc(0, s);
+  B.reserve(1024, 0);
+  Scanner S(s);
+
+  // root
+  const int nparts = 296;
+  DevBuf<double> part((size_t)nparts * 2 * D, s), d_bs0(1, s);
+  klaunch(k_bbox_partial<D>, nparts, TB, 0, s, d_src, ns, d_targ, nt, part.get());
+  klaunch(k_root<D>, 1, 1, 0, s, part.get(), nparts, B.centers.get(), d_bs0.get(), B.ilevel.get(),
+                            B.iparent.get(), B.nchild.get(), B.ichild.get(), B.nsrc.get(),
+                            B.ntarg.get(), ns, nt);
+  ZF_LAUNCH_CHECK();
+  std::vector<double> bsz(p.nlmax + 2, 0.0);
+  ZF_CUDA(cudaMemcpyAsync(bsz.data(), d_bs0.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+  DevBuf<int> pbs(ns, s), pbt(nt, s);
+  pbs.zero();
+  pbt.zero();
+  ZF_CUDA(cudaStreamSynchronize(s));
+
+  std::vector<int> laddr(2 * (p.nlmax + 1), 0);
+  laddr[0] = 0;
+  laddr[1] = 0;
+  int n = 1, ilev;
+  for (ilev = 0; ilev < p.nlmax; ilev++) {
+    int lo = laddr[2 * ilev], hi = laddr[2 * ilev + 1], nb = hi - lo + 1;
+    klaunch(k_level_flags, div_up(nb, TB), TB, 0, s, lo, nb, B.nsrc.get(), B.ntarg.get(), p.idivflag,
+                                                 p.ndiv, ilev < p.nlmin, B.iflag.get());
+    int nref = S.scan(B.iflag.get() + lo, nb);
+    if (nref == 0) break;
+    bsz[ilev + 1] = bsz[ilev] / 2;
+    B.reserve((size_t)n + (size_t)nref * NC, n);
+    klaunch(k_make_children<D>, div_up(nb, TB), TB, 0, s, 
+        lo, nb, S.flag01.get(), S.rank.get(), n, bsz[ilev + 1], ilev + 1, 0, B.centers.get(),
+        B.ilevel.get(), B.iparent.get(), B.nchild.get(), B.ichild.get(), B.iflag.get(),
+        B.nsrc.get(), B.ntarg.get());
+    klaunch(k_assign<D>, div_up(ns, TB), TB, 0, s, d_src, ns, pbs.get(), B.ilevel.get(), B.nchild.get(),
+                                              B.ichild.get(), B.centers.get(), ilev, B.nsrc.get());
+    klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, d_targ, nt, pbt.get(), B.ilevel.get(),
+                                              B.nchild.get(), B.ichild.get(), B.centers.get(), ilev,
+                                              B.ntarg.get());
+    ZF_LAUNCH_CHECK();
+    laddr[2 * (ilev + 1)] = n;
+    laddr[2 * (ilev + 1) + 1] = n + nref * NC - 1;
+    n += nref * NC;
+  }
+  int nlevels = ilev;
+  laddr.resize(2 * (nlevels + 1));
+  pbs.release();
+  pbt.release();
+
+  DevBuf<int> ncoll(B.cap, s), coll(B.cap * mnbors, s);
+  colleagues_all<D>(B, nlevels, laddr, bsz, p.isep, mnbors, ncoll, coll, s);
+
+  if (nlevels >= 2) {
+    // flag and flag+ passes
+    B.iflag.zero();
+    for (int l = nlevels; l >= 2; l--) {
+      int lo = laddr[2 * l], hi = laddr[2 * l + 1];
+      double distest = 1.05 * (bsz[l - 1] + bsz[l - 2]) / 2.0;
+      distest = distest * p.isep;
+      klaunch(k_lr_flag1<D>, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, distest, B.iparent.get(),
+                                                          B.nchild.get(), B.centers.get(),
+                                                          ncoll.get(), coll.get(), mnbors,
+                                                          B.iflag.get());
+    }
+    for (int l = nlevels; l >= 1; l--) {
+      int lo = laddr[2 * l], hi = laddr[2 * l + 1];
+      double distest = 1.05 * (bsz[l] + bsz[l - 1]) / 2.0;
+      if (!p.lr_isep_quirk) distest = distest * p.isep;
+      klaunch(k_lr_flag2<D>, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, distest, B.iparent.get(),
+                                                          B.nchild.get(), B.centers.get(),
+                                                          ncoll.get(), coll.get(), mnbors,
+                                                          B.iflag.get());
+    }
+    ZF_LAUNCH_CHECK();
+    std::vector<int> tail(2 * (nlevels + 1));
+    for (int l = 0; l <= nlevels; l++) { tail[2 * l] = 0; tail[2 * l + 1] = -1; }
+    for (int l = 1; l <= nlevels - 2; l++) {
+      tail[2 * (l + 1)] = n;
+      refine_flag_range<D>(B, S, n, laddr[2 * l], laddr[2 * l + 1], bsz[l + 1], l, ncoll, coll,
+                           mnbors, s);
+      tail[2 * (l + 1) + 1] = n - 1;
+    }
+    reorg<D>(B, n, nlevels, laddr, tail, s);
+    ncoll.grow(B.cap, 0);
+    coll.grow(B.cap * mnbors, 0);
+    colleagues_all<D>(B, nlevels, laddr, bsz, p.isep, mnbors, ncoll, coll, s);
+
+    klaunch(k_reset_flags, div_up(n, TB), TB, 0, s, n, B.iflag.get());
+    for (int l = 0; l <= nlevels; l++) { tail[2 * l] = 0; tail[2 * l + 1] = -1; }
+    for (int l = 2; l <= nlevels - 2; l++) {
+      double distest = 1.05 * (bsz[l] + bsz[l + 1]) / 2.0;
+      distest = distest * p.isep;
+      int lo = laddr[2 * l], hi = laddr[2 * l + 1];
+      if (hi >= lo)
+        klaunch(k_updateflags<D>, div_up(hi - lo + 1, TB), TB, 0, s, 
+            lo, hi, distest, B.nchild.get(), B.ichild.get(), B.centers.get(), ncoll.get(),
+            coll.get(), mnbors, B.iflag.get());
+      int tlo = tail[2 * l], thi = tail[2 * l + 1];
+      if (thi >= tlo)
+        klaunch(k_updateflags<D>, div_up(thi - tlo + 1, TB), TB, 0, s, 
+            tlo, thi, distest, B.nchild.get(), B.ichild.get(), B.centers.get(), ncoll.get(),
+            coll.get(), mnbors, B.iflag.get());
+      tail[2 * (l + 1)] = n;
+      refine_flag_range<D>(B, S, n, lo, hi, bsz[l + 1], l, ncoll, coll, mnbors, s);
+      refine_flag_range<D>(B, S, n, tlo, thi, bsz[l + 1], l, ncoll, coll, mnbors, s);
+      tail[2 * (l + 1) + 1] = n - 1;
+      int nlo = tail[2 * (l + 1)], nhi = tail[2 * (l + 1) + 1];
+      if (nhi >= nlo) {
+        double tol = (double)((float)p.isep * 1.05f) * bsz[l + 1];
+        klaunch(k_coll<D>, div_up(nhi - nlo + 1, TB), TB, 0, s, nlo, nhi, tol, B.iparent.get(),
+                                                          B.ichild.get(), B.centers.get(), mnbors,
+                                                          ncoll.get(), coll.get());
+      }
+      ZF_LAUNCH_CHECK();
+    }
+    reorg<D>(B, n, nlevels, laddr, tail, s);
+    ncoll.grow(B.cap, 0);
+    coll.grow(B.cap * mnbors, 0);
+    colleagues_all<D>(B, nlevels, laddr, bsz, p.isep, mnbors, ncoll, coll, s);
+  }
+
+  t.D = D;
+  t.NC = NC;
+  t.isep = p.isep;
+  t.mnbors = mnbors;
+  t.nlevels = nlevels;
+  t.nboxes = n;
+  t.laddr = laddr;
+  t.boxsize.assign(bsz.begin(), bsz.begin() + nlevels + 1);
+  t.boxsize.push_back(0.0);
+  t.ilevel = std::move(B.ilevel);
+  t.iparent = std::move(B.iparent);
+  t.nchild = std::move(B.nchild);
+  t.ichild = std::move(B.ichild);
+  t.centers = std::move(B.centers);
+  t.ncoll = std::move(ncoll);
+  t.coll = std::move(coll);
+  t.bsz.alloc(t.boxsize.size(), s);
+  ZF_CUDA(cudaMemcpyAsync(t.bsz.get(), t.boxsize.data(), t.boxsize.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaStreamSynchronize(s));
+}
+
+template <int D>
+void sort_points_t(const DevTree& t, const double* d_pts, int n, DevBuf<int>& perm,
+                   DevBuf<int>& se, cudaStream_t s) {
+  int nb = t.nboxes;
+  DevBuf<int> leaf(n, s), cnt(nb, s), start(nb, s), key(n, s), idx(n, s), key2(n, s);
+  cnt.zero();
+  perm.alloc(n, s);
+  se.alloc(2 * (size_t)nb, s);
+  klaunch(k_descend<D>, div_up(n, TB), TB, 0, s, d_pts, n, t.nchild.get(), t.ichild.get(),
+                                            t.centers.get(), leaf.get(), cnt.get());
+  for (int l = t.nlevels - 1; l >= 0; l--) {
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    klaunch(k_sum_children<D>, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, t.nchild.get(),
+                                                            t.ichild.get(), cnt.get());
+  }
+  ZF_CUDA(cudaMemsetAsync(start.get(), 0, sizeof(int), s));
+  for (int l = 0; l < t.nlevels; l++) {
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    klaunch(k_child_starts<D>, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, t.nchild.get(),
+                                                            t.ichild.get(), cnt.get(), start.get());
+  }
+  klaunch(k_sort_keys, div_up(n, TB), TB, 0, s, n, leaf.get(), start.get(), key.get(), idx.get());
+  ZF_LAUNCH_CHECK();
+  int bits = 1;
+  while ((1L << bits) <= (long)n) bits++;
+  size_t bytes = 0;
+  ZF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key.get(), key2.get(), idx.get(),
+                                          perm.get(), n, 0, bits, s));
+  DevBuf<char> tmp(bytes, s);
+  ZF_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, key.get(), key2.get(), idx.get(),
+                                          perm.get(), n, 0, bits, s));
+  klaunch(k_ranges, div_up(nb, TB), TB, 0, s, nb, start.get(), cnt.get(), se.get());
+  ZF_LAUNCH_CHECK();
+}
+
+template <int D>
+void build_lists_t(const DevTree& t, DevLists& L, cudaStream_t s) {
+  int nb = t.nboxes;
+  for (int k = 0; k < 4; k++) L.n[k].alloc(nb, s);
+  DevBuf<int> mx(4, s);
+  int dummy_m = 0;
+  klaunch(k_lists<D>, div_up(nb, TB), TB, 0, s, 
+      nb, 0, t.ilevel.get(), t.iparent.get(), t.nchild.get(), t.ichild.get(), t.centers.get(),
+      t.ncoll.get(), t.coll.get(), t.mnbors, t.bsz.get(), t.isep, L.n[0].get(), L.n[1].get(),
+      L.n[2].get(), L.n[3].get(), nullptr, nullptr, nullptr, nullptr, dummy_m, dummy_m, dummy_m,
+      dummy_m);
+  klaunch(k_max4, 1, TB, 0, s, nb, L.n[0].get(), L.n[1].get(), L.n[2].get(), L.n[3].get(), mx.get());
+  ZF_LAUNCH_CHECK();
+  ZF_CUDA(cudaMemcpyAsync(L.mn, mx.get(), 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ZF_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < 4; k++) {
+    L.list[k].alloc((size_t)(L.mn[k] > 0 ? L.mn[k] : 1) * nb, s);
+    L.list[k].fill_bytes(0xff);
+  }
+  klaunch(k_lists<D>, div_up(nb, TB), TB, 0, s, 
+      nb, 1, t.ilevel.get(), t.iparent.get(), t.nchild.get(), t.ichild.get(), t.centers.get(),
+      t.ncoll.get(), t.coll.get(), t.mnbors, t.bsz.get(), t.isep, L.n[0].get(), L.n[1].get(),
+      L.n[2].get(), L.n[3].get(), L.list[0].get(), L.list[1].get(), L.list[2].get(),
+      L.list[3].get(), L.mn[0], L.mn[1], L.mn[2], L.mn[3]);
+  ZF_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void build_tree(const double* d_src, int ns, const double* d_targ, int nt, const TreeParams& p,
+                DevTree& t, cudaStream_t s) {
+  if (p.D == 2) build_tree_t<2>(d_src, ns, d_targ, nt, p, t, s);
+  else if (p.D == 3) build_tree_t<3>(d_src, ns, d_targ, nt, p, t, s);
+  else throw zf_error(ZF_ERR_ARG, "D must be 2 or 3");
+}
+
+void sort_points(const DevTree& t, const double* d_pts, int n, DevBuf<int>& perm, DevBuf<int>& se,
+                 cudaStream_t s) {
+  if (t.D == 2) sort_points_t<2>(t, d_pts, n, perm, se, s);
+  else sort_points_t<3>(t, d_pts, n, perm, se, s);
+}
+
+void build_lists(const DevTree& t, DevLists& L, cudaStream_t s) {
+  if (t.D == 2) build_lists_t<2>(t, L, s);
+  else build_lists_t<3>(t, L, s);
+}
+
+}  // namespace zf

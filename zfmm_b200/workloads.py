@@ -1,0 +1,49 @@
+"""Seeded synthetic inputs with the shapes and distributions of the benchmark
+configurations (no external data).  Arrays are returned in the reference's
+layouts: points (d, n) complex, strengths (n,) complex.
+"""
+import numpy as np
+
+
+def cnormal(rng, *shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) / np.sqrt(2.0)
+
+
+def lap2d_uniform(n=20000, seed=0):
+    """zlfmm2d plain solve: real parts U[-1,1]^2, imaginary parts
+    0.1*sin(pi x1)*cos(pi x2) on each coordinate, complex normal charges and
+    dipole strengths, real unit dipole vectors at uniform angles."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1.0, 1.0, size=(2, n))
+    im = 0.1 * np.sin(np.pi * x[0]) * np.cos(np.pi * x[1])
+    z = x + 1j * im[None, :]
+    q = cnormal(rng, n)
+    ds = cnormal(rng, n)
+    phi = rng.uniform(0.0, 2 * np.pi, n)
+    dv = np.stack([np.cos(phi), np.sin(phi)]).astype(np.complex128)
+    return dict(zsrc=z, charge=q, dipstr=ds, dipvec=dv)
+
+
+def curve2d(n=2_000_000, seed=0, scale=1.0, shift=(0.0, 0.0), amp=0.05):
+    """Complex-deformed closed curve r(t) = (1+0.3cos5t)(cos t, sin t)
+    + amp*i*(cos3t, sin3t), t uniform on [0, 2pi)."""
+    rng = np.random.default_rng(seed)
+    t = rng.uniform(0.0, 2 * np.pi, n)
+    r = 1.0 + 0.3 * np.cos(5 * t)
+    z = np.stack([scale * r * np.cos(t) + shift[0], scale * r * np.sin(t) + shift[1]]) \
+        + 1j * amp * np.stack([np.cos(3 * t), np.sin(3 * t)])
+    return dict(zsrc=z.astype(np.complex128), charge=cnormal(rng, n), dipstr=cnormal(rng, n),
+                dipvec=cnormal(rng, 2, n))
+
+
+def clustered2d(n, seed=0, nclusters=5):
+    """Strongly non-uniform points (Gaussian clusters of different widths):
+    exercises deep adaptive refinement and the level-restriction passes."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-1, 1, size=(nclusters, 2))
+    w = 10.0 ** rng.uniform(-3, -1, nclusters)
+    k = rng.integers(0, nclusters, n)
+    x = c[k].T + w[k][None, :] * rng.standard_normal((2, n))
+    im = 0.05 * np.sin(3 * x[0]) * np.cos(2 * x[1])
+    z = x + 1j * im[None, :]
+    return dict(zsrc=z, charge=cnormal(rng, n), dipstr=cnormal(rng, n), dipvec=cnormal(rng, 2, n))
