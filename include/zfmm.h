@@ -67,6 +67,26 @@ int zfmm_zl2devaldirect_dev(int nt, const double *ztarg, int ns, const double *z
                             int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh,
                             void *stream);
 
+/* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
+ * the reference.  For callers that cannot allocate device memory during a
+ * solve: code whose device memory is owned by another allocator (a
+ * framework's caching pool that has reserved the GPU), or that runs under a
+ * fixed memory budget.  Inputs and outputs are the caller's device arrays, as
+ * in zfmm_zl2devaldirect_dev; the partial sums of the source-split kernel use
+ * a fixed 8 MiB device array inside the library (kept by every GPU that loads
+ * the library until the process exits).  No cudaMalloc/cudaFree and no
+ * allocating library routine is called.  Problems whose scratch would exceed
+ * the array are rejected with status 1 and a message; the capacity in bytes is
+ * returned by zfmm_zl2devaldirect_noalloc_capacity().  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (different streams or host threads) race. */
+int zfmm_zl2devaldirect_dev_noalloc(int nt, const double *ztarg, int ns, const double *zsrc,
+                                    const double *charge, const double *dipstr,
+                                    const double *dipvec, int ifcharge, double *pot, double *grad,
+                                    int ifdipole, int ifpgh, void *stream);
+long zfmm_zl2devaldirect_noalloc_capacity(void);
+
 /* Per-step device times (ms) of the last FMM call on this host thread:
  * [set-up, P2M, M2M, M2L+P2L, L2L, P2P+M2T+L2T, unsort], plus nboxes, nlevels
  * and the expansion order.  Recording adds CUDA events; enable with

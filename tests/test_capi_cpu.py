@@ -15,7 +15,7 @@ HEADER = os.path.join(ROOT, "include", "zfmm.h")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = re.findall(r"^\s*(?:const\s+)?(?:void|int|double|char)\s*\*?\s*(\w+)\s*\(", src,
+    names = re.findall(r"^\s*(?:const\s+)?(?:void|int|long|double|char)\s*\*?\s*(\w+)\s*\(", src,
                        flags=re.M)
     return sorted(set(names))
 

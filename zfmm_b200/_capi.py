@@ -30,6 +30,10 @@ SIGNATURES = {
     "zfmm_zl2devaldirect_dev": (c_int, [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
                                         c_void_p, c_int, c_void_p, c_void_p, c_int, c_int,
                                         c_void_p]),
+    "zfmm_zl2devaldirect_dev_noalloc": (c_int, [c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                                c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                                c_int, c_int, c_void_p]),
+    "zfmm_zl2devaldirect_noalloc_capacity": (ctypes.c_long, []),
     "zfmm_set_step_timing": (None, [c_int]),
     "zfmm_last_step_times": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p]),
     "zfmm_last_counts": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_long)]),

@@ -266,6 +266,27 @@ int zfmm_zl2devaldirect_dev(int nt, const double* ztarg, int ns, const double* z
   });
 }
 
+int zfmm_zl2devaldirect_dev_noalloc(int nt, const double* ztarg, int ns, const double* zsrc,
+                                    const double* charge, const double* dipstr,
+                                    const double* dipvec, int ifcharge, double* pot, double* grad,
+                                    int ifdipole, int ifpgh, void* stream) {
+  return guarded([&] {
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs2D in = make_inputs(ns, zsrc, ifcharge == 1, charge, ifdipole == 1, dipstr, dipvec, nt,
+                              ztarg, ifpgh);
+    zl2ddirect_device_noalloc(in, (zdc*)pot, (zdc*)grad, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+long zfmm_zl2devaldirect_noalloc_capacity(void) {
+  return (long)(direct2d_noalloc_capacity() * sizeof(zdc));
+}
+
 int zfmm_tree_dump(int D, int ndiv, int isep, int ns, const double* zsrc, int nt,
                    const double* ztarg, int box_cap, int list_cap, int* nboxes, int* nlevels,
                    int* laddr, int* ilevel, int* iparent, int* nchild, int* ichild,

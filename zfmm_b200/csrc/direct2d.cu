@@ -8,6 +8,7 @@
 // memory and a second kernel adds the slices into pot/grad.  Like the
 // reference routine, the sums are unscaled and are ADDED to pot/grad.
 #include <algorithm>
+#include <mutex>
 #include "lap2d_pair.cuh"
 #include "lfmm2d.cuh"
 
@@ -132,6 +133,48 @@ void zl2ddirect_device(const Inputs2D& in, zdc* pot, zdc* grad, zdc* scratch, cu
     if (part) klaunch(k_direct2d_reduce<false>, div_up(in.nt, 256), 256, 0, s, in.nt, nsplit, part, pot, grad);
   }
   ZF_LAUNCH_CHECK();
+}
+
+// ---- allocation-free variant ----------------------------------------------
+// Scratch of the source-split direct sum lives in this fixed device array
+// (8 MiB, held by every GPU that loads the library until the process exits).
+// Each call overwrites every partial it reads, so nothing has to be cleared
+// between calls; calls that overlap on the GPU (two streams, or two host
+// threads) share the array and race.
+constexpr size_t kNoAllocScratchElems = (size_t)1 << 19;  // complex elements = 8 MiB
+static __device__ __align__(256) zdc g_direct2d_scratch[kNoAllocScratchElems];
+
+namespace {
+std::mutex g_scratch_mu;
+zdc* g_scratch_ptr[64] = {nullptr};
+}  // namespace
+
+size_t direct2d_noalloc_capacity() { return kNoAllocScratchElems; }
+
+// Device address of the scratch array on the current device.  The array's
+// name is only a host-side stand-in, so the address is taken once per device
+// with cudaGetSymbolAddress (on the first call made on that device).
+static zdc* noalloc_scratch() {
+  int dev = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw zf_error(ZF_ERR_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    ZF_CUDA(cudaGetSymbolAddress(&p, g_direct2d_scratch));
+    g_scratch_ptr[dev] = static_cast<zdc*>(p);
+  }
+  return g_scratch_ptr[dev];
+}
+
+void zl2ddirect_device_noalloc(const Inputs2D& in, zdc* pot, zdc* grad, cudaStream_t s) {
+  size_t need = direct2d_scratch_elems(in.nt, in.ns, in.ifpgh);
+  if (need > kNoAllocScratchElems)
+    throw zf_error(ZF_ERR_ARG, "problem needs " + std::to_string(need * sizeof(zdc)) +
+                                   " bytes of scratch, more than the fixed " +
+                                   std::to_string(kNoAllocScratchElems * sizeof(zdc)) +
+                                   " bytes of the allocation-free entry point");
+  zl2ddirect_device(in, pot, grad, noalloc_scratch(), s);
 }
 
 }  // namespace zf

@@ -31,4 +31,9 @@ void zlfmm2d_device(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* gra
 size_t direct2d_scratch_elems(int nt, int ns, int ifpgh);
 void zl2ddirect_device(const Inputs2D& in, zdc* pot, zdc* grad, zdc* scratch, cudaStream_t s);
 
+// Same sum with its scratch in a fixed device array of the library (no device
+// allocation); throws when the problem needs more than that array holds.
+size_t direct2d_noalloc_capacity();
+void zl2ddirect_device_noalloc(const Inputs2D& in, zdc* pot, zdc* grad, cudaStream_t s);
+
 }  // namespace zf
