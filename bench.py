@@ -36,39 +36,47 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # zlfmm2d plain single solve, 20,000 points (sources = targets), charges +
     # dipoles, pot + grad, isep=1, eps=1e-9
-    "zlfmm2d_uniform_20k": dict(kind="lap2d", n=20000, eps=1e-9, ifpgh=2, isep=1),
+    "zlfmm2d_uniform_20k": dict(kind="lap2d", n=20000, eps=1e-9, ifpgh=2, isep=1, cpu_n=20000),
+    # zhfmm2d single solve, 2,000,000 points on the complex-deformed curve,
+    # zk = 40+0.5i, charges + dipoles, pot + grad, isep=1, eps=1e-9
+    "zhfmm2d_curve_2m": dict(kind="helm2d", n=2_000_000, eps=1e-9, zk=40 + 0.5j, ifpgh=2, isep=1,
+                             cpu_n=200_000),
+    "zhfmm2d_curve_2m_eps1e-6": dict(kind="helm2d", n=2_000_000, eps=1e-6, zk=40 + 0.5j, ifpgh=2,
+                                     isep=1, cpu_n=200_000),
+    "zhfmm2d_curve_2m_eps1e-12": dict(kind="helm2d", n=2_000_000, eps=1e-12, zk=40 + 0.5j,
+                                      ifpgh=2, isep=1, cpu_n=200_000),
 }
-DEFAULT_WORKLOAD = "zlfmm2d_uniform_20k"
+DEFAULT_WORKLOAD = "zhfmm2d_curve_2m"
 
 # Algorithmic work per interaction (real flops; complex add 2, mul 6, div 11;
 # transcendental functions are not counted), per the frozen convention of the
-# project's measurement plan.  P = 2p+1 coefficients.
-#   P2P 2D Laplace pair (pot+grad, charge+dipole): 70 flops
+# project's measurement plan.  P = 2p+1 coefficients of the level.
+#   P2P pair (pot+grad, charge+dipole): 70 flops (2D Laplace), 650 (2D Helmholtz:
+#     two ~35-term complex polynomial evaluations for H0, H1 plus 90)
 #   M2T / L2T (target, expansion) with gradient: 3 complex MACs per coefficient = 24 P
-#   M2L / M2M / L2L 2D: one dense P x P complex operator = 8 P^2
+#   M2L: one dense P x P complex operator = 8 P^2;  M2M / L2L: 8 P_parent P_child
 #   P2M / P2L per source: 2 complex MACs per coefficient = 16 P
-def flop_model(kind, counts, p):
-    P = 2 * p + 1
-    if kind == "lap2d":
-        per = dict(p2p_pairs=70, m2t=24 * P, l2t=24 * P, m2l_pairs=8 * P * P, p2l=16 * P,
-                   m2m_pairs=8 * P * P, l2l_pairs=8 * P * P, p2m=16 * P)
-    else:
-        raise ValueError(kind)
+def flop_model(kind, counts):
+    pair = {"lap2d": 70, "helm2d": 650}[kind]
     steps = {
-        "p2m": counts["p2m"] * per["p2m"],
-        "m2m": counts["m2m_pairs"] * per["m2m_pairs"],
-        "m2l_p2l": counts["m2l_pairs"] * per["m2l_pairs"] + counts["p2l"] * per["p2l"],
-        "l2l": counts["l2l_pairs"] * per["l2l_pairs"],
-        "eval": counts["p2p_pairs"] * per["p2p_pairs"] + counts["m2t"] * per["m2t"]
-        + counts["l2t"] * per["l2t"],
+        "p2m": 16 * counts["p2m_P"],
+        "m2m": 8 * counts["m2m_pairs_P"],
+        "m2l_p2l": 8 * counts["m2l_pairs_P"] + 16 * counts["p2l_P"],
+        "l2l": 8 * counts["l2l_pairs_P"],
+        "eval": pair * counts["p2p_pairs"] + 24 * counts["m2t_P"] + 24 * counts["l2t_P"],
     }
+    per = {"p2p_pair": pair, "m2t_per_P": 24, "l2t_per_P": 24, "m2l_per_P2": 8,
+           "m2m_l2l_per_P1P2": 8, "p2m_p2l_per_P": 16}
     return steps, per
 
 
-def make_inputs(wl, seed):
+def make_inputs(wl, seed, n=None):
     from zfmm_b200 import workloads as W
+    n = wl["n"] if n is None else n
     if wl["kind"] == "lap2d":
-        return W.lap2d_uniform(wl["n"], seed=seed)
+        return W.lap2d_uniform(n, seed=seed)
+    if wl["kind"] == "helm2d":
+        return W.curve2d(n, seed=seed)
     raise ValueError(wl["kind"])
 
 
@@ -151,6 +159,9 @@ def cpu_time_oracle(wl, inp, reps_min=1, budget_s=15.0):
         if wl["kind"] == "lap2d":
             O.zlfmm2d(wl["eps"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
                       ifpgh=wl["ifpgh"], isep=wl["isep"])
+        else:
+            O.zhfmm2d(wl["eps"], wl["zk"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
+                      ifpgh=wl["ifpgh"], isep=wl["isep"])
         times.append(time.perf_counter() - t0)
         if len(times) == 1 and times[0] > budget_s:
             break
@@ -161,9 +172,9 @@ def run_reference(args, wl, ws, rank):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    inp = make_inputs(wl, seed=0)
-    nt = wl["n"]
-    for _ in range(args.warmup):
+    nt = wl["cpu_n"]
+    inp = make_inputs(wl, seed=0, n=nt)
+    for _ in range(min(args.warmup, 1)):
         cpu_time_oracle(wl, inp, reps_min=1, budget_s=0.0)
     per = []
     for _ in range(args.steps):
@@ -176,10 +187,12 @@ def run_reference(args, wl, ws, rank):
         "unit": "targets/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "n": nt, "eps": wl["eps"], "ifpgh": wl["ifpgh"],
+        "config": {"workload": args.workload, "n": wl["n"], "n_timed_sample": nt,
+                   "eps": wl["eps"], "zk": str(wl.get("zk")), "ifpgh": wl["ifpgh"],
                    "isep": wl["isep"], "l2": "n/a (host)"},
         "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "port",
-                         "sample": f"full workload, {args.steps} solves"},
+                         "sample": (f"{nt} points of the workload's distribution "
+                                    f"(full workload: {wl['n']}), {args.steps} solves")},
         "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -210,9 +223,17 @@ def run_ours(args, wl, ws, rank, local):
     sp = ctypes.c_void_p(stream.cuda_stream)
     P = lambda x: ctypes.c_void_p(x.data_ptr())
 
+    helm = wl["kind"] == "helm2d"
+    zkv = np.array([complex(wl.get("zk", 0)).real, complex(wl.get("zk", 0)).imag])
+    zkp = zkv.ctypes.data_as(ctypes.c_void_p)
+
     def solve():
-        _capi.check(L.zfmm_zlfmm2d_dev(eps, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot), P(grad),
-                                       n, P(zs), ifpgh, isep, sp))
+        if helm:
+            _capi.check(L.zfmm_zhfmm2d_dev(eps, zkp, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot),
+                                           P(grad), n, P(zs), ifpgh, isep, sp))
+        else:
+            _capi.check(L.zfmm_zlfmm2d_dev(eps, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot),
+                                           P(grad), n, P(zs), ifpgh, isep, sp))
 
     for _ in range(max(args.warmup, 3)):
         solve()
@@ -259,8 +280,12 @@ def run_ours(args, wl, ws, rank, local):
     hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
 
     def solve_host():
-        _capi.check(L.zfmm_zlfmm2d(eps, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv), hp(hpot),
-                                   hp(hgrad), n, hp(hz), ifpgh, isep, 0))
+        if helm:
+            _capi.check(L.zfmm_zhfmm2d(eps, zkp, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv),
+                                       hp(hpot), hp(hgrad), n, hp(hz), ifpgh, isep, 0))
+        else:
+            _capi.check(L.zfmm_zlfmm2d(eps, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv), hp(hpot),
+                                       hp(hgrad), n, hp(hz), ifpgh, isep, 0))
 
     solve_host()
     if ws > 1:
@@ -279,17 +304,24 @@ def run_ours(args, wl, ws, rank, local):
         e2e_tot = float(tt.item())
     h2d = hz.nbytes * 1 + hq.nbytes + hds.nbytes + hdv.nbytes + hz.nbytes  # zsrc, ztarg
     d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
-    # accuracy against the direct sum on a seeded subset of targets (device direct sum)
+    # accuracy against the FP64 direct sum on a seeded subset of targets (device direct sum)
     pg = pot.cpu().numpy()
     rng = np.random.default_rng(1234)
-    sub = np.sort(rng.choice(n, size=min(n, 4096), replace=False))
-    pd, _ = zfmm_b200.zl2devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
-                                     inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
-    relerr = float(np.linalg.norm(pg[sub] * 2 * np.pi - pd) / np.linalg.norm(pd))
+    nsub = min(n, 4096 if n <= 100_000 else 1024)
+    sub = np.sort(rng.choice(n, size=nsub, replace=False))
+    if helm:
+        pd, _ = zfmm_b200.zh2devaldirect(wl["zk"], len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                         inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
+        pd = pd * 0.25j
+    else:
+        pd, _ = zfmm_b200.zl2devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                         inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
+        pd = pd / (2 * np.pi)
+    relerr = float(np.linalg.norm(pg[sub] - pd) / np.linalg.norm(pd))
 
     # roofline of the dominant kernel (FP64 pipe bound)
     p = info["nterms"]
-    flops, per = flop_model(wl["kind"], counts, p)
+    flops, per = flop_model(wl["kind"], counts)
     avg = {k: v / args.steps for k, v in step_ms.items()}
     top = max(flops, key=lambda k: avg[k])
     achieved = flops[top] / (avg[top] * 1e-3) / 1e12
@@ -301,9 +333,12 @@ def run_ours(args, wl, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-        t_cpu, cores, nrep = cpu_time_oracle(wl, inp, reps_min=1, budget_s=12.0)
-        cpu = {"value": n / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
-               "sample": f"full workload (n={n}), median of {nrep} solves"}
+        ncpu = wl["cpu_n"]
+        cinp = inp if ncpu == n else make_inputs(wl, seed=0, n=ncpu)
+        t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
+        cpu = {"value": ncpu / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
+               "sample": (f"{ncpu} points of the workload's distribution (full workload: {n}), "
+                          f"median of {nrep} solves")}
     if rank != 0:
         return
     line = {
@@ -311,7 +346,8 @@ def run_ours(args, wl, ws, rank, local):
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "n": n, "eps": eps, "ifpgh": ifpgh, "isep": isep,
+        "config": {"workload": args.workload, "n": n, "eps": eps, "zk": str(wl.get("zk")),
+                   "ifpgh": ifpgh, "isep": isep,
                    "charges": True, "dipoles": True, "l2": "flushed (256 MiB write) between steps",
                    "parallelism": f"replicas x{ws}", "nboxes": info["nboxes"],
                    "nlevels": info["nlevels"], "nterms": p},

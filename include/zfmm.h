@@ -46,12 +46,35 @@ void zl2devaldirect_(const int *nt, const double *ztarg, const int *ns, const do
                      const int *ifcharge, double *pot, double *grad, const int *ifdipole,
                      const int *ifpgh);
 
+/* Replaces zhfmm2d (zfmm2d/src/helmholtz/zhfmm2d.f:14-15; MATLAB spec
+ * zfmm2d/matlab_linux/zhfmm2d.mw:7).  zk points to one complex (re, im).
+ * pot = sum (i/4) q H0(zk R) + dipole terms (zhfmm2d.f:1-12). */
+void zhfmm2d_(const double *eps, const double *zk, const int *ns, const double *zsrc,
+              int *ifcharge, const double *charge, int *ifdipole, const double *dipstr,
+              const double *dipvec, double *pot, double *grad, const int *nt,
+              const double *ztarg, int *ifpgh, const int *isep, const int *ifprint);
+
+/* Replaces zh2devaldirect (zfmm2d/src/helmholtz/zhfmm2d.f:773-774; MATLAB spec
+ * zfmm2d/matlab_linux/zh2devaldirect.mw:6).  Adds the UNSCALED sums (no i/4). */
+void zh2devaldirect_(const double *zk, const int *nt, const double *ztarg, const int *ns,
+                     const double *zsrc, const double *charge, const double *dipstr,
+                     const double *dipvec, const int *ifcharge, double *pot, double *grad,
+                     const int *ifdipole, const int *ifpgh);
+
 /* C forms of the above (host arrays).  Flags are not modified; out-of-range
  * flags are clamped the same way as the reference (zlfmm2d.f:58-68). */
 int zfmm_zlfmm2d(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
                  int ifdipole, const double *dipstr, const double *dipvec, double *pot,
                  double *grad, int nt, const double *ztarg, int ifpgh, int isep, int ifprint);
 int zfmm_zl2devaldirect(int nt, const double *ztarg, int ns, const double *zsrc,
+                        const double *charge, const double *dipstr, const double *dipvec,
+                        int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
+
+int zfmm_zhfmm2d(double eps, const double *zk, int ns, const double *zsrc, int ifcharge,
+                 const double *charge, int ifdipole, const double *dipstr, const double *dipvec,
+                 double *pot, double *grad, int nt, const double *ztarg, int ifpgh, int isep,
+                 int ifprint);
+int zfmm_zh2devaldirect(const double *zk, int nt, const double *ztarg, int ns, const double *zsrc,
                         const double *charge, const double *dipstr, const double *dipvec,
                         int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
 
@@ -66,6 +89,15 @@ int zfmm_zl2devaldirect_dev(int nt, const double *ztarg, int ns, const double *z
                             const double *charge, const double *dipstr, const double *dipvec,
                             int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh,
                             void *stream);
+
+int zfmm_zhfmm2d_dev(double eps, const double *zk, int ns, const double *zsrc, int ifcharge,
+                     const double *charge, int ifdipole, const double *dipstr,
+                     const double *dipvec, double *pot, double *grad, int nt, const double *ztarg,
+                     int ifpgh, int isep, void *stream);
+int zfmm_zh2devaldirect_dev(const double *zk, int nt, const double *ztarg, int ns,
+                            const double *zsrc, const double *charge, const double *dipstr,
+                            const double *dipvec, int ifcharge, double *pot, double *grad,
+                            int ifdipole, int ifpgh, void *stream);
 
 /* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory during a
@@ -94,10 +126,16 @@ long zfmm_zl2devaldirect_noalloc_capacity(void);
  * kernel and a stream synchronisation after the solve). */
 void zfmm_set_step_timing(int on);
 int zfmm_last_step_times(double *ms7, int *nboxes, int *nlevels, int *nterms);
-/* Interaction counts of the last timed FMM call: [P2P pairs, M2T (target,
- * box), L2T targets, M2L box pairs, P2L (box, source), M2M pairs, L2L pairs,
- * P2M sources], and the number of kernels the call launched. */
-int zfmm_last_counts(long long *counts8, long *launches);
+/* Interaction counts of the last FMM call made at timing level 2: [P2P pairs,
+ * M2T (target, box), L2T targets, M2L box pairs, P2L (box, source), M2M pairs,
+ * L2L pairs, P2M sources], then the same interactions weighted by the
+ * expansion lengths P = 2p+1 of their levels (M2L by P^2, M2M and L2L by
+ * P_parent P_child), and the number of kernels the call launched. */
+int zfmm_last_counts(long long *counts16, long *launches);
+/* Expansion order of the 2D Helmholtz FMM for boxes of size bsize (host
+ * computation, no GPU needed); replaces h2dterms
+ * (zfmm2d/src/helmholtz/h2dterms.f:35-97).  zk points to (re, im). */
+int zfmm_h2dterms(double bsize, const double *zk, double eps, int isep);
 /* Kernels launched by this library on the calling host thread so far. */
 long zfmm_launch_count(void);
 

@@ -64,3 +64,19 @@ def test_argument_errors_are_reported():
     rc = L.zfmm_zlfmm2d(1e-6, -1, None, 1, None, 0, None, None, None, None, 1, None, 1, 1, 0)
     assert rc == 1
     assert b"ns and nt" in L.zfmm_last_error()
+
+
+def test_h2dterms_matches_reference_log():
+    """The library's host-side h2dterms against the per-level expansion orders
+    of the reference's Helmholtz test (zfmm2d/test/helmholtz/fort.13:22-24)."""
+    import json
+    import zfmm_b200
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    g = json.load(open(os.path.join(gold, "golden.json")))["2d_helmholtz"]
+    z = np.load(os.path.join(gold, "fixture2d.npz"))["zsrc"].real
+    bs0 = max(np.ptp(z[:, 0]), np.ptp(z[:, 1]))
+    zk = np.array([3 * np.pi, 0.0])
+    L = zfmm_b200.lib()
+    got = [L.zfmm_h2dterms(bs0 / 2 ** l, zk.ctypes.data, float(np.float32(1e-12)), 1)
+           for l in range(11)]
+    assert got == g["nterms"]

@@ -19,8 +19,8 @@ import numpy as np
 
 from ._capi import ZfmmError, check, lib
 
-__all__ = ["zlfmm2d", "zl2devaldirect", "tree_dump", "ZfmmError", "set_step_timing",
-           "last_step_times", "version"]
+__all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "tree_dump", "ZfmmError",
+           "set_step_timing", "last_step_times", "last_counts", "version"]
 
 
 def _ptr(a):
@@ -61,16 +61,16 @@ def _torch_pts(x, d, n, name):
     return x
 
 
-def zlfmm2d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
-            isep=1):
-    """2D Laplace FMM with complex coordinates (reference zlfmm2d.f:14-234).
+def _zk(zk):
+    z = complex(zk)
+    return np.array([z.real, z.imag], np.float64)
 
-    pot(i) = sum_j charge_j log(R_ij)/(2 pi) - dipstr_j <dipvec_j, grad_y log R_ij>/(2 pi),
-    R = sqrt((x1-y1)^2 + (x2-y2)^2) on the principal branch.  Returns (pot, grad).
-    """
+
+def _fmm2d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh,
+           isep):
     if _is_torch(zsrc):
-        return _zlfmm2d_torch(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt,
-                              ztarg, ifpgh, isep)
+        return _fmm2d_torch(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt,
+                            ztarg, ifpgh, isep)
     ns, nt = int(ns), int(nt)
     zs = _pts(zsrc, 2, ns, "zsrc")
     zt = _pts(ztarg, 2, nt, "ztarg")
@@ -79,14 +79,42 @@ def zlfmm2d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg
     dv = _pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
     pot = np.zeros(nt, np.complex128)
     grad = np.zeros((2, nt), np.complex128, order="F")
-    check(lib().zfmm_zlfmm2d(float(eps), ns, _ptr(zs), int(ifcharge), _ptr(q), int(ifdipole),
-                             _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt, _ptr(zt), int(ifpgh),
-                             int(isep), 0))
+    if zk is None:
+        check(lib().zfmm_zlfmm2d(float(eps), ns, _ptr(zs), int(ifcharge), _ptr(q), int(ifdipole),
+                                 _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt, _ptr(zt),
+                                 int(ifpgh), int(isep), 0))
+    else:
+        k = _zk(zk)
+        check(lib().zfmm_zhfmm2d(float(eps), _ptr(k), ns, _ptr(zs), int(ifcharge), _ptr(q),
+                                 int(ifdipole), _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt,
+                                 _ptr(zt), int(ifpgh), int(isep), 0))
     return pot, grad
 
 
-def _zlfmm2d_torch(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh,
-                   isep):
+def zlfmm2d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
+            isep=1):
+    """2D Laplace FMM with complex coordinates (reference zlfmm2d.f:14-234).
+
+    pot(i) = sum_j charge_j log(R_ij)/(2 pi) - dipstr_j <dipvec_j, grad_y log R_ij>/(2 pi),
+    R = sqrt((x1-y1)^2 + (x2-y2)^2) on the principal branch.  Returns (pot, grad).
+    """
+    return _fmm2d(eps, None, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                  ifpgh, isep)
+
+
+def zhfmm2d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
+            isep=1):
+    """2D Helmholtz FMM with complex coordinates (reference zhfmm2d.f:14-227).
+
+    pot(i) = sum_j (i/4) charge_j H0(zk R_ij) + dipole terms, R as in zlfmm2d,
+    H0 = H0^(1) on its principal branch.  Argument order of zhfmm2d.mw:1.
+    """
+    return _fmm2d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                  ifpgh, isep)
+
+
+def _fmm2d_torch(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh,
+                 isep):
     import torch
     zs = _torch_pts(zsrc, 2, ns, "zsrc")
     zt = _torch_pts(ztarg, 2, nt, "ztarg")
@@ -96,16 +124,21 @@ def _zlfmm2d_torch(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt
     dv = _torch_pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
     pot = torch.empty(nt, dtype=torch.complex128, device=dev)
     grad = torch.empty((nt, 2), dtype=torch.complex128, device=dev)
-    stream = torch.cuda.current_stream(dev).cuda_stream
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
-    check(lib().zfmm_zlfmm2d_dev(float(eps), int(ns), p(zs), int(ifcharge), p(q), int(ifdipole),
-                                 p(ds), p(dv), p(pot), p(grad), int(nt), p(zt), int(ifpgh),
-                                 int(isep), ctypes.c_void_p(stream)))
+    if zk is None:
+        check(lib().zfmm_zlfmm2d_dev(float(eps), int(ns), p(zs), int(ifcharge), p(q),
+                                     int(ifdipole), p(ds), p(dv), p(pot), p(grad), int(nt), p(zt),
+                                     int(ifpgh), int(isep), stream))
+    else:
+        k = _zk(zk)
+        check(lib().zfmm_zhfmm2d_dev(float(eps), _ptr(k), int(ns), p(zs), int(ifcharge), p(q),
+                                     int(ifdipole), p(ds), p(dv), p(pot), p(grad), int(nt), p(zt),
+                                     int(ifpgh), int(isep), stream))
     return pot, grad.t()
 
 
-def zl2devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
-    """Unscaled 2D Laplace direct sum (reference zlfmm2d.f:600-654; no 1/(2 pi))."""
+def _direct2d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh):
     ns, nt = int(ns), int(nt)
     zs = _pts(zsrc, 2, ns, "zsrc")
     zt = _pts(ztarg, 2, nt, "ztarg")
@@ -114,10 +147,26 @@ def zl2devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipo
     dv = _pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
     pot = np.zeros(nt, np.complex128)
     grad = np.zeros((2, nt), np.complex128, order="F")
-    check(lib().zfmm_zl2devaldirect(nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds), _ptr(dv),
-                                    int(ifcharge), _ptr(pot), _ptr(grad), int(ifdipole),
-                                    int(ifpgh)))
+    if zk is None:
+        check(lib().zfmm_zl2devaldirect(nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds), _ptr(dv),
+                                        int(ifcharge), _ptr(pot), _ptr(grad), int(ifdipole),
+                                        int(ifpgh)))
+    else:
+        k = _zk(zk)
+        check(lib().zfmm_zh2devaldirect(_ptr(k), nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds),
+                                        _ptr(dv), int(ifcharge), _ptr(pot), _ptr(grad),
+                                        int(ifdipole), int(ifpgh)))
     return pot, grad
+
+
+def zl2devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
+    """Unscaled 2D Laplace direct sum (reference zlfmm2d.f:600-654; no 1/(2 pi))."""
+    return _direct2d(None, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
+
+
+def zh2devaldirect(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
+    """Unscaled 2D Helmholtz direct sum (reference zhfmm2d.f:773-838; no i/4)."""
+    return _direct2d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
 
 
 def tree_dump(D, ndiv, zsrc, ztarg=None, isep=1):
@@ -169,11 +218,13 @@ def last_step_times():
 
 def last_counts():
     """Interaction counts and kernel launches of the last timed FMM call."""
-    c = np.zeros(8, np.int64)
+    c = np.zeros(16, np.int64)
     nl = ctypes.c_long()
     lib().zfmm_last_counts(_ptr(c), ctypes.byref(nl))
     names = ["p2p_pairs", "m2t", "l2t", "m2l_pairs", "p2l", "m2m_pairs", "l2l_pairs", "p2m"]
-    return dict(zip(names, c.tolist())), nl.value
+    d = dict(zip(names, c[:8].tolist()))
+    d.update({k + "_P": v for k, v in zip(names, c[8:].tolist()) if k != "p2p_pairs"})
+    return d, nl.value
 
 
 def version():

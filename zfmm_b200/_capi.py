@@ -34,10 +34,24 @@ SIGNATURES = {
                                                 c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                                 c_int, c_int, c_void_p]),
     "zfmm_zl2devaldirect_noalloc_capacity": (ctypes.c_long, []),
+    "zhfmm2d_": (None, [c_void_p] * 16),
+    "zh2devaldirect_": (None, [c_void_p] * 13),
+    "zfmm_zhfmm2d": (c_int, [c_double, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int,
+                             c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                             c_int, c_int]),
+    "zfmm_zhfmm2d_dev": (c_int, [c_double, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int,
+                                 c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                                 c_int, c_void_p]),
+    "zfmm_zh2devaldirect": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                    c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int]),
+    "zfmm_zh2devaldirect_dev": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                        c_int, c_void_p]),
     "zfmm_set_step_timing": (None, [c_int]),
     "zfmm_last_step_times": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p]),
     "zfmm_last_counts": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_long)]),
     "zfmm_launch_count": (ctypes.c_long, []),
+    "zfmm_h2dterms": (c_int, [c_double, c_void_p, c_double, c_int]),
     "zfmm_tree_dump": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int,
                                c_int_p, c_int_p] + [c_void_p] * 12 + [c_int_p, c_void_p]),
     "zfmm_probe_fp64_tflops": (c_double, [c_int]),

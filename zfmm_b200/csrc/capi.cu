@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 #include "../../include/zfmm.h"
+#include "hfmm2d.cuh"
 #include "lfmm2d.cuh"
 
 using namespace zf;
@@ -96,8 +97,10 @@ void check_args2d(int ns, int nt, const double* zsrc, const double* ztarg, int i
   if (nt > 0 && ifpgh > 1 && !grad) throw zf_error(ZF_ERR_ARG, "ifpgh=2 needs grad");
 }
 
-// device path shared by host and device entry points
-void run_zlfmm2d(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* grad, cudaStream_t s) {
+// device path shared by host and device entry points; zk == nullptr selects
+// the Laplace FMM, otherwise Helmholtz with wavenumber *zk
+void run_fmm2d(double eps, const zdc* zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
+               cudaStream_t s) {
   if (in.nt > 0) {
     ZF_CUDA(cudaMemsetAsync(pot, 0, sizeof(zdc) * in.nt, s));
     if (grad) ZF_CUDA(cudaMemsetAsync(grad, 0, sizeof(zdc) * 2 * in.nt, s));
@@ -106,13 +109,14 @@ void run_zlfmm2d(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* grad, 
   if (isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
   StepTimes t;
   t.want_counts = g_timing >= 2;
-  zlfmm2d_device(eps, in, isep, pot, grad, s, g_timing ? &t : nullptr);
+  if (zk) zhfmm2d_device(eps, *zk, in, isep, pot, grad, s, g_timing ? &t : nullptr);
+  else zlfmm2d_device(eps, in, isep, pot, grad, s, g_timing ? &t : nullptr);
   if (g_timing) g_times = t;
 }
 
-int zlfmm2d_host(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
-                 int ifdipole, const double* dipstr, const double* dipvec, double* pot,
-                 double* grad, int nt, const double* ztarg, int ifpgh, int isep) {
+int fmm2d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifcharge,
+               const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+               double* pot, double* grad, int nt, const double* ztarg, int ifpgh, int isep) {
   return guarded([&] {
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
@@ -132,7 +136,7 @@ int zlfmm2d_host(double eps, int ns, const double* zsrc, int ifcharge, const dou
                               (const double*)h.charge.get(), ifdipole,
                               (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
                               (const double*)h.ztarg.get(), ifpgh);
-    run_zlfmm2d(eps, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
+    run_fmm2d(eps, zk, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
       if (grad) {
@@ -162,20 +166,29 @@ int zfmm_last_step_times(double* ms7, int* nboxes, int* nlevels, int* nterms) {
   return 0;
 }
 
-int zfmm_last_counts(long long* counts8, long* launches) {
-  for (int i = 0; i < 8; i++) counts8[i] = (long long)g_times.counts[i];
+int zfmm_last_counts(long long* counts16, long* launches) {
+  for (int i = 0; i < 16; i++) counts16[i] = (long long)g_times.counts[i];
   if (launches) *launches = g_times.launches;
   return 0;
 }
 
 long zfmm_launch_count(void) { return launch_counter(); }
 
+int zfmm_h2dterms(double bsize, const double* zk, double eps, int isep) {
+  if (!zk) return -1;
+  try {
+    return h2dterms_host(bsize, mkz(zk[0], zk[1]), eps, isep);
+  } catch (...) {
+    return -1;
+  }
+}
+
 int zfmm_zlfmm2d(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
                  int ifdipole, const double* dipstr, const double* dipvec, double* pot,
                  double* grad, int nt, const double* ztarg, int ifpgh, int isep, int ifprint) {
   (void)ifprint;
-  return zlfmm2d_host(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, nt,
-                      ztarg, ifpgh, isep);
+  return fmm2d_host(eps, nullptr, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot,
+                    grad, nt, ztarg, ifpgh, isep);
 }
 
 void zlfmm2d_(const double* eps, const int* ns, const double* zsrc, int* ifcharge,
@@ -183,8 +196,8 @@ void zlfmm2d_(const double* eps, const int* ns, const double* zsrc, int* ifcharg
               double* pot, double* grad, const int* nt, const double* ztarg, int* ifpgh,
               const int* isep, const int* ifprint) {
   clamp_flags(*ifcharge, *ifdipole, *ifpgh);  // written back, as the reference does
-  int rc = zlfmm2d_host(*eps, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec, pot, grad,
-                        *nt, ztarg, *ifpgh, *isep);
+  int rc = fmm2d_host(*eps, nullptr, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec,
+                      pot, grad, *nt, ztarg, *ifpgh, *isep);
   if (rc != 0 && *nt > 0) {
     memset(pot, 0, sizeof(double) * 2 * *nt);
     if (grad) memset(grad, 0, sizeof(double) * 4 * *nt);
@@ -204,14 +217,15 @@ int zfmm_zlfmm2d_dev(double eps, int ns, const double* zsrc, int ifcharge, const
     cudaStream_t s = (cudaStream_t)stream;
     Inputs2D in = make_inputs(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
                               ifpgh);
-    run_zlfmm2d(eps, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
+    run_fmm2d(eps, nullptr, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
     ZF_CUDA(cudaStreamSynchronize(s));
   });
 }
 
-int zfmm_zl2devaldirect(int nt, const double* ztarg, int ns, const double* zsrc,
-                        const double* charge, const double* dipstr, const double* dipvec,
-                        int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
+namespace {
+int direct2d_host(const zdc* zk, int nt, const double* ztarg, int ns, const double* zsrc,
+                  const double* charge, const double* dipstr, const double* dipvec, int ifcharge,
+                  double* pot, double* grad, int ifdipole, int ifpgh) {
   return guarded([&] {
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
@@ -233,12 +247,22 @@ int zfmm_zl2devaldirect(int nt, const double* ztarg, int ns, const double* zsrc,
                               (const double*)h.charge.get(), ifdipole == 1,
                               (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
                               (const double*)h.ztarg.get(), ifpgh);
-    zl2ddirect_device(in, dpot.get(), dgrad.get(), nullptr, s);
+    if (zk) zh2ddirect_device(*zk, in, dpot.get(), dgrad.get(), s);
+    else zl2ddirect_device(in, dpot.get(), dgrad.get(), nullptr, s);
     ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
     if (ifpgh > 1)
       ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 2 * nt, cudaMemcpyDeviceToHost, s));
     ZF_CUDA(cudaStreamSynchronize(s));
   });
+}
+
+}  // namespace
+
+int zfmm_zl2devaldirect(int nt, const double* ztarg, int ns, const double* zsrc,
+                        const double* charge, const double* dipstr, const double* dipvec,
+                        int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
+  return direct2d_host(nullptr, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, pot, grad,
+                       ifdipole, ifpgh);
 }
 
 void zl2devaldirect_(const int* nt, const double* ztarg, const int* ns, const double* zsrc,
@@ -262,6 +286,86 @@ int zfmm_zl2devaldirect_dev(int nt, const double* ztarg, int ns, const double* z
     Inputs2D in = make_inputs(ns, zsrc, ifcharge == 1, charge, ifdipole == 1, dipstr, dipvec, nt,
                               ztarg, ifpgh);
     zl2ddirect_device(in, (zdc*)pot, (zdc*)grad, nullptr, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_zhfmm2d(double eps, const double* zk, int ns, const double* zsrc, int ifcharge,
+                 const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                 double* pot, double* grad, int nt, const double* ztarg, int ifpgh, int isep,
+                 int ifprint) {
+  (void)ifprint;
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  zdc k = mkz(zk[0], zk[1]);
+  return fmm2d_host(eps, &k, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, nt,
+                    ztarg, ifpgh, isep);
+}
+
+void zhfmm2d_(const double* eps, const double* zk, const int* ns, const double* zsrc,
+              int* ifcharge, const double* charge, int* ifdipole, const double* dipstr,
+              const double* dipvec, double* pot, double* grad, const int* nt,
+              const double* ztarg, int* ifpgh, const int* isep, const int* ifprint) {
+  clamp_flags(*ifcharge, *ifdipole, *ifpgh);  // written back, as the reference does
+  zdc k = mkz(zk[0], zk[1]);
+  int rc = fmm2d_host(*eps, &k, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec, pot,
+                      grad, *nt, ztarg, *ifpgh, *isep);
+  if (rc != 0 && *nt > 0) {
+    memset(pot, 0, sizeof(double) * 2 * *nt);
+    if (grad) memset(grad, 0, sizeof(double) * 4 * *nt);
+  }
+  (void)ifprint;
+}
+
+int zfmm_zhfmm2d_dev(double eps, const double* zk, int ns, const double* zsrc, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr,
+                     const double* dipvec, double* pot, double* grad, int nt, const double* ztarg,
+                     int ifpgh, int isep, void* stream) {
+  return guarded([&] {
+    if (!zk) throw zf_error(ZF_ERR_ARG, "zk is null");
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs2D in = make_inputs(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                              ifpgh);
+    zdc k = mkz(zk[0], zk[1]);
+    run_fmm2d(eps, &k, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_zh2devaldirect(const double* zk, int nt, const double* ztarg, int ns, const double* zsrc,
+                        const double* charge, const double* dipstr, const double* dipvec,
+                        int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  zdc k = mkz(zk[0], zk[1]);
+  return direct2d_host(&k, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, pot, grad,
+                       ifdipole, ifpgh);
+}
+
+void zh2devaldirect_(const double* zk, const int* nt, const double* ztarg, const int* ns,
+                     const double* zsrc, const double* charge, const double* dipstr,
+                     const double* dipvec, const int* ifcharge, double* pot, double* grad,
+                     const int* ifdipole, const int* ifpgh) {
+  zfmm_zh2devaldirect(zk, *nt, ztarg, *ns, zsrc, charge, dipstr, dipvec, *ifcharge, pot, grad,
+                      *ifdipole, *ifpgh);
+}
+
+int zfmm_zh2devaldirect_dev(const double* zk, int nt, const double* ztarg, int ns,
+                            const double* zsrc, const double* charge, const double* dipstr,
+                            const double* dipvec, int ifcharge, double* pot, double* grad,
+                            int ifdipole, int ifpgh, void* stream) {
+  return guarded([&] {
+    if (!zk) throw zf_error(ZF_ERR_ARG, "zk is null");
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs2D in = make_inputs(ns, zsrc, ifcharge == 1, charge, ifdipole == 1, dipstr, dipvec, nt,
+                              ztarg, ifpgh);
+    zh2ddirect_device(mkz(zk[0], zk[1]), in, (zdc*)pot, (zdc*)grad, s);
     ZF_CUDA(cudaStreamSynchronize(s));
   });
 }

@@ -9,6 +9,8 @@
 // reference routine, the sums are unscaled and are ADDED to pot/grad.
 #include <algorithm>
 #include <mutex>
+#include "helm2d_pair.cuh"
+#include "hfmm2d.cuh"
 #include "lap2d_pair.cuh"
 #include "lfmm2d.cuh"
 
@@ -18,9 +20,9 @@ namespace {
 constexpr int DTB = 128;   // threads (targets) per block
 constexpr int TILE = 128;  // sources per shared-memory tile
 
-template <bool GRAD>
-__global__ void __launch_bounds__(DTB) k_direct2d(Inputs2D in, int chunk, zdc* pot, zdc* grad,
-                                                 zdc* part) {
+template <bool GRAD, bool HELM>
+__global__ void __launch_bounds__(DTB) k_direct2d(Inputs2D in, zdc zk, int chunk, zdc* pot,
+                                                 zdc* grad, zdc* part) {
   __shared__ zdc sy[TILE][6];  // y1, y2, q, ds, d1, d2
   int i = blockIdx.x * DTB + threadIdx.x;
   int j0 = blockIdx.y * chunk, j1 = min(in.ns, j0 + chunk);
@@ -49,9 +51,14 @@ __global__ void __launch_bounds__(DTB) k_direct2d(Inputs2D in, int chunk, zdc* p
     }
     __syncthreads();
     if (valid)
-      for (int k = 0; k < n; k++)
-        lap2d_pair<GRAD>(x1, x2, sy[k][0], sy[k][1], sy[k][2], sy[k][3], sy[k][4], sy[k][5],
-                         in.ifcharge, in.ifdipole, p, g1, g2);
+      for (int k = 0; k < n; k++) {
+        if (HELM)
+          helm_pair<GRAD>(zk, x1, x2, sy[k][0], sy[k][1], sy[k][2], sy[k][3], sy[k][4], sy[k][5],
+                          in.ifcharge, in.ifdipole, p, g1, g2);
+        else
+          lap2d_pair<GRAD>(x1, x2, sy[k][0], sy[k][1], sy[k][2], sy[k][3], sy[k][4], sy[k][5],
+                           in.ifcharge, in.ifdipole, p, g1, g2);
+      }
   }
   if (!valid) return;
   if (part == nullptr) {
@@ -108,7 +115,9 @@ size_t direct2d_scratch_elems(int nt, int ns, int ifpgh) {
   return (size_t)nsplit * nt * (ifpgh > 1 ? 3 : 1);
 }
 
-void zl2ddirect_device(const Inputs2D& in, zdc* pot, zdc* grad, zdc* scratch, cudaStream_t s) {
+namespace {
+template <bool HELM>
+void direct2d_run(const Inputs2D& in, zdc zk, zdc* pot, zdc* grad, zdc* scratch, cudaStream_t s) {
   if (in.nt <= 0 || in.ns <= 0) return;
   int nsplit = choose_split(in.nt, in.ns);
   int chunk = div_up(in.ns, nsplit);
@@ -126,13 +135,22 @@ void zl2ddirect_device(const Inputs2D& in, zdc* pot, zdc* grad, zdc* scratch, cu
   }
   dim3 grid(div_up(in.nt, DTB), nsplit);
   if (in.ifpgh > 1) {
-    klaunch(k_direct2d<true>, grid, DTB, 0, s, in, chunk, pot, grad, part);
+    klaunch(k_direct2d<true, HELM>, grid, DTB, 0, s, in, zk, chunk, pot, grad, part);
     if (part) klaunch(k_direct2d_reduce<true>, div_up(in.nt, 256), 256, 0, s, in.nt, nsplit, part, pot, grad);
   } else {
-    klaunch(k_direct2d<false>, grid, DTB, 0, s, in, chunk, pot, grad, part);
+    klaunch(k_direct2d<false, HELM>, grid, DTB, 0, s, in, zk, chunk, pot, grad, part);
     if (part) klaunch(k_direct2d_reduce<false>, div_up(in.nt, 256), 256, 0, s, in.nt, nsplit, part, pot, grad);
   }
   ZF_LAUNCH_CHECK();
+}
+}  // namespace
+
+void zl2ddirect_device(const Inputs2D& in, zdc* pot, zdc* grad, zdc* scratch, cudaStream_t s) {
+  direct2d_run<false>(in, mkz(0.0), pot, grad, scratch, s);
+}
+
+void zh2ddirect_device(zdc zk, const Inputs2D& in, zdc* pot, zdc* grad, cudaStream_t s) {
+  direct2d_run<true>(in, zk, pot, grad, nullptr, s);
 }
 
 // ---- allocation-free variant ----------------------------------------------

@@ -110,7 +110,77 @@ __global__ void k_unsort(int nt, const int* __restrict__ perm, const zdc* __rest
   }
 }
 
+// one thread per box; the same conditions as the eight steps of the drivers
+__global__ void k_count(int nb, const int* ilevel, const int* iparent, const int* nchild,
+                        const int* ichild, const int* isrcse, const int* itargse, const int* nl1,
+                        const int* l1, int m1, const int* nl2, const int* l2, int m2,
+                        const int* nl3, const int* l3, int m3, const int* nl4, const int* l4,
+                        int m4, const int* pl, unsigned long long* cnt) {
+  // cnt[0..7]: counts; cnt[8..15]: the same interactions weighted by the
+  // expansion lengths P = 2p+1 of their levels: [-, M2T sum P, L2T sum P,
+  // M2L sum P^2, P2L sum P, M2M sum P_parent P_child, L2L sum P_parent P_child,
+  // P2M sum P]
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  auto P_ = [&](int x) { return (unsigned long long)(2 * pl[ilevel[x]] + 1); };
+  unsigned long long w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  auto ns_ = [&](int x) { return isrcse[2 * x + 1] - isrcse[2 * x] + 1; };
+  auto nt_ = [&](int x) { return itargse[2 * x + 1] - itargse[2 * x] + 1; };
+  unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int ntb = nt_(b), nsb = ns_(b);
+  if (nchild[b] == 0 && ntb > 0) {
+    for (int i = 0; i < nl1[b]; i++) c[0] += (unsigned long long)ntb * max(0, ns_(l1[(size_t)b * m1 + i]));
+    for (int i = 0; i < nl3[b]; i++) {
+      int jb = l3[(size_t)b * m3 + i];
+      if (ns_(jb) > 0) { c[1] += ntb; w[1] += ntb * P_(jb); }
+    }
+    if (ilevel[b] >= 2) { c[2] = ntb; w[2] = ntb * P_(b); }
+  }
+  if (ntb > 0) {
+    for (int i = 0; i < nl2[b]; i++)
+      if (ns_(l2[(size_t)b * m2 + i]) > 0) { c[3]++; w[3] += P_(b) * P_(b); }
+    for (int i = 0; i < nl4[b]; i++) {
+      unsigned long long k = max(0, ns_(l4[(size_t)b * m4 + i]));
+      c[4] += k;
+      w[4] += k * P_(b);
+    }
+  }
+  if (nchild[b] > 0 && nsb > 0 && ilevel[b] >= 1)
+    for (int k = 0; k < 4; k++) {
+      int ch = ichild[4 * b + k];
+      if (ns_(ch) > 0) { c[5]++; w[5] += P_(b) * P_(ch); }
+    }
+  if (ilevel[b] >= 2 && ntb > 0) {
+    int pb = iparent[b];
+    if (nt_(pb) > 0 && (nl2[pb] > 0 || nl4[pb] > 0)) { c[6] = 1; w[6] = P_(pb) * P_(b); }
+  }
+  if (nchild[b] == 0 && nsb > 0 && ilevel[b] >= 1) { c[7] = nsb; w[7] = nsb * P_(b); }
+  for (int k = 0; k < 8; k++) {
+    if (c[k]) atomicAdd(&cnt[k], c[k]);
+    if (w[k]) atomicAdd(&cnt[8 + k], w[k]);
+  }
+}
+
 }  // namespace
+
+void count_interactions2d(const Setup2D& S, const int* p_per_level, unsigned long long* counts,
+                          cudaStream_t s) {
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  int nb = t.nboxes;
+  DevBuf<unsigned long long> cnt(16, s);
+  DevBuf<int> pl(t.nlevels + 1, s);
+  ZF_CUDA(cudaMemcpyAsync(pl.get(), p_per_level, (t.nlevels + 1) * sizeof(int),
+                          cudaMemcpyHostToDevice, s));
+  cnt.zero();
+  klaunch(k_count, div_up(nb, 256), 256, 0, s, nb, t.ilevel.get(), t.iparent.get(),
+          t.nchild.get(), t.ichild.get(), S.isrcse.get(), S.itargse.get(), L.n[0].get(),
+          L.list[0].get(), L.mn[0], L.n[1].get(), L.list[1].get(), L.mn[1], L.n[2].get(),
+          L.list[2].get(), L.mn[2], L.n[3].get(), L.list[3].get(), L.mn[3], pl.get(), cnt.get());
+  ZF_CUDA(cudaMemcpyAsync(counts, cnt.get(), 16 * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, s));
+  ZF_CUDA(cudaStreamSynchronize(s));
+}
 
 void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t s) {
   int ns = in.ns, nt = in.nt;

@@ -35,6 +35,13 @@ struct Setup2D {
 // builds everything above for the given tree parameters (ndiv, idivflag, isep)
 void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t s);
 
+// interaction counts of the FMM on this tree (host array of 16): [P2P pairs,
+// M2T (target, box), L2T targets, M2L box pairs, P2L (box, source), M2M pairs,
+// L2L pairs, P2M sources], then the same weighted by the expansion lengths
+// P = 2p+1 of their levels (M2L by P^2, M2M/L2L by P_parent P_child)
+void count_interactions2d(const Setup2D& S, const int* p_per_level, unsigned long long* counts,
+                          cudaStream_t s);
+
 // potsort/gradsort (sorted order) -> pot/grad (user order), times `scale`
 void unsort2d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc scale,
               int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);

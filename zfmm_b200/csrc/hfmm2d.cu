@@ -22,9 +22,13 @@
 //               accumulating pot and grad without storing the function table;
 //   P2P:        group of lanes per target over the list-1 sources, shuffle
 //               reduction.
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 #include "fmm2d_common.cuh"
 #include "hank2d.cuh"
+#include "helm2d_pair.cuh"
 #include "hfmm2d.cuh"
 #include "lfmm2d.cuh"
 
@@ -233,14 +237,14 @@ __device__ void form_expansion(const HelmArgs& A, int s0, int s1, zdc c1, zdc c2
 
 constexpr int MAXR = 8;  // coefficient slots per lane: p <= 255
 
-__global__ void __launch_bounds__(32 * WPB) k_hp2m(int nb, HelmArgs A) {
+__global__ void __launch_bounds__(32 * WPB) k_hp2m(int nb, HelmArgs A, int pmax) {
   extern __shared__ zdc sh[];
   int b = blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b >= nb) return;
   int s0 = A.isrcse[2 * b], s1 = A.isrcse[2 * b + 1];
-  if (A.nchild[b] > 0 || s1 < s0 || A.ilevel[b] < 1) return;
+  if (A.nchild[b] > 0 || s1 < s0 || A.ilevel[b] < 2) return;
   int l = A.ilevel[b], p = A.T.p[l];
-  zdc* tab = sh + (threadIdx.x >> 5) * FCH * (A.T.p[0] + 2);
+  zdc* tab = sh + (threadIdx.x >> 5) * FCH * (pmax + 2);
   zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
 #pragma unroll
   for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
@@ -429,42 +433,6 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
 
 // ---- steps 3, 5, 8: P2P (list1), M2T (list3), L2T per target leaf --------------
 template <bool GRAD>
-__device__ __forceinline__ void helm_pair(zdc zk, zdc x1, zdc x2, zdc y1, zdc y2, zdc q, zdc ds,
-                                          zdc d1, zdc d2, int ifcharge, int ifdipole, zdc& pot,
-                                          zdc& g1, zdc& g2) {
-  // zh2devaldirect (zhfmm2d.f:773-838), unscaled
-  zdc y1mx1 = y1 - x1, y2mx2 = y2 - x2;
-  zdc rz = zsqrt_p(y1mx1 * y1mx1 + y2mx2 * y2mx2);
-  zdc z = rz * zk;
-  if (!(zabs(z) > (double)1e-16f && z.im > -32.0)) return;  // REAL*4 literal 1E-16
-  zdc h0, h1;
-  hank01(z, h0, h1);
-  zdc irz = zinv(rz);
-  zdc zh1 = zk * h1;
-  if (ifcharge) {
-    pot += q * h0;
-    if (GRAD) {
-      zdc f = q * (zh1 * irz);
-      g1 += f * y1mx1;  // -q zk h1 (x - y)/rz
-      g2 += f * y2mx2;
-    }
-  }
-  if (ifdipole) {
-    zdc tmp = d1 * y1mx1 + d2 * y2mx2;
-    pot += ds * (tmp * (zh1 * irz));
-    if (GRAD) {
-      zdc h2 = (2.0 * zinv(z)) * h1 - h0;
-      zdc dh1 = 0.5 * (h0 - h2);
-      zdc irz2 = irz * irz, irz3 = irz2 * irz;
-      zdc a = zk * dh1 * irz2 - h1 * irz3;  // multiplies x - y = -(y - x)
-      zdc dsz = ds * zk;
-      g1 += dsz * ((-a * y1mx1) * tmp) - ds * (zh1 * irz) * d1;
-      g2 += dsz * ((-a * y2mx2) * tmp) - ds * (zh1 * irz) * d2;
-    }
-  }
-}
-
-template <bool GRAD>
 __global__ void __launch_bounds__(32 * WPB) k_heval(int nb, HelmArgs A, const int* nl1,
                                                    const int* l1, int m1, const int* nl3,
                                                    const int* l3, int m3, zdc* potsort,
@@ -639,26 +607,62 @@ __global__ void __launch_bounds__(32 * WPB) k_heval(int nb, HelmArgs A, const in
 
 }  // namespace
 
-int h2dterms_host(double bsize, zdc zk, double eps, int isep) {
-  // h2dterms.f:35-97: decay of |J_n(z2) H_n(z1)| with z1 = zk bsize (isep + 1/2),
-  // z2 = zk bsize sqrt(2)/2, n up to 50000
+namespace {
+// h2dterms for one level.  The reference evaluates H_n(z1) and J_n(z2) up to
+// n = 50000 and returns the first n where the product has decayed below eps;
+// the answer is found at a few times |z1|.  Here the tables are built to a
+// bound that doubles until the criterion fires: J_n from Miller's recurrence
+// does not depend on how far above n the recurrence started once it has
+// converged, so the values, and the answer, are those of the full tables.
+int h2dterms_eval(double bsize, zdc zk, double eps, int isep) {
   const int ntmax = 50000;
   zdc z1 = (zk * bsize) * (0.5 + isep * 1.0);
   double rscale = 1.0;
   const double pi2 = 8 * atan(1.0);
   if (zabs(zk * bsize) < pi2) rscale = zabs(zk * bsize);
-  std::vector<zdc> hfun(ntmax + 2), jfun(ntmax + 2);
-  h2dall(ntmax, z1, rscale, hfun.data(), 0, nullptr);
   zdc z2 = (zk * bsize) * (sqrt(2.0) / 2.0);
-  int ntop = jbessel_top(ntmax, z2);
-  std::vector<zdc> tmp(ntop + 2);
-  jbessel2d(ntmax, z2, rscale, jfun.data(), 0, nullptr, tmp.data(), ntop);
-  double x0 = zabs(jfun[0] * hfun[0]) + zabs(jfun[1] * hfun[1]);
-  for (int j = 2; j <= ntmax; j++) {
-    double x = (zabs(jfun[j] * hfun[j]) + zabs(jfun[j - 1] * hfun[j - 1])) * zabs(hfun[0]);
-    if (x < eps * x0) return j + 1;
+  int nb = 64;
+  while (true) {
+    int n = nb < ntmax ? nb : ntmax;
+    std::vector<zdc> hfun(n + 2), jfun(n + 2);
+    h2dall(n, z1, rscale, hfun.data(), 0, nullptr);
+    int ntop = jbessel_top(n, z2);
+    std::vector<zdc> tmp(ntop + 2);
+    jbessel2d(n, z2, rscale, jfun.data(), 0, nullptr, tmp.data(), ntop);
+    double x0 = zabs(jfun[0] * hfun[0]) + zabs(jfun[1] * hfun[1]);
+    for (int j = 2; j <= n; j++) {
+      double x = (zabs(jfun[j] * hfun[j]) + zabs(jfun[j - 1] * hfun[j - 1])) * zabs(hfun[0]);
+      if (x < eps * x0) return j + 1;
+    }
+    if (n >= ntmax) return 10001;  // the reference's "box too big" value
+    nb *= 4;
   }
-  return 10001;
+}
+
+struct TermsKey {
+  double bsize, zr, zi, eps;
+  int isep;
+  bool operator<(const TermsKey& o) const {
+    return std::tie(bsize, zr, zi, eps, isep) < std::tie(o.bsize, o.zr, o.zi, o.eps, o.isep);
+  }
+};
+std::mutex g_terms_mu;
+std::map<TermsKey, int> g_terms_cache;
+}  // namespace
+
+int h2dterms_host(double bsize, zdc zk, double eps, int isep) {
+  // h2dterms.f:35-97, results cached per (box size, zk, eps, isep)
+  TermsKey key{bsize, zk.re, zk.im, eps, isep};
+  {
+    std::lock_guard<std::mutex> lk(g_terms_mu);
+    auto it = g_terms_cache.find(key);
+    if (it != g_terms_cache.end()) return it->second;
+  }
+  int n = h2dterms_eval(bsize, zk, eps, isep);
+  std::lock_guard<std::mutex> lk(g_terms_mu);
+  if (g_terms_cache.size() > 4096) g_terms_cache.clear();
+  g_terms_cache[key] = n;
+  return n;
 }
 
 void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
@@ -687,17 +691,20 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   A.zk = zk;
   long tot = 0;
   int pmax = 0;
+  // Expansions of levels 0 and 1 are never read: lists 2-4 of those levels are
+  // empty (the four level-1 boxes touch), so no box translates or evaluates
+  // them.  They are not formed here (the reference forms the level-1
+  // multipoles and never uses them); p of levels >= 2 bounds the work.
   for (int l = 0; l <= nlev; l++) {
     double a = zabs(zk * (t.boxsize[l] / (2.0 * ZF_PI)));
     A.T.rs[l] = a < 1.0 ? a : 1.0;
-    A.T.p[l] = h2dterms_host(t.boxsize[l], zk, eps, isep);
+    A.T.p[l] = l >= 2 ? h2dterms_host(t.boxsize[l], zk, eps, isep) : 0;
     if (A.T.p[l] > 32 * MAXR - 1) throw zf_error(ZF_ERR_ARG, "expansion order too large");
     A.T.lo[l] = t.laddr[2 * l];
     A.T.base[l] = tot;
     tot += (long)(t.laddr[2 * l + 1] - t.laddr[2 * l] + 1) * (2 * A.T.p[l] + 1);
     if (A.T.p[l] > pmax) pmax = A.T.p[l];
   }
-  // the reference forces nothing here (2D); p is used per level as computed
   DevBuf<zdc> mp(tot, s), loc(tot, s), potsort(nt, s), gradsort(in.ifpgh > 1 ? 2 * (size_t)nt : 1, s);
   mp.zero();
   loc.zero();
@@ -711,13 +718,12 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   int grid_all = div_up(nb, WPB);
   // shared-memory strides (complex elements per warp)
   auto dense_stride = [](int ntt) { return (ntt + 2) + (2 * ntt + 1) + (ntt + 1 + 1); };
-  int p0 = A.T.p[0];
-  size_t sm_p2m = (size_t)WPB * FCH * (p0 + 2) * sizeof(zdc);
+  size_t sm_p2m = (size_t)WPB * FCH * (pmax + 2) * sizeof(zdc);
   ZF_CUDA(cudaFuncSetAttribute(k_hp2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
-  klaunch(k_hp2m, grid_all, 32 * WPB, sm_p2m, s, nb, A);
+  klaunch(k_hp2m, grid_all, 32 * WPB, sm_p2m, s, nb, A, pmax);
   ZF_LAUNCH_CHECK();
   mark(2);
-  for (int l = nlev - 1; l >= 1; l--) {
+  for (int l = nlev - 1; l >= 2; l--) {
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
     int stride = dense_stride(A.T.p[l] + A.T.p[l + 1]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
@@ -736,7 +742,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   }
   ZF_LAUNCH_CHECK();
   mark(4);
-  for (int l = 1; l <= nlev - 1; l++) {
+  for (int l = 2; l <= nlev - 1; l++) {
     int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
     int stride = dense_stride(A.T.p[l] + A.T.p[l + 1]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
@@ -769,6 +775,10 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
     times->nterms = pmax;
     for (auto& e : ev) cudaEventDestroy(e);
     times->launches = launch_counter() - launches0;
+  }
+  if (timing && times->want_counts) {
+    std::vector<int> pl(A.T.p, A.T.p + nlev + 1);
+    count_interactions2d(S, pl.data(), times->counts, s);
   }
 }
 

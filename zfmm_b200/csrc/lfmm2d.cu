@@ -449,36 +449,6 @@ __global__ void __launch_bounds__(32 * WPB) k_eval(int nb, LapArgs A, const int*
   }
 }
 
-// interaction counts for the roofline bookkeeping (one thread per box)
-__global__ void k_count(int nb, LapArgs A, const int* nl1, const int* l1, int m1, const int* nl2,
-                        const int* l2, int m2, const int* nl3, const int* l3, int m3,
-                        const int* nl4, const int* l4, int m4, unsigned long long* cnt) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb) return;
-  auto ns_ = [&](int x) { return A.isrcse[2 * x + 1] - A.isrcse[2 * x] + 1; };
-  auto nt_ = [&](int x) { return A.itargse[2 * x + 1] - A.itargse[2 * x] + 1; };
-  unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int ntb = nt_(b), nsb = ns_(b);
-  if (A.nchild[b] == 0 && ntb > 0) {
-    for (int i = 0; i < nl1[b]; i++) c[0] += (unsigned long long)ntb * max(0, ns_(l1[(size_t)b * m1 + i]));
-    for (int i = 0; i < nl3[b]; i++) c[1] += ns_(l3[(size_t)b * m3 + i]) > 0 ? ntb : 0;
-    c[2] = ntb;
-  }
-  if (ntb > 0) {
-    for (int i = 0; i < nl2[b]; i++) c[3] += ns_(l2[(size_t)b * m2 + i]) > 0;
-    for (int i = 0; i < nl4[b]; i++) c[4] += max(0, ns_(l4[(size_t)b * m4 + i]));
-  }
-  if (A.nchild[b] > 0 && nsb > 0 && A.ilevel[b] >= 1)
-    for (int k = 0; k < 4; k++) c[5] += ns_(A.ichild[4 * b + k]) > 0;
-  if (A.ilevel[b] >= 2 && ntb > 0) {
-    int pb = A.iparent[b];
-    if (nt_(pb) > 0 && (nl2[pb] > 0 || nl4[pb] > 0)) c[6] = 1;
-  }
-  if (A.nchild[b] == 0 && nsb > 0) c[7] = nsb;
-  for (int k = 0; k < 8; k++)
-    if (c[k]) atomicAdd(&cnt[k], c[k]);
-}
-
 }  // namespace
 
 int l2dterms(double eps) {
@@ -609,14 +579,8 @@ void zlfmm2d_device(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* gra
     times->launches = launch_counter() - launches0;
   }
   if (timing && times->want_counts) {
-    DevBuf<unsigned long long> cnt(8, s);
-    cnt.zero();
-    klaunch(k_count, div_up(nb, 256), 256, 0, s, nb, A, L.n[0].get(), L.list[0].get(), L.mn[0],
-            L.n[1].get(), L.list[1].get(), L.mn[1], L.n[2].get(), L.list[2].get(), L.mn[2],
-            L.n[3].get(), L.list[3].get(), L.mn[3], cnt.get());
-    ZF_CUDA(cudaMemcpyAsync(times->counts, cnt.get(), sizeof(times->counts),
-                            cudaMemcpyDeviceToHost, s));
-    ZF_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> pl(nlev + 1, p);
+    count_interactions2d(S, pl.data(), times->counts, s);
   }
 }
 

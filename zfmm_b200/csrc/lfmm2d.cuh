@@ -12,7 +12,7 @@ struct StepTimes {
   // interaction counts of the call: 0 P2P pairs, 1 M2T (target, box), 2 L2T
   // targets, 3 M2L box pairs, 4 P2L (box, source), 5 M2M pairs, 6 L2L pairs,
   // 7 P2M sources
-  unsigned long long counts[8] = {0};
+  unsigned long long counts[16] = {0};  // [8..15]: weighted by P (see count_interactions2d)
   long launches = 0;  // kernels of this library launched by the call
   bool want_counts = false;  // also count interactions (extra kernel + sync)
 };
