@@ -41,6 +41,9 @@ WORKLOADS = {
     # zk = 40+0.5i, charges + dipoles, pot + grad, isep=1, eps=1e-9
     "zhfmm2d_curve_2m": dict(kind="helm2d", n=2_000_000, eps=1e-9, zk=40 + 0.5j, ifpgh=2, isep=1,
                              cpu_n=200_000),
+    # smaller case of the same distribution, for kernel-level profiling
+    "zhfmm2d_curve_500k": dict(kind="helm2d", n=500_000, eps=1e-9, zk=40 + 0.5j, ifpgh=2, isep=1,
+                               cpu_n=200_000),
     "zhfmm2d_curve_2m_eps1e-6": dict(kind="helm2d", n=2_000_000, eps=1e-6, zk=40 + 0.5j, ifpgh=2,
                                      isep=1, cpu_n=200_000),
     "zhfmm2d_curve_2m_eps1e-12": dict(kind="helm2d", n=2_000_000, eps=1e-12, zk=40 + 0.5j,

@@ -61,6 +61,23 @@ void zh2devaldirect_(const double *zk, const int *nt, const double *ztarg, const
                      const double *dipvec, const int *ifcharge, double *pot, double *grad,
                      const int *ifdipole, const int *ifpgh);
 
+/* Replaces zlfmm3d (zfmm3d/src/laplace/zlfmm3d.f:14-15; MATLAB spec
+ * zfmm3d/matlab_linux/zlfmm3d.mw:1).  pot = sum q/(4 pi R) + dipole terms;
+ * the driver rescales the geometry to a unit root box internally and returns
+ * grad in the caller's units (zlfmm3d.f:187-200, :236-240). */
+void zlfmm3d_(const double *eps, const int *ns, const double *zsrc, int *ifcharge,
+              const double *charge, int *ifdipole, const double *dipstr, const double *dipvec,
+              double *pot, double *grad, const int *nt, const double *ztarg, int *ifpgh,
+              const int *isep, const int *ifprint);
+
+/* Replaces zl3devaldirect (zfmm3d/src/laplace/zlfmm3d.f:628-629; MATLAB spec
+ * zfmm3d/matlab_linux/zl3devaldirect.mw:1).  ADDS the sums (with 1/(4 pi))
+ * into pot/grad, as the reference routine does. */
+void zl3devaldirect_(const int *nt, const double *ztarg, const int *ns, const double *zsrc,
+                     const double *charge, const double *dipstr, const double *dipvec,
+                     const int *ifcharge, double *pot, double *grad, const int *ifdipole,
+                     const int *ifpgh);
+
 /* C forms of the above (host arrays).  Flags are not modified; out-of-range
  * flags are clamped the same way as the reference (zlfmm2d.f:58-68). */
 int zfmm_zlfmm2d(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
@@ -98,6 +115,25 @@ int zfmm_zh2devaldirect_dev(const double *zk, int nt, const double *ztarg, int n
                             const double *zsrc, const double *charge, const double *dipstr,
                             const double *dipvec, int ifcharge, double *pot, double *grad,
                             int ifdipole, int ifpgh, void *stream);
+
+/* 3D Laplace, C forms: host arrays, then device pointers on `stream`. */
+int zfmm_zlfmm3d(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
+                 int ifdipole, const double *dipstr, const double *dipvec, double *pot,
+                 double *grad, int nt, const double *ztarg, int ifpgh, int isep, int ifprint);
+int zfmm_zl3devaldirect(int nt, const double *ztarg, int ns, const double *zsrc,
+                        const double *charge, const double *dipstr, const double *dipvec,
+                        int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
+int zfmm_zlfmm3d_dev(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
+                     int ifdipole, const double *dipstr, const double *dipvec, double *pot,
+                     double *grad, int nt, const double *ztarg, int ifpgh, int isep,
+                     void *stream);
+int zfmm_zl3devaldirect_dev(int nt, const double *ztarg, int ns, const double *zsrc,
+                            const double *charge, const double *dipstr, const double *dipvec,
+                            int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh,
+                            void *stream);
+/* Expansion order of the 3D Laplace FMM for eps; replaces zl3dterms
+ * (zfmm3d/src/laplace/zlfmm3d.f:1283-1321).  Host computation. */
+int zfmm_zl3dterms(double eps);
 
 /* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory during a
@@ -138,6 +174,10 @@ int zfmm_last_counts(long long *counts16, long *launches);
 int zfmm_h2dterms(double bsize, const double *zk, double eps, int isep);
 /* Kernels launched by this library on the calling host thread so far. */
 long zfmm_launch_count(void);
+/* Device scratch comes from a library-owned memory pool per device that keeps
+ * freed memory mapped between calls; this returns the cached memory of the
+ * current device's pool to the driver (no reference counterpart). */
+int zfmm_trim_pool(void);
 
 /* Tree inspection (tests and tools): builds the device tree for real parts of
  * zsrc/ztarg (host arrays, dimension D = 2 or 3) exactly as the D-dimensional

@@ -84,6 +84,15 @@ int o_zhfmm2d(double eps, const double *zk, int ns, const double *zsrc, int ifch
               double *pot, double *grad, int nt, const double *ztarg, int ifpgh, int isep,
               int ifprint);
 
+/* 3D Laplace: direct sum (with 1/(4 pi), zlfmm3d.f:628-683) and FMM */
+int o_zl3dterms(double eps);
+void o_zl3devaldirect(int nt, const double *ztarg, int ns, const double *zsrc,
+                      const double *charge, const double *dipstr, const double *dipvec,
+                      int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
+int o_zlfmm3d(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
+              int ifdipole, const double *dipstr, const double *dipvec, double *pot,
+              double *grad, int nt, const double *ztarg, int ifpgh, int isep, int ifprint);
+
 /* tree inspection helpers for tests: build the tree exactly as the 2D/3D drivers
  * do and copy out summary arrays.  Returns nboxes; fills nlevels. */
 int o_tree_info(int D, double eps_ndiv, int ndiv_override, const double *zsrc, int ns,

@@ -212,3 +212,46 @@ def zh2ddirect(zk, zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpg
     f(_p(zkv), nt, _p(ztarg), ns, _p(zsrc), _p(q), _p(ds), _p(dv), ifc, _p(pot), _p(grad), ifd,
       ifpgh)
     return pot, grad
+
+
+def zlfmm3d(eps, zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1, isep=1):
+    """Oracle zlfmm3d; arrays (n,3) complex."""
+    zsrc = c128(zsrc)
+    ns = zsrc.shape[0]
+    ztarg = zsrc if ztarg is None else c128(ztarg)
+    nt = ztarg.shape[0]
+    ifc = 0 if charge is None else 1
+    ifd = 0 if dipstr is None else 1
+    q = c128(charge) if ifc else np.zeros(1, np.complex128)
+    ds = c128(dipstr) if ifd else np.zeros(1, np.complex128)
+    dv = c128(dipvec) if ifd else np.zeros((1, 3), np.complex128)
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((nt, 3), np.complex128)
+    f = lib().o_zlfmm3d
+    f.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_int]
+    rc = f(eps, ns, _p(zsrc), ifc, _p(q), ifd, _p(ds), _p(dv), _p(pot), _p(grad), nt, _p(ztarg),
+           ifpgh, isep, 0)
+    assert rc == 0
+    return pot, grad
+
+
+def zl3ddirect(zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1):
+    zsrc = c128(zsrc)
+    ztarg = zsrc if ztarg is None else c128(ztarg)
+    ns, nt = zsrc.shape[0], ztarg.shape[0]
+    ifc = 0 if charge is None else 1
+    ifd = 0 if dipstr is None else 1
+    q = c128(charge) if ifc else np.zeros(1, np.complex128)
+    ds = c128(dipstr) if ifd else np.zeros(1, np.complex128)
+    dv = c128(dipvec) if ifd else np.zeros((1, 3), np.complex128)
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((nt, 3), np.complex128)
+    f = lib().o_zl3devaldirect
+    f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    f(nt, _p(ztarg), ns, _p(zsrc), _p(q), _p(ds), _p(dv), ifc, _p(pot), _p(grad), ifd, ifpgh)
+    return pot, grad

@@ -87,3 +87,26 @@ def test_fmm2d_laplace_fixture_matches_direct():
     pd, _ = O.zl2ddirect(z, q, ztarg=z[sub])
     err = np.linalg.norm(pot[sub] * 2 * np.pi - pd) / np.linalg.norm(pd)
     assert err < 1e-11
+
+
+def test_direct3d_laplace_first12():
+    z, q = fx("fixture3d.npz")
+    pot, _ = O.zl3ddirect(z, q, ztarg=z[:12])
+    for p, (re, im) in zip(pot, G["3d_laplace"]["pot0"]):
+        assert close5(p.real, re) and close5(p.imag, im)
+
+
+def test_fmm3d_laplace_fixture_matches_log():
+    """The reference's 3D Laplace test (test9.f:78-133): eps = 1e-12, charges,
+    pot only; its log shows the first 12 potentials and err/(|pot0|+|q|) =
+    1.4130e-10 (fort.13:57-76)."""
+    z, q = fx("fixture3d.npz")
+    pot, _ = O.zlfmm3d(EPS12, z, q)
+    for p, (re, im) in zip(pot[:12], G["3d_laplace"]["pot"]):
+        assert close5(p.real, re) and close5(p.imag, im)
+    pd, _ = O.zl3ddirect(z, q)
+    err = np.linalg.norm(pot - pd)
+    assert close5(np.linalg.norm(pd), G["3d_laplace"]["pot0_norm"][0])
+    assert close5(np.linalg.norm(q), G["3d_laplace"]["charge_norm"][0])
+    rel = err / (np.linalg.norm(pd) + np.linalg.norm(q))
+    assert rel < 3 * 1.4130e-10

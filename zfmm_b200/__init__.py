@@ -19,7 +19,8 @@ import numpy as np
 
 from ._capi import ZfmmError, check, lib
 
-__all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "tree_dump", "ZfmmError",
+__all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "zlfmm3d", "zl3devaldirect",
+           "zl3dterms", "tree_dump", "ZfmmError",
            "set_step_timing", "last_step_times", "last_counts", "version"]
 
 
@@ -167,6 +168,66 @@ def zl2devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipo
 def zh2devaldirect(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
     """Unscaled 2D Helmholtz direct sum (reference zhfmm2d.f:773-838; no i/4)."""
     return _direct2d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
+
+
+def zlfmm3d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
+            isep=1):
+    """3D Laplace FMM with complex coordinates (reference zlfmm3d.f:14-245).
+
+    pot(i) = sum_j charge_j / (4 pi R_ij) + dipole terms, R = sqrt(sum_k (x_k - y_k)^2)
+    on the principal branch.  zsrc, ztarg, dipvec: (3, n) or (n, 3) complex.
+    Returns (pot, grad) with grad of shape (3, nt).  numpy inputs run through the
+    host-array entry point, complex128 CUDA tensors through the device entry point
+    on the current stream (grad then is a (3, nt) view).
+    """
+    if _is_torch(zsrc):
+        import torch
+        zs = _torch_pts(zsrc, 3, ns, "zsrc")
+        zt = _torch_pts(ztarg, 3, nt, "ztarg")
+        q = charge.contiguous() if ifcharge == 1 else None
+        ds = dipstr.contiguous() if ifdipole == 1 else None
+        dv = _torch_pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
+        pot = torch.empty(nt, dtype=torch.complex128, device=zs.device)
+        grad = torch.empty((nt, 3), dtype=torch.complex128, device=zs.device)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
+        p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+        check(lib().zfmm_zlfmm3d_dev(float(eps), int(ns), p(zs), int(ifcharge), p(q),
+                                     int(ifdipole), p(ds), p(dv), p(pot), p(grad), int(nt), p(zt),
+                                     int(ifpgh), int(isep), stream))
+        return pot, grad.t()
+    ns, nt = int(ns), int(nt)
+    zs = _pts(zsrc, 3, ns, "zsrc")
+    zt = _pts(ztarg, 3, nt, "ztarg")
+    q = _vec(charge, ns, "charge") if ifcharge == 1 else None
+    ds = _vec(dipstr, ns, "dipstr") if ifdipole == 1 else None
+    dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((3, nt), np.complex128, order="F")
+    check(lib().zfmm_zlfmm3d(float(eps), ns, _ptr(zs), int(ifcharge), _ptr(q), int(ifdipole),
+                             _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt, _ptr(zt), int(ifpgh),
+                             int(isep), 0))
+    return pot, grad
+
+
+def zl3devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
+    """3D Laplace direct sum with 1/(4 pi) (reference zlfmm3d.f:628-683)."""
+    ns, nt = int(ns), int(nt)
+    zs = _pts(zsrc, 3, ns, "zsrc")
+    zt = _pts(ztarg, 3, nt, "ztarg")
+    q = _vec(charge, ns, "charge") if ifcharge == 1 else None
+    ds = _vec(dipstr, ns, "dipstr") if ifdipole == 1 else None
+    dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((3, nt), np.complex128, order="F")
+    check(lib().zfmm_zl3devaldirect(nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds), _ptr(dv),
+                                    int(ifcharge), _ptr(pot), _ptr(grad), int(ifdipole),
+                                    int(ifpgh)))
+    return pot, grad
+
+
+def zl3dterms(eps):
+    """Expansion order of the 3D Laplace FMM (reference zlfmm3d.f:1283-1321)."""
+    return int(lib().zfmm_zl3dterms(float(eps)))
 
 
 def tree_dump(D, ndiv, zsrc, ztarg=None, isep=1):

@@ -47,10 +47,24 @@ SIGNATURES = {
     "zfmm_zh2devaldirect_dev": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
                                         c_int, c_void_p]),
+    "zlfmm3d_": (None, [c_void_p] * 15),
+    "zl3devaldirect_": (None, [c_void_p] * 12),
+    "zfmm_zlfmm3d": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                             c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int]),
+    "zfmm_zl3devaldirect": (c_int, [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_int, c_void_p, c_void_p, c_int, c_int]),
+    "zfmm_zlfmm3d_dev": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                                 c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
+                                 c_void_p]),
+    "zfmm_zl3devaldirect_dev": (c_int, [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_int, c_void_p, c_void_p, c_int, c_int,
+                                        c_void_p]),
+    "zfmm_zl3dterms": (c_int, [c_double]),
     "zfmm_set_step_timing": (None, [c_int]),
     "zfmm_last_step_times": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p]),
     "zfmm_last_counts": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_long)]),
     "zfmm_launch_count": (ctypes.c_long, []),
+    "zfmm_trim_pool": (ctypes.c_int, []),
     "zfmm_h2dterms": (c_int, [c_double, c_void_p, c_double, c_int]),
     "zfmm_tree_dump": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int,
                                c_int_p, c_int_p] + [c_void_p] * 12 + [c_int_p, c_void_p]),

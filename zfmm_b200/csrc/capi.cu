@@ -5,11 +5,13 @@
 // they are synchronous and reentrant across host threads.  Exceptions never
 // cross the ABI: they become status codes plus a thread-local message.
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "../../include/zfmm.h"
 #include "hfmm2d.cuh"
 #include "lfmm2d.cuh"
+#include "lfmm3d.cuh"
 
 using namespace zf;
 
@@ -17,6 +19,32 @@ namespace zf {
 long& launch_counter() {
   static thread_local long n = 0;
   return n;
+}
+
+namespace {
+constexpr int kMaxDev = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxDev] = {};
+}  // namespace
+
+cudaMemPool_t pool() {
+  int dev = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDev) throw zf_error(ZF_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p;
+    ZF_CUDA(cudaMemPoolCreate(&p, &props));
+    unsigned long long keep = ~0ull;
+    ZF_CUDA(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = p;
+  }
+  return g_pools[dev];
 }
 }  // namespace zf
 
@@ -173,6 +201,14 @@ int zfmm_last_counts(long long* counts16, long* launches) {
 }
 
 long zfmm_launch_count(void) { return launch_counter(); }
+
+int zfmm_trim_pool(void) {
+  return guarded([&] {
+    check_device();
+    ZF_CUDA(cudaDeviceSynchronize());
+    ZF_CUDA(cudaMemPoolTrimTo(pool(), 0));
+  });
+}
 
 int zfmm_h2dterms(double bsize, const double* zk, double eps, int isep) {
   if (!zk) return -1;
@@ -456,5 +492,186 @@ int zfmm_tree_dump(int D, int ndiv, int isep, int ns, const double* zsrc, int nt
     ZF_CUDA(cudaStreamSynchronize(s));
   });
 }
+
+}  // extern "C"
+
+// ---- 3D Laplace -------------------------------------------------------------
+namespace {
+
+Inputs3D make_inputs3(int ns, const double* zsrc, int ifcharge, const double* charge,
+                      int ifdipole, const double* dipstr, const double* dipvec, int nt,
+                      const double* ztarg, int ifpgh) {
+  Inputs3D in;
+  in.ns = ns;
+  in.nt = nt;
+  in.zsrc = reinterpret_cast<const zdc*>(zsrc);
+  in.charge = reinterpret_cast<const zdc*>(charge);
+  in.dipstr = reinterpret_cast<const zdc*>(dipstr);
+  in.dipvec = reinterpret_cast<const zdc*>(dipvec);
+  in.ztarg = reinterpret_cast<const zdc*>(ztarg);
+  in.ifcharge = ifcharge;
+  in.ifdipole = ifdipole;
+  in.ifpgh = ifpgh;
+  return in;
+}
+
+void run_fmm3d(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad, cudaStream_t s) {
+  // zlfmm3d.f:36-37: pot and grad are zeroed first
+  if (in.nt > 0) {
+    ZF_CUDA(cudaMemsetAsync(pot, 0, sizeof(zdc) * in.nt, s));
+    if (grad) ZF_CUDA(cudaMemsetAsync(grad, 0, sizeof(zdc) * 3 * in.nt, s));
+  }
+  if (in.ns == 0 || in.nt == 0) return;
+  if (isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
+  StepTimes t;
+  t.want_counts = g_timing >= 2;
+  zlfmm3d_device(eps, in, isep, pot, grad, s, g_timing ? &t : nullptr);
+  if (g_timing) g_times = t;
+}
+
+int fmm3d_host(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
+               int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+               double* grad, int nt, const double* ztarg, int ifpgh, int isep) {
+  return guarded([&] {
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    check_device();
+    cudaStream_t s = cudaStreamPerThread;
+    HostIn h;
+    upload(h.zsrc, zsrc, 3 * (size_t)ns, s);
+    upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
+    if (ifcharge == 1) upload(h.charge, charge, ns, s);
+    if (ifdipole == 1) {
+      upload(h.dipstr, dipstr, ns, s);
+      upload(h.dipvec, dipvec, 3 * (size_t)ns, s);
+    }
+    DevBuf<zdc> dpot(nt, s), dgrad(ifpgh > 1 ? 3 * (size_t)nt : 0, s);
+    Inputs3D in = make_inputs3(ns, (const double*)h.zsrc.get(), ifcharge,
+                               (const double*)h.charge.get(), ifdipole,
+                               (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
+                               (const double*)h.ztarg.get(), ifpgh);
+    run_fmm3d(eps, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
+    if (nt > 0) {
+      ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
+      if (grad) {
+        if (ifpgh > 1)
+          ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 3 * nt, cudaMemcpyDeviceToHost, s));
+        else
+          memset(grad, 0, sizeof(zdc) * 3 * nt);
+      }
+    }
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int direct3d_host(int nt, const double* ztarg, int ns, const double* zsrc, const double* charge,
+                  const double* dipstr, const double* dipvec, int ifcharge, double* pot,
+                  double* grad, int ifdipole, int ifpgh) {
+  return guarded([&] {
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = cudaStreamPerThread;
+    HostIn h;
+    upload(h.zsrc, zsrc, 3 * (size_t)ns, s);
+    upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
+    if (ifcharge == 1) upload(h.charge, charge, ns, s);
+    if (ifdipole == 1) {
+      upload(h.dipstr, dipstr, ns, s);
+      upload(h.dipvec, dipvec, 3 * (size_t)ns, s);
+    }
+    DevBuf<zdc> dpot, dgrad;
+    upload(dpot, pot, nt, s);
+    if (ifpgh > 1) upload(dgrad, grad, 3 * (size_t)nt, s);
+    Inputs3D in = make_inputs3(ns, (const double*)h.zsrc.get(), ifcharge == 1,
+                               (const double*)h.charge.get(), ifdipole == 1,
+                               (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
+                               (const double*)h.ztarg.get(), ifpgh);
+    zl3ddirect_device(in, dpot.get(), dgrad.get(), s);
+    ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
+    if (ifpgh > 1)
+      ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 3 * nt, cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int zfmm_zlfmm3d(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
+                 int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+                 double* grad, int nt, const double* ztarg, int ifpgh, int isep, int ifprint) {
+  (void)ifprint;
+  return fmm3d_host(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, nt,
+                    ztarg, ifpgh, isep);
+}
+
+void zlfmm3d_(const double* eps, const int* ns, const double* zsrc, int* ifcharge,
+              const double* charge, int* ifdipole, const double* dipstr, const double* dipvec,
+              double* pot, double* grad, const int* nt, const double* ztarg, int* ifpgh,
+              const int* isep, const int* ifprint) {
+  clamp_flags(*ifcharge, *ifdipole, *ifpgh);  // written back, as the reference does
+  int rc = fmm3d_host(*eps, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec, pot, grad,
+                      *nt, ztarg, *ifpgh, *isep);
+  if (rc != 0 && *nt > 0) {
+    memset(pot, 0, sizeof(double) * 2 * *nt);
+    if (grad) memset(grad, 0, sizeof(double) * 6 * *nt);
+  }
+  (void)ifprint;
+}
+
+int zfmm_zlfmm3d_dev(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
+                     int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+                     double* grad, int nt, const double* ztarg, int ifpgh, int isep,
+                     void* stream) {
+  return guarded([&] {
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs3D in = make_inputs3(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                               ifpgh);
+    run_fmm3d(eps, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_zl3devaldirect(int nt, const double* ztarg, int ns, const double* zsrc,
+                        const double* charge, const double* dipstr, const double* dipvec,
+                        int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
+  return direct3d_host(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, pot, grad, ifdipole,
+                       ifpgh);
+}
+
+void zl3devaldirect_(const int* nt, const double* ztarg, const int* ns, const double* zsrc,
+                     const double* charge, const double* dipstr, const double* dipvec,
+                     const int* ifcharge, double* pot, double* grad, const int* ifdipole,
+                     const int* ifpgh) {
+  zfmm_zl3devaldirect(*nt, ztarg, *ns, zsrc, charge, dipstr, dipvec, *ifcharge, pot, grad,
+                      *ifdipole, *ifpgh);
+}
+
+int zfmm_zl3devaldirect_dev(int nt, const double* ztarg, int ns, const double* zsrc,
+                            const double* charge, const double* dipstr, const double* dipvec,
+                            int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh,
+                            void* stream) {
+  return guarded([&] {
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs3D in = make_inputs3(ns, zsrc, ifcharge == 1, charge, ifdipole == 1, dipstr, dipvec, nt,
+                               ztarg, ifpgh);
+    zl3ddirect_device(in, (zdc*)pot, (zdc*)grad, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_zl3dterms(double eps) { return zl3dterms(eps); }
 
 }  // extern "C"

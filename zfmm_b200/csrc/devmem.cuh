@@ -1,8 +1,10 @@
 // Stream-ordered device buffers and error plumbing for the host orchestration.
 //
-// All scratch is taken from the device's default memory pool with
-// cudaMallocAsync/cudaFreeAsync on the call's stream, so repeated calls reuse
-// pool memory instead of hitting the driver allocator.  Errors are thrown as
+// All scratch is taken from a library-owned stream-ordered memory pool per
+// device (cudaMallocFromPoolAsync / cudaFreeAsync on the call's stream).  The
+// pool keeps freed memory mapped between calls (release threshold = max), so a
+// repeated solve of the same size maps no new pages; zfmm_trim_pool() returns
+// the cached memory to the driver.  Errors are thrown as
 // zf_error inside the library and turned into status codes at the C ABI.
 #pragma once
 #include <cuda_runtime.h>
@@ -24,6 +26,9 @@ enum Status {
   ZF_ERR_NOMEM = 3,
   ZF_ERR_INTERNAL = 4,
 };
+
+// the calling thread's current device's pool (created on first use)
+cudaMemPool_t pool();
 
 inline void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -51,13 +56,13 @@ class DevBuf {
     release();
     s_ = s;
     n_ = n;
-    if (n) ZF_CUDA(cudaMallocAsync((void**)&p_, n * sizeof(T), s));
+    if (n) ZF_CUDA(cudaMallocFromPoolAsync((void**)&p_, n * sizeof(T), pool(), s));
   }
   // grow to at least n elements keeping the first `keep` elements
   void grow(size_t n, size_t keep) {
     if (n <= n_) return;
     T* q = nullptr;
-    ZF_CUDA(cudaMallocAsync((void**)&q, n * sizeof(T), s_));
+    ZF_CUDA(cudaMallocFromPoolAsync((void**)&q, n * sizeof(T), pool(), s_));
     if (keep && p_) ZF_CUDA(cudaMemcpyAsync(q, p_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s_));
     if (p_) cudaFreeAsync(p_, s_);
     p_ = q;

@@ -1,0 +1,44 @@
+// Shared set-up of the 3D complex-coordinate FMMs (zlfmm3d / zhfmm3d):
+// real parts -> device octree -> sort -> reorder -> complex box centres ->
+// rescaling to the unit root box.
+//
+// Reference: zfmm3d/src/laplace/zlfmm3d.f:60-200 (identical steps in
+// zfmm3d/src/helmholtz/zhfmm3d.f:60-200).  After the centres are formed, every
+// coordinate, centre and box size is multiplied by b0inv = 1/boxsize(0),
+// charges by b0inv and dipole vectors by b0inv^2 (zlfmm3d.f:187-200).
+#pragma once
+#include <vector>
+#include "tree.cuh"
+#include "zcomplex.cuh"
+
+namespace zf {
+
+struct Inputs3D {
+  int ns = 0, nt = 0;
+  const zdc* zsrc = nullptr;    // zsrc(3,ns)
+  const zdc* charge = nullptr;
+  const zdc* dipstr = nullptr;
+  const zdc* dipvec = nullptr;  // dipvec(3,ns)
+  const zdc* ztarg = nullptr;   // ztarg(3,nt)
+  int ifcharge = 0, ifdipole = 0, ifpgh = 1;
+};
+
+struct Setup3D {
+  DevTree tree;
+  DevLists lists;
+  DevBuf<int> isrc, isrcse, itarg, itargse;
+  DevBuf<zdc> zsrcsort, ztargsort, chargesort, dipstrsort, dipvecsort;
+  DevBuf<zdc> zcsrc, zctarg;  // [3*nboxes], rescaled
+  double b0 = 1.0;            // boxsize(0) before rescaling
+  std::vector<double> bsz;    // rescaled box sizes per level
+};
+
+// `charge_scale` / `dipvec_scale`: the factors applied to the sorted strengths
+// (the Laplace driver uses b0inv and b0inv^2).
+void setup3d(const Inputs3D& in, const TreeParams& tp, Setup3D& S, bool rescale_charge,
+             bool rescale_dipvec, cudaStream_t s);
+
+void unsort3d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc pscale,
+              zdc gscale, int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);
+
+}  // namespace zf

@@ -1,0 +1,21 @@
+// 3D Laplace FMM and direct sum entry points (device pointers).
+#pragma once
+#include "fmm3d_common.cuh"
+#include "lfmm2d.cuh"
+
+namespace zf {
+
+// zl3dterms (zfmm3d/src/laplace/zlfmm3d.f:1283-1321)
+int zl3dterms(double eps);
+// lndiv (zfmm3d/src/common/lndiv_fast.f:17-35)
+int lndiv3d(double eps, int ns, int nt);
+
+// pot(nt), grad(3,nt) are overwritten; the 1/(4 pi) is included as in the
+// reference.  `times` as in the 2D drivers (counts[] of the 3D passes).
+void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
+                    cudaStream_t s, StepTimes* times);
+
+// zl3devaldirect over all pairs: ADDS the sums (with 1/(4 pi)) into pot/grad
+void zl3ddirect_device(const Inputs3D& in, zdc* pot, zdc* grad, cudaStream_t s);
+
+}  // namespace zf

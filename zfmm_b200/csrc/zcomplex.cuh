@@ -46,6 +46,7 @@ ZF_HD zdc operator/(zdc a, zdc b) {
   }
 }
 ZF_HD zdc zinv(zdc b) { return mkz(1.0) / b; }
+ZF_HD zdc operator/(double a, zdc b) { return mkz(a) / b; }
 
 ZF_HD zdc zsqrt_p(zdc z) {
   double x = z.re, y = z.im;

@@ -47,3 +47,34 @@ def clustered2d(n, seed=0, nclusters=5):
     im = 0.05 * np.sin(3 * x[0]) * np.cos(2 * x[1])
     z = x + 1j * im[None, :]
     return dict(zsrc=z, charge=cnormal(rng, n), dipstr=cnormal(rng, n), dipvec=cnormal(rng, 2, n))
+
+
+def lap3d_uniform(n=1_000_000, seed=0, nrhs=1, amp=0.05):
+    """zlfmm3d batched solve: real parts U[-1,1]^3, imaginary parts
+    amp*(sin 2pi x2, sin 2pi x3, sin 2pi x1) (amp = 0.05 in the benchmark); nrhs complex normal charge
+    vectors (charge has shape (n,) for nrhs == 1, else (nrhs, n)); dipole
+    strengths complex normal and real unit dipole vectors for the tests that
+    use them."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1.0, 1.0, size=(3, n))
+    im = amp * np.stack([np.sin(2 * np.pi * x[1]), np.sin(2 * np.pi * x[2]),
+                         np.sin(2 * np.pi * x[0])])
+    z = x + 1j * im
+    q = cnormal(rng, n) if nrhs == 1 else cnormal(rng, nrhs, n)
+    ds = cnormal(rng, n)
+    v = rng.standard_normal((3, n))
+    v /= np.linalg.norm(v, axis=0, keepdims=True)
+    return dict(zsrc=z, charge=q, dipstr=ds, dipvec=v.astype(np.complex128))
+
+
+def clustered3d(n, seed=0, nclusters=4):
+    """Gaussian clusters of different widths in 3D (adaptive octree with
+    non-empty lists 3 and 4), small smooth imaginary parts, complex dipoles."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-1, 1, size=(nclusters, 3))
+    w = 10.0 ** rng.uniform(-2, -0.5, nclusters)
+    k = rng.integers(0, nclusters, n)
+    x = c[k].T + w[k][None, :] * rng.standard_normal((3, n))
+    im = 0.03 * np.stack([np.sin(3 * x[1]), np.cos(2 * x[2]), np.sin(x[0] + x[1])])
+    z = x + 1j * im
+    return dict(zsrc=z, charge=cnormal(rng, n), dipstr=cnormal(rng, n), dipvec=cnormal(rng, 3, n))
