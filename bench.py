@@ -48,8 +48,44 @@ WORKLOADS = {
                                      isep=1, cpu_n=200_000),
     "zhfmm2d_curve_2m_eps1e-12": dict(kind="helm2d", n=2_000_000, eps=1e-12, zk=40 + 0.5j,
                                       ifpgh=2, isep=1, cpu_n=200_000),
+    # zlfmm3d single solve on the geometry of the batched configuration:
+    # 1,000,000 points U[-1,1]^3 with imaginary parts 0.05 sin(2 pi .), one
+    # charge vector, charges only, pot + grad, eps=1e-9
+    "zlfmm3d_uniform_1m": dict(kind="lap3d", n=1_000_000, eps=1e-9, ifpgh=2, isep=1,
+                               cpu_n=30_000, dipoles=False),
+    "zlfmm3d_uniform_200k": dict(kind="lap3d", n=200_000, eps=1e-9, ifpgh=2, isep=1,
+                                 cpu_n=30_000, dipoles=False),
 }
 DEFAULT_WORKLOAD = "zhfmm2d_curve_2m"
+
+def m2l3d_flops(p):
+    """Real flops of one point-and-shoot 3D Laplace translation at order p, as
+    implemented: two y-rotations, each sampling 2p+1 meridian points with 92
+    flops per (n, m >= 0, sample) and projecting with (p+1)^2 (2p+1) complex
+    MACs, plus the axial shift (one complex MAC per term of its Toeplitz sums)."""
+    ns = 2 * p + 1
+    sample = 92 * ns * (p + 1) * (p + 2) // 2
+    project = 8 * (p + 1) ** 2 * ns
+    shift = 8 * sum(p + 1 - abs(k) for j in range(p + 1) for k in range(-j, j + 1))
+    return 2 * (sample + project) + shift
+
+
+def flop_model3d(counts, p):
+    # per source (P2M/P2L): 42 flops per (n, m >= 0); per target and expansion
+    # (M2T/L2T with gradient): 80 flops per (n, m >= 0); P2P pair 90 flops
+    nm = (p + 1) * (p + 2) // 2
+    tr = m2l3d_flops(p)
+    steps = {
+        "p2m": 42 * nm * counts["p2m"],
+        "m2m": tr * counts["m2m_pairs"],
+        "m2l_p2l": tr * counts["m2l_pairs"] + 42 * nm * counts["p2l"],
+        "l2l": tr * counts["l2l_pairs"],
+        "eval": 90 * counts["p2p_pairs"] + 80 * nm * (counts["m2t"] + counts["l2t"]),
+    }
+    per = {"p2p_pair": 90, "translation": tr, "p2m_p2l_per_source": 42 * nm,
+           "m2t_l2t_per_target": 80 * nm}
+    return steps, per
+
 
 # Algorithmic work per interaction (real flops; complex add 2, mul 6, div 11;
 # transcendental functions are not counted), per the frozen convention of the
@@ -80,6 +116,8 @@ def make_inputs(wl, seed, n=None):
         return W.lap2d_uniform(n, seed=seed)
     if wl["kind"] == "helm2d":
         return W.curve2d(n, seed=seed)
+    if wl["kind"] == "lap3d":
+        return W.lap3d_uniform(n, seed=seed)
     raise ValueError(wl["kind"])
 
 
@@ -162,6 +200,10 @@ def cpu_time_oracle(wl, inp, reps_min=1, budget_s=15.0):
         if wl["kind"] == "lap2d":
             O.zlfmm2d(wl["eps"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
                       ifpgh=wl["ifpgh"], isep=wl["isep"])
+        elif wl["kind"] == "lap3d":
+            dip = wl.get("dipoles", True)
+            O.zlfmm3d(wl["eps"], z, inp["charge"], inp["dipstr"] if dip else None,
+                      inp["dipvec"].T if dip else None, ifpgh=wl["ifpgh"], isep=wl["isep"])
         else:
             O.zhfmm2d(wl["eps"], wl["zk"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
                       ifpgh=wl["ifpgh"], isep=wl["isep"])
@@ -215,12 +257,14 @@ def run_ours(args, wl, ws, rank, local):
     inp = make_inputs(wl, seed=rank)
     n = wl["n"]
     ifpgh, isep, eps = wl["ifpgh"], wl["isep"], wl["eps"]
-    # device-resident inputs (Fortran layout = (n, 2) row-major complex128)
+    d = 3 if wl["kind"] == "lap3d" else 2
+    ifd = 1 if wl.get("dipoles", True) else 0
+    # device-resident inputs (Fortran layout = (n, d) row-major complex128)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     zs = t(inp["zsrc"].T)
     q, ds, dv = t(inp["charge"]), t(inp["dipstr"]), t(inp["dipvec"].T)
     pot = torch.empty(n, dtype=torch.complex128, device=dev)
-    grad = torch.empty((n, 2), dtype=torch.complex128, device=dev)
+    grad = torch.empty((n, d), dtype=torch.complex128, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sp = ctypes.c_void_p(stream.cuda_stream)
@@ -233,6 +277,9 @@ def run_ours(args, wl, ws, rank, local):
     def solve():
         if helm:
             _capi.check(L.zfmm_zhfmm2d_dev(eps, zkp, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot),
+                                           P(grad), n, P(zs), ifpgh, isep, sp))
+        elif d == 3:
+            _capi.check(L.zfmm_zlfmm3d_dev(eps, n, P(zs), 1, P(q), ifd, P(ds), P(dv), P(pot),
                                            P(grad), n, P(zs), ifpgh, isep, sp))
         else:
             _capi.check(L.zfmm_zlfmm2d_dev(eps, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot),
@@ -279,12 +326,15 @@ def run_ours(args, wl, ws, rank, local):
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     hz, hq, hds, hdv = pin(inp["zsrc"].T), pin(inp["charge"]), pin(inp["dipstr"]), pin(inp["dipvec"].T)
     hpot = torch.empty(n, dtype=torch.complex128).pin_memory().numpy()
-    hgrad = torch.empty((n, 2), dtype=torch.complex128).pin_memory().numpy()
+    hgrad = torch.empty((n, d), dtype=torch.complex128).pin_memory().numpy()
     hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
 
     def solve_host():
         if helm:
             _capi.check(L.zfmm_zhfmm2d(eps, zkp, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv),
+                                       hp(hpot), hp(hgrad), n, hp(hz), ifpgh, isep, 0))
+        elif d == 3:
+            _capi.check(L.zfmm_zlfmm3d(eps, n, hp(hz), 1, hp(hq), ifd, hp(hds), hp(hdv),
                                        hp(hpot), hp(hgrad), n, hp(hz), ifpgh, isep, 0))
         else:
             _capi.check(L.zfmm_zlfmm2d(eps, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv), hp(hpot),
@@ -305,7 +355,7 @@ def run_ours(args, wl, ws, rank, local):
         tt = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_tot = float(tt.item())
-    h2d = hz.nbytes * 1 + hq.nbytes + hds.nbytes + hdv.nbytes + hz.nbytes  # zsrc, ztarg
+    h2d = hz.nbytes * 2 + hq.nbytes + (hds.nbytes + hdv.nbytes if ifd else 0)  # zsrc, ztarg
     d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
     # accuracy against the FP64 direct sum on a seeded subset of targets (device direct sum)
     pg = pot.cpu().numpy()
@@ -316,6 +366,9 @@ def run_ours(args, wl, ws, rank, local):
         pd, _ = zfmm_b200.zh2devaldirect(wl["zk"], len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
                                          inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
         pd = pd * 0.25j
+    elif d == 3:
+        pd, _ = zfmm_b200.zl3devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                         inp["charge"], inp["dipstr"], inp["dipvec"], 1, ifd, 1)
     else:
         pd, _ = zfmm_b200.zl2devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
                                          inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
@@ -324,7 +377,10 @@ def run_ours(args, wl, ws, rank, local):
 
     # roofline of the dominant kernel (FP64 pipe bound)
     p = info["nterms"]
-    flops, per = flop_model(wl["kind"], counts)
+    if d == 3:
+        flops, per = flop_model3d(counts, p)
+    else:
+        flops, per = flop_model(wl["kind"], counts)
     avg = {k: v / args.steps for k, v in step_ms.items()}
     top = max(flops, key=lambda k: avg[k])
     achieved = flops[top] / (avg[top] * 1e-3) / 1e12
@@ -351,7 +407,8 @@ def run_ours(args, wl, ws, rank, local):
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": {"workload": args.workload, "n": n, "eps": eps, "zk": str(wl.get("zk")),
                    "ifpgh": ifpgh, "isep": isep,
-                   "charges": True, "dipoles": True, "l2": "flushed (256 MiB write) between steps",
+                   "charges": True, "dipoles": bool(ifd),
+                   "l2": "flushed (256 MiB write) between steps",
                    "parallelism": f"replicas x{ws}", "nboxes": info["nboxes"],
                    "nlevels": info["nlevels"], "nterms": p},
         "e2e": {"value": ws * n * args.steps / e2e_tot, "unit": "targets/s",

@@ -93,6 +93,17 @@ int o_zlfmm3d(double eps, int ns, const double *zsrc, int ifcharge, const double
               int ifdipole, const double *dipstr, const double *dipvec, double *pot,
               double *grad, int nt, const double *ztarg, int ifpgh, int isep, int ifprint);
 
+/* 3D Helmholtz: direct sum (with 1/(4 pi), zhfmm3d.f:606-693) and FMM; zk = (re, im) */
+int o_h3dterms(double size, double zkr, double zki, double eps, int isep);
+void o_gauss_legendre(int n, double *x, double *w);
+void o_zh3devaldirect(const double *zk, int nt, const double *ztarg, int ns, const double *zsrc,
+                      const double *charge, const double *dipstr, const double *dipvec,
+                      int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
+int o_zhfmm3d(double eps, const double *zk, int ns, const double *zsrc, int ifcharge,
+              const double *charge, int ifdipole, const double *dipstr, const double *dipvec,
+              double *pot, double *grad, int nt, const double *ztarg, int ifpgh, int isep,
+              int ifprint);
+
 /* tree inspection helpers for tests: build the tree exactly as the 2D/3D drivers
  * do and copy out summary arrays.  Returns nboxes; fills nlevels. */
 int o_tree_info(int D, double eps_ndiv, int ndiv_override, const double *zsrc, int ns,

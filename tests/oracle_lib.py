@@ -255,3 +255,66 @@ def zl3ddirect(zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1)
                   ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     f(nt, _p(ztarg), ns, _p(zsrc), _p(q), _p(ds), _p(dv), ifc, _p(pot), _p(grad), ifd, ifpgh)
     return pot, grad
+
+
+def h3dterms(size, zk, eps, isep=1):
+    f = lib().o_h3dterms
+    f.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    f.restype = ctypes.c_int
+    zk = complex(zk)
+    return f(size, zk.real, zk.imag, eps, isep)
+
+
+def gauss_legendre(n):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    f = lib().o_gauss_legendre
+    f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    f(n, _p(x), _p(w))
+    return x, w
+
+
+def zhfmm3d(eps, zk, zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1, isep=1):
+    """Oracle zhfmm3d; arrays (n,3) complex."""
+    zsrc = c128(zsrc)
+    ns = zsrc.shape[0]
+    ztarg = zsrc if ztarg is None else c128(ztarg)
+    nt = ztarg.shape[0]
+    ifc = 0 if charge is None else 1
+    ifd = 0 if dipstr is None else 1
+    q = c128(charge) if ifc else np.zeros(1, np.complex128)
+    ds = c128(dipstr) if ifd else np.zeros(1, np.complex128)
+    dv = c128(dipvec) if ifd else np.zeros((1, 3), np.complex128)
+    k = np.array([complex(zk).real, complex(zk).imag])
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((nt, 3), np.complex128)
+    f = lib().o_zhfmm3d
+    f.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_int, ctypes.c_int]
+    rc = f(eps, _p(k), ns, _p(zsrc), ifc, _p(q), ifd, _p(ds), _p(dv), _p(pot), _p(grad), nt,
+           _p(ztarg), ifpgh, isep, 0)
+    assert rc == 0
+    return pot, grad
+
+
+def zh3ddirect(zk, zsrc, charge=None, dipstr=None, dipvec=None, ztarg=None, ifpgh=1):
+    zsrc = c128(zsrc)
+    ztarg = zsrc if ztarg is None else c128(ztarg)
+    ns, nt = zsrc.shape[0], ztarg.shape[0]
+    ifc = 0 if charge is None else 1
+    ifd = 0 if dipstr is None else 1
+    q = c128(charge) if ifc else np.zeros(1, np.complex128)
+    ds = c128(dipstr) if ifd else np.zeros(1, np.complex128)
+    dv = c128(dipvec) if ifd else np.zeros((1, 3), np.complex128)
+    k = np.array([complex(zk).real, complex(zk).imag])
+    pot = np.zeros(nt, np.complex128)
+    grad = np.zeros((nt, 3), np.complex128)
+    f = lib().o_zh3devaldirect
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    f(_p(k), nt, _p(ztarg), ns, _p(zsrc), _p(q), _p(ds), _p(dv), ifc, _p(pot), _p(grad), ifd,
+      ifpgh)
+    return pot, grad

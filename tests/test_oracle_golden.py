@@ -110,3 +110,42 @@ def test_fmm3d_laplace_fixture_matches_log():
     assert close5(np.linalg.norm(q), G["3d_laplace"]["charge_norm"][0])
     rel = err / (np.linalg.norm(pd) + np.linalg.norm(q))
     assert rel < 3 * 1.4130e-10
+
+
+def test_direct3d_helmholtz_first12():
+    z, q = fx("fixture3d.npz")
+    g = G["3d_helmholtz"]
+    assert abs(complex(*g["zk"]) - np.pi) < 1e-4
+    pot, _ = O.zh3ddirect(np.pi, z, q, ztarg=z[:12])  # test9.f: zk = pi
+    for p, (re, im) in zip(pot, g["pot0"]):
+        assert close5(p.real, re) and close5(p.imag, im)
+
+
+def test_fmm3d_helmholtz_fixture_matches_log():
+    """The reference's 3D Helmholtz test: zk = pi, eps = 1e-12, charges, pot
+    only; its log shows the first 12 potentials, |pot0| = 13.215 and
+    err/(|pot0|+|q|) = 8.8576e-10 (zfmm3d/test/helmholtz/fort.13:1-40)."""
+    z, q = fx("fixture3d.npz")
+    g = G["3d_helmholtz"]
+    zk = complex(*g["zk"])
+    assert abs(zk - np.pi) < 1e-4
+    zk = np.pi  # test9.f: zk = pi (the log prints 5 digits)
+    pot, _ = O.zhfmm3d(EPS12, zk, z, q)
+    for p, (re, im) in zip(pot[:12], g["pot"]):
+        assert close5(p.real, re) and close5(p.imag, im)
+    pd, _ = O.zh3ddirect(zk, z, q)
+    assert close5(np.linalg.norm(pd), g["pot0_norm"][0])
+    rel = np.linalg.norm(pot - pd) / (np.linalg.norm(pd) + np.linalg.norm(q))
+    assert rel < 3 * 8.8576e-10
+
+
+def test_h3dterms_levels_and_quadrature():
+    """h3dterms on the rescaled boxes of the fixture run, and the Gauss-Legendre
+    rule of the z-shifts against numpy's."""
+    import numpy.polynomial.legendre as leg
+    for n in [5, 30, 92, 125]:
+        x, w = O.gauss_legendre(n)
+        xr, wr = leg.leggauss(n)
+        assert np.abs(x - xr).max() < 1e-14 and np.abs(w - wr).max() < 1e-13
+    p = [O.h3dterms(2.0 ** -l, np.pi * G["3d_laplace"]["b0"][0], EPS12) for l in range(4)]
+    assert min(p) > 10 and max(p) < 200
