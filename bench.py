@@ -55,6 +55,13 @@ WORKLOADS = {
                                cpu_n=30_000, dipoles=False),
     "zlfmm3d_uniform_200k": dict(kind="lap3d", n=200_000, eps=1e-9, ifpgh=2, isep=1,
                                  cpu_n=30_000, dipoles=False),
+    # zhfmm3d single instance at the largest size of the batched configuration:
+    # 500,000 points on the unit sphere displaced by 0.1i times the normal
+    # scaled by a degree-4 field, zk = 10+0.2i, charges + dipoles, pot + grad
+    "zhfmm3d_sphere_500k": dict(kind="helm3d", n=500_000, eps=1e-9, zk=10 + 0.2j, ifpgh=2,
+                                isep=1, cpu_n=30_000),
+    "zhfmm3d_sphere_100k": dict(kind="helm3d", n=100_000, eps=1e-9, zk=10 + 0.2j, ifpgh=2,
+                                isep=1, cpu_n=30_000),
 }
 DEFAULT_WORKLOAD = "zhfmm2d_curve_2m"
 
@@ -70,20 +77,50 @@ def m2l3d_flops(p):
     return 2 * (sample + project) + shift
 
 
-def flop_model3d(counts, p):
-    # per source (P2M/P2L): 42 flops per (n, m >= 0); per target and expansion
-    # (M2T/L2T with gradient): 80 flops per (n, m >= 0); P2P pair 90 flops
-    nm = (p + 1) * (p + 2) // 2
-    tr = m2l3d_flops(p)
-    steps = {
-        "p2m": 42 * nm * counts["p2m"],
-        "m2m": tr * counts["m2m_pairs"],
-        "m2l_p2l": tr * counts["m2l_pairs"] + 42 * nm * counts["p2l"],
-        "l2l": tr * counts["l2l_pairs"],
-        "eval": 90 * counts["p2p_pairs"] + 80 * nm * (counts["m2t"] + counts["l2t"]),
-    }
-    per = {"p2p_pair": 90, "translation": tr, "p2m_p2l_per_source": 42 * nm,
-           "m2t_l2t_per_target": 80 * nm}
+def rot3d_flops(p):
+    """One point-and-shoot y-rotation of order p: 2p+1 meridian samples with 92
+    flops per (n, m >= 0, sample), then the (p+1)^2 (2p+1) complex-MAC DFT
+    projection."""
+    ns = 2 * p + 1
+    return 92 * ns * (p + 1) * (p + 2) // 2 + 8 * (p + 1) ** 2 * ns
+
+
+def h3d_trans_flops(p1, p2):
+    """One 3D Helmholtz translation (order p1 -> p2) as implemented: the two
+    rotations plus the quadrature z-shift at nquad = 2.5 p2 nodes: 70 flops per
+    (node, n, m >= 0) for the value/derivative sums, 5 per projection Legendre
+    term and 8 per (node, output coefficient) for the projection."""
+    nq = int(2.5 * p2)
+    quad = nq * (70 * (p1 + 1) * (p1 + 2) // 2 + 5 * (p2 + 1) * (p2 + 2) // 2
+                 + 8 * (p2 + 1) ** 2)
+    return rot3d_flops(p1) + rot3d_flops(p2) + quad
+
+
+def flop_model3d(kind, lvl, orders):
+    """Per-step flops from the per-level interaction counts (last_level_counts)
+    and the order of each level.  Per source (P2M/P2L) 42 (Laplace) or 50
+    (Helmholtz) flops per (n, m >= 0); per target and expansion (M2T/L2T with
+    gradient) 80; P2P pair 90 (Laplace) or 130 (Helmholtz)."""
+    L = len(orders)
+    nm = lambda p: (p + 1) * (p + 2) // 2
+    helm = kind == "helm3d"
+    src, pair = (50, 130) if helm else (42, 90)
+    tr = h3d_trans_flops if helm else (lambda p1, p2: m2l3d_flops(p1))
+    steps = {"p2m": 0, "m2m": 0, "m2l_p2l": 0, "l2l": 0, "eval": 0}
+    for l in range(L):
+        p = orders[l]
+        pc = orders[min(l + 1, L - 1)]
+        pp = orders[max(l - 1, 0)]
+        steps["p2m"] += src * nm(p) * lvl["p2m"][l]
+        steps["m2m"] += tr(pc, p) * lvl["m2m_pairs"][l]
+        steps["m2l_p2l"] += tr(p, p) * lvl["m2l_pairs"][l] + src * nm(p) * lvl["p2l"][l]
+        steps["l2l"] += tr(pp, p) * lvl["l2l_pairs"][l]
+        steps["eval"] += (pair * lvl["p2p_pairs"][l] + 80 * nm(pc) * lvl["m2t"][l]
+                          + 80 * nm(p) * lvl["l2t"][l])
+    pm = max(orders) if orders else 0
+    per = {"p2p_pair": pair, "translation_at_pmax": tr(pm, pm),
+           "p2m_p2l_per_source_per_nm": src, "m2t_l2t_per_target_per_nm": 80,
+           "orders_per_level": orders}
     return steps, per
 
 
@@ -118,6 +155,8 @@ def make_inputs(wl, seed, n=None):
         return W.curve2d(n, seed=seed)
     if wl["kind"] == "lap3d":
         return W.lap3d_uniform(n, seed=seed)
+    if wl["kind"] == "helm3d":
+        return W.sphere3d(n, seed=seed)
     raise ValueError(wl["kind"])
 
 
@@ -204,6 +243,9 @@ def cpu_time_oracle(wl, inp, reps_min=1, budget_s=15.0):
             dip = wl.get("dipoles", True)
             O.zlfmm3d(wl["eps"], z, inp["charge"], inp["dipstr"] if dip else None,
                       inp["dipvec"].T if dip else None, ifpgh=wl["ifpgh"], isep=wl["isep"])
+        elif wl["kind"] == "helm3d":
+            O.zhfmm3d(wl["eps"], wl["zk"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
+                      ifpgh=wl["ifpgh"], isep=wl["isep"])
         else:
             O.zhfmm2d(wl["eps"], wl["zk"], z, inp["charge"], inp["dipstr"], inp["dipvec"].T,
                       ifpgh=wl["ifpgh"], isep=wl["isep"])
@@ -257,7 +299,7 @@ def run_ours(args, wl, ws, rank, local):
     inp = make_inputs(wl, seed=rank)
     n = wl["n"]
     ifpgh, isep, eps = wl["ifpgh"], wl["isep"], wl["eps"]
-    d = 3 if wl["kind"] == "lap3d" else 2
+    d = 3 if wl["kind"] in ("lap3d", "helm3d") else 2
     ifd = 1 if wl.get("dipoles", True) else 0
     # device-resident inputs (Fortran layout = (n, d) row-major complex128)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -271,6 +313,7 @@ def run_ours(args, wl, ws, rank, local):
     P = lambda x: ctypes.c_void_p(x.data_ptr())
 
     helm = wl["kind"] == "helm2d"
+    helm3 = wl["kind"] == "helm3d"
     zkv = np.array([complex(wl.get("zk", 0)).real, complex(wl.get("zk", 0)).imag])
     zkp = zkv.ctypes.data_as(ctypes.c_void_p)
 
@@ -278,6 +321,9 @@ def run_ours(args, wl, ws, rank, local):
         if helm:
             _capi.check(L.zfmm_zhfmm2d_dev(eps, zkp, n, P(zs), 1, P(q), 1, P(ds), P(dv), P(pot),
                                            P(grad), n, P(zs), ifpgh, isep, sp))
+        elif helm3:
+            _capi.check(L.zfmm_zhfmm3d_dev(eps, zkp, n, P(zs), 1, P(q), ifd, P(ds), P(dv),
+                                           P(pot), P(grad), n, P(zs), ifpgh, isep, sp))
         elif d == 3:
             _capi.check(L.zfmm_zlfmm3d_dev(eps, n, P(zs), 1, P(q), ifd, P(ds), P(dv), P(pot),
                                            P(grad), n, P(zs), ifpgh, isep, sp))
@@ -293,6 +339,7 @@ def run_ours(args, wl, ws, rank, local):
     solve()
     counts, _ = zfmm_b200.last_counts()
     _, info = zfmm_b200.last_step_times()
+    lvl, orders = zfmm_b200.last_level_counts() if d == 3 else (None, None)
     L.zfmm_set_step_timing(1)
     ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -333,6 +380,9 @@ def run_ours(args, wl, ws, rank, local):
         if helm:
             _capi.check(L.zfmm_zhfmm2d(eps, zkp, n, hp(hz), 1, hp(hq), 1, hp(hds), hp(hdv),
                                        hp(hpot), hp(hgrad), n, hp(hz), ifpgh, isep, 0))
+        elif helm3:
+            _capi.check(L.zfmm_zhfmm3d(eps, zkp, n, hp(hz), 1, hp(hq), ifd, hp(hds), hp(hdv),
+                                       hp(hpot), hp(hgrad), n, hp(hz), ifpgh, isep, 0))
         elif d == 3:
             _capi.check(L.zfmm_zlfmm3d(eps, n, hp(hz), 1, hp(hq), ifd, hp(hds), hp(hdv),
                                        hp(hpot), hp(hgrad), n, hp(hz), ifpgh, isep, 0))
@@ -366,6 +416,10 @@ def run_ours(args, wl, ws, rank, local):
         pd, _ = zfmm_b200.zh2devaldirect(wl["zk"], len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
                                          inp["charge"], inp["dipstr"], inp["dipvec"], 1, 1, 1)
         pd = pd * 0.25j
+    elif helm3:
+        pd, _ = zfmm_b200.zh3devaldirect(wl["zk"], len(sub), inp["zsrc"][:, sub], n,
+                                         inp["zsrc"], inp["charge"], inp["dipstr"],
+                                         inp["dipvec"], 1, ifd, 1)
     elif d == 3:
         pd, _ = zfmm_b200.zl3devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
                                          inp["charge"], inp["dipstr"], inp["dipvec"], 1, ifd, 1)
@@ -378,7 +432,7 @@ def run_ours(args, wl, ws, rank, local):
     # roofline of the dominant kernel (FP64 pipe bound)
     p = info["nterms"]
     if d == 3:
-        flops, per = flop_model3d(counts, p)
+        flops, per = flop_model3d(wl["kind"], lvl, orders)
     else:
         flops, per = flop_model(wl["kind"], counts)
     avg = {k: v / args.steps for k, v in step_ms.items()}

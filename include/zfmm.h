@@ -78,6 +78,22 @@ void zl3devaldirect_(const int *nt, const double *ztarg, const int *ns, const do
                      const int *ifcharge, double *pot, double *grad, const int *ifdipole,
                      const int *ifpgh);
 
+/* Replaces zhfmm3d (zfmm3d/src/helmholtz/zhfmm3d.f:1-2; MATLAB spec
+ * zfmm3d/matlab_linux/zhfmm3d.mw:1).  zk points to one complex (re, im).
+ * pot = sum q e^{i k R}/(4 pi R) + dipole terms; the driver rescales the
+ * geometry to a unit root box (wavenumber zk*boxsize(0)) internally. */
+void zhfmm3d_(const double *eps, const double *zk, const int *ns, const double *zsrc,
+              int *ifcharge, const double *charge, int *ifdipole, const double *dipstr,
+              const double *dipvec, double *pot, double *grad, const int *nt,
+              const double *ztarg, int *ifpgh, const int *isep, const int *ifprint);
+
+/* Replaces zh3devaldirect (zfmm3d/src/helmholtz/zhfmm3d.f:606-607; MATLAB spec
+ * zfmm3d/matlab_linux/zh3devaldirect.mw:1).  ADDS the sums (with 1/(4 pi)). */
+void zh3devaldirect_(const double *zk, const int *nt, const double *ztarg, const int *ns,
+                     const double *zsrc, const double *charge, const double *dipstr,
+                     const double *dipvec, const int *ifcharge, double *pot, double *grad,
+                     const int *ifdipole, const int *ifpgh);
+
 /* C forms of the above (host arrays).  Flags are not modified; out-of-range
  * flags are clamped the same way as the reference (zlfmm2d.f:58-68). */
 int zfmm_zlfmm2d(double eps, int ns, const double *zsrc, int ifcharge, const double *charge,
@@ -135,6 +151,27 @@ int zfmm_zl3devaldirect_dev(int nt, const double *ztarg, int ns, const double *z
  * (zfmm3d/src/laplace/zlfmm3d.f:1283-1321).  Host computation. */
 int zfmm_zl3dterms(double eps);
 
+/* 3D Helmholtz, C forms: host arrays, then device pointers on `stream`. */
+int zfmm_zhfmm3d(double eps, const double *zk, int ns, const double *zsrc, int ifcharge,
+                 const double *charge, int ifdipole, const double *dipstr, const double *dipvec,
+                 double *pot, double *grad, int nt, const double *ztarg, int ifpgh, int isep,
+                 int ifprint);
+int zfmm_zh3devaldirect(const double *zk, int nt, const double *ztarg, int ns, const double *zsrc,
+                        const double *charge, const double *dipstr, const double *dipvec,
+                        int ifcharge, double *pot, double *grad, int ifdipole, int ifpgh);
+int zfmm_zhfmm3d_dev(double eps, const double *zk, int ns, const double *zsrc, int ifcharge,
+                     const double *charge, int ifdipole, const double *dipstr,
+                     const double *dipvec, double *pot, double *grad, int nt, const double *ztarg,
+                     int ifpgh, int isep, void *stream);
+int zfmm_zh3devaldirect_dev(const double *zk, int nt, const double *ztarg, int ns,
+                            const double *zsrc, const double *charge, const double *dipstr,
+                            const double *dipvec, int ifcharge, double *pot, double *grad,
+                            int ifdipole, int ifpgh, void *stream);
+/* Expansion order of the 3D Helmholtz FMM for a box of (rescaled) size
+ * `size` and wavenumber zk = (re, im); replaces h3dterms
+ * (zfmm3d/src/helmholtz/h3dterms.f:16-75).  Host computation. */
+int zfmm_h3dterms(double size, const double *zk, double eps, int isep);
+
 /* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory during a
  * solve: code whose device memory is owned by another allocator (a
@@ -172,6 +209,11 @@ int zfmm_last_counts(long long *counts16, long *launches);
  * computation, no GPU needed); replaces h2dterms
  * (zfmm2d/src/helmholtz/h2dterms.f:35-97).  zk points to (re, im). */
 int zfmm_h2dterms(double bsize, const double *zk, double eps, int isep);
+/* 3D FMMs with step timing level 2: the eight interaction counts of
+ * zfmm_last_counts per tree level, counts8x64[k*64 + level] (target level for
+ * P2P/M2T/L2T/M2L/P2L, parent level for M2M, child level for L2L), and the
+ * expansion order of each level, orders64[level]. */
+int zfmm_last_level_counts(long long *counts8x64, int *orders64, int *nlevels);
 /* Kernels launched by this library on the calling host thread so far. */
 long zfmm_launch_count(void);
 /* Device scratch comes from a library-owned memory pool per device that keeps

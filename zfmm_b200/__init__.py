@@ -20,7 +20,7 @@ import numpy as np
 from ._capi import ZfmmError, check, lib
 
 __all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "zlfmm3d", "zl3devaldirect",
-           "zl3dterms", "tree_dump", "ZfmmError",
+           "zhfmm3d", "zh3devaldirect", "zl3dterms", "h3dterms", "tree_dump", "ZfmmError",
            "set_step_timing", "last_step_times", "last_counts", "version"]
 
 
@@ -170,16 +170,8 @@ def zh2devaldirect(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, if
     return _direct2d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
 
 
-def zlfmm3d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
-            isep=1):
-    """3D Laplace FMM with complex coordinates (reference zlfmm3d.f:14-245).
-
-    pot(i) = sum_j charge_j / (4 pi R_ij) + dipole terms, R = sqrt(sum_k (x_k - y_k)^2)
-    on the principal branch.  zsrc, ztarg, dipvec: (3, n) or (n, 3) complex.
-    Returns (pot, grad) with grad of shape (3, nt).  numpy inputs run through the
-    host-array entry point, complex128 CUDA tensors through the device entry point
-    on the current stream (grad then is a (3, nt) view).
-    """
+def _fmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh,
+           isep):
     if _is_torch(zsrc):
         import torch
         zs = _torch_pts(zsrc, 3, ns, "zsrc")
@@ -191,9 +183,15 @@ def zlfmm3d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg
         grad = torch.empty((nt, 3), dtype=torch.complex128, device=zs.device)
         stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
         p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
-        check(lib().zfmm_zlfmm3d_dev(float(eps), int(ns), p(zs), int(ifcharge), p(q),
-                                     int(ifdipole), p(ds), p(dv), p(pot), p(grad), int(nt), p(zt),
-                                     int(ifpgh), int(isep), stream))
+        if zk is None:
+            check(lib().zfmm_zlfmm3d_dev(float(eps), int(ns), p(zs), int(ifcharge), p(q),
+                                         int(ifdipole), p(ds), p(dv), p(pot), p(grad), int(nt),
+                                         p(zt), int(ifpgh), int(isep), stream))
+        else:
+            k = _zk(zk)
+            check(lib().zfmm_zhfmm3d_dev(float(eps), _ptr(k), int(ns), p(zs), int(ifcharge),
+                                         p(q), int(ifdipole), p(ds), p(dv), p(pot), p(grad),
+                                         int(nt), p(zt), int(ifpgh), int(isep), stream))
         return pot, grad.t()
     ns, nt = int(ns), int(nt)
     zs = _pts(zsrc, 3, ns, "zsrc")
@@ -203,14 +201,44 @@ def zlfmm3d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg
     dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
     pot = np.zeros(nt, np.complex128)
     grad = np.zeros((3, nt), np.complex128, order="F")
-    check(lib().zfmm_zlfmm3d(float(eps), ns, _ptr(zs), int(ifcharge), _ptr(q), int(ifdipole),
-                             _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt, _ptr(zt), int(ifpgh),
-                             int(isep), 0))
+    if zk is None:
+        check(lib().zfmm_zlfmm3d(float(eps), ns, _ptr(zs), int(ifcharge), _ptr(q), int(ifdipole),
+                                 _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt, _ptr(zt),
+                                 int(ifpgh), int(isep), 0))
+    else:
+        k = _zk(zk)
+        check(lib().zfmm_zhfmm3d(float(eps), _ptr(k), ns, _ptr(zs), int(ifcharge), _ptr(q),
+                                 int(ifdipole), _ptr(ds), _ptr(dv), _ptr(pot), _ptr(grad), nt,
+                                 _ptr(zt), int(ifpgh), int(isep), 0))
     return pot, grad
 
 
-def zl3devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
-    """3D Laplace direct sum with 1/(4 pi) (reference zlfmm3d.f:628-683)."""
+def zlfmm3d(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
+            isep=1):
+    """3D Laplace FMM with complex coordinates (reference zlfmm3d.f:14-245).
+
+    pot(i) = sum_j charge_j / (4 pi R_ij) + dipole terms, R = sqrt(sum_k (x_k - y_k)^2)
+    on the principal branch.  zsrc, ztarg, dipvec: (3, n) or (n, 3) complex.
+    Returns (pot, grad) with grad of shape (3, nt).  numpy inputs run through the
+    host-array entry point, complex128 CUDA tensors through the device entry point
+    on the current stream (grad then is a (3, nt) view).
+    """
+    return _fmm3d(eps, None, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                  ifpgh, isep)
+
+
+def zhfmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg, ifpgh=1,
+            isep=1):
+    """3D Helmholtz FMM with complex coordinates (reference zhfmm3d.f:1-249).
+
+    pot(i) = sum_j charge_j e^{i zk R_ij} / (4 pi R_ij) + dipole terms, R as in
+    zlfmm3d.  Same layouts and return values as zlfmm3d.
+    """
+    return _fmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                  ifpgh, isep)
+
+
+def _direct3d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh):
     ns, nt = int(ns), int(nt)
     zs = _pts(zsrc, 3, ns, "zsrc")
     zt = _pts(ztarg, 3, nt, "ztarg")
@@ -219,10 +247,32 @@ def zl3devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipo
     dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
     pot = np.zeros(nt, np.complex128)
     grad = np.zeros((3, nt), np.complex128, order="F")
-    check(lib().zfmm_zl3devaldirect(nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds), _ptr(dv),
-                                    int(ifcharge), _ptr(pot), _ptr(grad), int(ifdipole),
-                                    int(ifpgh)))
+    if zk is None:
+        check(lib().zfmm_zl3devaldirect(nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds), _ptr(dv),
+                                        int(ifcharge), _ptr(pot), _ptr(grad), int(ifdipole),
+                                        int(ifpgh)))
+    else:
+        k = _zk(zk)
+        check(lib().zfmm_zh3devaldirect(_ptr(k), nt, _ptr(zt), ns, _ptr(zs), _ptr(q), _ptr(ds),
+                                        _ptr(dv), int(ifcharge), _ptr(pot), _ptr(grad),
+                                        int(ifdipole), int(ifpgh)))
     return pot, grad
+
+
+def zl3devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
+    """3D Laplace direct sum with 1/(4 pi) (reference zlfmm3d.f:628-683)."""
+    return _direct3d(None, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
+
+
+def zh3devaldirect(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
+    """3D Helmholtz direct sum with 1/(4 pi) (reference zhfmm3d.f:606-693)."""
+    return _direct3d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
+
+
+def h3dterms(size, zk, eps, isep=1):
+    """Expansion order of the 3D Helmholtz FMM (reference h3dterms.f:16-75)."""
+    k = _zk(zk)
+    return int(lib().zfmm_h3dterms(float(size), _ptr(k), float(eps), int(isep)))
 
 
 def zl3dterms(eps):
@@ -286,6 +336,20 @@ def last_counts():
     d = dict(zip(names, c[:8].tolist()))
     d.update({k + "_P": v for k, v in zip(names, c[8:].tolist()) if k != "p2p_pairs"})
     return d, nl.value
+
+
+def last_level_counts():
+    """Per-level interaction counts and expansion orders of the last 3D FMM
+    call made with set_step_timing(2): ({name: [count per level]}, [order per
+    level])."""
+    c = np.zeros(8 * 64, np.int64)
+    o = np.zeros(64, np.int32)
+    nl = ctypes.c_int()
+    lib().zfmm_last_level_counts(_ptr(c), _ptr(o), ctypes.byref(nl))
+    L = nl.value + 1
+    names = ["p2p_pairs", "m2t", "l2t", "m2l_pairs", "p2l", "m2m_pairs", "l2l_pairs", "p2m"]
+    c = c.reshape(8, 64)
+    return {k: c[i, :L].tolist() for i, k in enumerate(names)}, o[:L].tolist()
 
 
 def version():

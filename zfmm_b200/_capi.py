@@ -60,10 +60,25 @@ SIGNATURES = {
                                         c_void_p, c_int, c_void_p, c_void_p, c_int, c_int,
                                         c_void_p]),
     "zfmm_zl3dterms": (c_int, [c_double]),
+    "zhfmm3d_": (None, [c_void_p] * 16),
+    "zh3devaldirect_": (None, [c_void_p] * 13),
+    "zfmm_zhfmm3d": (c_int, [c_double, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int,
+                             c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                             c_int, c_int]),
+    "zfmm_zh3devaldirect": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                    c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int]),
+    "zfmm_zhfmm3d_dev": (c_int, [c_double, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int,
+                                 c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                                 c_int, c_void_p]),
+    "zfmm_zh3devaldirect_dev": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                        c_int, c_void_p]),
+    "zfmm_h3dterms": (c_int, [c_double, c_void_p, c_double, c_int]),
     "zfmm_set_step_timing": (None, [c_int]),
     "zfmm_last_step_times": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p]),
     "zfmm_last_counts": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_long)]),
     "zfmm_launch_count": (ctypes.c_long, []),
+    "zfmm_last_level_counts": (c_int, [c_void_p, c_void_p, c_int_p]),
     "zfmm_trim_pool": (ctypes.c_int, []),
     "zfmm_h2dterms": (c_int, [c_double, c_void_p, c_double, c_int]),
     "zfmm_tree_dump": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int,

@@ -12,6 +12,7 @@
 #include "hfmm2d.cuh"
 #include "lfmm2d.cuh"
 #include "lfmm3d.cuh"
+#include "hfmm3d.cuh"
 
 using namespace zf;
 
@@ -201,6 +202,14 @@ int zfmm_last_counts(long long* counts16, long* launches) {
 }
 
 long zfmm_launch_count(void) { return launch_counter(); }
+
+int zfmm_last_level_counts(long long* counts8x64, int* orders64, int* nlevels) {
+  for (int k = 0; k < 8; k++)
+    for (int l = 0; l < 64; l++) counts8x64[k * 64 + l] = (long long)g_times.lvl_counts[k][l];
+  for (int l = 0; l < 64; l++) orders64[l] = g_times.lvl_p[l];
+  if (nlevels) *nlevels = g_times.nlevels;
+  return 0;
+}
 
 int zfmm_trim_pool(void) {
   return guarded([&] {
@@ -515,7 +524,9 @@ Inputs3D make_inputs3(int ns, const double* zsrc, int ifcharge, const double* ch
   return in;
 }
 
-void run_fmm3d(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad, cudaStream_t s) {
+// zk == nullptr selects the Laplace FMM, otherwise Helmholtz with wavenumber *zk
+void run_fmm3d(double eps, const zdc* zk, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
+               cudaStream_t s) {
   // zlfmm3d.f:36-37: pot and grad are zeroed first
   if (in.nt > 0) {
     ZF_CUDA(cudaMemsetAsync(pot, 0, sizeof(zdc) * in.nt, s));
@@ -525,13 +536,14 @@ void run_fmm3d(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad, cu
   if (isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
   StepTimes t;
   t.want_counts = g_timing >= 2;
-  zlfmm3d_device(eps, in, isep, pot, grad, s, g_timing ? &t : nullptr);
+  if (zk) zhfmm3d_device(eps, *zk, in, isep, pot, grad, s, g_timing ? &t : nullptr);
+  else zlfmm3d_device(eps, in, isep, pot, grad, s, g_timing ? &t : nullptr);
   if (g_timing) g_times = t;
 }
 
-int fmm3d_host(double eps, int ns, const double* zsrc, int ifcharge, const double* charge,
-               int ifdipole, const double* dipstr, const double* dipvec, double* pot,
-               double* grad, int nt, const double* ztarg, int ifpgh, int isep) {
+int fmm3d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifcharge,
+               const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+               double* pot, double* grad, int nt, const double* ztarg, int ifpgh, int isep) {
   return guarded([&] {
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
@@ -551,7 +563,7 @@ int fmm3d_host(double eps, int ns, const double* zsrc, int ifcharge, const doubl
                                (const double*)h.charge.get(), ifdipole,
                                (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
                                (const double*)h.ztarg.get(), ifpgh);
-    run_fmm3d(eps, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
+    run_fmm3d(eps, zk, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
       if (grad) {
@@ -565,9 +577,9 @@ int fmm3d_host(double eps, int ns, const double* zsrc, int ifcharge, const doubl
   });
 }
 
-int direct3d_host(int nt, const double* ztarg, int ns, const double* zsrc, const double* charge,
-                  const double* dipstr, const double* dipvec, int ifcharge, double* pot,
-                  double* grad, int ifdipole, int ifpgh) {
+int direct3d_host(const zdc* zk, int nt, const double* ztarg, int ns, const double* zsrc,
+                  const double* charge, const double* dipstr, const double* dipvec, int ifcharge,
+                  double* pot, double* grad, int ifdipole, int ifpgh) {
   return guarded([&] {
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
@@ -589,7 +601,8 @@ int direct3d_host(int nt, const double* ztarg, int ns, const double* zsrc, const
                                (const double*)h.charge.get(), ifdipole == 1,
                                (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
                                (const double*)h.ztarg.get(), ifpgh);
-    zl3ddirect_device(in, dpot.get(), dgrad.get(), s);
+    if (zk) zh3ddirect_device(*zk, in, dpot.get(), dgrad.get(), s);
+    else zl3ddirect_device(in, dpot.get(), dgrad.get(), s);
     ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
     if (ifpgh > 1)
       ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 3 * nt, cudaMemcpyDeviceToHost, s));
@@ -605,8 +618,8 @@ int zfmm_zlfmm3d(double eps, int ns, const double* zsrc, int ifcharge, const dou
                  int ifdipole, const double* dipstr, const double* dipvec, double* pot,
                  double* grad, int nt, const double* ztarg, int ifpgh, int isep, int ifprint) {
   (void)ifprint;
-  return fmm3d_host(eps, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, nt,
-                    ztarg, ifpgh, isep);
+  return fmm3d_host(eps, nullptr, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot,
+                    grad, nt, ztarg, ifpgh, isep);
 }
 
 void zlfmm3d_(const double* eps, const int* ns, const double* zsrc, int* ifcharge,
@@ -614,8 +627,8 @@ void zlfmm3d_(const double* eps, const int* ns, const double* zsrc, int* ifcharg
               double* pot, double* grad, const int* nt, const double* ztarg, int* ifpgh,
               const int* isep, const int* ifprint) {
   clamp_flags(*ifcharge, *ifdipole, *ifpgh);  // written back, as the reference does
-  int rc = fmm3d_host(*eps, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec, pot, grad,
-                      *nt, ztarg, *ifpgh, *isep);
+  int rc = fmm3d_host(*eps, nullptr, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec,
+                      pot, grad, *nt, ztarg, *ifpgh, *isep);
   if (rc != 0 && *nt > 0) {
     memset(pot, 0, sizeof(double) * 2 * *nt);
     if (grad) memset(grad, 0, sizeof(double) * 6 * *nt);
@@ -635,7 +648,7 @@ int zfmm_zlfmm3d_dev(double eps, int ns, const double* zsrc, int ifcharge, const
     cudaStream_t s = (cudaStream_t)stream;
     Inputs3D in = make_inputs3(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
                                ifpgh);
-    run_fmm3d(eps, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
+    run_fmm3d(eps, nullptr, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
     ZF_CUDA(cudaStreamSynchronize(s));
   });
 }
@@ -643,8 +656,8 @@ int zfmm_zlfmm3d_dev(double eps, int ns, const double* zsrc, int ifcharge, const
 int zfmm_zl3devaldirect(int nt, const double* ztarg, int ns, const double* zsrc,
                         const double* charge, const double* dipstr, const double* dipvec,
                         int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
-  return direct3d_host(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, pot, grad, ifdipole,
-                       ifpgh);
+  return direct3d_host(nullptr, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, pot, grad,
+                       ifdipole, ifpgh);
 }
 
 void zl3devaldirect_(const int* nt, const double* ztarg, const int* ns, const double* zsrc,
@@ -673,5 +686,93 @@ int zfmm_zl3devaldirect_dev(int nt, const double* ztarg, int ns, const double* z
 }
 
 int zfmm_zl3dterms(double eps) { return zl3dterms(eps); }
+
+// ---- 3D Helmholtz ----
+int zfmm_zhfmm3d(double eps, const double* zk, int ns, const double* zsrc, int ifcharge,
+                 const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                 double* pot, double* grad, int nt, const double* ztarg, int ifpgh, int isep,
+                 int ifprint) {
+  (void)ifprint;
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  zdc k = mkz(zk[0], zk[1]);
+  return fmm3d_host(eps, &k, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                    nt, ztarg, ifpgh, isep);
+}
+
+void zhfmm3d_(const double* eps, const double* zk, const int* ns, const double* zsrc,
+              int* ifcharge, const double* charge, int* ifdipole, const double* dipstr,
+              const double* dipvec, double* pot, double* grad, const int* nt,
+              const double* ztarg, int* ifpgh, const int* isep, const int* ifprint) {
+  clamp_flags(*ifcharge, *ifdipole, *ifpgh);  // written back, as the reference does
+  int rc = zfmm_zhfmm3d(*eps, zk, *ns, zsrc, *ifcharge, charge, *ifdipole, dipstr, dipvec, pot,
+                        grad, *nt, ztarg, *ifpgh, *isep, *ifprint);
+  if (rc != 0 && *nt > 0) {
+    memset(pot, 0, sizeof(double) * 2 * *nt);
+    if (grad) memset(grad, 0, sizeof(double) * 6 * *nt);
+  }
+}
+
+int zfmm_zhfmm3d_dev(double eps, const double* zk, int ns, const double* zsrc, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr,
+                     const double* dipvec, double* pot, double* grad, int nt, const double* ztarg,
+                     int ifpgh, int isep, void* stream) {
+  return guarded([&] {
+    if (!zk) throw zf_error(ZF_ERR_ARG, "zk is null");
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    zdc k = mkz(zk[0], zk[1]);
+    Inputs3D in = make_inputs3(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
+                               ifpgh);
+    run_fmm3d(eps, &k, in, isep, (zdc*)pot, ifpgh > 1 ? (zdc*)grad : nullptr, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_zh3devaldirect(const double* zk, int nt, const double* ztarg, int ns, const double* zsrc,
+                        const double* charge, const double* dipstr, const double* dipvec,
+                        int ifcharge, double* pot, double* grad, int ifdipole, int ifpgh) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  zdc k = mkz(zk[0], zk[1]);
+  return direct3d_host(&k, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, pot, grad,
+                       ifdipole, ifpgh);
+}
+
+void zh3devaldirect_(const double* zk, const int* nt, const double* ztarg, const int* ns,
+                     const double* zsrc, const double* charge, const double* dipstr,
+                     const double* dipvec, const int* ifcharge, double* pot, double* grad,
+                     const int* ifdipole, const int* ifpgh) {
+  zfmm_zh3devaldirect(zk, *nt, ztarg, *ns, zsrc, charge, dipstr, dipvec, *ifcharge, pot, grad,
+                      *ifdipole, *ifpgh);
+}
+
+int zfmm_zh3devaldirect_dev(const double* zk, int nt, const double* ztarg, int ns,
+                            const double* zsrc, const double* charge, const double* dipstr,
+                            const double* dipvec, int ifcharge, double* pot, double* grad,
+                            int ifdipole, int ifpgh, void* stream) {
+  return guarded([&] {
+    if (!zk) throw zf_error(ZF_ERR_ARG, "zk is null");
+    check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
+                 ifpgh);
+    if (nt == 0 || ns == 0) return;
+    check_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    Inputs3D in = make_inputs3(ns, zsrc, ifcharge == 1, charge, ifdipole == 1, dipstr, dipvec, nt,
+                               ztarg, ifpgh);
+    zh3ddirect_device(mkz(zk[0], zk[1]), in, (zdc*)pot, (zdc*)grad, s);
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int zfmm_h3dterms(double size, const double* zk, double eps, int isep) {
+  if (!zk) return -1;
+  try {
+    return h3dterms_host(size, mkz(zk[0], zk[1]), eps, isep);
+  } catch (...) {
+    return -1;
+  }
+}
 
 }  // extern "C"

@@ -15,6 +15,10 @@ struct StepTimes {
   unsigned long long counts[16] = {0};  // [8..15]: weighted by P (see count_interactions2d)
   long launches = 0;  // kernels of this library launched by the call
   bool want_counts = false;  // also count interactions (extra kernel + sync)
+  // 3D drivers: the counts above per level (see count_interactions3d) and the
+  // expansion order of each level
+  unsigned long long lvl_counts[8][64] = {};
+  int lvl_p[64] = {};
 };
 
 int l2dterms(double eps);

@@ -35,28 +35,11 @@
 #include <vector>
 #include "lap3d_pair.cuh"
 #include "lfmm3d.cuh"
+#include "sph3d.cuh"
 
 namespace zf {
+
 namespace {
-
-constexpr double kPi = 3.14159265358979323846;
-constexpr double kF16 = (double)1e-16f;  // REAL*4 literal 1E-16 of the reference
-constexpr int TNT = 256;                 // threads of the translation kernel
-constexpr int FNT = 128;                 // threads of the form kernel (4 warps)
-constexpr int ENT = 128;                 // threads of the eval / P2P kernels
-constexpr int PTILE = 128;               // sources per P2P shared-memory tile
-
-// ---- tables -----------------------------------------------------------------
-struct Tab3 {
-  int p, NC, NS, nmax;
-  const double* r1;    // [(p+1)^2] ylgndrini rat1, (n, m) at n*(p+1)+m
-  const double* r2;    // rat2
-  const double* sq;    // sqrt(2n+1), n <= 2p+1
-  const double* amat;  // get_amat, (n, m) at n*(2nmax+1)+m+nmax, n <= nmax = 2p
-  const double* dinv;  // y-rotation projection weights, (n, |m|) at n*(p+1)+|m|
-  const zdc* tw;       // exp(-2 pi i k / (2p+1)), k < 2p+1
-};
-
 Tab3 make_tab3(int p) {
   int L = p + 1, N = p, nmax = 2 * p, NS = 2 * p + 1;
   std::vector<double> r1((size_t)L * L, 0.0), r2((size_t)L * L, 0.0);
@@ -162,6 +145,8 @@ Tab3 make_tab3(int p) {
   return T;
 }
 
+}  // namespace
+
 std::mutex g_tab_mu;
 std::map<std::pair<int, int>, Tab3> g_tabs;
 
@@ -177,230 +162,12 @@ Tab3 get_tab3(int p) {
   return T;
 }
 
-// ---- device helpers ---------------------------------------------------------
-__device__ __forceinline__ int ix3(int n, int m) { return n * n + n + m; }
+namespace {
 
-// degree n of the compact index idx = n*n + n + m
-__device__ __forceinline__ int deg3(int idx) {
-  int n = (int)sqrtf((float)idx);
-  if (n * n > idx) n--;
-  if ((n + 1) * (n + 1) <= idx) n++;
-  return n;
-}
-
-// x^n for n >= 0 by binary powering
-__device__ __forceinline__ double ipow(double x, int n) {
-  double r = 1.0;
-  while (n > 0) {
-    if (n & 1) r *= x;
-    x *= x;
-    n >>= 1;
-  }
-  return r;
-}
-
-// zsqrt (ztoolbox.f:110-124): phase atan2 in (-pi, pi] with -pi taken as pi
-__device__ __forceinline__ zdc zsqrt_r(zdc z2) {
-  double r = sqrt(zabs(z2));
-  double ph = atan2(z2.im, z2.re);
-  if (ph == -kPi) ph = kPi;
-  ph = ph * 0.5;
-  double s, c;
-  sincos(ph, &s, &c);
-  return mkz(r * c, r * s);
-}
-
-struct Sph {
-  zdc rz, ct, st, cp, sp, eip;
-};
-
-// zcart2sph (ztoolbox.f:132-160)
-__device__ __forceinline__ Sph zcart2sph(zdc x0, zdc x1, zdc x2, const zdc* c0) {
-  Sph s;
-  zdc z1 = x0 - c0[0], z2 = x1 - c0[1], z3 = x2 - c0[2];
-  zdc r2 = z1 * z1 + z2 * z2 + z3 * z3;
-  s.rz = zsqrt_r(r2);
-  s.ct = z3 / s.rz;
-  zdc zrxy = zsqrt_r(z1 * z1 + z2 * z2);
-  s.st = zrxy / s.rz;
-  if (zabs(zrxy) <= kF16) {
-    s.cp = mkz(1.0);
-    s.sp = mkz(0.0);
-    s.eip = mkz(1.0);
-  } else {
-    s.cp = z1 / zrxy;
-    s.sp = z2 / zrxy;
-    s.eip = s.cp + zmul_i(s.sp);
-  }
-  return s;
-}
-
-__device__ __forceinline__ void shfl_sum(zdc& v) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) v += shfl_xor_z(v, o);
-}
-
-// ---- translations -----------------------------------------------------------
-struct Geo {
-  bool zr, yr;
-  zdc cb, sb, ca, sa, zshift;
-};
-
-// geometry of zl3dmpmp / zl3dmploc / zl3dlocloc (zl3dtrans.f:1-321)
-__device__ __forceinline__ Geo geo3(const zdc* c0, const zdc* c) {
-  Geo g;
-  zdc x0 = c[0] - c0[0], x1 = c[1] - c0[1], x2 = c[2] - c0[2];
-  g.cb = mkz(1.0);
-  g.sb = mkz(0.0);
-  g.ca = mkz(1.0);
-  g.sa = mkz(0.0);
-  double e2 = zabs(x1);
-  g.zr = !(e2 <= kF16);
-  if (g.zr) {
-    zdc rxy = zsqrt_r(x0 * x0 + x1 * x1);
-    g.cb = -x0 / rxy;
-    g.sb = -x1 / rxy;
-    x0 = -rxy;
-  }
-  double e1 = zabs(x0);
-  g.yr = !(e1 <= kF16);
-  zdc zz = x2;
-  if (g.yr) {
-    zdc rxz = zsqrt_r(x0 * x0 + x2 * x2);
-    g.ca = x2 / rxz;
-    g.sa = x0 / rxz;
-    zz = rxz;
-  }
-  g.zshift = -zz;
-  return g;
-}
-
-// z3dyrot sampling (zrotate.f:94-239): thread jj < 2p+1 evaluates the
-// expansion `a` on the rotated meridian at angle 2 pi (jj-p)/(2p+1) and
-// writes F[n][jj] for every degree n.  Legendre columns stream in registers.
-__device__ void yrot_sample(const Tab3& T, const zdc* __restrict__ a, zdc* __restrict__ F,
-                            zdc ca, zdc sa) {
-  const int p = T.p, NS = T.NS, L = p + 1;
-  const int jj = threadIdx.x;
-  if (jj >= NS) return;
-  const int j = jj - p;
-  const double s4i = 1.0 / sqrt(4 * kPi);
-  double ph = j * 2 * kPi / (2 * p + 1);
-  double sph, cph;
-  sincos(ph, &sph, &cph);
-  zdc x1 = cph * ca, x2 = mkz(sph);
-  zdc zrxy = zsqrt_r(x1 * x1 + x2 * x2);
-  zdc ct = (-cph) * sa;
-  zdc st = zsqrt_r(mkz(1.0) - (cph * cph) * (mkz(1.0) - ca * ca));
-  if (ph == 0) st = (zabs(st + ca) <= zabs(st - ca)) ? -ca : ca;
-  zdc cp, sp, eip;
-  if (zabs(zrxy) >= kF16) {
-    cp = x1 / zrxy;
-    sp = x2 / zrxy;
-    eip = cp + zmul_i(sp);
-  } else {
-    cp = mkz(1.0);
-    sp = mkz(0.0);
-    eip = mkz(1.0);
-  }
-  zdc z1 = s4i * st, z2 = (st * ca - ct * cp * sa) * s4i, z3 = zmul_i(sp * sa * s4i);
-  // myzylgndr2sf (ztoolbox.f:273-327) with z = ct, stheta = st
-  const zdc z = ct, zz1 = mkz(1.0) - z * z;
-  const zdc u = (zabs(zz1) >= (double)1e-12f) ? -zsqrt_r(zz1) : -st;
-  const double* __restrict__ r1 = T.r1;
-  const double* __restrict__ r2 = T.r2;
-  const double* __restrict__ sq = T.sq;
-  zdc* Fj = F + jj;
-  // m = 0
-  {
-    zdc Ypp = mkz(1.0), Dpp = mkz(0.0), Yp = Ypp, Dp = Dpp;
-    {
-      zdc a0 = a[0];
-      Fj[0] = a0 * (Yp * s4i) - a0 * (Dp * z2 * st);
-    }
-    if (p >= 1) {
-      double c = __ldg(&r1[L]);
-      Yp = z * Ypp * c;
-      Dp = (z * Dpp + Ypp) * c;
-      zdc an = a[ix3(1, 0)];
-      zdc y = Yp * sq[1], d = Dp * sq[1];
-      Fj[NS] = an * (y * s4i) - an * (d * z2 * st);
-    }
-    for (int n = 2; n <= p; n++) {
-      double c1 = __ldg(&r1[n * L]), c2 = __ldg(&r2[n * L]);
-      zdc Y = (c1 * z) * Yp - c2 * Ypp;
-      zdc D = c1 * (z * Dp + Yp) - c2 * Dpp;
-      Ypp = Yp; Dpp = Dp; Yp = Y; Dp = D;
-      zdc an = a[ix3(n, 0)];
-      double s = __ldg(&sq[n]);
-      zdc y = Y * s, d = D * s;
-      Fj[n * NS] = an * (y * s4i) - an * (d * z2 * st);
-    }
-  }
-  zdc Ydiag = mkz(1.0), em = mkz(1.0);
-  for (int m = 1; m <= p; m++) {
-    double cmm = __ldg(&r1[m * L + m]);
-    Ydiag = (m == 1) ? mkz(-cmm) : (Ydiag * u) * cmm;
-    em = em * eip;
-    zdc emi = zinv(em);
-    double sg = (m & 1) ? -1.0 : 1.0;
-    double dm = (double)m;
-    zdc Yp = Ydiag, Dp = (Ydiag * (double)(-m)) * z;
-    zdc Ypp = mkz(0.0), Dpp = mkz(0.0);
-    for (int n = m; n <= p; n++) {
-      zdc Y, D;
-      if (n == m) {
-        Y = Yp;
-        D = Dp;
-      } else if (n == m + 1) {
-        double c = __ldg(&r1[n * L + m]);
-        Y = (z * Yp) * c;
-        D = (z * Dp + zz1 * Yp) * c;
-        Ypp = Yp; Dpp = Dp; Yp = Y; Dp = D;
-      } else {
-        double c1 = __ldg(&r1[n * L + m]), c2 = __ldg(&r2[n * L + m]);
-        Y = (c1 * z) * Yp - c2 * Ypp;
-        D = c1 * (z * Dp + zz1 * Yp) - c2 * Dpp;
-        Ypp = Yp; Dpp = Dp; Yp = Y; Dp = D;
-      }
-      double s = __ldg(&sq[n]);
-      zdc y = Y * s, d = D * s;
-      zdc z4 = a[ix3(n, m)] * em, z5 = a[ix3(n, -m)] * emi;
-      zdc z6 = z4 + z5;
-      zdc add = z6 * (z1 * y - z2 * d) + (dm * y) * (z3 * (z4 - z5));
-      Fj[n * NS] += sg * add;
-    }
-  }
-}
-
-// projection of z3dyrot: out(n, m) = dinv(n,|m|) * sum_j F[n][j] e^{-i m j 2 pi/(2p+1)}
-template <int KMAX>
-__device__ __forceinline__ void yrot_project(const Tab3& T, const zdc* __restrict__ F,
-                                             zdc* __restrict__ out, const zdc* __restrict__ tw) {
-  const int p = T.p, NS = T.NS, NC = T.NC;
-#pragma unroll
-  for (int k = 0; k < KMAX; k++) {
-    int idx = threadIdx.x + k * TNT;
-    if (idx < NC) {
-      int n = deg3(idx), m = idx - n * n - n;
-      int step = ((m % NS) + NS) % NS;
-      int kk = (int)((((long)m * (-p)) % NS + NS) % NS);
-      const zdc* Fn = F + n * NS;
-      zdc c0 = mkz(0.0), c1 = mkz(0.0);
-      int jj = 0;
-      for (; jj + 1 < NS; jj += 2) {
-        c0 += Fn[jj] * tw[kk];
-        kk += step;
-        if (kk >= NS) kk -= NS;
-        c1 += Fn[jj + 1] * tw[kk];
-        kk += step;
-        if (kk >= NS) kk -= NS;
-      }
-      if (jj < NS) c0 += Fn[jj] * tw[kk];
-      out[idx] = (c0 + c1) * __ldg(&T.dinv[n * (p + 1) + (m < 0 ? -m : m)]);
-    }
-  }
-}
+constexpr int TNT = 256;                 // threads of the translation kernel
+constexpr int FNT = 128;                 // threads of the form kernel (4 warps)
+constexpr int ENT = 128;                 // threads of the eval / P2P kernels
+constexpr int PTILE = 128;               // sources per P2P shared-memory tile
 
 struct TransArgs {
   Tab3 T;
@@ -414,7 +181,6 @@ struct TransArgs {
   int lo, hi;
 };
 
-__device__ __forceinline__ int nsrc(const int* se, int b) { return se[2 * b + 1] - se[2 * b] + 1; }
 
 // KIND 0: M2M into parent box, 1: M2L into target box, 2: L2L into child box
 template <int KIND, int KMAX>
@@ -533,9 +299,9 @@ __global__ void __launch_bounds__(TNT, 2) k_trans3(TransArgs A) {
     zdc* cur = sA;
     zdc* oth = sB;
     if (g.yr) {
-      yrot_sample(T, cur, sF, g.ca, g.sa);
+      yrot_sample(p, p + 1, T.r1, T.r2, T.sq, cur, sF, g.ca, g.sa);
       __syncthreads();
-      yrot_project<KMAX>(T, sF, oth, sTw);
+      yrot_project<KMAX, TNT>(p, p + 1, T.dinv, 1.0, sF, oth, sTw);
       __syncthreads();
       zdc* t = cur; cur = oth; oth = t;
     }
@@ -576,9 +342,9 @@ __global__ void __launch_bounds__(TNT, 2) k_trans3(TransArgs A) {
       zdc* t = cur; cur = oth; oth = t;
     }
     if (g.yr) {
-      yrot_sample(T, cur, sF, g.ca, -g.sa);
+      yrot_sample(p, p + 1, T.r1, T.r2, T.sq, cur, sF, g.ca, -g.sa);
       __syncthreads();
-      yrot_project<KMAX>(T, sF, oth, sTw);
+      yrot_project<KMAX, TNT>(p, p + 1, T.dinv, 1.0, sF, oth, sTw);
       __syncthreads();
       zdc* t = cur; cur = oth; oth = t;
     }
@@ -1066,38 +832,46 @@ __global__ void k_direct3d_reduce(int nt, int nsplit, const zdc* part, zdc* pot,
 }
 
 // ---- interaction counts ---------------------------------------------------------
+// per box: the interactions the drivers run, in totals cnt[0..7] and per
+// level cnt[16 + k*64 + level] (target level for P2P/M2T/L2T/M2L/P2L, parent
+// level for M2M, child level for L2L, leaf level for P2M); lmin: the coarsest
+// level at which P2M runs, M2M parents sit, and L2L children sit
 __global__ void k_count3(int nb, const int* ilevel, const int* iparent, const int* nchild,
                          const int* ichild, const int* isrcse, const int* itargse, const int* nl1,
                          const int* l1, int m1, const int* nl2, const int* l2, int m2,
                          const int* nl3, const int* l3, int m3, const int* nl4, const int* l4,
-                         int m4, unsigned long long* cnt) {
+                         int m4, int p2m_lmin, int m2m_lmin, int l2l_lmin,
+                         unsigned long long* cnt) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
   auto ns_ = [&](int x) { return isrcse[2 * x + 1] - isrcse[2 * x] + 1; };
   auto nt_ = [&](int x) { return itargse[2 * x + 1] - itargse[2 * x] + 1; };
   unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int ntb = nt_(b), nsb = ns_(b);
+  int ntb = nt_(b), nsb = ns_(b), lb = ilevel[b];
   if (nchild[b] == 0 && ntb > 0) {
     for (int i = 0; i < nl1[b]; i++) c[0] += (unsigned long long)ntb * max(0, ns_(l1[(size_t)b * m1 + i]));
     for (int i = 0; i < nl3[b]; i++)
       if (ns_(l3[(size_t)b * m3 + i]) > 0) c[1] += ntb;
-    if (ilevel[b] >= 2) c[2] = ntb;
+    if (lb >= 2) c[2] = ntb;
   }
   if (ntb > 0) {
     for (int i = 0; i < nl2[b]; i++)
       if (ns_(l2[(size_t)b * m2 + i]) > 0) c[3]++;
     for (int i = 0; i < nl4[b]; i++) c[4] += max(0, ns_(l4[(size_t)b * m4 + i]));
   }
-  if (nchild[b] > 0 && nsb > 0 && ilevel[b] >= 1)
+  if (nchild[b] > 0 && nsb > 0 && lb >= m2m_lmin)
     for (int k = 0; k < 8; k++)
       if (ns_(ichild[8 * b + k]) > 0) c[5]++;
-  if (ilevel[b] >= 2 && ntb > 0) {
+  if (lb >= l2l_lmin && ntb > 0) {
     int pb = iparent[b];
     if (nt_(pb) > 0 && (nl2[pb] > 0 || nl4[pb] > 0)) c[6] = 1;
   }
-  if (nchild[b] == 0 && nsb > 0 && ilevel[b] >= 1) c[7] = nsb;
+  if (nchild[b] == 0 && nsb > 0 && lb >= p2m_lmin) c[7] = nsb;
   for (int k = 0; k < 8; k++)
-    if (c[k]) atomicAdd(&cnt[k], c[k]);
+    if (c[k]) {
+      atomicAdd(&cnt[k], c[k]);
+      atomicAdd(&cnt[16 + k * 64 + lb], c[k]);
+    }
 }
 
 // ---- host helpers ---------------------------------------------------------------
@@ -1324,17 +1098,32 @@ void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* gra
     for (auto& e : ev) cudaEventDestroy(e);
     times->launches = launch_counter() - launches0;
     if (times->want_counts) {
-      DevBuf<unsigned long long> cnt(16, s);
-      cnt.zero();
-      klaunch(k_count3, div_up(nb, 256), 256, 0, s, nb, t.ilevel.get(), t.iparent.get(),
-              t.nchild.get(), t.ichild.get(), S.isrcse.get(), S.itargse.get(), L.n[0].get(),
-              L.list[0].get(), L.mn[0], L.n[1].get(), L.list[1].get(), L.mn[1], L.n[2].get(),
-              L.list[2].get(), L.mn[2], L.n[3].get(), L.list[3].get(), L.mn[3], cnt.get());
-      ZF_CUDA(cudaMemcpyAsync(times->counts, cnt.get(), 16 * sizeof(unsigned long long),
-                              cudaMemcpyDeviceToHost, s));
-      ZF_CUDA(cudaStreamSynchronize(s));
+      std::vector<int> pl(nlev + 1, p);
+      count_interactions3d(S, pl.data(), 1, 1, 2, times, s);
     }
   }
+}
+
+void count_interactions3d(const Setup3D& S, const int* p_per_level, int p2m_lmin, int m2m_lmin,
+                          int l2l_lmin, StepTimes* times, cudaStream_t s) {
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  int nb = t.nboxes;
+  DevBuf<unsigned long long> cnt(16 + 8 * 64, s);
+  cnt.zero();
+  klaunch(k_count3, div_up(nb, 256), 256, 0, s, nb, t.ilevel.get(), t.iparent.get(),
+          t.nchild.get(), t.ichild.get(), S.isrcse.get(), S.itargse.get(), L.n[0].get(),
+          L.list[0].get(), L.mn[0], L.n[1].get(), L.list[1].get(), L.mn[1], L.n[2].get(),
+          L.list[2].get(), L.mn[2], L.n[3].get(), L.list[3].get(), L.mn[3], p2m_lmin, m2m_lmin,
+          l2l_lmin, cnt.get());
+  std::vector<unsigned long long> h(16 + 8 * 64);
+  ZF_CUDA(cudaMemcpyAsync(h.data(), cnt.get(), h.size() * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, s));
+  ZF_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < 16; i++) times->counts[i] = h[i];
+  for (int k = 0; k < 8; k++)
+    for (int l = 0; l < 64; l++) times->lvl_counts[k][l] = h[16 + k * 64 + l];
+  for (int l = 0; l < 64; l++) times->lvl_p[l] = l <= t.nlevels ? p_per_level[l] : 0;
 }
 
 }  // namespace zf

@@ -15,6 +15,12 @@ int lndiv3d(double eps, int ns, int nt);
 void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
                     cudaStream_t s, StepTimes* times);
 
+// interaction counts of a 3D FMM on this set-up, totals and per level, into
+// times (counts, lvl_counts, lvl_p); p2m_lmin / m2m_lmin / l2l_lmin: the
+// coarsest level with P2M leaves / M2M parents / L2L children
+void count_interactions3d(const Setup3D& S, const int* p_per_level, int p2m_lmin, int m2m_lmin,
+                          int l2l_lmin, StepTimes* times, cudaStream_t s);
+
 // zl3devaldirect over all pairs: ADDS the sums (with 1/(4 pi)) into pot/grad
 void zl3ddirect_device(const Inputs3D& in, zdc* pot, zdc* grad, cudaStream_t s);
 

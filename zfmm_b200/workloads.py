@@ -78,3 +78,22 @@ def clustered3d(n, seed=0, nclusters=4):
     im = 0.03 * np.stack([np.sin(3 * x[1]), np.cos(2 * x[2]), np.sin(x[0] + x[1])])
     z = x + 1j * im
     return dict(zsrc=z, charge=cnormal(rng, n), dipstr=cnormal(rng, n), dipvec=cnormal(rng, 3, n))
+
+
+def sphere3d(n, seed=0, amp=0.1):
+    """Points uniform on the unit sphere, displaced by amp*i times the outward
+    normal scaled by a random smooth field of degree 4 (a seeded polynomial
+    of degree <= 4 in x, y, z, normalised to max |f| = 1 on the points);
+    complex normal charges and dipole strengths, complex normal dipole
+    vectors."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((3, n))
+    v /= np.linalg.norm(v, axis=0, keepdims=True)
+    f = np.zeros(n)
+    for a in range(5):
+        for b in range(5 - a):
+            for c in range(5 - a - b):
+                f += rng.standard_normal() * v[0] ** a * v[1] ** b * v[2] ** c
+    f /= np.abs(f).max()
+    z = v + 1j * amp * f[None, :] * v
+    return dict(zsrc=z, charge=cnormal(rng, n), dipstr=cnormal(rng, n), dipvec=cnormal(rng, 3, n))
