@@ -259,6 +259,12 @@ __global__ void __launch_bounds__(32 * WPB) k_hp2m(int nb, HelmArgs A, int pmax)
 
 // ---- dense translations --------------------------------------------------------
 // M2M (zh2dmpmp): children -> parent, level lev
+// M2M (zh2dmpmp): the reference's sum over child coefficients n,
+//   mp(m) += sum_n (-1)^(m+n) J_(m-n) e^{i(n-m) theta} mp_child(n) w(m, n),
+//   w = rs2^|n| rs1^|m-n| / rs1^|m|   (rs1 parent, rs2 child scale, rs2 <= rs1)
+// is a Toeplitz product in k = m - n once w is split by the signs of m, n:
+// opposite signs (or n = 0): (rs1 rs2)^|n|; same sign, |n| <= |m|:
+// (rs2/rs1)^|n|; same sign, |n| > |m|: (rs2/rs1)^|m| (rs1 rs2)^|k|.
 __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, HelmArgs A,
                                                   int stride) {
   extern __shared__ zdc sh[];
@@ -268,15 +274,18 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
   int n1 = A.T.p[lev], n2 = A.T.p[lev + 1], nt = n1 + n2;
   double rs1 = A.T.rs[lev], rs2 = A.T.rs[lev + 1];
   zdc* fj = sh + (threadIdx.x >> 5) * stride;   // [nt+2]
-  zdc* ez = fj + (nt + 2);                       // ez^k, k = -nt..nt at ez[nt + k]
-  double* r1 = (double*)(ez + 2 * nt + 1);       // rs1^k, k = 0..nt
-  double* r2 = r1 + nt + 1;
+  zdc* S1 = fj + (nt + 2) + nt;                  // S1[k], k = -nt..nt
+  zdc* S2 = S1 + nt + 1 + nt;                    // S1[k] (rs1 rs2)^|k|
+  zdc* uu = S2 + nt + 1 + n2;                    // (rs2/rs1)^|n| mp_child(n), n = -n2..n2
+  zdc* ww = uu + n2 + 1 + n2;                    // (rs1 rs2)^|n| mp_child(n)
+  double* qa = (double*)(ww + n2 + 1);           // (rs1 rs2)^k, k = 0..nt
+  double* qb = qa + nt + 1;                      // (rs2/rs1)^k, k = 0..nt
   zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
 #pragma unroll
   for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
   for (int k = lane; k <= nt; k += 32) {
-    r1[k] = pow(rs1, (double)k);
-    r2[k] = pow(rs2, (double)k);
+    qa[k] = pow(rs1 * rs2, (double)k);
+    qb[k] = pow(rs2 / rs1, (double)k);
   }
   for (int jc = 0; jc < 4; jc++) {
     int jb = A.ichild[4 * b + jc];
@@ -285,29 +294,47 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
     polar(A.zcsrc[2 * b] - A.zcsrc[2 * jb], A.zcsrc[2 * b + 1] - A.zcsrc[2 * jb + 1], rz, e);
     __syncwarp();
     if (lane == 0) jbessel_stream(nt, rz * A.zk, rs1, fj);
+    __syncwarp();
     zdc ie = zinv(e);
+    // S1[k] = (-1)^k t(k) e^{-ik theta}, t(k) = J_k (k >= 0), (-1)^k J_-k (k < 0)
     for (int k = lane; k <= nt; k += 32) {
-      ez[nt + k] = zpown(e, k);
-      ez[nt - k] = zpown(ie, k);
+      zdc f = fj[k];
+      S1[k] = (sgn(k) * f) * zpown(ie, k);
+      S1[-k] = f * zpown(e, k);
+      S2[k] = S1[k] * qa[k];
+      S2[-k] = S1[-k] * qa[k];
+    }
+    const zdc* M2 = expo(A, A.mp, jb);
+    for (int n = lane - n2; n <= n2; n += 32) {
+      zdc v = M2[n];
+      int an = abs(n);
+      uu[n] = qb[an] * v;
+      ww[n] = qa[an] * v;
     }
     __syncwarp();
-    const zdc* M2 = expo(A, A.mp, jb);
-    for (int m = lane - 0, r = 0; m <= n1; m += 32, r++) {
-      for (int half = 0; half < 2; half++) {
-        int mm = half ? -m : m;
-        if (half && m == 0) continue;
-        zdc s = mkz(0.0);
-        for (int n = -n2; n <= n2; n++) {
-          int k = mm - n;
-          double rfrac = r2[abs(n)] * r1[abs(k)] / r1[abs(mm)];
-          zdc t = (k >= 0) ? fj[k] : sgn(-k) * fj[-k];
-          t = (rfrac * sgn(mm + n)) * t;
-          s += t * (M2[n] * ez[nt + n - mm]);
-        }
-        if (mm == 0) acc0 += s;
-        else if (half) accm[r] += s;
-        else accp[r] += s;
+    for (int m = lane, r = 0; m <= n1; m += 32, r++) {
+      zdc a1 = mkz(0.0), a2 = mkz(0.0);
+      for (int n = -n2; n <= n2; n++) {
+        int k = m - n;
+        if (n <= 0) a1 += S1[k] * ww[n];
+        else if (n <= m) a1 += S1[k] * uu[n];
+        else a2 += S2[k] * M2[n];
       }
+      zdc sp = a1 + qb[m] * a2;
+      if (m == 0) {
+        acc0 += sp;
+        continue;
+      }
+      a1 = mkz(0.0);
+      a2 = mkz(0.0);
+      for (int n = -n2; n <= n2; n++) {
+        int k = -m - n;
+        if (n >= 0) a1 += S1[k] * ww[n];
+        else if (n >= -m) a1 += S1[k] * uu[n];
+        else a2 += S2[k] * M2[n];
+      }
+      accp[r] += sp;
+      accm[r] += a1 + qb[m] * a2;
     }
   }
   zdc* M = expo(A, A.mp, b);
@@ -330,8 +357,10 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const
   int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
   double rs = A.T.rs[l];
   zdc* fh = sh + (threadIdx.x >> 5) * stride;  // [n2+2]
-  zdc* ez = fh + (n2 + 2);                      // [2*n2+1]
-  double* rp = (double*)(ez + 2 * n2 + 1);      // rs^k, k = 0..n2
+  zdc* T = fh + (n2 + 2);                       // [2*n2+1]
+  double* rp = (double*)(T + 2 * n2 + 1);       // rs^k, k = 0..n2
+  zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;      // b(n), n = -p..p
+  zdc* cc = bb + 2 * p + 1;                     // c(n)
   zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
 #pragma unroll
   for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
@@ -345,28 +374,49 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const
     __syncwarp();
     h2dall_warp(n2, rz * A.zk, rs, fh);
     zdc ie = zinv(e);
+    // Toeplitz symbol T[k] = H_k e^{ik theta} (k = -2p..2p, H_-k = (-1)^k H_k,
+    // scaled) and the source coefficients without (b) and with (c) the factor
+    // rs^(2|n|): the reference's weight rs^|m| rs^|n| / rs^|n-m| is 1 for n, m
+    // of opposite signs and rs^(2 min(|m|,|n|)) otherwise, so
+    //   loc(m) = sum_{n<0} T[n-m] b(n) + sum_{0<=n<=m} T[n-m] c(n)
+    //          + rs^(2m) sum_{n>m} T[n-m] b(n)        (m >= 0, mirrored for m < 0)
     for (int k = lane; k <= n2; k += 32) {
-      ez[n2 + k] = zpown(e, k);
-      ez[n2 - k] = zpown(ie, k);
+      zdc f = fh[k];
+      T[n2 + k] = f * zpown(e, k);
+      T[n2 - k] = (sgn(k) * f) * zpown(ie, k);
+    }
+    const zdc* M = expo(A, A.mp, jb);
+    for (int n = lane - p; n <= p; n += 32) {
+      zdc v = M[n];
+      bb[n] = v;
+      cc[n] = rp[2 * abs(n)] * v;
     }
     __syncwarp();
-    const zdc* M = expo(A, A.mp, jb);
     for (int m = lane, r = 0; m <= p; m += 32, r++) {
-      for (int half = 0; half < 2; half++) {
-        int mm = half ? -m : m;
-        if (half && m == 0) continue;
-        zdc s = mkz(0.0);
-        for (int n = -p; n <= p; n++) {
-          int k = n - mm;
-          zdc t = (k >= 0) ? fh[k] : sgn(k) * fh[-k];
-          double f = rp[abs(mm)] * rp[abs(n)] / rp[abs(k)];
-          s += (f * t) * (M[n] * ez[n2 + k]);
-        }
-        if (mm == 0) acc0 += s;
-        else if (half) accm[r] += s;
-        else accp[r] += s;
+      zdc a1 = mkz(0.0), a2 = mkz(0.0);
+      const zdc* Tm = T + n2 - m;  // Tm[n] = T[n - m]
+      for (int n = -p; n <= p; n++) {
+        zdc t = Tm[n];
+        if (n > m) a2 += t * bb[n];
+        else a1 += t * (n < 0 ? bb[n] : cc[n]);
       }
+      zdc sp = a1 + rp[2 * m] * a2;
+      if (m == 0) {
+        acc0 += sp;
+        continue;
+      }
+      a1 = mkz(0.0);
+      a2 = mkz(0.0);
+      const zdc* Tq = T + n2 + m;  // Tq[n] = T[n + m]
+      for (int n = -p; n <= p; n++) {
+        zdc t = Tq[n];
+        if (n < -m) a2 += t * bb[n];
+        else a1 += t * (n > 0 ? bb[n] : cc[n]);
+      }
+      accp[r] += sp;
+      accm[r] += a1 + rp[2 * m] * a2;
     }
+    __syncwarp();
   }
   if (n4c > 0) {
     zdc* tab = fh;  // reuse: needs FCH*(p+2) <= stride
@@ -386,6 +436,10 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const
 }
 
 // L2L (zh2dlocloc) into the children at level lev+1
+// L2L (zh2dlocloc): loc_child(m) += sum_n t(n-m) e^{i(n-m) theta} loc(n)
+//   rs1^|m| rs1^|n-m| / rs2^|n|   (rs1 child, rs2 parent scale, rs1 <= rs2)
+// split by signs: same sign with |n| >= |m|: (rs1/rs2)^|n|; same sign with
+// |n| < |m| (and n = 0): (rs1/rs2)^|n| rs1^(2|k|); opposite: (rs1/rs2)^|n| rs1^(2|m|).
 __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, HelmArgs A,
                                                   const int* nl2, const int* nl4, int stride) {
   extern __shared__ zdc sh[];
@@ -396,38 +450,51 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
   if (A.itargse[2 * jb + 1] < A.itargse[2 * jb]) return;
   int n1 = A.T.p[lev + 1], n2 = A.T.p[lev], nt = n1 + n2;
   double rs1 = A.T.rs[lev + 1], rs2 = A.T.rs[lev];
-  zdc* fj = sh + (threadIdx.x >> 5) * stride;
-  zdc* ez = fj + (nt + 2);
-  double* r1 = (double*)(ez + 2 * nt + 1);
-  double* r2 = r1 + nt + 1;
+  zdc* fj = sh + (threadIdx.x >> 5) * stride;   // [nt+2]
+  zdc* S1 = fj + (nt + 2) + nt;                  // S1[k] = t(k) e^{ik theta}, k = -nt..nt
+  zdc* S3 = S1 + nt + 1 + nt;                    // S1[k] rs1^(2|k|)
+  zdc* uu = S3 + nt + 1 + n2;                    // (rs1/rs2)^|n| loc_parent(n)
+  double* qa = (double*)(uu + n2 + 1);           // rs1^(2k), k = 0..nt
+  double* qb = qa + nt + 1;                      // (rs1/rs2)^k, k = 0..nt
   for (int k = lane; k <= nt; k += 32) {
-    r1[k] = pow(rs1, (double)k);
-    r2[k] = pow(rs2, (double)k);
+    qa[k] = pow(rs1, 2.0 * k);
+    qb[k] = pow(rs1 / rs2, (double)k);
   }
   zdc rz, e;
   polar(A.zctarg[2 * jb] - A.zctarg[2 * b], A.zctarg[2 * jb + 1] - A.zctarg[2 * b + 1], rz, e);
   if (lane == 0) jbessel_stream(nt, rz * A.zk, rs1, fj);
+  __syncwarp();
   zdc ie = zinv(e);
   for (int k = lane; k <= nt; k += 32) {
-    ez[nt + k] = zpown(e, k);
-    ez[nt - k] = zpown(ie, k);
+    zdc f = fj[k];
+    S1[k] = f * zpown(e, k);
+    S1[-k] = (sgn(k) * f) * zpown(ie, k);
+    S3[k] = S1[k] * qa[k];
+    S3[-k] = S1[-k] * qa[k];
   }
-  __syncwarp();
   const zdc* L2 = expo(A, A.loc, b);
+  for (int n = lane - n2; n <= n2; n += 32) uu[n] = qb[abs(n)] * L2[n];
+  __syncwarp();
   zdc* L1 = expo(A, A.loc, jb);
   for (int m = lane; m <= n1; m += 32) {
-    for (int half = 0; half < 2; half++) {
-      int mm = half ? -m : m;
-      if (half && m == 0) continue;
-      zdc s = mkz(0.0);
-      for (int n = -n2; n <= n2; n++) {
-        int k = n - mm;
-        double rfrac = r1[abs(mm)] * r1[abs(k)] / r2[abs(n)];
-        zdc t = (k >= 0) ? fj[k] : sgn(k) * fj[-k];
-        s += (rfrac * t) * (L2[n] * ez[nt + k]);
-      }
-      L1[mm] += s;
+    zdc a1 = mkz(0.0), a2 = mkz(0.0);
+    for (int n = -n2; n <= n2; n++) {
+      int k = n - m;
+      if (n >= m) a1 += S1[k] * uu[n];
+      else if (n >= 0) a1 += S3[k] * uu[n];
+      else a2 += S1[k] * uu[n];
     }
+    L1[m] += a1 + qa[m] * a2;
+    if (m == 0) continue;
+    a1 = mkz(0.0);
+    a2 = mkz(0.0);
+    for (int n = -n2; n <= n2; n++) {
+      int k = n + m;
+      if (n <= -m) a1 += S1[k] * uu[n];
+      else if (n <= 0) a1 += S3[k] * uu[n];
+      else a2 += S1[k] * uu[n];
+    }
+    L1[-m] += a1 + qa[m] * a2;
   }
 }
 
@@ -718,6 +785,11 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   int grid_all = div_up(nb, WPB);
   // shared-memory strides (complex elements per warp)
   auto dense_stride = [](int ntt) { return (ntt + 2) + (2 * ntt + 1) + (ntt + 1 + 1); };
+  // M2M / L2L: J table, two Toeplitz symbols, two weighted input vectors and
+  // two real power tables
+  auto trans_stride = [](int ntt, int nin) {
+    return (ntt + 2) + 2 * (2 * ntt + 1) + 2 * (2 * nin + 1) + (ntt + 1);
+  };
   size_t sm_p2m = (size_t)WPB * FCH * (pmax + 2) * sizeof(zdc);
   ZF_CUDA(cudaFuncSetAttribute(k_hp2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
   klaunch(k_hp2m, grid_all, 32 * WPB, sm_p2m, s, nb, A, pmax);
@@ -725,7 +797,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   mark(2);
   for (int l = nlev - 1; l >= 2; l--) {
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
-    int stride = dense_stride(A.T.p[l] + A.T.p[l + 1]);
+    int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l + 1]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     ZF_CUDA(cudaFuncSetAttribute(k_hm2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     klaunch(k_hm2m, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, l, A, stride);
@@ -733,7 +805,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   ZF_LAUNCH_CHECK();
   mark(3);
   {
-    int stride = dense_stride(2 * pmax);
+    int stride = dense_stride(2 * pmax) + 2 * (2 * pmax + 1);
     if (stride < FCH * (pmax + 2)) stride = FCH * (pmax + 2);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     ZF_CUDA(cudaFuncSetAttribute(k_hm2l_p2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -744,7 +816,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   mark(4);
   for (int l = 2; l <= nlev - 1; l++) {
     int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
-    int stride = dense_stride(A.T.p[l] + A.T.p[l + 1]);
+    int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     ZF_CUDA(cudaFuncSetAttribute(k_hl2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     klaunch(k_hl2l, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, l, A, L.n[1].get(),
