@@ -237,10 +237,10 @@ __device__ void form_expansion(const HelmArgs& A, int s0, int s1, zdc c1, zdc c2
 
 constexpr int MAXR = 8;  // coefficient slots per lane: p <= 255
 
-__global__ void __launch_bounds__(32 * WPB) k_hp2m(int nb, HelmArgs A, int pmax) {
+__global__ void __launch_bounds__(32 * WPB) k_hp2m(int lo, int hi, HelmArgs A, int pmax) {
   extern __shared__ zdc sh[];
-  int b = blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b >= nb) return;
+  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (b > hi) return;
   int s0 = A.isrcse[2 * b], s1 = A.isrcse[2 * b + 1];
   if (A.nchild[b] > 0 || s1 < s0 || A.ilevel[b] < 2) return;
   int l = A.ilevel[b], p = A.T.p[l];
@@ -344,16 +344,17 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
   }
 }
 
-// M2L (zh2dmploc) over list2, then P2L (zh2dformloc) over list4
-__global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const int* nl2,
-                                                      const int* l2, int m2, const int* nl4,
-                                                      const int* l4, int m4, int stride) {
+// M2L (zh2dmploc) over list 2; R coefficient slots per lane (p < 32 R).  The
+// local expansion is written here; P2L (k_hp2l) adds to it afterwards.
+template <int R>
+__global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A, const int* nl2,
+                                                  const int* l2, int m2, int stride) {
   extern __shared__ zdc sh[];
-  int b = blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b >= nb) return;
+  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (b > hi) return;
   if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
-  int n2c = nl2[b], n4c = nl4[b];
-  if (n2c == 0 && n4c == 0) return;
+  int n2c = nl2[b];
+  if (n2c == 0) return;
   int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
   double rs = A.T.rs[l];
   zdc* fh = sh + (threadIdx.x >> 5) * stride;  // [n2+2]
@@ -361,9 +362,9 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const
   double* rp = (double*)(T + 2 * n2 + 1);       // rs^k, k = 0..n2
   zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;      // b(n), n = -p..p
   zdc* cc = bb + 2 * p + 1;                     // c(n)
-  zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
+  zdc accp[R], accm[R], acc0 = mkz(0.0);
 #pragma unroll
-  for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
+  for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
   for (int k = lane; k <= n2; k += 32) rp[k] = pow(rs, (double)k);
   zdc c1 = A.zctarg[2 * b], c2 = A.zctarg[2 * b + 1];
   for (int il = 0; il < n2c; il++) {
@@ -392,7 +393,10 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const
       cc[n] = rp[2 * abs(n)] * v;
     }
     __syncwarp();
-    for (int m = lane, r = 0; m <= p; m += 32, r++) {
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int m = lane + 32 * r;
+      if (m > p) break;
       zdc a1 = mkz(0.0), a2 = mkz(0.0);
       const zdc* Tm = T + n2 - m;  // Tm[n] = T[n - m]
       for (int n = -p; n <= p; n++) {
@@ -418,20 +422,49 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2l_p2l(int nb, HelmArgs A, const
     }
     __syncwarp();
   }
-  if (n4c > 0) {
-    zdc* tab = fh;  // reuse: needs FCH*(p+2) <= stride
-    for (int il = 0; il < n4c; il++) {
-      int jb = l4[(size_t)b * m4 + il];
-      int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
-      if (s1 < s0) continue;
-      __syncwarp();
-      form_expansion(A, s0, s1, c1, c2, rs, p, true, tab, accp, accm, acc0);
+  zdc* L = expo(A, A.loc, b);
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    int m = lane + 32 * r;
+    if (m > p) break;
+    if (m == 0) L[0] = acc0;
+    else {
+      L[m] = accp[r];
+      L[-m] = accm[r];
     }
+  }
+}
+
+// P2L (zh2dformloc) over list 4, added to the local expansion
+__global__ void __launch_bounds__(32 * WPB) k_hp2l(int lo, int hi, HelmArgs A, const int* nl4,
+                                                  const int* l4, int m4, int stride) {
+  extern __shared__ zdc sh[];
+  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (b > hi) return;
+  if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
+  int n4c = nl4[b];
+  if (n4c == 0) return;
+  int l = A.ilevel[b], p = A.T.p[l];
+  double rs = A.T.rs[l];
+  zdc* tab = sh + (threadIdx.x >> 5) * stride;  // FCH*(p+2)
+  zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
+#pragma unroll
+  for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
+  zdc c1 = A.zctarg[2 * b], c2 = A.zctarg[2 * b + 1];
+  for (int il = 0; il < n4c; il++) {
+    int jb = l4[(size_t)b * m4 + il];
+    int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
+    if (s1 < s0) continue;
+    __syncwarp();
+    form_expansion(A, s0, s1, c1, c2, rs, p, true, tab, accp, accm, acc0);
   }
   zdc* L = expo(A, A.loc, b);
   for (int m = lane, r = 0; m <= p; m += 32, r++) {
-    if (m == 0) L[0] = acc0;
-    else { L[m] = accp[r]; L[-m] = accm[r]; }
+    if (m == 0) L[0] += acc0;
+    else {
+      L[m] += accp[r];
+      L[-m] += accm[r];
+    }
   }
 }
 
@@ -790,9 +823,14 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   auto trans_stride = [](int ntt, int nin) {
     return (ntt + 2) + 2 * (2 * ntt + 1) + 2 * (2 * nin + 1) + (ntt + 1);
   };
-  size_t sm_p2m = (size_t)WPB * FCH * (pmax + 2) * sizeof(zdc);
-  ZF_CUDA(cudaFuncSetAttribute(k_hp2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
-  klaunch(k_hp2m, grid_all, 32 * WPB, sm_p2m, s, nb, A, pmax);
+  // P2M per level (leaves of levels >= 2), shared memory sized by the level's order
+  for (int l = 2; l <= nlev; l++) {
+    int pl = A.T.p[l];
+    size_t sm_p2m = (size_t)WPB * FCH * (pl + 2) * sizeof(zdc);
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    ZF_CUDA(cudaFuncSetAttribute(k_hp2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
+    klaunch(k_hp2m, div_up(hi - lo + 1, WPB), 32 * WPB, sm_p2m, s, lo, hi, A, pl);
+  }
   ZF_LAUNCH_CHECK();
   mark(2);
   for (int l = nlev - 1; l >= 2; l--) {
@@ -804,14 +842,36 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   }
   ZF_LAUNCH_CHECK();
   mark(3);
-  {
-    int stride = dense_stride(2 * pmax) + 2 * (2 * pmax + 1);
-    if (stride < FCH * (pmax + 2)) stride = FCH * (pmax + 2);
+  // one launch per level (lists 2 and 4 are empty on levels 0 and 1): the
+  // shared-memory stride and the register slots follow the level's order, so
+  // the many fine-level boxes run at full occupancy
+  for (int l = 2; l <= nlev; l++) {
+    int pl = A.T.p[l];
+    int stride = dense_stride(2 * pl) + 2 * (2 * pl + 1);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
-    ZF_CUDA(cudaFuncSetAttribute(k_hm2l_p2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    klaunch(k_hm2l_p2l, grid_all, 32 * WPB, sm, s, nb, A, L.n[1].get(), L.list[1].get(), L.mn[1],
-            L.n[3].get(), L.list[3].get(), L.mn[3], stride);
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+    auto go = [&](auto kern) {
+      ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, L.n[1].get(), L.list[1].get(), L.mn[1],
+              stride);
+    };
+    int R = (pl + 32) / 32;
+    if (R <= 1) go(k_hm2l<1>);
+    else if (R <= 2) go(k_hm2l<2>);
+    else if (R <= 4) go(k_hm2l<4>);
+    else go(k_hm2l<MAXR>);
   }
+  ZF_LAUNCH_CHECK();
+  if (L.mn[3] > 0)
+    for (int l = 2; l <= nlev; l++) {
+      int pl = A.T.p[l];
+      int stride = FCH * (pl + 2);
+      size_t sm = (size_t)WPB * stride * sizeof(zdc);
+      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+      ZF_CUDA(cudaFuncSetAttribute(k_hp2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      klaunch(k_hp2l, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, A, L.n[3].get(),
+              L.list[3].get(), L.mn[3], stride);
+    }
   ZF_LAUNCH_CHECK();
   mark(4);
   for (int l = 2; l <= nlev - 1; l++) {
