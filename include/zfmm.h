@@ -238,6 +238,9 @@ int zfmm_tree_dump(int D, int ndiv, int isep, int ns, const double *zsrc, int nt
 /* Measured FP64 FMA throughput of the current device in TFLOP/s (roofline
  * denominator for the FP64-bound kernels); -1 on error. */
 double zfmm_probe_fp64_tflops(int iters);
+/* Measured FP64 tensor-core (mma.sync m8n8k4 f64) throughput, TFLOP/s; -1 on
+ * error. */
+double zfmm_probe_dmma_tflops(int iters);
 
 /* Last error message of this host thread ("" when none). */
 const char *zfmm_last_error(void);

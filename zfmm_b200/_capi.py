@@ -84,6 +84,7 @@ SIGNATURES = {
     "zfmm_tree_dump": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int,
                                c_int_p, c_int_p] + [c_void_p] * 12 + [c_int_p, c_void_p]),
     "zfmm_probe_fp64_tflops": (c_double, [c_int]),
+    "zfmm_probe_dmma_tflops": (c_double, [c_int]),
     "zfmm_last_error": (ctypes.c_char_p, []),
     "zfmm_version": (ctypes.c_char_p, []),
 }
