@@ -62,6 +62,14 @@ WORKLOADS = {
                                 isep=1, cpu_n=30_000),
     "zhfmm3d_sphere_100k": dict(kind="helm3d", n=100_000, eps=1e-9, zk=10 + 0.2j, ifpgh=2,
                                 isep=1, cpu_n=30_000),
+    # zlfmm3d batched right-hand sides: one geometry of 1,000,000 points (the
+    # distribution above), 64 complex normal charge vectors, charges only,
+    # pot + grad, eps=1e-9; one step = plan (tree, lists, centres) + one
+    # 64-right-hand-side solve
+    "zlfmm3d_batched_1m_64": dict(kind="lap3d", n=1_000_000, nrhs=64, eps=1e-9, ifpgh=2, isep=1,
+                                  cpu_n=30_000, dipoles=False),
+    "zlfmm3d_batched_200k_64": dict(kind="lap3d", n=200_000, nrhs=64, eps=1e-9, ifpgh=2,
+                                    isep=1, cpu_n=30_000, dipoles=False),
 }
 DEFAULT_WORKLOAD = "zhfmm2d_curve_2m"
 
@@ -124,6 +132,24 @@ def flop_model3d(kind, lvl, orders):
     return steps, per
 
 
+def nd_trans3_flops(p, nd, kind=1):
+    """Real flops of one batched 3D Laplace translation of nd right-hand sides
+    at order p, as implemented: per 32-right-hand-side pass and rotation, the
+    (angle >= 0, order) recurrences and sample coefficients (100 flops per
+    angle, n, m >= 0); per right-hand side and rotation, the sample product on
+    sums / differences (2 (p+1) sum_n (n+1) complex MACs) and the cosine / sine
+    projection (2 (p+1) sum_n (n+1) real-by-complex MACs); per right-hand side
+    the axial shift (M2L: sum_m (p+1-|m|)^2 complex MACs, M2M / L2L half)."""
+    L = p + 1
+    tri = L * (L + 1) // 2
+    passes = -(-nd // 32)
+    gen = 2 * passes * 100 * L * tri
+    rot = 2 * nd * (2 * L * tri * 8 + 2 * L * tri * 4)
+    sh = sum((p + 1 - abs(m)) ** 2 for m in range(-p, p + 1))
+    shift = nd * 8 * (sh if kind == 1 else sh // 2)
+    return gen + rot + shift
+
+
 # Algorithmic work per interaction (real flops; complex add 2, mul 6, div 11;
 # transcendental functions are not counted), per the frozen convention of the
 # project's measurement plan.  P = 2p+1 coefficients of the level.
@@ -146,9 +172,11 @@ def flop_model(kind, counts):
     return steps, per
 
 
-def make_inputs(wl, seed, n=None):
+def make_inputs(wl, seed, n=None, nrhs=1):
     from zfmm_b200 import workloads as W
     n = wl["n"] if n is None else n
+    if wl["kind"] == "lap3d" and nrhs > 1:
+        return W.lap3d_uniform(n, seed=seed, nrhs=nrhs)
     if wl["kind"] == "lap2d":
         return W.lap2d_uniform(n, seed=seed)
     if wl["kind"] == "helm2d":
@@ -482,6 +510,189 @@ def run_ours(args, wl, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_ours_batched(args, wl, ws, rank, local):
+    """One step = plan (tree, lists, centres) + one nd-right-hand-side solve."""
+    import ctypes
+
+    import torch
+
+    import zfmm_b200
+    from zfmm_b200 import _capi
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _capi.lib()
+    n, nd = wl["n"], wl["nrhs"]
+    ifpgh, isep, eps = wl["ifpgh"], wl["isep"], wl["eps"]
+    inp = make_inputs(wl, seed=rank, nrhs=nd)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    zs = t(inp["zsrc"].T)
+    q = t(inp["charge"].T)  # (n, nd): right-hand side fastest
+    pot = torch.empty((n, nd), dtype=torch.complex128, device=dev)
+    grad = torch.empty((n, 3, nd), dtype=torch.complex128, device=dev)
+    pot1 = torch.empty(n, dtype=torch.complex128, device=dev)
+    grad1 = torch.empty((n, 3), dtype=torch.complex128, device=dev)
+    q0 = t(inp["charge"][0])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+    plan_ms = []
+
+    def solve():
+        h = ctypes.c_void_p()
+        _capi.check(L.zfmm_plan3d_create_dev(eps, n, P(zs), n, P(zs), isep, sp, ctypes.byref(h)))
+        _capi.check(L.zfmm_zlfmm3d_plan_dev(h, nd, 1, P(q), 0, None, None, ifpgh, P(pot),
+                                            P(grad), sp))
+        _capi.check(L.zfmm_plan3d_destroy(h))
+
+    def solve_plain():
+        _capi.check(L.zfmm_zlfmm3d_dev(eps, n, P(zs), 1, P(q0), 0, None, None, P(pot1),
+                                       P(grad1), n, P(zs), ifpgh, isep, sp))
+
+    for _ in range(max(args.warmup, 3)):
+        solve()
+    torch.cuda.synchronize()
+    L.zfmm_set_step_timing(2)
+    solve()
+    counts, _ = zfmm_b200.last_counts()
+    _, info = zfmm_b200.last_step_times()
+    lvl, orders = zfmm_b200.last_level_counts()
+    L.zfmm_set_step_timing(1)
+    step_ms = {k: 0.0 for k in ["setup", "p2m", "m2m", "m2l_p2l", "l2l", "eval", "unsort"]}
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.zfmm_launch_count()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            ev0[k].record(stream)
+            solve()
+            ev1[k].record(stream)
+            st, _ = zfmm_b200.last_step_times()
+            for kk in step_ms:
+                step_ms[kk] += st[kk]
+        torch.cuda.synchronize()
+    launches = L.zfmm_launch_count() - launches0
+    tot_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    # the plain single-right-hand-side solve on the same geometry, same run
+    for _ in range(2):
+        solve_plain()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nplain = 3
+    flush.fill_(1)
+    e0.record(stream)
+    for _ in range(nplain):
+        solve_plain()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / nplain
+    L.zfmm_set_step_timing(0)
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    value = ws * n * nd * args.steps / (tot_ms * 1e-3)
+    plain_value = n / (plain_ms * 1e-3)
+
+    # end to end: host arrays in pinned memory through the host entry points
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hz, hq = pin(inp["zsrc"].T), pin(inp["charge"].T)
+    hpot = torch.empty((n, nd), dtype=torch.complex128).pin_memory().numpy()
+    hgrad = torch.empty((n, 3, nd), dtype=torch.complex128).pin_memory().numpy()
+    hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def solve_host():
+        h = ctypes.c_void_p()
+        _capi.check(L.zfmm_plan3d_create(eps, n, hp(hz), n, hp(hz), isep, ctypes.byref(h)))
+        _capi.check(L.zfmm_zlfmm3d_plan(h, nd, 1, hp(hq), 0, None, None, ifpgh, hp(hpot),
+                                        hp(hgrad)))
+        _capi.check(L.zfmm_plan3d_destroy(h))
+
+    solve_host()
+    e2e_t = []
+    for k in range(args.steps):
+        flush.fill_(k & 255)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solve_host()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_tot = sum(e2e_t)
+    if ws > 1:
+        tt = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_tot = float(tt.item())
+    h2d = 2 * hz.nbytes + hq.nbytes
+    d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
+    # accuracy: right-hand sides 0 and nd-1 against the FP64 direct sum on a subset
+    rng = np.random.default_rng(1234)
+    sub = np.sort(rng.choice(n, size=min(n, 1024), replace=False))
+    pg = pot.cpu().numpy()
+    errs = []
+    for r in (0, nd - 1):
+        pd, _ = zfmm_b200.zl3devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                         inp["charge"][r], None, None, 1, 0, 1)
+        errs.append(float(np.linalg.norm(pg[sub, r] - pd) / np.linalg.norm(pd)))
+    # plain vs batched agreement on right-hand side 0 (same tree, same algorithm)
+    p1 = pot1.cpu().numpy()
+    agree = float(np.linalg.norm(pg[:, 0] - p1) / np.linalg.norm(p1))
+    # roofline: batched translations (M2L) against the FP64 peak
+    p = info["nterms"]
+    avg = {k: v / args.steps for k, v in step_ms.items()}
+    m2l_pairs = sum(lvl["m2l_pairs"])
+    flops_m2l = nd_trans3_flops(p, nd, 1) * m2l_pairs
+    achieved = flops_m2l / (avg["m2l_p2l"] * 1e-3) / 1e12
+    peak = float(L.zfmm_probe_fp64_tflops(20000))
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        ncpu = wl["cpu_n"]
+        cinp = make_inputs(wl, seed=0, n=ncpu)
+        t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
+        cpu = {"value": ncpu / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
+               "sample": (f"one right-hand side on {ncpu} points of the workload's distribution "
+                          f"(full workload: {n} points x {nd} right-hand sides, which the "
+                          f"reference solves as {nd} sequential calls), median of {nrep}")}
+    if rank != 0:
+        return
+    line = {
+        "metric": "targets/sec at eps=1e-9", "value": value, "unit": "targets/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "nrhs": nd, "eps": eps, "ifpgh": ifpgh,
+                   "isep": isep, "charges": True, "dipoles": False,
+                   "step": "plan (tree, lists, centres) + one solve of all right-hand sides",
+                   "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": f"replicas x{ws}", "nboxes": info["nboxes"],
+                   "nlevels": info["nlevels"], "nterms": p},
+        "e2e": {"value": ws * n * nd * args.steps / e2e_tot, "unit": "targets/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "plain_single_rhs": {"value": plain_value, "unit": "targets/s", "ms_per_solve": plain_ms,
+                             "batched_per_rhs_speedup": value / ws / plain_value},
+        "rel_l2_err_vs_direct": max(errs),
+        "rel_l2_batched_vs_plain_rhs0": agree,
+        "step_ms": {k: round(v, 4) for k, v in avg.items()},
+        "roofline": {"bound": "fp64", "kernel": "m2l_p2l (k_trans3nd)", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None,
+                     "peak_source": "measured FP64 FMA probe (zfmm_probe_fp64_tflops)",
+                     "traffic": None, "flops_per_step": flops_m2l,
+                     "flop_model": {"translation_nd": nd_trans3_flops(p, nd, 1),
+                                    "m2l_pairs": m2l_pairs}},
+        "interactions": counts,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -496,6 +707,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, wl, ws, rank)
+        elif wl.get("nrhs", 1) > 1:
+            run_ours_batched(args, wl, ws, rank, local)
         else:
             run_ours(args, wl, ws, rank, local)
     finally:

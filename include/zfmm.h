@@ -172,6 +172,32 @@ int zfmm_zh3devaldirect_dev(const double *zk, int nt, const double *ztarg, int n
  * (zfmm3d/src/helmholtz/h3dterms.f:16-75).  Host computation. */
 int zfmm_h3dterms(double size, const double *zk, double eps, int isep);
 
+/* 3D plans (no counterpart in the reference, whose drivers rebuild the tree
+ * on every call): the octree, sorted points, complex box centres and
+ * interaction lists of one geometry, built once (zlfmm3d.f:60-200 /
+ * zhfmm3d.f:60-200 up to the expansions) and reused by any number of solves,
+ * each with nd right-hand sides.  The tree depends on eps, the points and isep
+ * only, so one plan serves both kernels and every wavenumber.  Arrays of a
+ * solve follow the right-hand-side-fastest convention: charge(nd, ns),
+ * dipstr(nd, ns), pot(nd, nt), grad(nd, 3, nt); dipvec(3, ns) is shared by all
+ * right-hand sides.  A solve with nd = 1 gives the same values as
+ * zfmm_zlfmm3d on the same points (to rounding).  create: host arrays, or
+ * device pointers on `stream` for _dev; destroy waits for the device. */
+typedef struct zfmm_plan3d_s *zfmm_plan3d;
+int zfmm_plan3d_create(double eps, int ns, const double *zsrc, int nt, const double *ztarg,
+                       int isep, zfmm_plan3d *plan);
+int zfmm_plan3d_create_dev(double eps, int ns, const double *zsrc, int nt, const double *ztarg,
+                           int isep, void *stream, zfmm_plan3d *plan);
+int zfmm_plan3d_destroy(zfmm_plan3d plan);
+int zfmm_plan3d_info(zfmm_plan3d plan, int *nboxes, int *nlevels, int *ns, int *nt);
+/* 3D Laplace solves on a plan: host arrays, or device pointers on `stream`. */
+int zfmm_zlfmm3d_plan(zfmm_plan3d plan, int nd, int ifcharge, const double *charge,
+                      int ifdipole, const double *dipstr, const double *dipvec, int ifpgh,
+                      double *pot, double *grad);
+int zfmm_zlfmm3d_plan_dev(zfmm_plan3d plan, int nd, int ifcharge, const double *charge,
+                          int ifdipole, const double *dipstr, const double *dipvec, int ifpgh,
+                          double *pot, double *grad, void *stream);
+
 /* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory during a
  * solve: code whose device memory is owned by another allocator (a

@@ -21,7 +21,7 @@ from ._capi import ZfmmError, check, lib
 
 __all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "zlfmm3d", "zl3devaldirect",
            "zhfmm3d", "zh3devaldirect", "zl3dterms", "h3dterms", "tree_dump", "ZfmmError",
-           "set_step_timing", "last_step_times", "last_counts", "version"]
+           "set_step_timing", "last_step_times", "last_counts", "version", "Plan3D"]
 
 
 def _ptr(a):
@@ -267,6 +267,96 @@ def zl3devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipo
 def zh3devaldirect(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
     """3D Helmholtz direct sum with 1/(4 pi) (reference zhfmm3d.f:606-693)."""
     return _direct3d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
+
+
+def _mat(v, nd, n, name):
+    """(nd, n) complex, right-hand side fastest in memory (Fortran order)."""
+    a = np.asarray(v, dtype=np.complex128)
+    if nd == 1 and a.ndim == 1:
+        a = a.reshape(1, -1)
+    if a.shape != (nd, n):
+        raise ValueError(f"{name} must have shape ({nd}, {n}), got {a.shape}")
+    return np.asfortranarray(a)
+
+
+class Plan3D:
+    """Geometry of a 3D complex-coordinate FMM built once and reused.
+
+    The octree on the real parts, the sorted and rescaled points, the complex
+    box centres and the interaction lists (the set-up of zlfmm3d.f:60-200) are
+    built on the GPU when the plan is created; every solve then only forms,
+    translates and evaluates expansions, for nd right-hand sides at a time.
+
+        plan = Plan3D(eps, ns, zsrc, nt, ztarg, isep=1)
+        pot, grad = plan.zlfmm3d(nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh)
+
+    numpy: zsrc (3, ns), ztarg (3, nt); charge and dipstr (nd, ns); dipvec (3, ns),
+    shared by the right-hand sides; returns pot (nd, nt) and grad (nd, 3, nt).
+    torch (complex128 CUDA): zsrc (ns, 3), charge (ns, nd) contiguous; returns
+    views shaped (nd, nt) and (nd, 3, nt) of right-hand-side-fastest storage.
+    """
+
+    def __init__(self, eps, ns, zsrc, nt, ztarg, isep=1):
+        self._h = ctypes.c_void_p()
+        self.ns, self.nt, self.eps = int(ns), int(nt), float(eps)
+        if _is_torch(zsrc):
+            import torch
+            zs = _torch_pts(zsrc, 3, self.ns, "zsrc")
+            zt = _torch_pts(ztarg, 3, self.nt, "ztarg")
+            self.device = zs.device
+            stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
+            check(lib().zfmm_plan3d_create_dev(self.eps, self.ns, ctypes.c_void_p(zs.data_ptr()),
+                                               self.nt, ctypes.c_void_p(zt.data_ptr()),
+                                               int(isep), stream, ctypes.byref(self._h)))
+        else:
+            self.device = None
+            zs = _pts(zsrc, 3, self.ns, "zsrc")
+            zt = _pts(ztarg, 3, self.nt, "ztarg")
+            check(lib().zfmm_plan3d_create(self.eps, self.ns, _ptr(zs), self.nt, _ptr(zt),
+                                           int(isep), ctypes.byref(self._h)))
+
+    def info(self):
+        """(nboxes, nlevels) of the plan's tree."""
+        nb, nl, a, b = (ctypes.c_int() for _ in range(4))
+        check(lib().zfmm_plan3d_info(self._h, ctypes.byref(nb), ctypes.byref(nl),
+                                     ctypes.byref(a), ctypes.byref(b)))
+        return nb.value, nl.value
+
+    def zlfmm3d(self, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh=1):
+        """3D Laplace FMM of nd right-hand sides on the plan's points."""
+        nd, ns, nt = int(nd), self.ns, self.nt
+        if _is_torch(charge if ifcharge == 1 else dipstr):
+            import torch
+            dev = self.device
+            q = charge.contiguous() if ifcharge == 1 else None
+            ds = dipstr.contiguous() if ifdipole == 1 else None
+            dv = _torch_pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
+            pot = torch.empty((nt, nd), dtype=torch.complex128, device=dev)
+            grad = torch.empty((nt, 3, nd), dtype=torch.complex128, device=dev)
+            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+            p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+            check(lib().zfmm_zlfmm3d_plan_dev(self._h, nd, int(ifcharge), p(q), int(ifdipole),
+                                              p(ds), p(dv), int(ifpgh), p(pot), p(grad), stream))
+            return pot.t(), grad.permute(2, 1, 0)
+        q = _mat(charge, nd, ns, "charge") if ifcharge == 1 else None
+        ds = _mat(dipstr, nd, ns, "dipstr") if ifdipole == 1 else None
+        dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
+        pot = np.zeros((nd, nt), np.complex128, order="F")
+        grad = np.zeros((nd, 3, nt), np.complex128, order="F")
+        check(lib().zfmm_zlfmm3d_plan(self._h, nd, int(ifcharge), _ptr(q), int(ifdipole),
+                                      _ptr(ds), _ptr(dv), int(ifpgh), _ptr(pot), _ptr(grad)))
+        return pot, grad
+
+    def close(self):
+        if self._h:
+            check(lib().zfmm_plan3d_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def h3dterms(size, zk, eps, isep=1):

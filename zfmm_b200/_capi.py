@@ -83,6 +83,16 @@ SIGNATURES = {
     "zfmm_h2dterms": (c_int, [c_double, c_void_p, c_double, c_int]),
     "zfmm_tree_dump": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int,
                                c_int_p, c_int_p] + [c_void_p] * 12 + [c_int_p, c_void_p]),
+    "zfmm_plan3d_create": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int,
+                                   ctypes.POINTER(c_void_p)]),
+    "zfmm_plan3d_create_dev": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int,
+                                       c_void_p, ctypes.POINTER(c_void_p)]),
+    "zfmm_plan3d_destroy": (c_int, [c_void_p]),
+    "zfmm_plan3d_info": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p, c_int_p]),
+    "zfmm_zlfmm3d_plan": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                  c_int, c_void_p, c_void_p]),
+    "zfmm_zlfmm3d_plan_dev": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                      c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "zfmm_probe_fp64_tflops": (c_double, [c_int]),
     "zfmm_probe_dmma_tflops": (c_double, [c_int]),
     "zfmm_last_error": (ctypes.c_char_p, []),

@@ -114,7 +114,80 @@ __global__ void k_unsort3(int nt, const int* __restrict__ perm, const zdc* __res
     for (int d = 0; d < 3; d++) grad[3 * j + d] = gs[3 * i + d] * gscale;
 }
 
+__global__ void k_gather_nd(int ns, int nd, const int* __restrict__ perm,
+                            const zdc* __restrict__ q, const zdc* __restrict__ ds,
+                            const zdc* __restrict__ dv, const double* __restrict__ b0,
+                            int rescale_q, int rescale_dv, zdc* qs, zdc* dss, zdc* dvs) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= (long)ns * nd) return;
+  int i = (int)(k / nd), r = (int)(k - (long)i * nd);
+  double bi = 1.0 / b0[0];
+  long src = (long)perm[i] * nd + r;
+  qs[k] = q ? q[src] * (rescale_q ? bi : 1.0) : mkz(0.0);
+  dss[k] = ds ? ds[src] : mkz(0.0);
+  if (r == 0)
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      dvs[3 * i + d] = dv ? dv[3 * perm[i] + d] * (rescale_dv ? bi * bi : 1.0) : mkz(0.0);
+}
+
+__global__ void k_unsort_nd(int nt, int nd, const int* __restrict__ perm,
+                            const zdc* __restrict__ ps, const zdc* __restrict__ gs, zdc pscale,
+                            zdc gscale, int ifpgh, zdc* pot, zdc* grad) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= (long)nt * nd) return;
+  int i = (int)(k / nd), r = (int)(k - (long)i * nd);
+  long j = perm[i];
+  pot[j * nd + r] = ps[k] * pscale;
+  if (ifpgh > 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      grad[(3 * j + d) * nd + r] = gs[(3L * i + d) * nd + r] * gscale;
+}
+
 }  // namespace
+
+void setup3d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
+                  Setup3D& S, cudaStream_t s) {
+  DevBuf<double> srcR(3 * (size_t)ns, s), targR(3 * (size_t)nt, s);
+  klaunch(k_real3, div_up(3L * ns, TB), TB, 0, s, zsrc, 3L * ns, srcR.get());
+  klaunch(k_real3, div_up(3L * nt, TB), TB, 0, s, ztarg, 3L * nt, targR.get());
+  ZF_LAUNCH_CHECK();
+  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
+  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  S.b0 = S.tree.boxsize[0];
+  const double* b0 = S.tree.bsz.get();
+  S.zsrcsort.alloc(3 * (size_t)ns, s);
+  S.ztargsort.alloc(3 * (size_t)nt, s);
+  klaunch(k_gather3t, div_up(ns, TB), TB, 0, s, ns, S.isrc.get(), zsrc, b0, S.zsrcsort.get());
+  klaunch(k_gather3t, div_up(nt, TB), TB, 0, s, nt, S.itarg.get(), ztarg, b0,
+          S.ztargsort.get());
+  ZF_LAUNCH_CHECK();
+  centres3(S.tree, S.isrcse, S.zsrcsort, b0, S.zcsrc, s);
+  centres3(S.tree, S.itargse, S.ztargsort, b0, S.zctarg, s);
+  build_lists(S.tree, S.lists, s);
+  S.bsz.resize(S.tree.nlevels + 1);
+  for (int l = 0; l <= S.tree.nlevels; l++) S.bsz[l] = S.tree.boxsize[l] / S.b0;
+}
+
+void gather_strengths_nd(const Setup3D& S, int ns, int nd, const zdc* charge,
+                         const zdc* dipstr, const zdc* dipvec, bool rescale_charge,
+                         bool rescale_dipvec, zdc* q, zdc* ds, zdc* dv, cudaStream_t s) {
+  if (ns <= 0) return;
+  klaunch(k_gather_nd, div_up((long)ns * nd, TB), TB, 0, s, ns, nd, S.isrc.get(), charge,
+          dipstr, dipvec, S.tree.bsz.get(), rescale_charge ? 1 : 0, rescale_dipvec ? 1 : 0, q,
+          ds, dv);
+  ZF_LAUNCH_CHECK();
+}
+
+void unsort3d_nd(int nt, int nd, const int* itarg, const zdc* potsort, const zdc* gradsort,
+                 zdc pscale, zdc gscale, int ifpgh, zdc* pot, zdc* grad, cudaStream_t s) {
+  if (nt <= 0) return;
+  klaunch(k_unsort_nd, div_up((long)nt * nd, TB), TB, 0, s, nt, nd, itarg, potsort, gradsort,
+          pscale, gscale, ifpgh, pot, grad);
+  ZF_LAUNCH_CHECK();
+}
 
 void setup3d(const Inputs3D& in, const TreeParams& tp, Setup3D& S, bool rescale_charge,
              bool rescale_dipvec, cudaStream_t s) {

@@ -38,6 +38,24 @@ struct Setup3D {
 void setup3d(const Inputs3D& in, const TreeParams& tp, Setup3D& S, bool rescale_charge,
              bool rescale_dipvec, cudaStream_t s);
 
+// the geometric part of setup3d only (tree, sort, sorted rescaled points,
+// complex centres, lists); the strength arrays of S stay empty
+void setup3d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
+                  Setup3D& S, cudaStream_t s);
+
+// strengths of nd right-hand sides in tree order: charge(nd, ns) and
+// dipstr(nd, ns) (right-hand side fastest) -> q[i*nd + r], ds[i*nd + r];
+// dipvec(3, ns), shared by the right-hand sides -> dv[3*i + d]; the rescaling
+// flags as in setup3d.  Null inputs give zeros.
+void gather_strengths_nd(const Setup3D& S, int ns, int nd, const zdc* charge, const zdc* dipstr,
+                         const zdc* dipvec, bool rescale_charge, bool rescale_dipvec, zdc* q,
+                         zdc* ds, zdc* dv, cudaStream_t s);
+
+// pot(nd, nt) = pscale * potsort, grad(nd, 3, nt) = gscale * gradsort, from
+// tree order back to the caller's order
+void unsort3d_nd(int nt, int nd, const int* itarg, const zdc* potsort, const zdc* gradsort,
+                 zdc pscale, zdc gscale, int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);
+
 void unsort3d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc pscale,
               zdc gscale, int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);
 

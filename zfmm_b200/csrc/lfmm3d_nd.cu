@@ -1,0 +1,1286 @@
+// 3D Laplace FMM for many right-hand sides on one geometry (a plan).
+//
+// The same algorithm as zlfmm3d (zfmm3d/src/laplace/zlfmm3d.f:252-622) with
+// every expansion, strength and output carrying a right-hand-side index r
+// fastest: expansion (box, coefficient n*n+n+m, r) at
+// (box * (p+1)^2 + n*n+n+m) * nd + r, strengths q[i*nd + r], potentials
+// pot[i*nd + r], gradients grad[(3i+d)*nd + r].  Geometry-dependent work
+// (Legendre recurrences, rotation samples, shift tables, pair distances) is
+// computed once per box pair, source or target and applied to every
+// right-hand side.
+//
+// Kernels:
+//   k_trans3nd  M2M / M2L / L2L.  The point-and-shoot translation of
+//               zl3dmpmp / zl3dmploc / zl3dlocloc (zl3dtrans.f:1-540): z-rotation,
+//               y-rotation by sampling on the rotated meridian (the
+//               recurrences of myzylgndr2sf, ztoolbox.f:273-327) and projection
+//               by a DFT (z3dyrot, zrotate.f:94-239), axial shift, inverse
+//               rotations.  The y-rotation is streamed one degree n at a time:
+//               the sample coefficients of degree n for all angles come from
+//               (angle, order) recurrence states held in registers (one state per
+//               thread slot), and are applied to 32 right-hand sides (one per
+//               lane) as two small complex products, sample then project.  The
+//               samples at angles +j and -j share their Legendre values, so the
+//               product is formed on sums and differences of the +m / -m
+//               coefficients and the projection on the cosine / sine halves of
+//               the DFT (a quarter of the direct product's work).  The shifted and
+//               rotated expansions of the 32 right-hand sides pass through a
+//               per-CTA scratch in global memory (L2-resident).
+//   k_form3nd   P2M / P2L: one warp per (box, 32 right-hand sides); lanes
+//               stream the source recurrences (lane = source) into a small
+//               shared buffer, then sum it against the staged strengths
+//               (lane = right-hand side).
+//   k_eval3nd   L2T / M2T: a thread per target, the recurrence values applied to
+//               RB right-hand sides held in registers.
+//   k_p2p3nd    list-1 direct interactions, pair geometry once for RB
+//               right-hand sides.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+#include "lfmm3d.cuh"
+#include "plan3d.cuh"
+#include "sph3d.cuh"
+
+namespace zf {
+
+namespace {
+
+constexpr int XNT = 512;      // threads of the batched translation kernel
+constexpr int XW = XNT / 32;  // its warps
+constexpr int RC = 32;        // right-hand sides per translation pass (one per lane)
+constexpr int JT = 5;         // sample product: angles per warp task
+constexpr int MT = 3;         // projection: orders per warp task
+constexpr int JB = 8;         // shift: output degrees per warp task
+
+// cos / sin of 2 pi (jc m mod (2p+1)) / (2p+1), [jc][m] for jc, m <= p
+struct RotTab {
+  const double* cw;
+  const double* sw;
+};
+
+std::mutex g_rot_mu;
+std::map<std::pair<int, int>, RotTab> g_rot;
+
+RotTab get_rottab(int p) {
+  int dev = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_rot_mu);
+  auto key = std::make_pair(dev, p);
+  auto it = g_rot.find(key);
+  if (it != g_rot.end()) return it->second;
+  int L = p + 1, NS = 2 * p + 1;
+  std::vector<double> h(2 * (size_t)L * L);
+  for (int jc = 0; jc <= p; jc++)
+    for (int m = 0; m <= p; m++) {
+      int k = (jc * m) % NS;
+      double a = 2 * kPi * k / NS;
+      h[(size_t)jc * L + m] = cos(a);
+      h[(size_t)L * L + (size_t)jc * L + m] = sin(a);
+    }
+  double* d = nullptr;
+  ZF_CUDA(cudaMalloc((void**)&d, h.size() * sizeof(double)));
+  ZF_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  RotTab R{d, d + (size_t)L * L};
+  g_rot[key] = R;
+  return R;
+}
+
+// per-angle constants of one y-rotation (the set-up of myzylgndr2sf in z3dyrot)
+struct JCc {
+  zdc z, zz1, u, z1, z2, z3, st, eip;
+};
+
+struct XSm {
+  JCc* jc;
+  zdc *Cs, *Cd, *As, *Ad, *Ss, *Sd, *Ef, *Eb, *G, *T1, *T2;
+};
+
+__device__ __forceinline__ XSm carve_xsm(zdc* sm, int p) {
+  const int L = p + 1, NS = 2 * p + 1;
+  XSm S;
+  S.jc = (JCc*)sm;
+  zdc* q = sm + 8 * L;
+  S.Cs = q; q += L * L;
+  S.Cd = q; q += L * L;
+  S.As = q; q += L * RC;
+  S.Ad = q; q += L * RC;
+  S.Ss = q; q += L * RC;
+  S.Sd = q; q += L * RC;
+  S.Ef = q; q += NS;
+  S.Eb = q; q += NS;
+  S.G = q; q += NS;
+  S.T1 = q; q += L;
+  S.T2 = q;
+  return S;
+}
+
+size_t xsm_bytes(int p) {
+  size_t L = p + 1, NS = 2 * p + 1;
+  return (8 * L + 2 * L * L + 4 * L * RC + 3 * NS + 2 * L) * sizeof(zdc);
+}
+
+struct TransNdArgs {
+  Tab3 T;
+  RotTab R;
+  const int *ilevel, *iparent, *nchild, *ichild, *isrcse, *itargse;
+  const zdc *zcs, *zct;
+  const double* rsc;
+  const zdc* in;
+  zdc* out;
+  zdc* scratch;  // 2 (p+1)^2 RC per CTA
+  const int *nl2, *l2, *nl4;
+  int mn2, nd, lo, hi;
+};
+
+// amat-based factor applied after the first rotation (the prescale of the
+// axial shift, zl3dtrans.f)
+template <int KIND>
+__device__ __forceinline__ zdc prescale(const Tab3& T, const XSm& S, int n, int m, zdc v) {
+  const int nmax = T.nmax, ldA = 2 * nmax + 1;
+  double an = __ldg(&T.amat[n * ldA + m + nmax]);
+  if (KIND == 0) return v * an;
+  if (KIND == 1) return v * (((n + m) & 1) ? -an : an);
+  return v * S.T2[n] / an;
+}
+
+// One y-rotation by the angle (ca, sa) of the 32 right-hand sides of an
+// expansion of order p.  MODE 0: input from a box expansion in global memory
+// (row stride ldin, z-rotated by Ef on load), output written to the scratch
+// (row stride RC) with the shift prescale.  MODE 1: input from the scratch,
+// output added to a box expansion (row stride ldout) with the inverse
+// z-rotation Eb.  nval: right-hand sides of this pass that exist.
+template <int SLOTS, int MODE, int KIND>
+__device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc sa, bool zr,
+                       const zdc* gin, long ldin, zdc* gout, long ldout, int nval) {
+  const int p = T.p, L = p + 1, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const double s4i = 1.0 / sqrt(4 * kPi);
+  __syncthreads();
+  if (tid < L) {
+    const int j = tid;
+    double ph = j * 2 * kPi / (2 * p + 1);
+    double sph, cph;
+    sincos(ph, &sph, &cph);
+    zdc x1 = cph * ca, x2 = mkz(sph);
+    zdc zrxy = zsqrt_r(x1 * x1 + x2 * x2);
+    zdc ct = (-cph) * sa;
+    zdc st = zsqrt_r(mkz(1.0) - (cph * cph) * (mkz(1.0) - ca * ca));
+    if (ph == 0) st = (zabs(st + ca) <= zabs(st - ca)) ? -ca : ca;
+    zdc cp, sp, eip;
+    if (zabs(zrxy) >= kF16) {
+      cp = x1 / zrxy;
+      sp = x2 / zrxy;
+      eip = cp + zmul_i(sp);
+    } else {
+      cp = mkz(1.0);
+      sp = mkz(0.0);
+      eip = mkz(1.0);
+    }
+    JCc c;
+    c.z1 = s4i * st;
+    c.z2 = (st * ca - ct * cp * sa) * s4i;
+    c.z3 = zmul_i(sp * sa * s4i);
+    c.z = ct;
+    c.zz1 = mkz(1.0) - ct * ct;
+    c.u = (zabs(c.zz1) >= (double)1e-12f) ? -zsqrt_r(c.zz1) : -st;
+    c.st = st;
+    c.eip = eip;
+    S.jc[j] = c;
+  }
+  zdc Yp[SLOTS], Ypp[SLOTS], Dp[SLOTS], Dpp[SLOTS], em[SLOTS];
+#pragma unroll
+  for (int s = 0; s < SLOTS; s++) Yp[s] = Ypp[s] = Dp[s] = Dpp[s] = em[s] = mkz(0.0);
+  __syncthreads();
+
+  // sample coefficients of degree n: Cs = C(j,m) + C(j,-m), Cd = C(j,m) - C(j,-m)
+  auto gen = [&](int n) {
+#pragma unroll
+    for (int s = 0; s < SLOTS; s++) {
+      int idx = tid + s * XNT;
+      if (idx >= L * L) continue;
+      int m = idx / L, jc = idx - m * L;
+      if (m > n) continue;
+      const JCc& J = S.jc[jc];
+      zdc z = J.z;
+      zdc Y, D;
+      if (n == m) {
+        if (m == 0) {
+          Y = mkz(1.0);
+          D = mkz(0.0);
+          em[s] = mkz(1.0);
+        } else {
+          zdc u = J.u, e = J.eip, Yd = mkz(-__ldg(&T.r1[L + 1])), ee = e;
+          for (int k = 2; k <= m; k++) {
+            Yd = (Yd * u) * __ldg(&T.r1[k * L + k]);
+            ee = ee * e;
+          }
+          Y = Yd;
+          D = (Yd * (double)(-m)) * z;
+          em[s] = ee;
+        }
+      } else if (n == m + 1) {
+        double c = __ldg(&T.r1[n * L + m]);
+        Y = (z * Yp[s]) * c;
+        D = (m == 0) ? (z * Dp[s] + Yp[s]) * c : (z * Dp[s] + J.zz1 * Yp[s]) * c;
+      } else {
+        double c1 = __ldg(&T.r1[n * L + m]), c2 = __ldg(&T.r2[n * L + m]);
+        Y = (c1 * z) * Yp[s] - c2 * Ypp[s];
+        D = (m == 0) ? c1 * (z * Dp[s] + Yp[s]) - c2 * Dpp[s]
+                     : c1 * (z * Dp[s] + J.zz1 * Yp[s]) - c2 * Dpp[s];
+      }
+      Ypp[s] = Yp[s];
+      Dpp[s] = Dp[s];
+      Yp[s] = Y;
+      Dp[s] = D;
+      double sqn = __ldg(&T.sq[n]);
+      zdc y = Y * sqn, d = D * sqn;
+      if (m == 0) {
+        zdc c0 = y * s4i - (d * J.z2) * J.st;
+        S.Cs[jc] = c0 * 2.0;
+        S.Cd[jc] = mkz(0.0);
+      } else {
+        double sg = (m & 1) ? -1.0 : 1.0;
+        zdc P = sg * (J.z1 * y - J.z2 * d);
+        zdc Q = (sg * m) * (y * J.z3);
+        zdc Cp = (P + Q) * em[s], Cm = (P - Q) * zinv(em[s]);
+        S.Cs[m * L + jc] = Cp + Cm;
+        S.Cd[m * L + jc] = Cp - Cm;
+      }
+    }
+  };
+  // inputs of degree n: As = a(n,m) + a(n,-m), Ad = a(n,m) - a(n,-m)
+  auto load = [&](int n) {
+    for (int m = w; m <= n; m += XW) {
+      zdc a = mkz(0.0), b = mkz(0.0);
+      if (MODE == 0) {
+        if (lane < nval) {
+          a = gin[(long)ix3(n, m) * ldin + lane];
+          if (m > 0) b = gin[(long)ix3(n, -m) * ldin + lane];
+          if (zr) {
+            a = a * S.Ef[p + m];
+            b = b * S.Ef[p - m];
+          }
+        }
+      } else {
+        a = gin[ix3(n, m) * RC + lane];
+        if (m > 0) b = gin[ix3(n, -m) * RC + lane];
+      }
+      if (m == 0) {
+        S.As[lane] = a;
+        S.Ad[lane] = mkz(0.0);
+      } else {
+        S.As[m * RC + lane] = a + b;
+        S.Ad[m * RC + lane] = a - b;
+      }
+    }
+  };
+  auto store = [&](int n, int m, zdc v) {
+    if (MODE == 0) {
+      gout[ix3(n, m) * RC + lane] = prescale<KIND>(T, S, n, m, v);
+    } else if (lane < nval) {
+      zdc* o = gout + (long)ix3(n, m) * ldout + lane;
+      *o += zr ? v * S.Eb[p + m] : v;
+    }
+  };
+
+  gen(0);
+  load(0);
+  __syncthreads();
+  const int ngrp = (L + JT - 1) / JT;
+  for (int n = 0; n <= p; n++) {
+    // samples at angles >= 0: S = F(j) + F(-j), D = F(j) - F(-j)
+    for (int t = w; t < 2 * ngrp; t += XW) {
+      const int which = t & 1, jc0 = (t >> 1) * JT;
+      const zdc* C = which ? S.Cd : S.Cs;
+      const zdc* Av = which ? S.Ad : S.As;
+      zdc acc[JT];
+#pragma unroll
+      for (int k = 0; k < JT; k++) acc[k] = mkz(0.0);
+      for (int m = which; m <= n; m++) {
+        zdc a = Av[m * RC + lane];
+        const zdc* Cr = C + m * L + jc0;
+#pragma unroll
+        for (int k = 0; k < JT; k++)
+          if (jc0 + k < L) acc[k] += Cr[k] * a;
+      }
+      zdc* O = which ? S.Sd : S.Ss;
+#pragma unroll
+      for (int k = 0; k < JT; k++)
+        if (jc0 + k < L) O[(jc0 + k) * RC + lane] = acc[k];
+    }
+    __syncthreads();
+    // projection: out(n, +-m) = dinv(n, m) (X -+ i Y)
+    const int ng2 = (n + MT) / MT;
+    for (int t = w; t < ng2; t += XW) {
+      const int m0 = t * MT;
+      zdc X[MT], Yv[MT];
+      zdc x0 = (S.Ss[lane] + S.Sd[lane]) * 0.5;
+#pragma unroll
+      for (int k = 0; k < MT; k++) {
+        X[k] = x0;
+        Yv[k] = mkz(0.0);
+      }
+      for (int jc = 1; jc <= p; jc++) {
+        zdc sv = S.Ss[jc * RC + lane], dv = S.Sd[jc * RC + lane];
+        const double* cr = R.cw + jc * L + m0;
+        const double* sr = R.sw + jc * L + m0;
+#pragma unroll
+        for (int k = 0; k < MT; k++)
+          if (m0 + k <= n) {
+            X[k] += sv * __ldg(&cr[k]);
+            Yv[k] += dv * __ldg(&sr[k]);
+          }
+      }
+#pragma unroll
+      for (int k = 0; k < MT; k++) {
+        int m = m0 + k;
+        if (m > n) break;
+        double dn = __ldg(&T.dinv[n * L + m]);
+        zdc iy = zmul_i(Yv[k]);
+        store(n, m, (X[k] - iy) * dn);
+        if (m > 0) store(n, -m, (X[k] + iy) * dn);
+      }
+    }
+    if (n < p) {
+      gen(n + 1);
+      load(n + 1);
+    }
+    __syncthreads();
+  }
+}
+
+// the y-rotation skipped (translation along z): z-rotation and prescale only
+template <int MODE, int KIND>
+__device__ void copy_nd(const Tab3& T, const XSm& S, bool zr, const zdc* gin, long ldin,
+                        zdc* gout, long ldout, int nval) {
+  const int p = T.p, NC = T.NC, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  for (int idx = w; idx < NC; idx += XW) {
+    int n = deg3(idx), m = idx - n * n - n;
+    if (MODE == 0) {
+      zdc a = mkz(0.0);
+      if (lane < nval) {
+        a = gin[(long)idx * ldin + lane];
+        if (zr) a = a * S.Ef[p + m];
+      }
+      gout[idx * RC + lane] = prescale<KIND>(T, S, n, m, a);
+    } else if (lane < nval) {
+      zdc v = gin[idx * RC + lane];
+      gout[(long)idx * ldout + lane] += zr ? v * S.Eb[p + m] : v;
+    }
+  }
+  __syncthreads();
+}
+
+// axial shift X1 -> X2 (scratch, row stride RC)
+template <int KIND>
+__device__ void shift_nd(const Tab3& T, const XSm& S, const zdc* X1, zdc* X2) {
+  const int p = T.p, nmax = T.nmax, ldA = 2 * nmax + 1, lane = threadIdx.x & 31,
+            w = threadIdx.x >> 5;
+  int t = 0;
+  for (int mm = -p; mm <= p; mm++) {
+    const int am_ = mm < 0 ? -mm : mm, nbk = (p + 1 - am_ + JB - 1) / JB;
+    for (int bk = 0; bk < nbk; bk++, t++) {
+      if (t % XW != w) continue;
+      const int j0 = am_ + bk * JB;
+      zdc acc[JB];
+#pragma unroll
+      for (int k = 0; k < JB; k++) acc[k] = mkz(0.0);
+      if (KIND == 1) {
+        for (int n = am_; n <= p; n++) {
+          zdc a = X1[ix3(n, mm) * RC + lane];
+#pragma unroll
+          for (int k = 0; k < JB; k++)
+            if (j0 + k <= p) acc[k] += a * S.G[n + j0 + k];
+        }
+      } else if (KIND == 0) {
+        int nhi = min(p, j0 + JB - 1);
+        for (int n = am_; n <= nhi; n++) {
+          zdc a = X1[ix3(n, mm) * RC + lane];
+#pragma unroll
+          for (int k = 0; k < JB; k++) {
+            int j = j0 + k;
+            if (j <= p && n <= j) acc[k] += a * S.G[j - n];
+          }
+        }
+      } else {
+        for (int n = j0; n <= p; n++) {
+          zdc a = X1[ix3(n, mm) * RC + lane];
+#pragma unroll
+          for (int k = 0; k < JB; k++) {
+            int j = j0 + k;
+            if (j <= p && n >= j) acc[k] += a * S.G[n - j];
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < JB; k++) {
+        int j = j0 + k;
+        if (j > p) break;
+        double ajk = __ldg(&T.amat[j * ldA + mm + nmax]);
+        zdc v = (KIND == 0) ? S.T1[j] * acc[k] / ajk : S.T1[j] * acc[k] * ajk;
+        X2[ix3(j, mm) * RC + lane] = v;
+      }
+    }
+  }
+}
+
+template <int KIND, int SLOTS>
+__global__ void __launch_bounds__(XNT, 1) k_trans3nd(TransNdArgs A) {
+  extern __shared__ zdc sm[];
+  const Tab3& T = A.T;
+  const int p = T.p, NC = T.NC, tid = threadIdx.x;
+  const XSm S = carve_xsm(sm, p);
+  zdc* X1 = A.scratch + (size_t)blockIdx.x * 2 * NC * RC;
+  zdc* X2 = X1 + (size_t)NC * RC;
+  const double s4 = sqrt(4 * kPi);
+  const int nmax = T.nmax, ldA = 2 * nmax + 1;
+  const double* __restrict__ am = T.amat;
+  const long nd = A.nd;
+  for (int b = A.lo + blockIdx.x; b <= A.hi; b += gridDim.x) {
+    int nin = 0, par = -1;
+    if (KIND == 0) {
+      if (nsrc(A.isrcse, b) <= 0 || A.nchild[b] == 0) continue;
+      nin = A.nchild[b];
+    } else if (KIND == 1) {
+      if (nsrc(A.itargse, b) <= 0 || A.nl2[b] == 0) continue;
+      nin = A.nl2[b];
+    } else {
+      par = A.iparent[b];
+      if (par < 0 || nsrc(A.itargse, b) <= 0 || nsrc(A.itargse, par) <= 0 ||
+          (A.nl2[par] == 0 && A.nl4[par] == 0))
+        continue;
+      nin = 1;
+    }
+    const int lb = A.ilevel[b];
+    for (int r0 = 0; r0 < A.nd; r0 += RC) {
+      const int nval = min(RC, A.nd - r0);
+      for (int it = 0; it < nin; it++) {
+        int src;
+        const zdc *c0, *c;
+        double rs0, rs;
+        if (KIND == 0) {
+          src = A.ichild[8 * b + it];
+          if (nsrc(A.isrcse, src) <= 0) continue;
+          c0 = A.zcs + 3 * src;
+          c = A.zcs + 3 * b;
+          rs0 = A.rsc[lb + 1];
+          rs = A.rsc[lb];
+        } else if (KIND == 1) {
+          src = A.l2[(size_t)b * A.mn2 + it];
+          if (nsrc(A.isrcse, src) <= 0) continue;
+          c0 = A.zcs + 3 * src;
+          c = A.zct + 3 * b;
+          rs0 = rs = A.rsc[lb];
+        } else {
+          src = par;
+          c0 = A.zct + 3 * par;
+          c = A.zct + 3 * b;
+          rs0 = A.rsc[lb - 1];
+          rs = A.rsc[lb];
+        }
+        Geo g = geo3(c0, c);
+        zdc zsh = g.zshift;
+        bool flip = zabs(zsqrt_p(zsh * zsh) - zsh) > kF16;
+        zdc rzs = flip ? -zsh : zsh;
+        __syncthreads();
+        for (int m = tid; m <= p; m += XNT) {
+          zdc ef = zpown(g.cb + zmul_i(g.sb), m), eb = zpown(g.cb - zmul_i(g.sb), m);
+          S.Ef[p + m] = ef;
+          S.Ef[p - m] = zinv(ef);
+          S.Eb[p + m] = eb;
+          S.Eb[p - m] = zinv(eb);
+        }
+        if (KIND == 0) {
+          zdc rz = rzs / rs0;
+          for (int n = tid; n <= p; n += XNT) {
+            double yl = __ldg(&T.sq[n]) * ((flip && (n & 1)) ? -1.0 : 1.0);
+            S.G[n] = (zpown(rz, n) * (__ldg(&am[n * ldA + nmax]) * yl)) / (2 * n + 1.0);
+            S.T1[n] = mkz(s4 * (ipow(rs0, n) / ipow(rs, n)));
+          }
+        } else if (KIND == 1) {
+          zdc rz = rzs / rs0;
+          for (int m = tid; m <= 2 * p; m += XNT) {
+            double yl = __ldg(&T.sq[m]) * ((flip && (m & 1)) ? -1.0 : 1.0);
+            S.G[m] = yl / (zpown(rz, m) * __ldg(&am[m * ldA + nmax]));
+          }
+          for (int j = tid; j <= p; j += XNT) S.T1[j] = (s4 / (2 * j + 1.0)) / rz;
+        } else {
+          zdc rz = rzs / rs;
+          for (int n = tid; n <= p; n += XNT) {
+            double yl = __ldg(&T.sq[n]) * ((flip && (n & 1)) ? -1.0 : 1.0);
+            S.G[n] = (zpown(rz, n) * (__ldg(&am[n * ldA + nmax]) * yl)) / (2 * n + 1.0);
+            S.T1[n] = mkz(s4 / (2 * n + 1.0) * ((n & 1) ? -1.0 : 1.0));
+            S.T2[n] = mkz((2 * n + 1.0) * (ipow(rs, n + 1) / ipow(rs0, n + 1)) *
+                          ((n & 1) ? -1.0 : 1.0));
+          }
+        }
+        __syncthreads();
+        const zdc* gin = A.in + (size_t)src * NC * nd + r0;
+        if (g.yr) rot_nd<SLOTS, 0, KIND>(T, A.R, S, g.ca, g.sa, g.zr, gin, nd, X1, RC, nval);
+        else copy_nd<0, KIND>(T, S, g.zr, gin, nd, X1, RC, nval);
+        __syncthreads();
+        shift_nd<KIND>(T, S, X1, X2);
+        __syncthreads();
+        zdc* gout = A.out + (size_t)b * NC * nd + r0;
+        if (g.yr) rot_nd<SLOTS, 1, KIND>(T, A.R, S, g.ca, -g.sa, g.zr, X2, RC, gout, nd, nval);
+        else copy_nd<1, KIND>(T, S, g.zr, X2, RC, gout, nd, nval);
+      }
+    }
+  }
+}
+
+// ---- P2M / P2L ---------------------------------------------------------------
+constexpr int FW = 4;  // warps per CTA of the form kernel, one work item each
+constexpr int KB = 8;  // (n, m) entries buffered per flush
+
+struct FormNdArgs {
+  Tab3 T;
+  const int *ilevel, *nchild, *isrcse, *itargse;
+  const zdc *zsrc, *q, *ds, *dv;
+  const zdc *zcs, *zct;
+  const double* rsc;
+  zdc* out;
+  const int *nl4, *l4;
+  int mn4, nb, nd, nchunk, ifcharge, ifdipole;
+};
+
+__host__ __device__ inline size_t form_nd_warp_elems(bool dip) { return (dip ? 2 : 1) * (32 * 32 + KB * 2 * 32); }
+
+// zl3dformmp (LOCAL = false) / zl3dformloc (LOCAL = true), zlfmm3d.f:689-1005,
+// sources s0..s1 about centre zc, into the 32 right-hand sides r0.. of `o`
+template <bool LOCAL, bool DIP>
+__device__ void form_range_nd(const FormNdArgs& A, int s0, int s1, const zdc* zc,
+                              double rscale, zdc* o, int r0, int nval, zdc* Qt, zdc* Dt,
+                              zdc* Gq, zdc* Gd) {
+  const Tab3& T = A.T;
+  const int p = T.p, L = p + 1, lane = threadIdx.x & 31;
+  const long nd = A.nd;
+  const double s4 = 1.0 / sqrt(4 * kPi);
+  const double* __restrict__ r1 = T.r1;
+  const double* __restrict__ r2 = T.r2;
+  const double* __restrict__ sq = T.sq;
+  for (int base = s0; base <= s1; base += 32) {
+    const int cnt = min(32, s1 - base + 1);
+    __syncwarp();
+    for (int k = 0; k < 32; k++) {
+      bool ok = k < cnt && lane < nval;
+      Qt[k * 32 + lane] = (ok && A.ifcharge) ? A.q[(long)(base + k) * nd + r0 + lane] : mkz(0.0);
+      if (DIP) Dt[k * 32 + lane] = ok ? A.ds[(long)(base + k) * nd + r0 + lane] : mkz(0.0);
+    }
+    const bool valid = lane < cnt;
+    const int ii = valid ? base + lane : base;
+    Sph s = zcart2sph(A.zsrc[3 * ii], A.zsrc[3 * ii + 1], A.zsrc[3 * ii + 2], zc);
+    zdc rz = s.rz / rscale;
+    zdc irz = zinv(rz);
+    zdc dzr_ = mkz(0.0), dthz = mkz(0.0), dphz = mkz(0.0);
+    if (DIP) {
+      zdc v0 = A.dv[3 * ii], v1 = A.dv[3 * ii + 1], v2 = A.dv[3 * ii + 2];
+      dzr_ = v0 * (s.st * s.cp) + v1 * (s.st * s.sp) + v2 * s.ct;
+      zdc dth_ = v0 * (s.ct * s.cp) + v1 * (s.ct * s.sp) - v2 * s.st;
+      zdc dph_ = -(v0 * s.sp) + v1 * s.cp;
+      dthz = dth_ / s.rz;
+      dphz = dph_ / s.rz;
+    }
+    const zdc z = s.ct, zz1 = mkz(1.0) - z * z;
+    const zdc u = -zsqrt_r(zz1);
+    zdc colp = LOCAL ? irz : mkz(1.0);
+    zdc Ydiag = mkz(1.0), em = mkz(1.0);
+    int e = 0, fm = 0, fn = 0;  // buffered entries and the first (m, n) among them
+    auto flush = [&]() {
+      __syncwarp();
+      int m = fm, n = fn;
+      for (int k = 0; k < e; k++) {
+        zdc ap = mkz(0.0), an = mkz(0.0);
+        const zdc* gq = Gq + k * 64;
+        const zdc* gd = Gd + k * 64;
+        for (int j = 0; j < 32; j++) {
+          zdc qv = Qt[j * 32 + lane];
+          ap += gq[j] * qv;
+          if (m > 0) an += gq[32 + j] * qv;
+          if (DIP) {
+            zdc dv = Dt[j * 32 + lane];
+            ap += gd[j] * dv;
+            if (m > 0) an += gd[32 + j] * dv;
+          }
+        }
+        if (lane < nval) {
+          o[(long)ix3(n, m) * nd + lane] += ap;
+          if (m > 0) o[(long)ix3(n, -m) * nd + lane] += an;
+        }
+        if (n < p) n++;
+        else {
+          m++;
+          n = m;
+        }
+      }
+      __syncwarp();
+      e = 0;
+    };
+    for (int m = 0; m <= p; m++) {
+      zdc emi = mkz(1.0);
+      if (m > 0) {
+        double cmm = __ldg(&r1[m * L + m]);
+        if (DIP) Ydiag = (m == 1) ? mkz(-cmm) : (Ydiag * u) * cmm;
+        else Ydiag = (Ydiag * u) * cmm;
+        em = em * s.eip;
+        emi = zinv(em);
+        colp = colp * (LOCAL ? irz : rz);
+      }
+      double sgm = (m & 1) ? -1.0 : 1.0;
+      zdc Yp = Ydiag, Dp = DIP ? (Ydiag * (double)(-m)) * z : mkz(0.0);
+      zdc Ypp = mkz(0.0), Dpp = mkz(0.0);
+      zdc rp = colp;
+      zdc rpm1 = (m > 0) ? colp * irz : mkz(0.0);
+      for (int n = m; n <= p; n++) {
+        zdc Y, D = mkz(0.0);
+        if (n == m) {
+          Y = Yp;
+          D = Dp;
+        } else {
+          if (n == m + 1) {
+            double c = __ldg(&r1[n * L + m]);
+            Y = (z * Yp) * c;
+            if (DIP) D = (m == 0) ? (z * Dp + Yp) * c : (z * Dp + zz1 * Yp) * c;
+          } else {
+            double c1 = __ldg(&r1[n * L + m]), c2 = __ldg(&r2[n * L + m]);
+            Y = (c1 * z) * Yp - c2 * Ypp;
+            if (DIP)
+              D = (m == 0) ? c1 * (z * Dp + Yp) - c2 * Dpp
+                           : c1 * (z * Dp + zz1 * Yp) - c2 * Dpp;
+          }
+          Ypp = Yp; Dpp = Dp; Yp = Y; Dp = D;
+          rpm1 = rp;
+          rp = rp * (LOCAL ? irz : rz);
+        }
+        double f = __ldg(&sq[n]) * (s4 * sgm / (2 * n + 1.0));
+        zdc y = Y * f, dy = D * f;
+        zdc qp, qn = mkz(0.0), dp = mkz(0.0), dn = mkz(0.0);
+        if (m == 0) {
+          qp = rp * y;
+          if (DIP) {
+            zdc dzr, dth;
+            if (!LOCAL) {
+              dzr = n == 0 ? mkz(0.0) : ((double)n * rpm1 / rscale) * y;
+              dth = -(rp * dy * s.st);
+            } else {
+              dzr = -((double)(n + 1) * y * rp / s.rz);
+              dth = -(dy * s.st * rp);
+            }
+            dp = -(dzr_ * dzr + dthz * dth);
+          }
+        } else {
+          zdc ys = DIP ? s.st * y : y;
+          zdc X = rp * ys;
+          qp = emi * X;
+          qn = em * X;
+          if (DIP) {
+            zdc DZ, DT, DP;
+            if (!LOCAL) {
+              DZ = ((double)n * rpm1 / rscale) * y * s.st;
+              DT = -(rp * dy);
+              DP = rp * y;
+            } else {
+              DZ = -((double)(n + 1) * y * s.st * rp / s.rz);
+              DT = -(dy * rp);
+              DP = y * rp;
+            }
+            zdc V = -(dzr_ * DZ + dthz * DT), W = dphz * zmul_i((double)m * DP);
+            dp = emi * (V + W);
+            dn = em * (V - W);
+          }
+        }
+        if (!valid) qp = qn = dp = dn = mkz(0.0);
+        if (e == 0) {
+          fm = m;
+          fn = n;
+        }
+        Gq[e * 64 + lane] = qp;
+        Gq[e * 64 + 32 + lane] = qn;
+        if (DIP) {
+          Gd[e * 64 + lane] = dp;
+          Gd[e * 64 + 32 + lane] = dn;
+        }
+        e++;
+        if (e == KB) flush();
+      }
+    }
+    if (e > 0) flush();
+  }
+}
+
+template <bool LOCAL, bool DIP>
+__global__ void __launch_bounds__(FW * 32) k_form3nd(FormNdArgs A) {
+  extern __shared__ zdc sm[];
+  const int w = threadIdx.x >> 5;
+  const long item = (long)blockIdx.x * FW + w;
+  if (item >= (long)A.nb * A.nchunk) return;
+  const int b = (int)(item / A.nchunk), r0 = (int)(item % A.nchunk) * 32;
+  const int nval = min(32, A.nd - r0);
+  const int NC = A.T.NC;
+  zdc* Qt = sm + (size_t)w * form_nd_warp_elems(DIP);
+  zdc* Dt = Qt + 32 * 32;
+  zdc* Gq = Dt + (DIP ? 32 * 32 : 0);
+  zdc* Gd = Gq + KB * 2 * 32;
+  int l = A.ilevel[b];
+  zdc* o = A.out + (size_t)b * NC * A.nd + r0;
+  if (!LOCAL) {
+    if (A.nchild[b] != 0 || nsrc(A.isrcse, b) <= 0 || l < 1) return;
+    form_range_nd<false, DIP>(A, A.isrcse[2 * b], A.isrcse[2 * b + 1], A.zcs + 3 * b, A.rsc[l],
+                              o, r0, nval, Qt, Dt, Gq, Gd);
+  } else {
+    if (nsrc(A.itargse, b) <= 0 || A.nl4[b] == 0) return;
+    for (int i = 0; i < A.nl4[b]; i++) {
+      int jb = A.l4[(size_t)b * A.mn4 + i];
+      if (nsrc(A.isrcse, jb) <= 0) continue;
+      form_range_nd<true, DIP>(A, A.isrcse[2 * jb], A.isrcse[2 * jb + 1], A.zct + 3 * b,
+                               A.rsc[l], o, r0, nval, Qt, Dt, Gq, Gd);
+    }
+  }
+}
+
+// ---- L2T / M2T -------------------------------------------------------------
+constexpr int ENT = 128;
+constexpr int RB = 8;  // right-hand sides per thread pass (eval, P2P)
+
+struct EvalNdArgs {
+  Tab3 T;
+  const int *ilevel, *nchild, *isrcse, *itargse;
+  const zdc *ztarg, *zcs, *zct;
+  const double* rsc;
+  const zdc *mp, *loc;
+  const int *nl3, *l3;
+  int mn3, nb, nd;
+  zdc *pot, *grad;
+};
+
+// zl3devalmp (LOCAL = false) / zl3devalloc (LOCAL = true), zlfmm3d.f:1011-1277,
+// for nv <= RB right-hand sides; e: coefficient rows of stride nd
+template <bool GRAD, bool LOCAL>
+__device__ __forceinline__ void eval_one_nd(const Tab3& T, const zdc* __restrict__ e, long nd,
+                                            int nv, const zdc* x, const zdc* zc, double rscale,
+                                            zdc* P, zdc* Gr, zdc* Gt, zdc* Gp) {
+  const int p = T.p, L = p + 1;
+  const double s4 = 1.0 / sqrt(4 * kPi);
+  const double* __restrict__ r1 = T.r1;
+  const double* __restrict__ r2 = T.r2;
+  const double* __restrict__ sq = T.sq;
+  Sph s = zcart2sph(x[0], x[1], x[2], zc);
+  zdc rz = s.rz / rscale, irz = zinv(rz);
+  const zdc z = s.ct, zz1 = mkz(1.0) - z * z;
+  const zdc u = -zsqrt_r(zz1);
+  zdc colp = LOCAL ? mkz(1.0) : irz;
+  zdc Ydiag = mkz(1.0), em = mkz(1.0);
+  for (int m = 0; m <= p; m++) {
+    zdc emi = mkz(1.0);
+    if (m > 0) {
+      double cmm = __ldg(&r1[m * L + m]);
+      if (GRAD) Ydiag = (m == 1) ? mkz(-cmm) : (Ydiag * u) * cmm;
+      else Ydiag = (Ydiag * u) * cmm;
+      em = em * s.eip;
+      emi = zinv(em);
+      colp = colp * (LOCAL ? rz : irz);
+    }
+    double sgm = (m & 1) ? -1.0 : 1.0;
+    double f0 = s4 * sgm / rscale;
+    zdc Yp = Ydiag, Dp = GRAD ? (Ydiag * (double)(-m)) * z : mkz(0.0);
+    zdc Ypp = mkz(0.0), Dpp = mkz(0.0);
+    zdc rf = colp;
+    zdc rfm1 = (LOCAL && m > 0) ? colp * irz : mkz(0.0);
+    for (int n = m; n <= p; n++) {
+      zdc Y, D = mkz(0.0);
+      if (n == m) {
+        Y = Yp;
+        D = Dp;
+      } else {
+        if (n == m + 1) {
+          double c = __ldg(&r1[n * L + m]);
+          Y = (z * Yp) * c;
+          if (GRAD) D = (m == 0) ? (z * Dp + Yp) * c : (z * Dp + zz1 * Yp) * c;
+        } else {
+          double c1 = __ldg(&r1[n * L + m]), c2 = __ldg(&r2[n * L + m]);
+          Y = (c1 * z) * Yp - c2 * Ypp;
+          if (GRAD)
+            D = (m == 0) ? c1 * (z * Dp + Yp) - c2 * Dpp : c1 * (z * Dp + zz1 * Yp) - c2 * Dpp;
+        }
+        Ypp = Yp; Dpp = Dp; Yp = Y; Dp = D;
+        rfm1 = rf;
+        rf = rf * (LOCAL ? rz : irz);
+      }
+      double f = __ldg(&sq[n]) * f0;
+      zdc y = Y * f;
+      if (m == 0) {
+        const zdc* row = e + (long)ix3(n, 0) * nd;
+        zdc yr = y * rf, dzr = mkz(0.0), dth = mkz(0.0);
+        if (GRAD) {
+          zdc dy = D * f;
+          if (!LOCAL) {
+            dzr = -((double)(n + 1) * y * rf / s.rz);
+            dth = -(dy * s.st * rf);
+          } else {
+            dzr = n == 0 ? mkz(0.0) : ((double)n * rfm1 / rscale) * y;
+            dth = -(rf * dy * s.st);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; r++)
+          if (r < nv) {
+            zdc c0 = ldz(&row[r]);
+            P[r] += c0 * yr;
+            if (GRAD) {
+              Gr[r] += c0 * dzr;
+              Gt[r] += c0 * dth;
+            }
+          }
+      } else {
+        const zdc* rowp = e + (long)ix3(n, m) * nd;
+        const zdc* rown = e + (long)ix3(n, -m) * nd;
+        zdc ys = GRAD ? y * s.st : y;
+        zdc ysr = ys * rf, DZ = mkz(0.0), DT = mkz(0.0), DPh = mkz(0.0);
+        if (GRAD) {
+          zdc dy = D * f;
+          if (!LOCAL) {
+            DZ = -((double)(n + 1) * ys * rf / s.rz);
+            DT = -(dy * rf);
+          } else {
+            DZ = ((double)n * rfm1 / rscale) * ys;
+            DT = -(rf * dy);
+          }
+          DPh = zmul_i((double)m * y * rf);
+        }
+#pragma unroll
+        for (int r = 0; r < RB; r++)
+          if (r < nv) {
+            zdc a = ldz(&rowp[r]) * em, bm = ldz(&rown[r]) * emi;
+            zdc Sp = a + bm;
+            P[r] += ysr * Sp;
+            if (GRAD) {
+              Gr[r] += DZ * Sp;
+              Gt[r] += DT * Sp;
+              Gp[r] += DPh * (a - bm);
+            }
+          }
+      }
+    }
+  }
+}
+
+template <bool GRAD>
+__global__ void __launch_bounds__(ENT) k_eval3nd(EvalNdArgs A) {
+  const Tab3& T = A.T;
+  const int NC = T.NC, tid = threadIdx.x;
+  const int b = blockIdx.x;
+  if (b >= A.nb) return;
+  const int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
+  if (A.nchild[b] != 0 || t1 < t0) return;
+  const int lb = A.ilevel[b];
+  const bool own = lb >= 2;
+  const int nexp = (own ? 1 : 0) + A.nl3[b];
+  if (nexp == 0) return;
+  const long nd = A.nd;
+  for (int c0 = t0; c0 <= t1; c0 += ENT) {
+    const int i = c0 + tid;
+    if (i > t1) continue;
+    zdc x[3] = {A.ztarg[3 * i], A.ztarg[3 * i + 1], A.ztarg[3 * i + 2]};
+    for (int rb = 0; rb < A.nd; rb += RB) {
+      const int nv = min(RB, A.nd - rb);
+      zdc P[RB], Gx[RB], Gy[RB], Gz[RB];
+#pragma unroll
+      for (int r = 0; r < RB; r++) P[r] = Gx[r] = Gy[r] = Gz[r] = mkz(0.0);
+      for (int e = 0; e < nexp; e++) {
+        int eb;
+        bool loc;
+        if (own && e == 0) {
+          eb = b;
+          loc = true;
+        } else {
+          eb = A.l3[(size_t)b * A.mn3 + e - (own ? 1 : 0)];
+          loc = false;
+          if (nsrc(A.isrcse, eb) <= 0) continue;
+        }
+        const zdc* zc = (loc ? A.zct : A.zcs) + 3 * eb;
+        const zdc* ex = (loc ? A.loc : A.mp) + (size_t)eb * NC * nd + rb;
+        zdc Gr[RB], Gt[RB], Gp[RB], Pe[RB];
+#pragma unroll
+        for (int r = 0; r < RB; r++) Pe[r] = Gr[r] = Gt[r] = Gp[r] = mkz(0.0);
+        double rscale = A.rsc[A.ilevel[eb]];
+        if (loc) eval_one_nd<GRAD, true>(T, ex, nd, nv, x, zc, rscale, Pe, Gr, Gt, Gp);
+        else eval_one_nd<GRAD, false>(T, ex, nd, nv, x, zc, rscale, Pe, Gr, Gt, Gp);
+#pragma unroll
+        for (int r = 0; r < RB; r++) P[r] += Pe[r];
+        if (GRAD) {
+          Sph s = zcart2sph(x[0], x[1], x[2], zc);
+          zdc ir = zinv(s.rz);
+          zdc ezr0 = s.st * s.cp, ezr1 = s.st * s.sp, ezr2 = s.ct;
+          zdc et0 = s.ct * s.cp * ir, et1 = s.ct * s.sp * ir, et2 = -(s.st * ir);
+          zdc ep0 = -(s.sp * ir), ep1 = s.cp * ir;
+#pragma unroll
+          for (int r = 0; r < RB; r++) {
+            Gx[r] += Gr[r] * ezr0 + Gt[r] * et0 + Gp[r] * ep0;
+            Gy[r] += Gr[r] * ezr1 + Gt[r] * et1 + Gp[r] * ep1;
+            Gz[r] += Gr[r] * ezr2 + Gt[r] * et2;
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (r < nv) {
+          A.pot[(long)i * nd + rb + r] += P[r];
+          if (GRAD) {
+            A.grad[(3L * i) * nd + rb + r] += Gx[r];
+            A.grad[(3L * i + 1) * nd + rb + r] += Gy[r];
+            A.grad[(3L * i + 2) * nd + rb + r] += Gz[r];
+          }
+        }
+    }
+  }
+}
+
+// ---- P2P (list 1) -------------------------------------------------------------
+constexpr int PT = 64;  // sources per shared-memory tile
+
+struct P2PNdArgs {
+  const int *nchild, *isrcse, *itargse;
+  const zdc *zsrc, *q, *ds, *dv, *ztarg;
+  const int *nl1, *l1;
+  int mn1, nb, nd, ifcharge, ifdipole;
+  zdc *pot, *grad;
+};
+
+struct SrcTileNd {
+  zdc y[PT][3];
+  zdc q[PT][RB];
+  zdc ds[PT][RB];
+  zdc v[PT][3];
+};
+
+template <bool GRAD, bool DIP>
+__global__ void __launch_bounds__(ENT) k_p2p3nd(P2PNdArgs A) {
+  extern __shared__ unsigned char smraw[];
+  SrcTileNd& S = *reinterpret_cast<SrcTileNd*>(smraw);
+  constexpr double PI4I = 0.079577471545947667884;
+  const int b = blockIdx.x;
+  if (b >= A.nb) return;
+  const int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
+  if (A.nchild[b] != 0 || t1 < t0 || A.nl1[b] == 0) return;
+  const long nd = A.nd;
+  for (int c0 = t0; c0 <= t1; c0 += ENT) {
+    const int i = c0 + threadIdx.x;
+    const bool valid = i <= t1;
+    zdc x[3] = {mkz(0.0), mkz(0.0), mkz(0.0)};
+    if (valid) {
+      x[0] = ldz(&A.ztarg[3 * i]);
+      x[1] = ldz(&A.ztarg[3 * i + 1]);
+      x[2] = ldz(&A.ztarg[3 * i + 2]);
+    }
+    for (int rb = 0; rb < A.nd; rb += RB) {
+      const int nv = min(RB, A.nd - rb);
+      zdc P[RB], G0[RB], G1[RB], G2[RB];
+#pragma unroll
+      for (int r = 0; r < RB; r++) P[r] = G0[r] = G1[r] = G2[r] = mkz(0.0);
+      for (int li = 0; li < A.nl1[b]; li++) {
+        const int jb = A.l1[(size_t)b * A.mn1 + li];
+        const int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
+        for (int j0 = s0; j0 <= s1; j0 += PT) {
+          const int n = min(PT, s1 - j0 + 1);
+          __syncthreads();
+          for (int k = threadIdx.x; k < n; k += ENT) {
+            const int j = j0 + k;
+            S.y[k][0] = ldz(&A.zsrc[3 * j]);
+            S.y[k][1] = ldz(&A.zsrc[3 * j + 1]);
+            S.y[k][2] = ldz(&A.zsrc[3 * j + 2]);
+            if (DIP) {
+              S.v[k][0] = ldz(&A.dv[3 * j]);
+              S.v[k][1] = ldz(&A.dv[3 * j + 1]);
+              S.v[k][2] = ldz(&A.dv[3 * j + 2]);
+            }
+          }
+          for (int k = threadIdx.x; k < n * RB; k += ENT) {
+            const int kk = k / RB, r = k - kk * RB;
+            const long off = (long)(j0 + kk) * nd + rb + r;
+            S.q[kk][r] = (r < nv && A.ifcharge) ? ldz(&A.q[off]) : mkz(0.0);
+            if (DIP) S.ds[kk][r] = r < nv ? ldz(&A.ds[off]) : mkz(0.0);
+          }
+          __syncthreads();
+          if (!valid) continue;
+          for (int k = 0; k < n; k++) {
+            zdc y0 = S.y[k][0] - x[0], y1 = S.y[k][1] - x[1], y2 = S.y[k][2] - x[2];
+            zdc rz = zsqrt_p(y0 * y0 + y1 * y1 + y2 * y2);
+            if (!(zabs(rz) > (double)1e-16f)) continue;
+            zdc ir = zinv(rz);
+            zdc r1 = ir * PI4I;
+            zdc r3 = r1 * (ir * ir);
+            if (A.ifcharge) {
+#pragma unroll
+              for (int r = 0; r < RB; r++) {
+                zdc qv = S.q[k][r];
+                P[r] += qv * r1;
+                if (GRAD) {
+                  zdc f = qv * r3;
+                  G0[r] += f * y0;
+                  G1[r] += f * y1;
+                  G2[r] += f * y2;
+                }
+              }
+            }
+            if (DIP) {
+              zdc dot = -(y0 * S.v[k][0] + y1 * S.v[k][1] + y2 * S.v[k][2]);
+              zdc w3 = r3 * dot;
+              zdc dd0 = mkz(0.0), dd1 = mkz(0.0), dd2 = mkz(0.0);
+              if (GRAD) {
+                zdc t = 3.0 * (dot * (r3 * (ir * ir)));
+                dd0 = r3 * S.v[k][0] + t * y0;
+                dd1 = r3 * S.v[k][1] + t * y1;
+                dd2 = r3 * S.v[k][2] + t * y2;
+              }
+#pragma unroll
+              for (int r = 0; r < RB; r++) {
+                zdc dsv = S.ds[k][r];
+                P[r] -= dsv * w3;
+                if (GRAD) {
+                  G0[r] -= dsv * dd0;
+                  G1[r] -= dsv * dd1;
+                  G2[r] -= dsv * dd2;
+                }
+              }
+            }
+          }
+        }
+      }
+      if (valid)
+#pragma unroll
+        for (int r = 0; r < RB; r++)
+          if (r < nv) {
+            A.pot[(long)i * nd + rb + r] += P[r];
+            if (GRAD) {
+              A.grad[(3L * i) * nd + rb + r] += G0[r];
+              A.grad[(3L * i + 1) * nd + rb + r] += G1[r];
+              A.grad[(3L * i + 2) * nd + rb + r] += G2[r];
+            }
+          }
+    }
+  }
+}
+
+// ---- host ------------------------------------------------------------------------
+template <int KIND, int SLOTS>
+void launch_trans_nd_k(const TransNdArgs& A, int grid, size_t sm, cudaStream_t s) {
+  ZF_CUDA(cudaFuncSetAttribute(k_trans3nd<KIND, SLOTS>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  klaunch(k_trans3nd<KIND, SLOTS>, grid, XNT, sm, s, A);
+}
+
+template <int KIND>
+void launch_trans_nd(const TransNdArgs& A, int grid, cudaStream_t s) {
+  if (A.hi < A.lo) return;
+  int L = A.T.p + 1;
+  size_t sm = xsm_bytes(A.T.p);
+  int slots = div_up(L * L, XNT);
+  if (slots <= 3) launch_trans_nd_k<KIND, 3>(A, grid, sm, s);
+  else if (slots <= 4) launch_trans_nd_k<KIND, 4>(A, grid, sm, s);
+  else if (slots <= 6) launch_trans_nd_k<KIND, 6>(A, grid, sm, s);
+  else throw zf_error(ZF_ERR_ARG, "expansion order too large for the batched translation");
+  ZF_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void plan3d_build(Plan3D& P, double eps, int ns, const zdc* zsrc, int nt, const zdc* ztarg,
+                  int isep, cudaStream_t s) {
+  if (isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
+  P.eps = eps;
+  P.isep = isep;
+  P.ns = ns;
+  P.nt = nt;
+  ZF_CUDA(cudaGetDevice(&P.device));
+  TreeParams tp;
+  tp.D = 3;
+  tp.isep = isep;
+  tp.idivflag = 0;
+  tp.ndiv = lndiv3d(eps, ns, nt);
+  tp.lr_isep_quirk = 1;
+  setup3d_geom(ns, zsrc, nt, ztarg, tp, P.S, s);
+  ZF_CUDA(cudaStreamSynchronize(s));
+}
+
+void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int ifpgh, zdc* pot,
+                          zdc* grad, cudaStream_t s, StepTimes* times) {
+  const Setup3D& S = P.S;
+  const int ns = P.ns, nt = P.nt;
+  long launches0 = launch_counter();
+  cudaEvent_t ev[8];
+  const bool timing = times != nullptr;
+  if (timing)
+    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  auto mark = [&](int i) {
+    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  mark(0);
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  const int nb = t.nboxes, nlev = t.nlevels;
+  const int p = zl3dterms(P.eps);
+  if (xsm_bytes(p) > 227 * 1024)
+    throw zf_error(ZF_ERR_ARG, "expansion order " + std::to_string(p) +
+                                   " too large for the batched 3D translation (eps too small)");
+  Tab3 T = get_tab3(p);
+  RotTab R = get_rottab(p);
+  const size_t NC = (size_t)T.NC;
+  std::vector<double> rsc_h(nlev + 2, 1.0);
+  for (int l = 0; l <= nlev; l++) rsc_h[l] = S.bsz[l] > 1.0 ? 1.0 : S.bsz[l];
+  DevBuf<double> rsc(rsc_h.size(), s);
+  ZF_CUDA(cudaMemcpyAsync(rsc.get(), rsc_h.data(), rsc_h.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, s));
+  // strengths in tree order, rescaled as the single right-hand-side driver
+  DevBuf<zdc> q((size_t)ns * nd, s), ds((size_t)ns * nd, s), dv(3 * (size_t)ns, s);
+  gather_strengths_nd(S, ns, nd, in.ifcharge ? in.charge : nullptr,
+                      in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
+                      true, true, q.get(), ds.get(), dv.get(), s);
+  mark(1);
+  DevBuf<zdc> mp(NC * nb * nd, s), loc(NC * nb * nd, s), potsort((size_t)nt * nd, s),
+      gradsort(ifpgh > 1 ? 3 * (size_t)nt * nd : 1, s);
+  mp.zero();
+  loc.zero();
+  potsort.zero();
+  gradsort.zero();
+  int dev = 0, nsm = 148;
+  ZF_CUDA(cudaGetDevice(&dev));
+  ZF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int nchunk = div_up(nd, 32);
+  // P2M
+  FormNdArgs F;
+  F.T = T;
+  F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
+  F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
+  F.zsrc = S.zsrcsort.get(); F.q = q.get(); F.ds = ds.get(); F.dv = dv.get();
+  F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get(); F.rsc = rsc.get();
+  F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
+  F.nb = nb; F.nd = nd; F.nchunk = nchunk; F.ifcharge = in.ifcharge; F.ifdipole = in.ifdipole;
+  const bool dip = in.ifdipole != 0;
+  const size_t smf = FW * form_nd_warp_elems(dip) * sizeof(zdc);
+  const int fgrid = (int)div_up((long)nb * nchunk, FW);
+  auto form = [&](bool local) {
+    if (local) {
+      if (dip) {
+        ZF_CUDA(cudaFuncSetAttribute(k_form3nd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+        klaunch(k_form3nd<true, true>, fgrid, FW * 32, smf, s, F);
+      } else {
+        ZF_CUDA(cudaFuncSetAttribute(k_form3nd<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+        klaunch(k_form3nd<true, false>, fgrid, FW * 32, smf, s, F);
+      }
+    } else {
+      if (dip) {
+        ZF_CUDA(cudaFuncSetAttribute(k_form3nd<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+        klaunch(k_form3nd<false, true>, fgrid, FW * 32, smf, s, F);
+      } else {
+        ZF_CUDA(cudaFuncSetAttribute(k_form3nd<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+        klaunch(k_form3nd<false, false>, fgrid, FW * 32, smf, s, F);
+      }
+    }
+    ZF_LAUNCH_CHECK();
+  };
+  F.out = mp.get();
+  if (nlev >= 1) form(false);
+  mark(2);
+  // translations: a persistent grid of one CTA per SM, scratch per CTA
+  const int xgrid = std::max(1, std::min(nsm, nb));
+  DevBuf<zdc> scratch((size_t)xgrid * 2 * NC * RC, s);
+  TransNdArgs A;
+  A.T = T;
+  A.R = R;
+  A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
+  A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
+  A.zcs = S.zcsrc.get(); A.zct = S.zctarg.get(); A.rsc = rsc.get();
+  A.nl2 = L.n[1].get(); A.l2 = L.list[1].get(); A.nl4 = L.n[3].get(); A.mn2 = L.mn[1];
+  A.scratch = scratch.get();
+  A.nd = nd;
+  A.in = mp.get();
+  A.out = mp.get();
+  for (int l = nlev - 1; l >= 1; l--) {
+    A.lo = t.laddr[2 * l];
+    A.hi = t.laddr[2 * l + 1];
+    launch_trans_nd<0>(A, std::min(xgrid, A.hi - A.lo + 1), s);
+  }
+  mark(3);
+  A.in = mp.get();
+  A.out = loc.get();
+  A.lo = 0;
+  A.hi = nb - 1;
+  launch_trans_nd<1>(A, xgrid, s);
+  if (L.mn[3] > 0) {
+    F.out = loc.get();
+    form(true);
+  }
+  mark(4);
+  A.in = loc.get();
+  A.out = loc.get();
+  for (int l = 1; l <= nlev - 1; l++) {
+    A.lo = t.laddr[2 * (l + 1)];
+    A.hi = t.laddr[2 * (l + 1) + 1];
+    launch_trans_nd<2>(A, std::min(xgrid, A.hi - A.lo + 1), s);
+  }
+  mark(5);
+  // P2P, then L2T / M2T
+  P2PNdArgs Pa;
+  Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
+  Pa.zsrc = S.zsrcsort.get(); Pa.q = q.get(); Pa.ds = ds.get(); Pa.dv = dv.get();
+  Pa.ztarg = S.ztargsort.get();
+  Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb; Pa.nd = nd;
+  Pa.ifcharge = in.ifcharge; Pa.ifdipole = in.ifdipole;
+  Pa.pot = potsort.get(); Pa.grad = gradsort.get();
+  const size_t smp = sizeof(SrcTileNd);
+  if (ifpgh > 1) {
+    if (dip) {
+      ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+      klaunch(k_p2p3nd<true, true>, nb, ENT, smp, s, Pa);
+    } else {
+      ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+      klaunch(k_p2p3nd<true, false>, nb, ENT, smp, s, Pa);
+    }
+  } else {
+    if (dip) {
+      ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+      klaunch(k_p2p3nd<false, true>, nb, ENT, smp, s, Pa);
+    } else {
+      ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+      klaunch(k_p2p3nd<false, false>, nb, ENT, smp, s, Pa);
+    }
+  }
+  ZF_LAUNCH_CHECK();
+  EvalNdArgs E;
+  E.T = T;
+  E.ilevel = t.ilevel.get(); E.nchild = t.nchild.get(); E.isrcse = S.isrcse.get();
+  E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
+  E.zct = S.zctarg.get(); E.rsc = rsc.get(); E.mp = mp.get(); E.loc = loc.get();
+  E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb; E.nd = nd;
+  E.pot = potsort.get(); E.grad = gradsort.get();
+  if (ifpgh > 1) klaunch(k_eval3nd<true>, nb, ENT, 0, s, E);
+  else klaunch(k_eval3nd<false>, nb, ENT, 0, s, E);
+  ZF_LAUNCH_CHECK();
+  mark(6);
+  unsort3d_nd(nt, nd, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0), mkz(1.0 / S.b0),
+              ifpgh, pot, grad, s);
+  mark(7);
+  if (timing) {
+    ZF_CUDA(cudaEventSynchronize(ev[7]));
+    float ms;
+    // steps as the single right-hand-side driver; set-up = the strength gather
+    for (int i = 0; i < 7; i++) {
+      ZF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      times->ms[i] = ms;
+    }
+    times->nboxes = nb;
+    times->nlevels = nlev;
+    times->nterms = p;
+    for (auto& e : ev) cudaEventDestroy(e);
+    times->launches = launch_counter() - launches0;
+    if (times->want_counts) {
+      std::vector<int> pl(nlev + 1, p);
+      count_interactions3d(S, pl.data(), 1, 1, 2, times, s);
+    }
+  }
+  (void)ns;
+}
+
+}  // namespace zf
