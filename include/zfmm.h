@@ -197,6 +197,15 @@ int zfmm_zlfmm3d_plan(zfmm_plan3d plan, int nd, int ifcharge, const double *char
 int zfmm_zlfmm3d_plan_dev(zfmm_plan3d plan, int nd, int ifcharge, const double *charge,
                           int ifdipole, const double *dipstr, const double *dipvec, int ifpgh,
                           double *pot, double *grad, void *stream);
+/* 3D Helmholtz solves on a plan, wavenumber zk = (re, im): the plan's tree is
+ * reused for every wavenumber and right-hand side. */
+int zfmm_zhfmm3d_plan(zfmm_plan3d plan, const double *zk, int nd, int ifcharge,
+                      const double *charge, int ifdipole, const double *dipstr,
+                      const double *dipvec, int ifpgh, double *pot, double *grad);
+int zfmm_zhfmm3d_plan_dev(zfmm_plan3d plan, const double *zk, int nd, int ifcharge,
+                          const double *charge, int ifdipole, const double *dipstr,
+                          const double *dipvec, int ifpgh, double *pot, double *grad,
+                          void *stream);
 
 /* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory during a

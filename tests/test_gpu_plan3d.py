@@ -7,7 +7,9 @@ solve (itself pinned to the oracle) to 10*eps relative L2, the parity bar of
 the FMMs.  One small case goes straight against the oracle.  The cases cover
 one and many right-hand sides (a ragged last pass of 32), charges and dipoles,
 ifpgh 1 and 2, adaptive trees with lists 3 and 4, plan reuse, and the device
-(torch) entry point."""
+(torch) entry point.  Helmholtz plan solves run the single-solve passes on
+the plan's tree for every right-hand side and wavenumber, so they must equal
+the single solves to rounding."""
 import numpy as np
 import pytest
 
@@ -137,3 +139,24 @@ def test_plan_device_entry_point():
     assert tuple(pt.shape) == (nd, n) and tuple(gt.shape) == (nd, 3, n)
     assert rel(pt.cpu().numpy(), p) < 1e-13
     assert rel(gt.cpu().numpy(), g) < 1e-13
+
+
+def test_helmholtz_plan_matches_single_two_wavenumbers():
+    import zfmm_b200
+    eps = 1e-9
+    w = W.sphere3d(15000, seed=18)
+    zs = w["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(8)
+    nd = 3
+    q, ds = cn(rng, nd, n), cn(rng, nd, n)
+    plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
+    for zk in (10 + 0.2j, 4 - 0.1j):
+        for ifc, ifd, ifpgh in [(1, 1, 2), (1, 0, 1)]:
+            p, g = plan.zhfmm3d(zk, nd, ifc, q, ifd, ds, w["dipvec"], ifpgh)
+            for r in range(nd):
+                p1, g1 = zfmm_b200.zhfmm3d(eps, zk, n, zs, ifc, q[r], ifd, ds[r], w["dipvec"],
+                                           n, zs, ifpgh, 1)
+                assert rel(p[r], p1) < 1e-13, (zk, ifc, ifd, r)
+                if ifpgh == 2:
+                    assert rel(g[r], g1) < 1e-13, (zk, ifc, ifd, r)

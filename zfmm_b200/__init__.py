@@ -324,7 +324,15 @@ class Plan3D:
 
     def zlfmm3d(self, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh=1):
         """3D Laplace FMM of nd right-hand sides on the plan's points."""
+        return self._solve(None, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh)
+
+    def zhfmm3d(self, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh=1):
+        """3D Helmholtz FMM (wavenumber zk) of nd right-hand sides on the plan's points."""
+        return self._solve(zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh)
+
+    def _solve(self, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh):
         nd, ns, nt = int(nd), self.ns, self.nt
+        k = None if zk is None else _zk(zk)
         if _is_torch(charge if ifcharge == 1 else dipstr):
             import torch
             dev = self.device
@@ -335,16 +343,28 @@ class Plan3D:
             grad = torch.empty((nt, 3, nd), dtype=torch.complex128, device=dev)
             stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
             p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
-            check(lib().zfmm_zlfmm3d_plan_dev(self._h, nd, int(ifcharge), p(q), int(ifdipole),
-                                              p(ds), p(dv), int(ifpgh), p(pot), p(grad), stream))
+            if k is None:
+                check(lib().zfmm_zlfmm3d_plan_dev(self._h, nd, int(ifcharge), p(q),
+                                                  int(ifdipole), p(ds), p(dv), int(ifpgh),
+                                                  p(pot), p(grad), stream))
+            else:
+                check(lib().zfmm_zhfmm3d_plan_dev(self._h, _ptr(k), nd, int(ifcharge), p(q),
+                                                  int(ifdipole), p(ds), p(dv), int(ifpgh),
+                                                  p(pot), p(grad), stream))
             return pot.t(), grad.permute(2, 1, 0)
         q = _mat(charge, nd, ns, "charge") if ifcharge == 1 else None
         ds = _mat(dipstr, nd, ns, "dipstr") if ifdipole == 1 else None
         dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
         pot = np.zeros((nd, nt), np.complex128, order="F")
         grad = np.zeros((nd, 3, nt), np.complex128, order="F")
-        check(lib().zfmm_zlfmm3d_plan(self._h, nd, int(ifcharge), _ptr(q), int(ifdipole),
-                                      _ptr(ds), _ptr(dv), int(ifpgh), _ptr(pot), _ptr(grad)))
+        if k is None:
+            check(lib().zfmm_zlfmm3d_plan(self._h, nd, int(ifcharge), _ptr(q), int(ifdipole),
+                                          _ptr(ds), _ptr(dv), int(ifpgh), _ptr(pot),
+                                          _ptr(grad)))
+        else:
+            check(lib().zfmm_zhfmm3d_plan(self._h, _ptr(k), nd, int(ifcharge), _ptr(q),
+                                          int(ifdipole), _ptr(ds), _ptr(dv), int(ifpgh),
+                                          _ptr(pot), _ptr(grad)))
         return pot, grad
 
     def close(self):

@@ -93,6 +93,10 @@ SIGNATURES = {
                                   c_int, c_void_p, c_void_p]),
     "zfmm_zlfmm3d_plan_dev": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
                                       c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "zfmm_zhfmm3d_plan": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                  c_void_p, c_int, c_void_p, c_void_p]),
+    "zfmm_zhfmm3d_plan_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
+                                      c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "zfmm_probe_fp64_tflops": (c_double, [c_int]),
     "zfmm_probe_dmma_tflops": (c_double, [c_int]),
     "zfmm_last_error": (ctypes.c_char_p, []),

@@ -802,9 +802,9 @@ void check_plan_args(zfmm_plan3d_s* plan, int nd, int ifcharge, const double* ch
 }
 
 // device path of the plan solves: pot / grad zeroed, then the FMM
-void run_plan3d(zfmm_plan3d_s* plan, int nd, int ifcharge, const zdc* charge, int ifdipole,
-                const zdc* dipstr, const zdc* dipvec, int ifpgh, zdc* pot, zdc* grad,
-                cudaStream_t s) {
+void run_plan3d(zfmm_plan3d_s* plan, const zdc* zk, int nd, int ifcharge, const zdc* charge,
+                int ifdipole, const zdc* dipstr, const zdc* dipvec, int ifpgh, zdc* pot,
+                zdc* grad, cudaStream_t s) {
   const Plan3D& P = plan->P;
   if (P.nt > 0) {
     ZF_CUDA(cudaMemsetAsync(pot, 0, sizeof(zdc) * P.nt * (size_t)nd, s));
@@ -819,8 +819,12 @@ void run_plan3d(zfmm_plan3d_s* plan, int nd, int ifcharge, const zdc* charge, in
   in.dipvec = dipvec;
   StepTimes t;
   t.want_counts = g_timing >= 2;
-  zlfmm3d_plan_execute(P, nd, in, ifpgh, pot, ifpgh > 1 ? grad : nullptr, s,
-                       g_timing ? &t : nullptr);
+  if (zk)
+    zhfmm3d_plan_execute(P, *zk, nd, in, ifpgh, pot, ifpgh > 1 ? grad : nullptr, s,
+                         g_timing ? &t : nullptr);
+  else
+    zlfmm3d_plan_execute(P, nd, in, ifpgh, pot, ifpgh > 1 ? grad : nullptr, s,
+                         g_timing ? &t : nullptr);
   if (g_timing) g_times = t;
 }
 
@@ -896,9 +900,13 @@ int zfmm_plan3d_info(zfmm_plan3d plan, int* nboxes, int* nlevels, int* ns, int* 
   });
 }
 
-int zfmm_zlfmm3d_plan(zfmm_plan3d plan, int nd, int ifcharge, const double* charge,
-                      int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
-                      double* pot, double* grad) {
+}  // extern "C"
+
+namespace {
+
+int plan_solve_host(zfmm_plan3d plan, const double* zk, int nd, int ifcharge,
+                    const double* charge, int ifdipole, const double* dipstr,
+                    const double* dipvec, int ifpgh, double* pot, double* grad) {
   return guarded([&] {
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_plan_args(plan, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot, grad);
@@ -911,8 +919,9 @@ int zfmm_zlfmm3d_plan(zfmm_plan3d plan, int nd, int ifcharge, const double* char
       upload(h.dipvec, dipvec, 3 * (size_t)ns, s);
     }
     DevBuf<zdc> dpot((size_t)nd * nt, s), dgrad(ifpgh > 1 ? 3 * (size_t)nd * nt : 0, s);
-    run_plan3d(plan, nd, ifcharge, h.charge.get(), ifdipole, h.dipstr.get(), h.dipvec.get(),
-               ifpgh, dpot.get(), dgrad.get(), s);
+    zdc k = zk ? mkz(zk[0], zk[1]) : mkz(0.0);
+    run_plan3d(plan, zk ? &k : nullptr, nd, ifcharge, h.charge.get(), ifdipole, h.dipstr.get(),
+               h.dipvec.get(), ifpgh, dpot.get(), dgrad.get(), s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt * (size_t)nd,
                               cudaMemcpyDeviceToHost, s));
@@ -928,17 +937,53 @@ int zfmm_zlfmm3d_plan(zfmm_plan3d plan, int nd, int ifcharge, const double* char
   });
 }
 
-int zfmm_zlfmm3d_plan_dev(zfmm_plan3d plan, int nd, int ifcharge, const double* charge,
-                          int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
-                          double* pot, double* grad, void* stream) {
+int plan_solve_dev(zfmm_plan3d plan, const double* zk, int nd, int ifcharge,
+                   const double* charge, int ifdipole, const double* dipstr,
+                   const double* dipvec, int ifpgh, double* pot, double* grad, void* stream) {
   return guarded([&] {
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_plan_args(plan, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot, grad);
     cudaStream_t s = (cudaStream_t)stream;
-    run_plan3d(plan, nd, ifcharge, (const zdc*)charge, ifdipole, (const zdc*)dipstr,
-               (const zdc*)dipvec, ifpgh, (zdc*)pot, (zdc*)grad, s);
+    zdc k = zk ? mkz(zk[0], zk[1]) : mkz(0.0);
+    run_plan3d(plan, zk ? &k : nullptr, nd, ifcharge, (const zdc*)charge, ifdipole,
+               (const zdc*)dipstr, (const zdc*)dipvec, ifpgh, (zdc*)pot, (zdc*)grad, s);
     ZF_CUDA(cudaStreamSynchronize(s));
   });
+}
+
+}  // namespace
+
+extern "C" {
+
+int zfmm_zlfmm3d_plan(zfmm_plan3d plan, int nd, int ifcharge, const double* charge,
+                      int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
+                      double* pot, double* grad) {
+  return plan_solve_host(plan, nullptr, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh,
+                         pot, grad);
+}
+
+int zfmm_zlfmm3d_plan_dev(zfmm_plan3d plan, int nd, int ifcharge, const double* charge,
+                          int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
+                          double* pot, double* grad, void* stream) {
+  return plan_solve_dev(plan, nullptr, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh,
+                        pot, grad, stream);
+}
+
+int zfmm_zhfmm3d_plan(zfmm_plan3d plan, const double* zk, int nd, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr,
+                      const double* dipvec, int ifpgh, double* pot, double* grad) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  return plan_solve_host(plan, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot,
+                         grad);
+}
+
+int zfmm_zhfmm3d_plan_dev(zfmm_plan3d plan, const double* zk, int nd, int ifcharge,
+                          const double* charge, int ifdipole, const double* dipstr,
+                          const double* dipvec, int ifpgh, double* pot, double* grad,
+                          void* stream) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  return plan_solve_dev(plan, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot,
+                        grad, stream);
 }
 
 }  // extern "C"

@@ -145,7 +145,52 @@ __global__ void k_unsort_nd(int nt, int nd, const int* __restrict__ perm,
       grad[(3 * j + d) * nd + r] = gs[(3L * i + d) * nd + r] * gscale;
 }
 
+__global__ void k_gather_col(int ns, int nd, int r, const int* __restrict__ perm,
+                             const zdc* __restrict__ q, const zdc* __restrict__ ds,
+                             const zdc* __restrict__ dv, const double* __restrict__ b0,
+                             int rescale_q, int rescale_dv, zdc* qs, zdc* dss, zdc* dvs) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  double bi = 1.0 / b0[0];
+  long j = perm[i];
+  qs[i] = q ? q[j * nd + r] * (rescale_q ? bi : 1.0) : mkz(0.0);
+  dss[i] = ds ? ds[j * nd + r] : mkz(0.0);
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    dvs[3 * i + d] = dv ? dv[3 * j + d] * (rescale_dv ? bi * bi : 1.0) : mkz(0.0);
+}
+
+__global__ void k_unsort_col(int nt, int nd, int r, const int* __restrict__ perm,
+                             const zdc* __restrict__ ps, const zdc* __restrict__ gs, zdc pscale,
+                             zdc gscale, int ifpgh, zdc* pot, zdc* grad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt) return;
+  long j = perm[i];
+  pot[j * nd + r] = ps[i] * pscale;
+  if (ifpgh > 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) grad[(3 * j + d) * nd + r] = gs[3 * i + d] * gscale;
+}
+
 }  // namespace
+
+void gather_strengths_col(const Setup3D& S, int ns, int nd, int r, const zdc* charge,
+                          const zdc* dipstr, const zdc* dipvec, bool rescale_charge,
+                          bool rescale_dipvec, zdc* q, zdc* ds, zdc* dv, cudaStream_t s) {
+  if (ns <= 0) return;
+  klaunch(k_gather_col, div_up(ns, TB), TB, 0, s, ns, nd, r, S.isrc.get(), charge, dipstr,
+          dipvec, S.tree.bsz.get(), rescale_charge ? 1 : 0, rescale_dipvec ? 1 : 0, q, ds, dv);
+  ZF_LAUNCH_CHECK();
+}
+
+void unsort3d_col(int nt, int nd, int r, const int* itarg, const zdc* potsort,
+                  const zdc* gradsort, zdc pscale, zdc gscale, int ifpgh, zdc* pot, zdc* grad,
+                  cudaStream_t s) {
+  if (nt <= 0) return;
+  klaunch(k_unsort_col, div_up(nt, TB), TB, 0, s, nt, nd, r, itarg, potsort, gradsort, pscale,
+          gscale, ifpgh, pot, grad);
+  ZF_LAUNCH_CHECK();
+}
 
 void setup3d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
                   Setup3D& S, cudaStream_t s) {

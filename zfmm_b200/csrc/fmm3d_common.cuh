@@ -56,6 +56,18 @@ void gather_strengths_nd(const Setup3D& S, int ns, int nd, const zdc* charge, co
 void unsort3d_nd(int nt, int nd, const int* itarg, const zdc* potsort, const zdc* gradsort,
                  zdc pscale, zdc gscale, int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);
 
+// right-hand side r of charge(nd, ns), dipstr(nd, ns) into tree order, as
+// setup3d's strengths (q[i], ds[i], dv[3i+d]); null inputs give zeros
+void gather_strengths_col(const Setup3D& S, int ns, int nd, int r, const zdc* charge,
+                          const zdc* dipstr, const zdc* dipvec, bool rescale_charge,
+                          bool rescale_dipvec, zdc* q, zdc* ds, zdc* dv, cudaStream_t s);
+
+// right-hand side r of pot(nd, nt) / grad(nd, 3, nt) from one right-hand
+// side's sorted potsort / gradsort
+void unsort3d_col(int nt, int nd, int r, const int* itarg, const zdc* potsort,
+                  const zdc* gradsort, zdc pscale, zdc gscale, int ifpgh, zdc* pot, zdc* grad,
+                  cudaStream_t s);
+
 void unsort3d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc pscale,
               zdc gscale, int ifpgh, zdc* pot, zdc* grad, cudaStream_t s);
 

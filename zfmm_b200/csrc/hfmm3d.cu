@@ -39,6 +39,7 @@
 #include "helm3d_special.cuh"
 #include "hfmm3d.cuh"
 #include "lfmm3d.cuh"
+#include "plan3d.cuh"
 #include "sph3d.cuh"
 
 namespace zf {
@@ -71,6 +72,19 @@ struct ShiftTab {
 };
 
 __device__ __forceinline__ int jdx(int n, int m) { return n * (n + 1) / 2 + m; }
+
+// per-wavenumber state of a solve: orders per level, expansion offsets,
+// tables of the largest order, quadrature z-shift configurations
+struct HelmPrep {
+  HLev lev;
+  int pmax = 0;
+  long tot = 0;
+  Tab3 T;
+  zdc kw;
+  DevBuf<double> dxw;
+  DevBuf<zdc> dcfd;
+  DevBuf<ShiftTab> dst;
+};
 
 // ---- translation kernel ------------------------------------------------------
 struct HTransArgs {
@@ -1022,33 +1036,15 @@ void zh3ddirect_device(zdc zk, const Inputs3D& in, zdc* pot, zdc* grad, cudaStre
   ZF_LAUNCH_CHECK();
 }
 
-void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
-                    cudaStream_t s, StepTimes* times) {
-  int ns = in.ns, nt = in.nt;
-  long launches0 = launch_counter();
-  cudaEvent_t ev[8];
-  bool timing = times != nullptr;
-  if (timing)
-    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
-  auto mark = [&](int i) {
-    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
-  };
-  mark(0);
-  TreeParams tp;
-  tp.D = 3;
-  tp.isep = isep;
-  tp.idivflag = 0;                 // hndiv resets the driver's idivflag = 2 (zhfmm3d.f:64-67)
-  tp.ndiv = lndiv3d(eps, ns, nt);  // hndiv_fast.f: the same table as lndiv
-  tp.lr_isep_quirk = 1;
-  Setup3D S;
-  setup3d(in, tp, S, true, true, s);
-  mark(1);
+// orders per level, tables and quadrature z-shift configurations of one
+// wavenumber on a set-up (zhfmm3d.f:200-240 and the zh3dtrans.f set-ups)
+void helm_prep(const Setup3D& S, double eps, zdc zk, int isep, HelmPrep& H, cudaStream_t s) {
   const DevTree& t = S.tree;
-  const DevLists& L = S.lists;
-  int nb = t.nboxes, nlev = t.nlevels;
+  const int nlev = t.nlevels;
   if (nlev + 1 > ML) throw zf_error(ZF_ERR_ARG, "too many tree levels");
   zdc kw = zk * S.b0;  // zkfmm
-  HLev lev;
+  H.kw = kw;
+  HLev& lev = H.lev;
   long tot = 0;
   int pmax = 0, pref = 0;
   for (int l = 0; l <= nlev; l++) {
@@ -1073,7 +1069,9 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
   }
   if (pmax > PMAXR)
     throw zf_error(ZF_ERR_ARG, "expansion order " + std::to_string(pmax) + " too large");
-  Tab3 T = get_tab3(pmax);
+  H.T = get_tab3(pmax);
+  H.pmax = pmax;
+  H.tot = tot;
   // quadrature z-shift tables per kind and output level
   std::vector<ShiftTab> sth(3 * ML);
   std::vector<double> xw;  // nodes and weights, all configurations
@@ -1128,8 +1126,10 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
       st.rs1 = lev.rs[l1];
       pend.push_back(pe);
     }
-  DevBuf<double> dxw(std::max<size_t>(xw.size(), 1), s);
-  DevBuf<zdc> dcfd(std::max<size_t>(cfd.size(), 1), s);
+  DevBuf<double>& dxw = H.dxw;
+  DevBuf<zdc>& dcfd = H.dcfd;
+  dxw.alloc(std::max<size_t>(xw.size(), 1), s);
+  dcfd.alloc(std::max<size_t>(cfd.size(), 1), s);
   if (!xw.empty())
     ZF_CUDA(cudaMemcpyAsync(dxw.get(), xw.data(), xw.size() * sizeof(double),
                             cudaMemcpyHostToDevice, s));
@@ -1143,32 +1143,51 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
     st.cF = dcfd.get() + pe.fo;
     st.cD = dcfd.get() + pe.dpo;
   }
-  DevBuf<ShiftTab> dst(3 * ML, s);
+  DevBuf<ShiftTab>& dst = H.dst;
+  dst.alloc(3 * ML, s);
   ZF_CUDA(cudaMemcpyAsync(dst.get(), sth.data(), sth.size() * sizeof(ShiftTab),
                           cudaMemcpyHostToDevice, s));
   ZF_CUDA(cudaStreamSynchronize(s));  // the host staging vectors go out of scope below
-  DevBuf<zdc> mp(std::max<long>(tot, 1), s), loc(std::max<long>(tot, 1), s), potsort(nt, s),
-      gradsort(in.ifpgh > 1 ? 3 * (size_t)nt : 1, s);
+}
+
+// P2M through L2T/M2T/P2P on a set-up and its wavenumber tables: adds the
+// sorted potentials (and gradients, unscaled) of one right-hand side with
+// sorted strengths q, ds, dv to potsort / gradsort; ev[2..5] (optional) get
+// the step boundaries recorded
+void helm_core(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds, const zdc* dv,
+               int ifcharge, int ifdipole, int ifpgh, zdc* potsort, zdc* gradsort,
+               cudaStream_t s, cudaEvent_t* ev) {
+  auto hmark = [&](int i) {
+    if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  const int nb = t.nboxes, nlev = t.nlevels;
+  const HLev& lev = H.lev;
+  const int pmax = H.pmax;
+  const long tot = H.tot;
+  const Tab3& T = H.T;
+  const zdc kw = H.kw;
+  const DevBuf<ShiftTab>& dst = H.dst;
+  DevBuf<zdc> mp(std::max<long>(tot, 1), s), loc(std::max<long>(tot, 1), s);
   mp.zero();
   loc.zero();
-  potsort.zero();
-  gradsort.zero();
   // P2M
   HFormArgs F;
   F.r1 = T.r1; F.r2 = T.r2; F.sq = T.sq; F.L = pmax + 1;
   F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
   F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
-  F.zsrc = S.zsrcsort.get(); F.charge = S.chargesort.get(); F.dipstr = S.dipstrsort.get();
-  F.dipvec = S.dipvecsort.get(); F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get();
+  F.zsrc = S.zsrcsort.get(); F.charge = q; F.dipstr = ds;
+  F.dipvec = dv; F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get();
   F.lev = lev; F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
-  F.nb = nb; F.ifcharge = in.ifcharge; F.ifdipole = in.ifdipole; F.pbuf = pmax; F.zk = kw;
+  F.nb = nb; F.ifcharge = ifcharge; F.ifdipole = ifdipole; F.pbuf = pmax; F.zk = kw;
   int fw = HFNT / 32;  // warps of the form kernel, one partial expansion each
   while (fw > 1 && (size_t)fw * (pmax + 1) * (pmax + 1) * sizeof(zdc) > kSmemMax) fw /= 2;
   size_t smf = (size_t)fw * (pmax + 1) * (pmax + 1) * sizeof(zdc);
   if (smf > kSmemMax) throw zf_error(ZF_ERR_ARG, "expansion order too large for P2M staging");
   F.out = mp.get();
   if (nlev >= 2) {
-    if (in.ifdipole) {
+    if (ifdipole) {
       ZF_CUDA(cudaFuncSetAttribute(k_hform3<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
       klaunch(k_hform3<false, true>, nb, 32 * fw, smf, s, F);
     } else {
@@ -1177,7 +1196,7 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
     }
     ZF_LAUNCH_CHECK();
   }
-  mark(2);
+  hmark(2);
   HTransArgs A;
   A.r1 = T.r1; A.r2 = T.r2; A.sq = T.sq; A.dinv = T.dinv; A.L = pmax + 1; A.pT = pmax;
   A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
@@ -1202,7 +1221,7 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
     A.hi = t.laddr[2 * l + 1];
     launch_htrans<0>(A, hscratch.get(), s);
   }
-  mark(3);
+  hmark(3);
   // M2L over levels >= 2, then P2L (list 4)
   A.in = mp.get();
   A.out = loc.get();
@@ -1214,7 +1233,7 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
   }
   if (L.mn[3] > 0) {
     F.out = loc.get();
-    if (in.ifdipole) {
+    if (ifdipole) {
       ZF_CUDA(cudaFuncSetAttribute(k_hform3<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
       klaunch(k_hform3<true, true>, nb, 32 * fw, smf, s, F);
     } else {
@@ -1223,7 +1242,7 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
     }
     ZF_LAUNCH_CHECK();
   }
-  mark(4);
+  hmark(4);
   // L2L, coarsest first: children at level l+1 of parents at level l >= 2
   A.in = loc.get();
   A.out = loc.get();
@@ -1233,15 +1252,15 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
     A.hi = t.laddr[2 * (l + 1) + 1];
     launch_htrans<2>(A, hscratch.get(), s);
   }
-  mark(5);
+  hmark(5);
   HP2PArgs Pa;
   Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
-  Pa.zsrc = S.zsrcsort.get(); Pa.charge = S.chargesort.get(); Pa.dipstr = S.dipstrsort.get();
-  Pa.dipvec = S.dipvecsort.get(); Pa.ztarg = S.ztargsort.get();
+  Pa.zsrc = S.zsrcsort.get(); Pa.charge = q; Pa.dipstr = ds;
+  Pa.dipvec = dv; Pa.ztarg = S.ztargsort.get();
   Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb;
-  Pa.ifcharge = in.ifcharge; Pa.ifdipole = in.ifdipole; Pa.zk = kw;
-  Pa.pot = potsort.get(); Pa.grad = gradsort.get();
-  if (in.ifpgh > 1) klaunch(k_hp2p3<true>, nb, HENT, 0, s, Pa);
+  Pa.ifcharge = ifcharge; Pa.ifdipole = ifdipole; Pa.zk = kw;
+  Pa.pot = potsort; Pa.grad = gradsort;
+  if (ifpgh > 1) klaunch(k_hp2p3<true>, nb, HENT, 0, s, Pa);
   else klaunch(k_hp2p3<false>, nb, HENT, 0, s, Pa);
   ZF_LAUNCH_CHECK();
   HEvalArgs E;
@@ -1250,9 +1269,9 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
   E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
   E.zct = S.zctarg.get(); E.lev = lev; E.mp = mp.get(); E.loc = loc.get();
   E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb; E.pbuf = pmax;
-  E.zk = kw; E.pot = potsort.get(); E.grad = gradsort.get();
+  E.zk = kw; E.pot = potsort; E.grad = gradsort;
   size_t sme = (size_t)(pmax + 1) * (pmax + 1) * sizeof(zdc);
-  if (in.ifpgh > 1) {
+  if (ifpgh > 1) {
     ZF_CUDA(cudaFuncSetAttribute(k_heval3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
     klaunch(k_heval3<true>, nb, HENT, sme, s, E);
   } else {
@@ -1260,6 +1279,36 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
     klaunch(k_heval3<false>, nb, HENT, sme, s, E);
   }
   ZF_LAUNCH_CHECK();
+}
+
+void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
+                    cudaStream_t s, StepTimes* times) {
+  int ns = in.ns, nt = in.nt;
+  long launches0 = launch_counter();
+  cudaEvent_t ev[8];
+  bool timing = times != nullptr;
+  if (timing)
+    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  auto mark = [&](int i) {
+    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  mark(0);
+  TreeParams tp;
+  tp.D = 3;
+  tp.isep = isep;
+  tp.idivflag = 0;                 // hndiv resets the driver's idivflag = 2 (zhfmm3d.f:64-67)
+  tp.ndiv = lndiv3d(eps, ns, nt);  // hndiv_fast.f: the same table as lndiv
+  tp.lr_isep_quirk = 1;
+  Setup3D S;
+  setup3d(in, tp, S, true, true, s);
+  mark(1);
+  HelmPrep H;
+  helm_prep(S, eps, zk, isep, H, s);
+  DevBuf<zdc> potsort(nt, s), gradsort(in.ifpgh > 1 ? 3 * (size_t)nt : 1, s);
+  potsort.zero();
+  gradsort.zero();
+  helm_core(S, H, S.chargesort.get(), S.dipstrsort.get(), S.dipvecsort.get(), in.ifcharge,
+            in.ifdipole, in.ifpgh, potsort.get(), gradsort.get(), s, timing ? ev : nullptr);
   mark(6);
   unsort3d(nt, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0), mkz(1.0 / S.b0), in.ifpgh,
            pot, grad, s);
@@ -1271,12 +1320,66 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
       ZF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
       times->ms[i] = ms;
     }
-    times->nboxes = nb;
-    times->nlevels = nlev;
-    times->nterms = pmax;
+    times->nboxes = S.tree.nboxes;
+    times->nlevels = S.tree.nlevels;
+    times->nterms = H.pmax;
     for (auto& e : ev) cudaEventDestroy(e);
     times->launches = launch_counter() - launches0;
-    if (times->want_counts) count_interactions3d(S, lev.p, 2, 2, 3, times, s);
+    if (times->want_counts) count_interactions3d(S, H.lev.p, 2, 2, 3, times, s);
+  }
+}
+
+void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in, int ifpgh,
+                          zdc* pot, zdc* grad, cudaStream_t s, StepTimes* times) {
+  const Setup3D& S = P.S;
+  const int ns = P.ns, nt = P.nt;
+  long launches0 = launch_counter();
+  const bool timing = times != nullptr;
+  cudaEvent_t ev[8];
+  if (timing)
+    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  float acc[8] = {0};
+  auto mark = [&](int i) {
+    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  auto take = [&](int a, int b, int slot) {
+    if (!timing) return;
+    ZF_CUDA(cudaEventSynchronize(ev[b]));
+    float ms;
+    ZF_CUDA(cudaEventElapsedTime(&ms, ev[a], ev[b]));
+    acc[slot] += ms;
+  };
+  mark(0);
+  HelmPrep H;
+  helm_prep(S, P.eps, zk, P.isep, H, s);
+  DevBuf<zdc> q(ns, s), ds(ns, s), dv(3 * (size_t)ns, s), potsort(nt, s),
+      gradsort(ifpgh > 1 ? 3 * (size_t)nt : 1, s);
+  mark(1);
+  take(0, 1, 0);
+  for (int r = 0; r < nd; r++) {
+    mark(0);
+    gather_strengths_col(S, ns, nd, r, in.ifcharge ? in.charge : nullptr,
+                         in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
+                         true, true, q.get(), ds.get(), dv.get(), s);
+    potsort.zero();
+    gradsort.zero();
+    mark(1);
+    helm_core(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, ifpgh, potsort.get(),
+              gradsort.get(), s, timing ? ev : nullptr);
+    mark(6);
+    unsort3d_col(nt, nd, r, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0),
+                 mkz(1.0 / S.b0), ifpgh, pot, grad, s);
+    mark(7);
+    for (int k = 0; k < 7; k++) take(k, k + 1, k);
+  }
+  if (timing) {
+    for (int k = 0; k < 7; k++) times->ms[k] = acc[k];
+    times->nboxes = S.tree.nboxes;
+    times->nlevels = S.tree.nlevels;
+    times->nterms = H.pmax;
+    for (auto& e : ev) cudaEventDestroy(e);
+    times->launches = launch_counter() - launches0;
+    if (times->want_counts) count_interactions3d(S, H.lev.p, 2, 2, 3, times, s);
   }
 }
 

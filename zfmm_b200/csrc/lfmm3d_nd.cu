@@ -47,12 +47,13 @@ namespace zf {
 
 namespace {
 
-constexpr int XNT = 512;      // threads of the batched translation kernel
+constexpr int XNT = 384;      // threads of the batched translation kernel
 constexpr int XW = XNT / 32;  // its warps
 constexpr int RC = 32;        // right-hand sides per translation pass (one per lane)
-constexpr int JT = 5;         // sample product: angles per warp task
-constexpr int MT = 3;         // projection: orders per warp task
+constexpr int JT = 7;         // sample product: angles per warp task
+constexpr int MT = 6;         // projection: orders per warp task
 constexpr int JB = 8;         // shift: output degrees per warp task
+constexpr int LR = 2;         // input rows per warp prefetched into registers
 
 // cos / sin of 2 pi (jc m mod (2p+1)) / (2p+1), [jc][m] for jc, m <= p
 struct RotTab {
@@ -90,18 +91,33 @@ RotTab get_rottab(int p) {
 // per-angle constants of one y-rotation (the set-up of myzylgndr2sf in z3dyrot)
 struct JCc {
   zdc z, zz1, u, z1, z2, z3, st, eip;
+  zdc yd[2], emr[2];  // Ydiag(m) and eip^m of the states starting at degree m, by parity
 };
+
+// global-memory streams of the translations (inputs, scratch, outputs) go
+// through L2 only, keeping L1 for the recurrence tables
+__device__ __forceinline__ zdc ldcg_z(const zdc* p) {
+  double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+  return mkz(v.x, v.y);
+}
+__device__ __forceinline__ void stcg_z(zdc* p, zdc v) {
+  __stcg(reinterpret_cast<double2*>(p), make_double2(v.re, v.im));
+}
+
+constexpr int kJCz = sizeof(JCc) / sizeof(zdc);  // complex slots per angle record
 
 struct XSm {
   JCc* jc;
   zdc *Cs, *Cd, *As, *Ad, *Ss, *Sd, *Ef, *Eb, *G, *T1, *T2;
+  zdc *Ypp, *Dpp;  // recurrence values of degree n-2 per (angle, order) state
+  zdc* Em;         // eip^m per (angle, order) state
 };
 
 __device__ __forceinline__ XSm carve_xsm(zdc* sm, int p) {
   const int L = p + 1, NS = 2 * p + 1;
   XSm S;
   S.jc = (JCc*)sm;
-  zdc* q = sm + 8 * L;
+  zdc* q = sm + kJCz * L;
   S.Cs = q; q += L * L;
   S.Cd = q; q += L * L;
   S.As = q; q += L * RC;
@@ -112,13 +128,16 @@ __device__ __forceinline__ XSm carve_xsm(zdc* sm, int p) {
   S.Eb = q; q += NS;
   S.G = q; q += NS;
   S.T1 = q; q += L;
-  S.T2 = q;
+  S.T2 = q; q += L;
+  S.Ypp = q; q += L * L;
+  S.Dpp = q; q += L * L;
+  S.Em = q;
   return S;
 }
 
 size_t xsm_bytes(int p) {
   size_t L = p + 1, NS = 2 * p + 1;
-  return (8 * L + 2 * L * L + 4 * L * RC + 3 * NS + 2 * L) * sizeof(zdc);
+  return (kJCz * L + 5 * L * L + 4 * L * RC + 3 * NS + 2 * L) * sizeof(zdc);
 }
 
 struct TransNdArgs {
@@ -132,6 +151,7 @@ struct TransNdArgs {
   zdc* scratch;  // 2 (p+1)^2 RC per CTA
   const int *nl2, *l2, *nl4;
   int mn2, nd, lo, hi;
+  int rot_smem;  // 1: the cos / sin tables are staged in shared memory
 };
 
 // amat-based factor applied after the first rotation (the prescale of the
@@ -186,11 +206,15 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
     c.u = (zabs(c.zz1) >= (double)1e-12f) ? -zsqrt_r(c.zz1) : -st;
     c.st = st;
     c.eip = eip;
+    c.yd[0] = mkz(1.0);
+    c.emr[0] = mkz(1.0);
+    c.yd[1] = mkz(p >= 1 ? -__ldg(&T.r1[L + 1]) : 0.0);
+    c.emr[1] = eip;
     S.jc[j] = c;
   }
-  zdc Yp[SLOTS], Ypp[SLOTS], Dp[SLOTS], Dpp[SLOTS], em[SLOTS];
+  zdc Yp[SLOTS], Dp[SLOTS];
 #pragma unroll
-  for (int s = 0; s < SLOTS; s++) Yp[s] = Ypp[s] = Dp[s] = Dpp[s] = em[s] = mkz(0.0);
+  for (int s = 0; s < SLOTS; s++) Yp[s] = Dp[s] = mkz(0.0);
   __syncthreads();
 
   // sample coefficients of degree n: Cs = C(j,m) + C(j,-m), Cd = C(j,m) - C(j,-m)
@@ -208,16 +232,10 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
         if (m == 0) {
           Y = mkz(1.0);
           D = mkz(0.0);
-          em[s] = mkz(1.0);
         } else {
-          zdc u = J.u, e = J.eip, Yd = mkz(-__ldg(&T.r1[L + 1])), ee = e;
-          for (int k = 2; k <= m; k++) {
-            Yd = (Yd * u) * __ldg(&T.r1[k * L + k]);
-            ee = ee * e;
-          }
-          Y = Yd;
-          D = (Yd * (double)(-m)) * z;
-          em[s] = ee;
+          Y = J.yd[m & 1];
+          D = (Y * (double)(-m)) * z;
+          S.Em[idx] = J.emr[m & 1];
         }
       } else if (n == m + 1) {
         double c = __ldg(&T.r1[n * L + m]);
@@ -225,12 +243,15 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
         D = (m == 0) ? (z * Dp[s] + Yp[s]) * c : (z * Dp[s] + J.zz1 * Yp[s]) * c;
       } else {
         double c1 = __ldg(&T.r1[n * L + m]), c2 = __ldg(&T.r2[n * L + m]);
-        Y = (c1 * z) * Yp[s] - c2 * Ypp[s];
-        D = (m == 0) ? c1 * (z * Dp[s] + Yp[s]) - c2 * Dpp[s]
-                     : c1 * (z * Dp[s] + J.zz1 * Yp[s]) - c2 * Dpp[s];
+        zdc ypp = S.Ypp[idx], dpp = S.Dpp[idx];
+        Y = (c1 * z) * Yp[s] - c2 * ypp;
+        D = (m == 0) ? c1 * (z * Dp[s] + Yp[s]) - c2 * dpp
+                     : c1 * (z * Dp[s] + J.zz1 * Yp[s]) - c2 * dpp;
       }
-      Ypp[s] = Yp[s];
-      Dpp[s] = Dp[s];
+      if (n > m) {
+        S.Ypp[idx] = Yp[s];
+        S.Dpp[idx] = Dp[s];
+      }
       Yp[s] = Y;
       Dp[s] = D;
       double sqn = __ldg(&T.sq[n]);
@@ -243,49 +264,83 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
         double sg = (m & 1) ? -1.0 : 1.0;
         zdc P = sg * (J.z1 * y - J.z2 * d);
         zdc Q = (sg * m) * (y * J.z3);
-        zdc Cp = (P + Q) * em[s], Cm = (P - Q) * zinv(em[s]);
+        zdc e = S.Em[idx];
+        zdc Cp = (P + Q) * e, Cm = (P - Q) * zinv(e);
         S.Cs[m * L + jc] = Cp + Cm;
         S.Cd[m * L + jc] = Cp - Cm;
       }
     }
+    // Ydiag and eip^m of the states that start at degree n+1 (the sequential
+    // products of myzylgndr2sf), one thread per angle
+    if (tid < L && n >= 1 && n + 1 <= p) {
+      JCc& J = S.jc[tid];
+      J.yd[(n + 1) & 1] = (J.yd[n & 1] * J.u) * __ldg(&T.r1[(n + 1) * L + n + 1]);
+      J.emr[(n + 1) & 1] = J.emr[n & 1] * J.eip;
+    }
   };
-  // inputs of degree n: As = a(n,m) + a(n,-m), Ad = a(n,m) - a(n,-m)
-  auto load = [&](int n) {
-    for (int m = w; m <= n; m += XW) {
-      zdc a = mkz(0.0), b = mkz(0.0);
-      if (MODE == 0) {
-        if (lane < nval) {
-          a = gin[(long)ix3(n, m) * ldin + lane];
-          if (m > 0) b = gin[(long)ix3(n, -m) * ldin + lane];
-          if (zr) {
-            a = a * S.Ef[p + m];
-            b = b * S.Ef[p - m];
-          }
-        }
-      } else {
-        a = gin[ix3(n, m) * RC + lane];
-        if (m > 0) b = gin[ix3(n, -m) * RC + lane];
+  // inputs of degree n: As = a(n,m) + a(n,-m), Ad = a(n,m) - a(n,-m).  The
+  // first LR rows of each warp are fetched into registers before the
+  // coefficient generation (hiding the global-memory latency behind it) and
+  // committed to shared memory after it; rows beyond (orders p >= LR*XW) load
+  // synchronously.
+  zdc fa[LR], fb[LR];
+  auto fetch_row = [&](int n, int m, zdc& a, zdc& b) {
+    a = mkz(0.0);
+    b = mkz(0.0);
+    if (MODE == 0) {
+      if (lane < nval) {
+        a = ldcg_z(gin + (long)ix3(n, m) * ldin + lane);
+        if (m > 0) b = ldcg_z(gin + (long)ix3(n, -m) * ldin + lane);
       }
-      if (m == 0) {
-        S.As[lane] = a;
-        S.Ad[lane] = mkz(0.0);
-      } else {
-        S.As[m * RC + lane] = a + b;
-        S.Ad[m * RC + lane] = a - b;
-      }
+    } else {
+      a = ldcg_z(gin + ix3(n, m) * RC + lane);
+      if (m > 0) b = ldcg_z(gin + ix3(n, -m) * RC + lane);
+    }
+  };
+  auto put_row = [&](int m, zdc a, zdc b) {
+    if (MODE == 0 && zr) {
+      a = a * S.Ef[p + m];
+      b = b * S.Ef[p - m];
+    }
+    if (m == 0) {
+      S.As[lane] = a;
+      S.Ad[lane] = mkz(0.0);
+    } else {
+      S.As[m * RC + lane] = a + b;
+      S.Ad[m * RC + lane] = a - b;
+    }
+  };
+  auto fetch = [&](int n) {
+#pragma unroll
+    for (int i = 0; i < LR; i++) {
+      int m = w + i * XW;
+      if (m <= n) fetch_row(n, m, fa[i], fb[i]);
+    }
+  };
+  auto commit = [&](int n) {
+#pragma unroll
+    for (int i = 0; i < LR; i++) {
+      int m = w + i * XW;
+      if (m <= n) put_row(m, fa[i], fb[i]);
+    }
+    for (int m = w + LR * XW; m <= n; m += XW) {
+      zdc a, b;
+      fetch_row(n, m, a, b);
+      put_row(m, a, b);
     }
   };
   auto store = [&](int n, int m, zdc v) {
     if (MODE == 0) {
-      gout[ix3(n, m) * RC + lane] = prescale<KIND>(T, S, n, m, v);
+      stcg_z(gout + ix3(n, m) * RC + lane, prescale<KIND>(T, S, n, m, v));
     } else if (lane < nval) {
       zdc* o = gout + (long)ix3(n, m) * ldout + lane;
-      *o += zr ? v * S.Eb[p + m] : v;
+      stcg_z(o, ldcg_z(o) + (zr ? v * S.Eb[p + m] : v));
     }
   };
 
+  fetch(0);
   gen(0);
-  load(0);
+  commit(0);
   __syncthreads();
   const int ngrp = (L + JT - 1) / JT;
   for (int n = 0; n <= p; n++) {
@@ -328,8 +383,8 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
 #pragma unroll
         for (int k = 0; k < MT; k++)
           if (m0 + k <= n) {
-            X[k] += sv * __ldg(&cr[k]);
-            Yv[k] += dv * __ldg(&sr[k]);
+            X[k] += sv * cr[k];
+            Yv[k] += dv * sr[k];
           }
       }
 #pragma unroll
@@ -343,8 +398,9 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
       }
     }
     if (n < p) {
+      fetch(n + 1);
       gen(n + 1);
-      load(n + 1);
+      commit(n + 1);
     }
     __syncthreads();
   }
@@ -361,13 +417,14 @@ __device__ void copy_nd(const Tab3& T, const XSm& S, bool zr, const zdc* gin, lo
     if (MODE == 0) {
       zdc a = mkz(0.0);
       if (lane < nval) {
-        a = gin[(long)idx * ldin + lane];
+        a = ldcg_z(gin + (long)idx * ldin + lane);
         if (zr) a = a * S.Ef[p + m];
       }
-      gout[idx * RC + lane] = prescale<KIND>(T, S, n, m, a);
+      stcg_z(gout + idx * RC + lane, prescale<KIND>(T, S, n, m, a));
     } else if (lane < nval) {
-      zdc v = gin[idx * RC + lane];
-      gout[(long)idx * ldout + lane] += zr ? v * S.Eb[p + m] : v;
+      zdc v = ldcg_z(gin + idx * RC + lane);
+      zdc* o = gout + (long)idx * ldout + lane;
+      stcg_z(o, ldcg_z(o) + (zr ? v * S.Eb[p + m] : v));
     }
   }
   __syncthreads();
@@ -388,16 +445,18 @@ __device__ void shift_nd(const Tab3& T, const XSm& S, const zdc* X1, zdc* X2) {
 #pragma unroll
       for (int k = 0; k < JB; k++) acc[k] = mkz(0.0);
       if (KIND == 1) {
+#pragma unroll 4
         for (int n = am_; n <= p; n++) {
-          zdc a = X1[ix3(n, mm) * RC + lane];
+          zdc a = ldcg_z(X1 + ix3(n, mm) * RC + lane);
 #pragma unroll
           for (int k = 0; k < JB; k++)
             if (j0 + k <= p) acc[k] += a * S.G[n + j0 + k];
         }
       } else if (KIND == 0) {
         int nhi = min(p, j0 + JB - 1);
+#pragma unroll 4
         for (int n = am_; n <= nhi; n++) {
-          zdc a = X1[ix3(n, mm) * RC + lane];
+          zdc a = ldcg_z(X1 + ix3(n, mm) * RC + lane);
 #pragma unroll
           for (int k = 0; k < JB; k++) {
             int j = j0 + k;
@@ -405,8 +464,9 @@ __device__ void shift_nd(const Tab3& T, const XSm& S, const zdc* X1, zdc* X2) {
           }
         }
       } else {
+#pragma unroll 4
         for (int n = j0; n <= p; n++) {
-          zdc a = X1[ix3(n, mm) * RC + lane];
+          zdc a = ldcg_z(X1 + ix3(n, mm) * RC + lane);
 #pragma unroll
           for (int k = 0; k < JB; k++) {
             int j = j0 + k;
@@ -420,7 +480,7 @@ __device__ void shift_nd(const Tab3& T, const XSm& S, const zdc* X1, zdc* X2) {
         if (j > p) break;
         double ajk = __ldg(&T.amat[j * ldA + mm + nmax]);
         zdc v = (KIND == 0) ? S.T1[j] * acc[k] / ajk : S.T1[j] * acc[k] * ajk;
-        X2[ix3(j, mm) * RC + lane] = v;
+        stcg_z(X2 + ix3(j, mm) * RC + lane, v);
       }
     }
   }
@@ -432,6 +492,14 @@ __global__ void __launch_bounds__(XNT, 1) k_trans3nd(TransNdArgs A) {
   const Tab3& T = A.T;
   const int p = T.p, NC = T.NC, tid = threadIdx.x;
   const XSm S = carve_xsm(sm, p);
+  RotTab Rt = A.R;
+  if (A.rot_smem) {
+    const int L = p + 1;
+    double* tab = reinterpret_cast<double*>(S.Em + L * L);
+    for (int k = tid; k < 2 * L * L; k += XNT) tab[k] = A.R.cw[k];  // cw then sw
+    Rt.cw = tab;
+    Rt.sw = tab + L * L;
+  }
   zdc* X1 = A.scratch + (size_t)blockIdx.x * 2 * NC * RC;
   zdc* X2 = X1 + (size_t)NC * RC;
   const double s4 = sqrt(4 * kPi);
@@ -518,13 +586,13 @@ __global__ void __launch_bounds__(XNT, 1) k_trans3nd(TransNdArgs A) {
         }
         __syncthreads();
         const zdc* gin = A.in + (size_t)src * NC * nd + r0;
-        if (g.yr) rot_nd<SLOTS, 0, KIND>(T, A.R, S, g.ca, g.sa, g.zr, gin, nd, X1, RC, nval);
+        if (g.yr) rot_nd<SLOTS, 0, KIND>(T, Rt, S, g.ca, g.sa, g.zr, gin, nd, X1, RC, nval);
         else copy_nd<0, KIND>(T, S, g.zr, gin, nd, X1, RC, nval);
         __syncthreads();
         shift_nd<KIND>(T, S, X1, X2);
         __syncthreads();
         zdc* gout = A.out + (size_t)b * NC * nd + r0;
-        if (g.yr) rot_nd<SLOTS, 1, KIND>(T, A.R, S, g.ca, -g.sa, g.zr, X2, RC, gout, nd, nval);
+        if (g.yr) rot_nd<SLOTS, 1, KIND>(T, Rt, S, g.ca, -g.sa, g.zr, X2, RC, gout, nd, nval);
         else copy_nd<1, KIND>(T, S, g.zr, X2, RC, gout, nd, nval);
       }
     }
@@ -1076,10 +1144,14 @@ void launch_trans_nd(const TransNdArgs& A, int grid, cudaStream_t s) {
   if (A.hi < A.lo) return;
   int L = A.T.p + 1;
   size_t sm = xsm_bytes(A.T.p);
+  TransNdArgs B = A;
+  size_t tab = 2 * (size_t)L * L * sizeof(double);
+  B.rot_smem = sm + tab <= 227 * 1024;
+  if (B.rot_smem) sm += tab;
   int slots = div_up(L * L, XNT);
-  if (slots <= 3) launch_trans_nd_k<KIND, 3>(A, grid, sm, s);
-  else if (slots <= 4) launch_trans_nd_k<KIND, 4>(A, grid, sm, s);
-  else if (slots <= 6) launch_trans_nd_k<KIND, 6>(A, grid, sm, s);
+  if (slots <= 4) launch_trans_nd_k<KIND, 4>(B, grid, sm, s);
+  else if (slots <= 6) launch_trans_nd_k<KIND, 6>(B, grid, sm, s);
+  else if (slots <= 8) launch_trans_nd_k<KIND, 8>(B, grid, sm, s);
   else throw zf_error(ZF_ERR_ARG, "expansion order too large for the batched translation");
   ZF_LAUNCH_CHECK();
 }

@@ -34,4 +34,11 @@ void plan3d_build(Plan3D& P, double eps, int ns, const zdc* zsrc, int nt, const 
 void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int ifpgh, zdc* pot,
                           zdc* grad, cudaStream_t s, StepTimes* times);
 
+// 3D Helmholtz with wavenumber zk on the plan's points: the orders, tables
+// and shift configurations of zk are built once per call and every
+// right-hand side runs the FMM passes on the plan's tree; same layouts as
+// zlfmm3d_plan_execute, scaling as zhfmm3d
+void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in, int ifpgh,
+                          zdc* pot, zdc* grad, cudaStream_t s, StepTimes* times);
+
 }  // namespace zf
