@@ -70,6 +70,21 @@ WORKLOADS = {
                                   cpu_n=30_000, dipoles=False),
     "zlfmm3d_batched_200k_64": dict(kind="lap3d", n=200_000, nrhs=64, eps=1e-9, ifpgh=2,
                                     isep=1, cpu_n=30_000, dipoles=False),
+    # zhfmm3d batched uneven instances: 200 independent FMMs, point counts
+    # log-uniform in [2,000, 500,000], points on unit spheres displaced by 0.1i
+    # times the normal scaled by a degree-4 field, zk = 10+0.2i, charges +
+    # dipoles, pot + grad, eps=1e-9; one step = all 200 solves in one call
+    # zhfmm2d adjoint: forward + reverse pass on 200,000 points of a two-curve
+    # interface (the curve above plus a copy scaled 0.6 and shifted by
+    # (0.2, 0.1)), imaginary displacement amplitude 0.05 per curve as a learnable
+    # parameter, zk = 20+0.3i, charges + dipoles, loss = mean |pot - ref|^2,
+    # eps=1e-10; one step = forward (pot and grad) + backward (gradients for
+    # charges, dipole strengths and both amplitudes)
+    "zhfmm2d_adjoint_200k": dict(kind="helm2d", adjoint=True, n=200_000, eps=1e-10,
+                                 zk=20 + 0.3j, ifpgh=2, isep=1, cpu_n=100_000),
+    "zhfmm3d_instances_200": dict(kind="helm3d", instances=200, nmin=2000, nmax=500_000,
+                                  n=500_000, eps=1e-9, zk=10 + 0.2j, ifpgh=2, isep=1,
+                                  cpu_n=30_000, nstreams=8),
 }
 DEFAULT_WORKLOAD = "zhfmm2d_curve_2m"
 
@@ -693,6 +708,333 @@ def run_ours_batched(args, wl, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_ours_many(args, wl, ws, rank, local):
+    """One step = all instances through the many-instance device entry point."""
+    import ctypes
+
+    import torch
+
+    import zfmm_b200
+    from zfmm_b200 import _capi
+    from zfmm_b200 import workloads as W
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _capi.lib()
+    rng = np.random.default_rng(2024 + rank)
+    ni = wl["instances"]
+    sizes = np.exp(rng.uniform(np.log(wl["nmin"]), np.log(wl["nmax"]), ni)).astype(np.int64)
+    eps, zk, ifpgh, isep = wl["eps"], wl["zk"], wl["ifpgh"], wl["isep"]
+    inst = [W.sphere3d(int(n), seed=1000 * rank + i) for i, n in enumerate(sizes)]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    dz = [t(w["zsrc"].T) for w in inst]
+    dq = [t(w["charge"]) for w in inst]
+    dd = [t(w["dipstr"]) for w in inst]
+    dv = [t(w["dipvec"].T) for w in inst]
+    dp = [torch.empty(int(n), dtype=torch.complex128, device=dev) for n in sizes]
+    dg = [torch.empty((int(n), 3), dtype=torch.complex128, device=dev) for n in sizes]
+    arr = lambda xs: (ctypes.c_void_p * ni)(*[x.data_ptr() for x in xs])
+    A = dict(zs=arr(dz), q=arr(dq), d=arr(dd), v=arr(dv), p=arr(dp), g=arr(dg))
+    ns = np.ascontiguousarray(sizes.astype(np.int32))
+    k = np.array([zk.real, zk.imag])
+    done = np.zeros(ni)
+    hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def solve(nstreams):
+        _capi.check(L.zfmm_zhfmm3d_many_dev(ni, eps, hp(k), hp(ns), A["zs"], 1, A["q"], 1, A["d"],
+                                            A["v"], hp(ns), A["zs"], ifpgh, isep, A["p"],
+                                            A["g"], nstreams, hp(done)))
+
+    nst = wl["nstreams"]
+    for _ in range(max(1, min(args.warmup, 1))):
+        solve(nst)
+    torch.cuda.synchronize()
+    launches0 = L.zfmm_launch_count()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    lat = []
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        for s_ in range(args.steps):
+            flush.fill_(s_ & 255)
+            torch.cuda.synchronize()
+            ev0[s_].record(stream)
+            solve(nst)
+            ev1[s_].record(stream)
+            torch.cuda.synchronize()
+            lat.append(done.copy())
+    tot_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    if ws > 1:
+        tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    npts = int(sizes.sum())
+    value = ws * npts * args.steps / (tot_ms * 1e-3)
+    lat_all = np.concatenate(lat)
+    # the same instances one after another on one stream (the plain calls)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solve(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    # end to end: host arrays through the host entry point
+    hz = [np.ascontiguousarray(w["zsrc"].T) for w in inst]
+    hq = [np.ascontiguousarray(w["charge"]) for w in inst]
+    hd = [np.ascontiguousarray(w["dipstr"]) for w in inst]
+    hv = [np.ascontiguousarray(w["dipvec"].T) for w in inst]
+    hpo = [np.zeros(int(n), np.complex128) for n in sizes]
+    hgr = [np.zeros((int(n), 3), np.complex128) for n in sizes]
+    harr = lambda xs: (ctypes.c_void_p * ni)(*[x.ctypes.data for x in xs])
+    H = dict(zs=harr(hz), q=harr(hq), d=harr(hd), v=harr(hv), p=harr(hpo), g=harr(hgr))
+    t0 = time.perf_counter()
+    _capi.check(L.zfmm_zhfmm3d_many(ni, eps, hp(k), hp(ns), H["zs"], 1, H["q"], 1, H["d"],
+                                    H["v"], hp(ns), H["zs"], ifpgh, isep, H["p"], H["g"], nst,
+                                    hp(done)))
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(a.nbytes for a in hz) * 2 + sum(a.nbytes for a in hq + hd + hv)
+    d2h = sum(a.nbytes for a in hpo + hgr)
+    # accuracy: the largest instance against the FP64 direct sum on 1024 targets
+    big = int(np.argmax(sizes))
+    w = inst[big]
+    n = int(sizes[big])
+    sub = np.sort(np.random.default_rng(1234).choice(n, size=min(n, 1024), replace=False))
+    pd, _ = zfmm_b200.zh3devaldirect(zk, len(sub), w["zsrc"][:, sub], n, w["zsrc"], w["charge"],
+                                     w["dipstr"], w["dipvec"], 1, 1, 1)
+    pg = dp[big].cpu().numpy()
+    relerr = float(np.linalg.norm(pg[sub] - pd) / np.linalg.norm(pd))
+    # roofline: the largest instance's M2L as a single instrumented call
+    L.zfmm_set_step_timing(2)
+    pb, gb = torch.empty_like(dp[big]), torch.empty_like(dg[big])
+    P_ = lambda x: ctypes.c_void_p(x.data_ptr())
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    _capi.check(L.zfmm_zhfmm3d_dev(eps, hp(k), n, P_(dz[big]), 1, P_(dq[big]), 1, P_(dd[big]),
+                                   P_(dv[big]), P_(pb), P_(gb), n, P_(dz[big]), ifpgh, isep, sp))
+    st, info = zfmm_b200.last_step_times()
+    lvl, orders = zfmm_b200.last_level_counts()
+    L.zfmm_set_step_timing(0)
+    launches = L.zfmm_launch_count() - launches0
+    flops, _per = flop_model3d("helm3d", lvl, orders)
+    achieved = flops["m2l_p2l"] / (st["m2l_p2l"] * 1e-3) / 1e12
+    peak = float(L.zfmm_probe_fp64_tflops(20000))
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        cinp = make_inputs(wl, seed=0, n=wl["cpu_n"])
+        t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
+        cpu = {"value": wl["cpu_n"] / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
+               "sample": (f"one {wl['cpu_n']}-point instance of the workload's distribution "
+                          f"(the reference runs the {ni} instances as sequential calls), "
+                          f"median of {nrep}")}
+    if rank != 0:
+        return
+    line = {
+        "metric": "targets/sec at eps=1e-9", "value": value, "unit": "targets/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, "instances": ni, "points_total": npts,
+                   "n_min": int(sizes.min()), "n_max": int(sizes.max()), "eps": eps,
+                   "zk": str(zk), "ifpgh": ifpgh, "isep": isep, "charges": True,
+                   "dipoles": True, "nstreams": nst,
+                   "timing": ("CUDA events on the current stream bracketing the call, which "
+                              "returns after every worker stream has finished"),
+                   "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": f"replicas x{ws}"},
+        "latency_ms": {"p50": float(np.percentile(lat_all, 50)),
+                       "p99": float(np.percentile(lat_all, 99)),
+                       "max": float(lat_all.max())},
+        "sequential_one_stream_ms": seq_ms,
+        "e2e": {"value": ws * npts / e2e_s, "unit": "targets/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "rel_l2_err_vs_direct": relerr,
+        "roofline": {"bound": "fp64", "kernel": "m2l_p2l of the largest instance",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None,
+                     "peak_source": "measured FP64 FMA probe (zfmm_probe_fp64_tflops)",
+                     "traffic": None, "flops_per_step": flops["m2l_p2l"]},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def two_curves(n, seed):
+    """The two-curve interface of the adjoint workload: real base points,
+    displacement directions (cos 3t, sin 3t), curve index, complex normal
+    charges, dipole strengths, dipole vectors and target field."""
+    rng = np.random.default_rng(seed)
+    m = n // 2
+    xr, disp, curve = [], [], []
+    for c, (sc, sh) in enumerate([(1.0, (0.0, 0.0)), (0.6, (0.2, 0.1))]):
+        t = rng.uniform(0, 2 * np.pi, m)
+        r = 1.0 + 0.3 * np.cos(5 * t)
+        xr.append(np.stack([sc * r * np.cos(t) + sh[0], sc * r * np.sin(t) + sh[1]], 1))
+        disp.append(np.stack([np.cos(3 * t), np.sin(3 * t)], 1))
+        curve.append(np.full(m, c))
+    cn = lambda *s: rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    return (np.concatenate(xr), np.concatenate(disp), np.concatenate(curve), cn(2 * m),
+            cn(2 * m), cn(2 * m, 2), cn(2 * m))
+
+
+def run_ours_adjoint(args, wl, ws, rank, local):
+    """One step = forward + backward of the differentiable two-curve zhfmm2d."""
+    import torch
+
+    import zfmm_b200
+    from zfmm_b200 import _capi
+    from zfmm_b200.adjoint import zhfmm2d_curves, points
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _capi.lib()
+    n, eps, zk = wl["n"], wl["eps"], wl["zk"]
+    xr, disp, curve, q, ds, dv, ref = two_curves(n, 7 + rank)
+    T = lambda x: torch.tensor(x, device=dev)
+    D = dict(xr=T(xr), disp=T(disp), curve=T(curve), q=T(q), ds=T(ds), dv=T(dv), ref=T(ref))
+    a0 = [0.05, 0.05]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def fwd_bwd(Dx, grads=True):
+        qq = Dx["q"].clone().requires_grad_(grads)
+        dd = Dx["ds"].clone().requires_grad_(grads)
+        a = torch.tensor(a0, device=dev, dtype=torch.float64, requires_grad=grads)
+        pot = zhfmm2d_curves(eps, zk, Dx["xr"], Dx["disp"], Dx["curve"], a, qq, dd, Dx["dv"])
+        Lv = torch.mean(torch.abs(pot - Dx["ref"]) ** 2)
+        if grads:
+            Lv.backward()
+            return Lv, qq.grad, dd.grad, a.grad
+        return Lv
+
+    for _ in range(max(args.warmup, 3)):
+        fwd_bwd(D)
+    torch.cuda.synchronize()
+    launches0 = L.zfmm_launch_count()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            ev0[k].record(stream)
+            out = fwd_bwd(D)
+            ev1[k].record(stream)
+        torch.cuda.synchronize()
+    launches = L.zfmm_launch_count() - launches0
+    tot_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    if ws > 1:
+        tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    value = ws * n * args.steps / (tot_ms * 1e-3)
+    # the plain forward solve (pot only) and the forward with gradients, same points
+    z = points(D["xr"], D["disp"], D["curve"], torch.tensor(a0, device=dev, dtype=torch.float64))
+    def timed(f, reps=3):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    plain_ms = timed(lambda: zfmm_b200._fmm2d_torch(eps, zk, n, z, 1, D["q"], 1, D["ds"], D["dv"],
+                                                     n, z, 1, 1))
+    fwd_ms = timed(lambda: fwd_bwd(D, grads=False))
+    step_ms = tot_ms / args.steps
+    # gradient checks at full size: central differences (h = 1e-6) of the FMM
+    # loss for both amplitudes and one charge
+    Lv, gq, gds, ga = out
+    h = 1e-6
+    fd_a = []
+    for c in range(2):
+        ap, am = list(a0), list(a0)
+        ap[c] += h
+        am[c] -= h
+        Lp = zhfmm2d_curves(eps, zk, D["xr"], D["disp"], D["curve"],
+                            torch.tensor(ap, device=dev, dtype=torch.float64), D["q"], D["ds"],
+                            D["dv"])
+        Lm = zhfmm2d_curves(eps, zk, D["xr"], D["disp"], D["curve"],
+                            torch.tensor(am, device=dev, dtype=torch.float64), D["q"], D["ds"],
+                            D["dv"])
+        fdv = (float(torch.mean(torch.abs(Lp - D["ref"]) ** 2))
+               - float(torch.mean(torch.abs(Lm - D["ref"]) ** 2))) / (2 * h)
+        fd_a.append(fdv)
+    ga = ga.cpu().numpy()
+    fd_rel = [abs(fd_a[c] - ga[c]) / abs(ga[c]) for c in range(2)]
+    # end to end: inputs from pinned host memory, gradients back to the host
+    hin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+           for k, v in dict(xr=xr, disp=disp, curve=curve, q=q, ds=ds, dv=dv, ref=ref).items()}
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        Dh = {kk: vv.to(dev, non_blocking=True) for kk, vv in hin.items()}
+        _, g1, g2, g3 = fwd_bwd(Dh)
+        g1.cpu(), g2.cpu(), g3.cpu()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(v.numel() * v.element_size() for v in hin.values())
+    d2h = 2 * n * 16 + 2 * 8
+    # roofline of the forward's dominant step (an instrumented forward solve)
+    L.zfmm_set_step_timing(2)
+    zfmm_b200._fmm2d_torch(eps, zk, n, z, 1, D["q"], 1, D["ds"], D["dv"], n, z, 2, 1)
+    torch.cuda.synchronize()
+    counts, _ = zfmm_b200.last_counts()
+    st, info = zfmm_b200.last_step_times()
+    L.zfmm_set_step_timing(0)
+    flops, _per = flop_model("helm2d", counts)
+    top = max(flops, key=lambda k: st[k])
+    achieved = flops[top] / (st[top] * 1e-3) / 1e12
+    peak = float(L.zfmm_probe_fp64_tflops(20000))
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        ncpu = wl["cpu_n"]
+        zc = points(*(torch.tensor(x) for x in (xr[:ncpu], disp[:ncpu], curve[:ncpu])),
+                    torch.tensor(a0, dtype=torch.float64)).numpy()
+        cinp = dict(zsrc=zc.T, charge=q[:ncpu], dipstr=ds[:ncpu], dipvec=dv[:ncpu].T)
+        t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
+        cpu = {"value": ncpu / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
+               "sample": (f"one forward solve (pot and grad) on the first {ncpu} points of the "
+                          f"workload (full: {n}); the reference has no adjoint"),
+               "median_of": nrep}
+    if rank != 0:
+        return
+    line = {
+        "metric": "targets/sec at eps=1e-10 (forward + adjoint)", "value": value,
+        "unit": "targets/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "eps": eps, "zk": str(zk), "ifpgh": 2,
+                   "isep": 1, "charges": True, "dipoles": True,
+                   "step": "forward (pot, grad) + backward (charge, dipstr, 2 amplitudes)",
+                   "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": f"replicas x{ws}"},
+        "forward_plain_ms": plain_ms, "forward_with_grad_ms": fwd_ms,
+        "backward_ms": step_ms - fwd_ms,
+        "backward_over_plain_forward": (step_ms - fwd_ms) / plain_ms,
+        "grad_check_fd_h1e-6_rel": fd_rel,
+        "e2e": {"value": ws * n * args.steps / e2e_s, "unit": "targets/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "fp64", "kernel": f"forward {top}", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None,
+                     "peak_source": "measured FP64 FMA probe (zfmm_probe_fp64_tflops)",
+                     "traffic": None, "flops_per_step": flops[top]},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -707,6 +1049,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, wl, ws, rank)
+        elif wl.get("adjoint"):
+            run_ours_adjoint(args, wl, ws, rank, local)
+        elif wl.get("instances"):
+            run_ours_many(args, wl, ws, rank, local)
         elif wl.get("nrhs", 1) > 1:
             run_ours_batched(args, wl, ws, rank, local)
         else:

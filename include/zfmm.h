@@ -207,6 +207,40 @@ int zfmm_zhfmm3d_plan_dev(zfmm_plan3d plan, const double *zk, int nd, int ifchar
                           const double *dipvec, int ifpgh, double *pot, double *grad,
                           void *stream);
 
+/* Many independent 3D FMMs in one call (no counterpart in the reference,
+ * where each instance is a separate zlfmm3d / zhfmm3d call): instance i has
+ * ns[i] sources zsrc[i](3, ns[i]), strengths charge[i], dipstr[i],
+ * dipvec[i](3, ns[i]), nt[i] targets ztarg[i](3, nt[i]) and outputs pot[i],
+ * grad[i](3, nt[i]), each exactly as the single call with the shared eps, zk,
+ * flags and isep.  Instances are taken largest first from a shared queue by
+ * `nstreams` host workers, each driving its own CUDA stream, so that small
+ * instances overlap on the GPU.  done_ms (optional, ninst entries) receives
+ * each instance's completion time in ms after the call started (its latency
+ * when all are submitted together).  Host arrays, or device pointers for
+ * _dev (the pointer arrays themselves are host memory). */
+int zfmm_zlfmm3d_many(int ninst, double eps, const int *ns, const double *const *zsrc,
+                      int ifcharge, const double *const *charge, int ifdipole,
+                      const double *const *dipstr, const double *const *dipvec, const int *nt,
+                      const double *const *ztarg, int ifpgh, int isep, double *const *pot,
+                      double *const *grad, int nstreams, double *done_ms);
+int zfmm_zhfmm3d_many(int ninst, double eps, const double *zk, const int *ns,
+                      const double *const *zsrc, int ifcharge, const double *const *charge,
+                      int ifdipole, const double *const *dipstr, const double *const *dipvec,
+                      const int *nt, const double *const *ztarg, int ifpgh, int isep,
+                      double *const *pot, double *const *grad, int nstreams, double *done_ms);
+int zfmm_zlfmm3d_many_dev(int ninst, double eps, const int *ns, const double *const *zsrc,
+                          int ifcharge, const double *const *charge, int ifdipole,
+                          const double *const *dipstr, const double *const *dipvec,
+                          const int *nt, const double *const *ztarg, int ifpgh, int isep,
+                          double *const *pot, double *const *grad, int nstreams,
+                          double *done_ms);
+int zfmm_zhfmm3d_many_dev(int ninst, double eps, const double *zk, const int *ns,
+                          const double *const *zsrc, int ifcharge, const double *const *charge,
+                          int ifdipole, const double *const *dipstr,
+                          const double *const *dipvec, const int *nt,
+                          const double *const *ztarg, int ifpgh, int isep, double *const *pot,
+                          double *const *grad, int nstreams, double *done_ms);
+
 /* Allocation-free form of zfmm_zl2devaldirect_dev; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory during a
  * solve: code whose device memory is owned by another allocator (a
@@ -249,7 +283,8 @@ int zfmm_h2dterms(double bsize, const double *zk, double eps, int isep);
  * P2P/M2T/L2T/M2L/P2L, parent level for M2M, child level for L2L), and the
  * expansion order of each level, orders64[level]. */
 int zfmm_last_level_counts(long long *counts8x64, int *orders64, int *nlevels);
-/* Kernels launched by this library on the calling host thread so far. */
+/* Kernels launched by this library so far, by all host threads of the
+ * process (the many-instance entry points launch from worker threads). */
 long zfmm_launch_count(void);
 /* Device scratch comes from a library-owned memory pool per device that keeps
  * freed memory mapped between calls; this returns the cached memory of the

@@ -80,3 +80,17 @@ def test_h2dterms_matches_reference_log():
     got = [L.zfmm_h2dterms(bs0 / 2 ** l, zk.ctypes.data, float(np.float32(1e-12)), 1)
            for l in range(11)]
     assert got == g["nterms"]
+
+
+def test_no_gpu_plans_and_batches_are_errors():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    import zfmm_b200
+    z = np.zeros((3, 5), np.complex128)
+    z[0] = np.arange(5)
+    with pytest.raises(zfmm_b200.ZfmmError, match="status 5"):
+        zfmm_b200.Plan3D(1e-6, 5, z, 5, z)
+    inst = [dict(zsrc=z, charge=np.ones(5))]
+    with pytest.raises(zfmm_b200.ZfmmError, match="status 5"):
+        zfmm_b200.zhfmm3d_many(1e-6, 1.0, inst, nstreams=2)

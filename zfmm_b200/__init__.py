@@ -21,7 +21,8 @@ from ._capi import ZfmmError, check, lib
 
 __all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "zlfmm3d", "zl3devaldirect",
            "zhfmm3d", "zh3devaldirect", "zl3dterms", "h3dterms", "tree_dump", "ZfmmError",
-           "set_step_timing", "last_step_times", "last_counts", "version", "Plan3D"]
+           "set_step_timing", "last_step_times", "last_counts", "version", "Plan3D",
+           "zlfmm3d_many", "zhfmm3d_many"]
 
 
 def _ptr(a):
@@ -377,6 +378,62 @@ class Plan3D:
             self.close()
         except Exception:
             pass
+
+
+def _many(eps, zk, instances, ifcharge, ifdipole, ifpgh, isep, nstreams):
+    n = len(instances)
+    keep = []
+    ns = np.zeros(n, np.int32)
+    nt = np.zeros(n, np.int32)
+    P = lambda: (ctypes.c_void_p * n)()
+    zs, zt, q, ds, dv, pot, grad = P(), P(), P(), P(), P(), P(), P()
+    outs = []
+    for i, inst in enumerate(instances):
+        a = _pts(inst["zsrc"], 3, np.asarray(inst["zsrc"]).shape[-1], "zsrc")
+        ns[i] = a.shape[1]
+        t = _pts(inst["ztarg"], 3, np.asarray(inst["ztarg"]).shape[-1], "ztarg") \
+            if inst.get("ztarg") is not None else a
+        nt[i] = t.shape[1]
+        zs[i], zt[i] = _ptr(a), _ptr(t)
+        keep += [a, t]
+        if ifcharge == 1:
+            c = _vec(inst["charge"], ns[i], "charge")
+            q[i] = _ptr(c)
+            keep.append(c)
+        if ifdipole == 1:
+            d = _vec(inst["dipstr"], ns[i], "dipstr")
+            v = _pts(inst["dipvec"], 3, ns[i], "dipvec")
+            ds[i], dv[i] = _ptr(d), _ptr(v)
+            keep += [d, v]
+        po = np.zeros(nt[i], np.complex128)
+        gr = np.zeros((3, nt[i]), np.complex128, order="F")
+        pot[i], grad[i] = _ptr(po), _ptr(gr)
+        outs.append((po, gr))
+    done = np.zeros(n, np.float64)
+    if zk is None:
+        check(lib().zfmm_zlfmm3d_many(n, float(eps), _ptr(ns), zs, int(ifcharge), q,
+                                      int(ifdipole), ds, dv, _ptr(nt), zt, int(ifpgh), int(isep),
+                                      pot, grad, int(nstreams), _ptr(done)))
+    else:
+        k = _zk(zk)
+        check(lib().zfmm_zhfmm3d_many(n, float(eps), _ptr(k), _ptr(ns), zs, int(ifcharge), q,
+                                      int(ifdipole), ds, dv, _ptr(nt), zt, int(ifpgh), int(isep),
+                                      pot, grad, int(nstreams), _ptr(done)))
+    return outs, done
+
+
+def zlfmm3d_many(eps, instances, ifcharge=1, ifdipole=0, ifpgh=1, isep=1, nstreams=8):
+    """Many independent zlfmm3d solves in one call.  instances: list of dicts
+    with zsrc (3, ns), charge, dipstr, dipvec (3, ns) and optional ztarg
+    (default: the sources).  Returns ([(pot, grad), ...], done_ms): each
+    instance's outputs as zlfmm3d's and its completion time (ms after the call
+    started)."""
+    return _many(eps, None, instances, ifcharge, ifdipole, ifpgh, isep, nstreams)
+
+
+def zhfmm3d_many(eps, zk, instances, ifcharge=1, ifdipole=0, ifpgh=1, isep=1, nstreams=8):
+    """Many independent zhfmm3d solves (shared zk) in one call; as zlfmm3d_many."""
+    return _many(eps, zk, instances, ifcharge, ifdipole, ifpgh, isep, nstreams)
 
 
 def h3dterms(size, zk, eps, isep=1):

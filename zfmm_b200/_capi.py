@@ -97,6 +97,18 @@ SIGNATURES = {
                                   c_void_p, c_int, c_void_p, c_void_p]),
     "zfmm_zhfmm3d_plan_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
                                       c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "zfmm_zlfmm3d_many": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                                  c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p,
+                                  c_void_p, c_int, c_void_p]),
+    "zfmm_zhfmm3d_many": (c_int, [c_int, c_double, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                                  c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                  c_void_p, c_void_p, c_int, c_void_p]),
+    "zfmm_zlfmm3d_many_dev": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_void_p,
+                                      c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                      c_void_p, c_void_p, c_int, c_void_p]),
+    "zfmm_zhfmm3d_many_dev": (c_int, [c_int, c_double, c_void_p, c_void_p, c_void_p, c_int,
+                                      c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      c_int, c_int, c_void_p, c_void_p, c_int, c_void_p]),
     "zfmm_probe_fp64_tflops": (c_double, [c_int]),
     "zfmm_probe_dmma_tflops": (c_double, [c_int]),
     "zfmm_last_error": (ctypes.c_char_p, []),

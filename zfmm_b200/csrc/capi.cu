@@ -4,7 +4,11 @@
 // per-thread default stream, run the device path and copy pot/grad back, so
 // they are synchronous and reentrant across host threads.  Exceptions never
 // cross the ABI: they become status codes plus a thread-local message.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -22,6 +26,11 @@ long& launch_counter() {
   static thread_local long n = 0;
   return n;
 }
+
+namespace {
+std::atomic<long> g_launch_total{0};
+}
+void count_launch_global() { g_launch_total.fetch_add(1, std::memory_order_relaxed); }
 
 namespace {
 constexpr int kMaxDev = 64;
@@ -202,7 +211,7 @@ int zfmm_last_counts(long long* counts16, long* launches) {
   return 0;
 }
 
-long zfmm_launch_count(void) { return launch_counter(); }
+long zfmm_launch_count(void) { return g_launch_total.load(); }
 
 int zfmm_last_level_counts(long long* counts8x64, int* orders64, int* nlevels) {
   for (int k = 0; k < 8; k++)
@@ -984,6 +993,186 @@ int zfmm_zhfmm3d_plan_dev(zfmm_plan3d plan, const double* zk, int nd, int ifchar
   if (!zk) return fail(ZF_ERR_ARG, "zk is null");
   return plan_solve_dev(plan, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot,
                         grad, stream);
+}
+
+}  // extern "C"
+
+// ---- many independent 3D FMMs in one call -------------------------------------
+namespace {
+
+struct ManyArgs {
+  int ninst = 0;
+  double eps = 0;
+  const zdc* zk = nullptr;
+  const int *ns = nullptr, *nt = nullptr;
+  const double* const* zsrc = nullptr;
+  const double* const* charge = nullptr;
+  const double* const* dipstr = nullptr;
+  const double* const* dipvec = nullptr;
+  const double* const* ztarg = nullptr;
+  double* const* pot = nullptr;
+  double* const* grad = nullptr;
+  int ifcharge = 1, ifdipole = 0, ifpgh = 1, isep = 1;
+  bool host = true;
+};
+
+// Instances are taken largest first from a shared counter by `nworkers` host
+// threads, each driving its own CUDA stream, so small instances overlap on the
+// GPU.  done_ms[i]: completion time of instance i after the call started.
+void run_many(const ManyArgs& M, int nworkers, double* done_ms) {
+  int dev = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  std::vector<int> order(M.ninst);
+  for (int i = 0; i < M.ninst; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (long)M.ns[a] + M.nt[a] > (long)M.ns[b] + M.nt[b];
+  });
+  std::atomic<int> next{0};
+  std::mutex err_mu;
+  std::string err;
+  int err_code = 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  auto worker = [&]() {
+    cudaStream_t s = nullptr;
+    try {
+      ZF_CUDA(cudaSetDevice(dev));
+      ZF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      for (;;) {
+        {
+          std::lock_guard<std::mutex> lk(err_mu);
+          if (err_code) break;
+        }
+        int k = next.fetch_add(1);
+        if (k >= M.ninst) break;
+        const int i = order[k];
+        const int ns = M.ns[i], nt = M.nt[i];
+        if (M.host) {
+          HostIn h;
+          upload(h.zsrc, M.zsrc[i], 3 * (size_t)ns, s);
+          upload(h.ztarg, M.ztarg[i], 3 * (size_t)nt, s);
+          if (M.ifcharge == 1) upload(h.charge, M.charge[i], ns, s);
+          if (M.ifdipole == 1) {
+            upload(h.dipstr, M.dipstr[i], ns, s);
+            upload(h.dipvec, M.dipvec[i], 3 * (size_t)ns, s);
+          }
+          DevBuf<zdc> dpot(nt, s), dgrad(M.ifpgh > 1 ? 3 * (size_t)nt : 0, s);
+          Inputs3D in = make_inputs3(ns, (const double*)h.zsrc.get(), M.ifcharge,
+                                     (const double*)h.charge.get(), M.ifdipole,
+                                     (const double*)h.dipstr.get(), (const double*)h.dipvec.get(),
+                                     nt, (const double*)h.ztarg.get(), M.ifpgh);
+          run_fmm3d(M.eps, M.zk, in, M.isep, dpot.get(), M.ifpgh > 1 ? dgrad.get() : nullptr, s);
+          if (nt > 0) {
+            ZF_CUDA(cudaMemcpyAsync(M.pot[i], dpot.get(), sizeof(zdc) * nt,
+                                    cudaMemcpyDeviceToHost, s));
+            if (M.ifpgh > 1)
+              ZF_CUDA(cudaMemcpyAsync(M.grad[i], dgrad.get(), sizeof(zdc) * 3 * nt,
+                                      cudaMemcpyDeviceToHost, s));
+          }
+          ZF_CUDA(cudaStreamSynchronize(s));
+        } else {
+          Inputs3D in = make_inputs3(ns, M.zsrc[i], M.ifcharge,
+                                     M.ifcharge == 1 ? M.charge[i] : nullptr, M.ifdipole,
+                                     M.ifdipole == 1 ? M.dipstr[i] : nullptr,
+                                     M.ifdipole == 1 ? M.dipvec[i] : nullptr, nt, M.ztarg[i],
+                                     M.ifpgh);
+          run_fmm3d(M.eps, M.zk, in, M.isep, (zdc*)M.pot[i],
+                    M.ifpgh > 1 ? (zdc*)M.grad[i] : nullptr, s);
+          ZF_CUDA(cudaStreamSynchronize(s));
+        }
+        if (done_ms)
+          done_ms[i] = std::chrono::duration<double, std::milli>(
+                           std::chrono::steady_clock::now() - t0).count();
+      }
+    } catch (const zf_error& e) {
+      std::lock_guard<std::mutex> lk(err_mu);
+      if (!err_code) {
+        err_code = e.code;
+        err = e.what();
+      }
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lk(err_mu);
+      if (!err_code) {
+        err_code = ZF_ERR_INTERNAL;
+        err = e.what();
+      }
+    }
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int w = 0; w < nworkers; w++) th.emplace_back(worker);
+  for (auto& t : th) t.join();
+  if (err_code) throw zf_error(err_code, err);
+}
+
+int many_impl(ManyArgs M, int nworkers, double* done_ms) {
+  return guarded([&] {
+    if (M.ninst < 0) throw zf_error(ZF_ERR_ARG, "ninst must be >= 0");
+    if (M.ninst == 0) return;
+    if (!M.ns || !M.nt || !M.zsrc || !M.ztarg || !M.pot)
+      throw zf_error(ZF_ERR_ARG, "null instance array");
+    clamp_flags(M.ifcharge, M.ifdipole, M.ifpgh);
+    if (M.isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
+    for (int i = 0; i < M.ninst; i++)
+      check_args2d(M.ns[i], M.nt[i], M.zsrc[i], M.ztarg[i], M.ifcharge,
+                   M.charge ? M.charge[i] : nullptr, M.ifdipole,
+                   M.dipstr ? M.dipstr[i] : nullptr, M.dipvec ? M.dipvec[i] : nullptr,
+                   M.pot[i], M.grad ? M.grad[i] : nullptr, M.ifpgh);
+    check_device();
+    run_many(M, std::max(1, std::min(nworkers, 64)), done_ms);
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int zfmm_zlfmm3d_many(int ninst, double eps, const int* ns, const double* const* zsrc,
+                      int ifcharge, const double* const* charge, int ifdipole,
+                      const double* const* dipstr, const double* const* dipvec, const int* nt,
+                      const double* const* ztarg, int ifpgh, int isep, double* const* pot,
+                      double* const* grad, int nstreams, double* done_ms) {
+  ManyArgs M{ninst, eps, nullptr, ns, nt, zsrc, charge, dipstr, dipvec, ztarg, pot, grad,
+             ifcharge, ifdipole, ifpgh, isep, true};
+  return many_impl(M, nstreams, done_ms);
+}
+
+int zfmm_zhfmm3d_many(int ninst, double eps, const double* zk, const int* ns,
+                      const double* const* zsrc, int ifcharge, const double* const* charge,
+                      int ifdipole, const double* const* dipstr, const double* const* dipvec,
+                      const int* nt, const double* const* ztarg, int ifpgh, int isep,
+                      double* const* pot, double* const* grad, int nstreams, double* done_ms) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  zdc k = mkz(zk[0], zk[1]);
+  ManyArgs M{ninst, eps, &k, ns, nt, zsrc, charge, dipstr, dipvec, ztarg, pot, grad,
+             ifcharge, ifdipole, ifpgh, isep, true};
+  return many_impl(M, nstreams, done_ms);
+}
+
+int zfmm_zlfmm3d_many_dev(int ninst, double eps, const int* ns, const double* const* zsrc,
+                          int ifcharge, const double* const* charge, int ifdipole,
+                          const double* const* dipstr, const double* const* dipvec,
+                          const int* nt, const double* const* ztarg, int ifpgh, int isep,
+                          double* const* pot, double* const* grad, int nstreams,
+                          double* done_ms) {
+  ManyArgs M{ninst, eps, nullptr, ns, nt, zsrc, charge, dipstr, dipvec, ztarg, pot, grad,
+             ifcharge, ifdipole, ifpgh, isep, false};
+  return many_impl(M, nstreams, done_ms);
+}
+
+int zfmm_zhfmm3d_many_dev(int ninst, double eps, const double* zk, const int* ns,
+                          const double* const* zsrc, int ifcharge, const double* const* charge,
+                          int ifdipole, const double* const* dipstr,
+                          const double* const* dipvec, const int* nt,
+                          const double* const* ztarg, int ifpgh, int isep, double* const* pot,
+                          double* const* grad, int nstreams, double* done_ms) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  zdc k = mkz(zk[0], zk[1]);
+  ManyArgs M{ninst, eps, &k, ns, nt, zsrc, charge, dipstr, dipvec, ztarg, pot, grad,
+             ifcharge, ifdipole, ifpgh, isep, false};
+  return many_impl(M, nstreams, done_ms);
 }
 
 }  // extern "C"

@@ -99,6 +99,8 @@ inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 // Kernel launches of this library go through klaunch, which counts them per
 // host thread (reported as the number of kernels a call launched).
 long& launch_counter();
+// launches of the library by all host threads of the process
+void count_launch_global();
 
 template <typename... KArgs, typename... Args>
 inline void klaunch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
@@ -106,6 +108,7 @@ inline void klaunch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem
   if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
   kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
   launch_counter()++;
+  count_launch_global();
 }
 
 }  // namespace zf
