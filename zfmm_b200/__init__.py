@@ -54,6 +54,7 @@ def _torch_pts(x, d, n, name):
     import torch
     if x.dtype != torch.complex128 or not x.is_cuda:
         raise ValueError(f"{name} must be a complex128 CUDA tensor")
+    x = x.resolve_conj()  # the C entry points read raw memory: no lazy conjugate views
     if tuple(x.shape) == (n, d):
         x = x.contiguous()
     elif tuple(x.shape) == (d, n):
@@ -121,8 +122,8 @@ def _fmm2d_torch(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, 
     zs = _torch_pts(zsrc, 2, ns, "zsrc")
     zt = _torch_pts(ztarg, 2, nt, "ztarg")
     dev = zs.device
-    q = charge.contiguous() if ifcharge == 1 else None
-    ds = dipstr.contiguous() if ifdipole == 1 else None
+    q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
+    ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
     dv = _torch_pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
     pot = torch.empty(nt, dtype=torch.complex128, device=dev)
     grad = torch.empty((nt, 2), dtype=torch.complex128, device=dev)
@@ -177,8 +178,8 @@ def _fmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, zt
         import torch
         zs = _torch_pts(zsrc, 3, ns, "zsrc")
         zt = _torch_pts(ztarg, 3, nt, "ztarg")
-        q = charge.contiguous() if ifcharge == 1 else None
-        ds = dipstr.contiguous() if ifdipole == 1 else None
+        q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
+        ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
         dv = _torch_pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
         pot = torch.empty(nt, dtype=torch.complex128, device=zs.device)
         grad = torch.empty((nt, 3), dtype=torch.complex128, device=zs.device)
@@ -337,8 +338,8 @@ class Plan3D:
         if _is_torch(charge if ifcharge == 1 else dipstr):
             import torch
             dev = self.device
-            q = charge.contiguous() if ifcharge == 1 else None
-            ds = dipstr.contiguous() if ifdipole == 1 else None
+            q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
+            ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
             dv = _torch_pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
             pot = torch.empty((nt, nd), dtype=torch.complex128, device=dev)
             grad = torch.empty((nt, 3, nd), dtype=torch.complex128, device=dev)
