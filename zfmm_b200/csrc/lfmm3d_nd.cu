@@ -55,7 +55,17 @@ constexpr int MT = 6;         // projection: orders per warp task
 constexpr int JB = 8;         // shift: output degrees per warp task
 constexpr int LR = 2;         // input rows per warp prefetched into registers
 
-// cos / sin of 2 pi (jc m mod (2p+1)) / (2p+1), [jc][m] for jc, m <= p
+// padded dimensions of the planar shared-memory operands of the rotation
+// products (rows of 8 / 4 for the m8n8k4 tiles; strides that spread a
+// fragment load over the banks)
+__host__ __device__ inline int rot_cp(int L) { return (L + 7) / 8 * 8; }  // angles / orders, padded
+__host__ __device__ inline int rot_kr(int L) { return (L + 3) / 4 * 4; }  // product depth, padded
+constexpr int RP = RC + 4;                                                // right-hand-side stride
+__host__ __device__ inline int rot_tp(int L) { return rot_cp(L) + 4; }    // table row stride
+
+// DFT halves of the projection, [m][jc] with row stride rot_tp(L), rows and
+// columns padded with zeros to rot_cp(L): CW(m, jc) = cos(2 pi (jc m mod NS) /
+// NS) with CW(m, 0) = 1/2, SW(m, jc) = sin(...) with SW(m, 0) = 0, NS = 2p+1
 struct RotTab {
   const double* cw;
   const double* sw;
@@ -71,21 +81,30 @@ RotTab get_rottab(int p) {
   auto key = std::make_pair(dev, p);
   auto it = g_rot.find(key);
   if (it != g_rot.end()) return it->second;
-  int L = p + 1, NS = 2 * p + 1;
-  std::vector<double> h(2 * (size_t)L * L);
-  for (int jc = 0; jc <= p; jc++)
-    for (int m = 0; m <= p; m++) {
+  const int L = p + 1, NS = 2 * p + 1, CP = rot_cp(L), TP = rot_tp(L);
+  const size_t one = (size_t)CP * TP;
+  std::vector<double> h(2 * one, 0.0);
+  for (int m = 0; m <= p; m++)
+    for (int jc = 0; jc <= p; jc++) {
       int k = (jc * m) % NS;
       double a = 2 * kPi * k / NS;
-      h[(size_t)jc * L + m] = cos(a);
-      h[(size_t)L * L + (size_t)jc * L + m] = sin(a);
+      h[(size_t)m * TP + jc] = jc == 0 ? 0.5 : cos(a);
+      h[one + (size_t)m * TP + jc] = jc == 0 ? 0.0 : sin(a);
     }
   double* d = nullptr;
   ZF_CUDA(cudaMalloc((void**)&d, h.size() * sizeof(double)));
   ZF_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
-  RotTab R{d, d + (size_t)L * L};
+  RotTab R{d, d + one};
   g_rot[key] = R;
   return R;
+}
+
+// one m8n8k4 FP64 tensor-core product, c += a b (fragments of the PTX layout:
+// a = A[lane/4][lane%4], b = B[lane%4][lane/4], c = C[lane/4][2(lane%4)+{0,1}])
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
 }
 
 // per-angle constants of one y-rotation (the set-up of myzylgndr2sf in z3dyrot)
@@ -104,40 +123,56 @@ __device__ __forceinline__ void stcg_z(zdc* p, zdc v) {
   __stcg(reinterpret_cast<double2*>(p), make_double2(v.re, v.im));
 }
 
-constexpr int kJCz = sizeof(JCc) / sizeof(zdc);  // complex slots per angle record
-
 struct XSm {
   JCc* jc;
-  zdc *Cs, *Cd, *As, *Ad, *Ss, *Sd, *Ef, *Eb, *G, *T1, *T2;
+  // planar operands of the rotation products: sample coefficients [m][jc]
+  // (stride CP), inputs [m][r] (stride RP), samples [jc][r] (stride RP)
+  double *Csr, *Csi, *Cdr, *Cdi, *Asr, *Asi, *Adr, *Adi, *Ssr, *Ssi, *Sdr, *Sdi;
+  double *cw, *sw;  // DFT tables staged in shared memory (null: read them from global)
+  zdc *Ef, *Eb, *G, *T1, *T2;
   zdc *Ypp, *Dpp;  // recurrence values of degree n-2 per (angle, order) state
-  zdc* Em;         // eip^m per (angle, order) state
 };
 
-__device__ __forceinline__ XSm carve_xsm(zdc* sm, int p) {
-  const int L = p + 1, NS = 2 * p + 1;
+// layout of the translation kernel's shared memory; returns its size in bytes
+// (with_tab: the DFT tables staged too)
+__host__ __device__ inline size_t xsm_layout(int p, bool with_tab, void* base, XSm* out) {
+  const size_t L = p + 1, NS = 2 * p + 1, CP = rot_cp(p + 1), KR = rot_kr(p + 1),
+               TP = rot_tp(p + 1);
+  char* b = (char*)base;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    void* q = b ? b + off : nullptr;
+    off += (bytes + 15) / 16 * 16;
+    return q;
+  };
   XSm S;
-  S.jc = (JCc*)sm;
-  zdc* q = sm + kJCz * L;
-  S.Cs = q; q += L * L;
-  S.Cd = q; q += L * L;
-  S.As = q; q += L * RC;
-  S.Ad = q; q += L * RC;
-  S.Ss = q; q += L * RC;
-  S.Sd = q; q += L * RC;
-  S.Ef = q; q += NS;
-  S.Eb = q; q += NS;
-  S.G = q; q += NS;
-  S.T1 = q; q += L;
-  S.T2 = q; q += L;
-  S.Ypp = q; q += L * L;
-  S.Dpp = q; q += L * L;
-  S.Em = q;
-  return S;
-}
-
-size_t xsm_bytes(int p) {
-  size_t L = p + 1, NS = 2 * p + 1;
-  return (kJCz * L + 5 * L * L + 4 * L * RC + 3 * NS + 2 * L) * sizeof(zdc);
+  S.jc = (JCc*)take(L * sizeof(JCc));
+  S.Csr = (double*)take(KR * CP * 8);
+  S.Csi = (double*)take(KR * CP * 8);
+  S.Cdr = (double*)take(KR * CP * 8);
+  S.Cdi = (double*)take(KR * CP * 8);
+  S.Asr = (double*)take(KR * RP * 8);
+  S.Asi = (double*)take(KR * RP * 8);
+  S.Adr = (double*)take(KR * RP * 8);
+  S.Adi = (double*)take(KR * RP * 8);
+  S.Ssr = (double*)take(CP * RP * 8);
+  S.Ssi = (double*)take(CP * RP * 8);
+  S.Sdr = (double*)take(CP * RP * 8);
+  S.Sdi = (double*)take(CP * RP * 8);
+  S.Ef = (zdc*)take(NS * 16);
+  S.Eb = (zdc*)take(NS * 16);
+  S.G = (zdc*)take(NS * 16);
+  S.T1 = (zdc*)take(L * 16);
+  S.T2 = (zdc*)take(L * 16);
+  S.Ypp = (zdc*)take(L * L * 16);
+  S.Dpp = (zdc*)take(L * L * 16);
+  S.cw = S.sw = nullptr;
+  if (with_tab) {
+    S.cw = (double*)take(CP * TP * 8);
+    S.sw = (double*)take(CP * TP * 8);
+  }
+  if (out) *out = S;
+  return off;
 }
 
 struct TransNdArgs {
@@ -175,6 +210,8 @@ template <int SLOTS, int MODE, int KIND>
 __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc sa, bool zr,
                        const zdc* gin, long ldin, zdc* gout, long ldout, int nval) {
   const int p = T.p, L = p + 1, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int CP = rot_cp(L), TP = rot_tp(L);
+  const int g8 = lane >> 2, t4 = lane & 3;  // fragment row / column of the m8n8k4 layout
   const double s4i = 1.0 / sqrt(4 * kPi);
   __syncthreads();
   if (tid < L) {
@@ -212,9 +249,9 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
     c.emr[1] = eip;
     S.jc[j] = c;
   }
-  zdc Yp[SLOTS], Dp[SLOTS];
+  zdc Yp[SLOTS], Dp[SLOTS], em[SLOTS];
 #pragma unroll
-  for (int s = 0; s < SLOTS; s++) Yp[s] = Dp[s] = mkz(0.0);
+  for (int s = 0; s < SLOTS; s++) Yp[s] = Dp[s] = em[s] = mkz(0.0);
   __syncthreads();
 
   // sample coefficients of degree n: Cs = C(j,m) + C(j,-m), Cd = C(j,m) - C(j,-m)
@@ -235,7 +272,7 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
         } else {
           Y = J.yd[m & 1];
           D = (Y * (double)(-m)) * z;
-          S.Em[idx] = J.emr[m & 1];
+          em[s] = J.emr[m & 1];
         }
       } else if (n == m + 1) {
         double c = __ldg(&T.r1[n * L + m]);
@@ -256,19 +293,22 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
       Dp[s] = D;
       double sqn = __ldg(&T.sq[n]);
       zdc y = Y * sqn, d = D * sqn;
+      zdc cs, cd;
       if (m == 0) {
-        zdc c0 = y * s4i - (d * J.z2) * J.st;
-        S.Cs[jc] = c0 * 2.0;
-        S.Cd[jc] = mkz(0.0);
+        cs = (y * s4i - (d * J.z2) * J.st) * 2.0;
+        cd = mkz(0.0);
       } else {
         double sg = (m & 1) ? -1.0 : 1.0;
         zdc P = sg * (J.z1 * y - J.z2 * d);
         zdc Q = (sg * m) * (y * J.z3);
-        zdc e = S.Em[idx];
-        zdc Cp = (P + Q) * e, Cm = (P - Q) * zinv(e);
-        S.Cs[m * L + jc] = Cp + Cm;
-        S.Cd[m * L + jc] = Cp - Cm;
+        zdc Cp = (P + Q) * em[s], Cm = (P - Q) * zinv(em[s]);
+        cs = Cp + Cm;
+        cd = Cp - Cm;
       }
+      S.Csr[m * CP + jc] = cs.re;
+      S.Csi[m * CP + jc] = cs.im;
+      S.Cdr[m * CP + jc] = cd.re;
+      S.Cdi[m * CP + jc] = cd.im;
     }
     // Ydiag and eip^m of the states that start at degree n+1 (the sequential
     // products of myzylgndr2sf), one thread per angle
@@ -302,13 +342,11 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
       a = a * S.Ef[p + m];
       b = b * S.Ef[p - m];
     }
-    if (m == 0) {
-      S.As[lane] = a;
-      S.Ad[lane] = mkz(0.0);
-    } else {
-      S.As[m * RC + lane] = a + b;
-      S.Ad[m * RC + lane] = a - b;
-    }
+    zdc s_ = m == 0 ? a : a + b, d_ = m == 0 ? mkz(0.0) : a - b;
+    S.Asr[m * RP + lane] = s_.re;
+    S.Asi[m * RP + lane] = s_.im;
+    S.Adr[m * RP + lane] = d_.re;
+    S.Adi[m * RP + lane] = d_.im;
   };
   auto fetch = [&](int n) {
 #pragma unroll
@@ -329,72 +367,87 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
       put_row(m, a, b);
     }
   };
-  auto store = [&](int n, int m, zdc v) {
+  auto store = [&](int n, int m, int r, zdc v) {
     if (MODE == 0) {
-      stcg_z(gout + ix3(n, m) * RC + lane, prescale<KIND>(T, S, n, m, v));
-    } else if (lane < nval) {
-      zdc* o = gout + (long)ix3(n, m) * ldout + lane;
+      stcg_z(gout + ix3(n, m) * RC + r, prescale<KIND>(T, S, n, m, v));
+    } else if (r < nval) {
+      zdc* o = gout + (long)ix3(n, m) * ldout + r;
       stcg_z(o, ldcg_z(o) + (zr ? v * S.Eb[p + m] : v));
     }
   };
+  const double* cwt = S.cw ? S.cw : R.cw;
+  const double* swt = S.sw ? S.sw : R.sw;
 
   fetch(0);
   gen(0);
   commit(0);
   __syncthreads();
-  const int ngrp = (L + JT - 1) / JT;
+  const int njt = CP / 8;
   for (int n = 0; n <= p; n++) {
-    // samples at angles >= 0: S = F(j) + F(-j), D = F(j) - F(-j)
-    for (int t = w; t < 2 * ngrp; t += XW) {
-      const int which = t & 1, jc0 = (t >> 1) * JT;
-      const zdc* C = which ? S.Cd : S.Cs;
-      const zdc* Av = which ? S.Ad : S.As;
-      zdc acc[JT];
-#pragma unroll
-      for (int k = 0; k < JT; k++) acc[k] = mkz(0.0);
-      for (int m = which; m <= n; m++) {
-        zdc a = Av[m * RC + lane];
-        const zdc* Cr = C + m * L + jc0;
-#pragma unroll
-        for (int k = 0; k < JT; k++)
-          if (jc0 + k < L) acc[k] += Cr[k] * a;
+    // samples at angles >= 0: S = F(j) + F(-j), D = F(j) - F(-j); complex
+    // [jc x m] x [m x r] products on m8n8k4 tiles (4 real MMAs per k-step)
+    for (int t = w; t < 2 * njt * 4; t += XW) {
+      const int which = t / (njt * 4), rem = t - which * njt * 4, jt = rem >> 2, rt = rem & 3;
+      const double* Cr = which ? S.Cdr : S.Csr;
+      const double* Ci = which ? S.Cdi : S.Csi;
+      const double* Ar = which ? S.Adr : S.Asr;
+      const double* Ai = which ? S.Adi : S.Asi;
+      double sr[2] = {0.0, 0.0}, si[2] = {0.0, 0.0};
+      const int jc = jt * 8 + g8, r = rt * 8 + g8;
+      for (int k0 = 0; k0 <= n; k0 += 4) {
+        const int m = k0 + t4;
+        double are = 0.0, aim = 0.0, bre = 0.0, bim = 0.0;
+        if (m <= n) {
+          are = Cr[m * CP + jc];
+          aim = Ci[m * CP + jc];
+          bre = Ar[m * RP + r];
+          bim = Ai[m * RP + r];
+        }
+        dmma(sr, are, bre);
+        dmma(sr, -aim, bim);
+        dmma(si, are, bim);
+        dmma(si, aim, bre);
       }
-      zdc* O = which ? S.Sd : S.Ss;
-#pragma unroll
-      for (int k = 0; k < JT; k++)
-        if (jc0 + k < L) O[(jc0 + k) * RC + lane] = acc[k];
+      double* Or = which ? S.Sdr : S.Ssr;
+      double* Oi = which ? S.Sdi : S.Ssi;
+      const int ro = (jt * 8 + g8) * RP + rt * 8 + 2 * t4;
+      Or[ro] = sr[0];
+      Or[ro + 1] = sr[1];
+      Oi[ro] = si[0];
+      Oi[ro + 1] = si[1];
     }
     __syncthreads();
-    // projection: out(n, +-m) = dinv(n, m) (X -+ i Y)
-    const int ng2 = (n + MT) / MT;
-    for (int t = w; t < ng2; t += XW) {
-      const int m0 = t * MT;
-      zdc X[MT], Yv[MT];
-      zdc x0 = (S.Ss[lane] + S.Sd[lane]) * 0.5;
-#pragma unroll
-      for (int k = 0; k < MT; k++) {
-        X[k] = x0;
-        Yv[k] = mkz(0.0);
+    // projection: X = CW (S + [jc = 0] D), Y = SW D on m8n8k4 tiles, then
+    // out(n, +-m) = dinv(n, m) (X -+ i Y)
+    const int nmt = (n + 8) / 8;
+    for (int t = w; t < nmt * 4; t += XW) {
+      const int mt = t >> 2, rt = t & 3;
+      double xr[2] = {0.0, 0.0}, xi[2] = {0.0, 0.0}, yr[2] = {0.0, 0.0}, yi[2] = {0.0, 0.0};
+      const int mrow = mt * 8 + g8, r = rt * 8 + g8;
+      for (int k0 = 0; k0 < CP; k0 += 4) {
+        const int jc = k0 + t4;
+        const double ac = cwt[mrow * TP + jc], as = swt[mrow * TP + jc];
+        double bsr = S.Ssr[jc * RP + r], bsi = S.Ssi[jc * RP + r];
+        const double bdr = S.Sdr[jc * RP + r], bdi = S.Sdi[jc * RP + r];
+        if (jc == 0) {
+          bsr += bdr;
+          bsi += bdi;
+        }
+        dmma(xr, ac, bsr);
+        dmma(xi, ac, bsi);
+        dmma(yr, as, bdr);
+        dmma(yi, as, bdi);
       }
-      for (int jc = 1; jc <= p; jc++) {
-        zdc sv = S.Ss[jc * RC + lane], dv = S.Sd[jc * RC + lane];
-        const double* cr = R.cw + jc * L + m0;
-        const double* sr = R.sw + jc * L + m0;
+      const int m = mt * 8 + g8;
+      if (m <= n) {
+        const double dn = __ldg(&T.dinv[n * L + m]);
 #pragma unroll
-        for (int k = 0; k < MT; k++)
-          if (m0 + k <= n) {
-            X[k] += sv * cr[k];
-            Yv[k] += dv * sr[k];
-          }
-      }
-#pragma unroll
-      for (int k = 0; k < MT; k++) {
-        int m = m0 + k;
-        if (m > n) break;
-        double dn = __ldg(&T.dinv[n * L + m]);
-        zdc iy = zmul_i(Yv[k]);
-        store(n, m, (X[k] - iy) * dn);
-        if (m > 0) store(n, -m, (X[k] + iy) * dn);
+        for (int i = 0; i < 2; i++) {
+          const int ro = rt * 8 + 2 * t4 + i;
+          const zdc X = mkz(xr[i], xi[i]), iy = zmul_i(mkz(yr[i], yi[i]));
+          store(n, m, ro, (X - iy) * dn);
+          if (m > 0) store(n, -m, ro, (X + iy) * dn);
+        }
       }
     }
     if (n < p) {
@@ -491,14 +544,22 @@ __global__ void __launch_bounds__(XNT, 1) k_trans3nd(TransNdArgs A) {
   extern __shared__ zdc sm[];
   const Tab3& T = A.T;
   const int p = T.p, NC = T.NC, tid = threadIdx.x;
-  const XSm S = carve_xsm(sm, p);
+  XSm S;
+  xsm_layout(p, A.rot_smem != 0, sm, &S);
   RotTab Rt = A.R;
-  if (A.rot_smem) {
-    const int L = p + 1;
-    double* tab = reinterpret_cast<double*>(S.Em + L * L);
-    for (int k = tid; k < 2 * L * L; k += XNT) tab[k] = A.R.cw[k];  // cw then sw
-    Rt.cw = tab;
-    Rt.sw = tab + L * L;
+  {
+    const int L = p + 1, CP = rot_cp(L), KR = rot_kr(L), TP = rot_tp(L);
+    if (S.cw) {
+      // tables staged once (cw then sw, contiguous in global memory)
+      for (int k = tid; k < 2 * CP * TP; k += XNT) S.cw[k] = A.R.cw[k];
+    }
+    // the padding columns (angles >= p+1) of the sample coefficients stay zero
+    for (int k = tid; k < KR * CP; k += XNT) {
+      S.Csr[k] = 0.0;
+      S.Csi[k] = 0.0;
+      S.Cdr[k] = 0.0;
+      S.Cdi[k] = 0.0;
+    }
   }
   zdc* X1 = A.scratch + (size_t)blockIdx.x * 2 * NC * RC;
   zdc* X2 = X1 + (size_t)NC * RC;
@@ -1143,11 +1204,10 @@ template <int KIND>
 void launch_trans_nd(const TransNdArgs& A, int grid, cudaStream_t s) {
   if (A.hi < A.lo) return;
   int L = A.T.p + 1;
-  size_t sm = xsm_bytes(A.T.p);
   TransNdArgs B = A;
-  size_t tab = 2 * (size_t)L * L * sizeof(double);
-  B.rot_smem = sm + tab <= 227 * 1024;
-  if (B.rot_smem) sm += tab;
+  size_t sm = xsm_layout(A.T.p, true, nullptr, nullptr);
+  B.rot_smem = sm <= 227 * 1024;
+  if (!B.rot_smem) sm = xsm_layout(A.T.p, false, nullptr, nullptr);
   int slots = div_up(L * L, XNT);
   if (slots <= 4) launch_trans_nd_k<KIND, 4>(B, grid, sm, s);
   else if (slots <= 6) launch_trans_nd_k<KIND, 6>(B, grid, sm, s);
@@ -1193,7 +1253,7 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   const DevLists& L = S.lists;
   const int nb = t.nboxes, nlev = t.nlevels;
   const int p = zl3dterms(P.eps);
-  if (xsm_bytes(p) > 227 * 1024)
+  if (xsm_layout(p, false, nullptr, nullptr) > 227 * 1024)
     throw zf_error(ZF_ERR_ARG, "expansion order " + std::to_string(p) +
                                    " too large for the batched 3D translation (eps too small)");
   Tab3 T = get_tab3(p);
