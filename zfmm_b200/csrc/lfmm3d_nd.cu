@@ -871,7 +871,8 @@ __global__ void __launch_bounds__(FW * 32) k_form3nd(FormNdArgs A) {
 
 // ---- L2T / M2T -------------------------------------------------------------
 constexpr int ENT = 128;
-constexpr int RB = 8;  // right-hand sides per thread pass (eval, P2P)
+constexpr int RB = 8;   // right-hand sides per thread pass of the P2P kernel
+constexpr int RBE = 4;  // right-hand sides per thread pass of the L2T / M2T kernel
 
 struct EvalNdArgs {
   Tab3 T;
@@ -885,7 +886,7 @@ struct EvalNdArgs {
 };
 
 // zl3devalmp (LOCAL = false) / zl3devalloc (LOCAL = true), zlfmm3d.f:1011-1277,
-// for nv <= RB right-hand sides; e: coefficient rows of stride nd
+// for nv <= RBE right-hand sides; e: coefficient rows of stride nd
 template <bool GRAD, bool LOCAL>
 __device__ __forceinline__ void eval_one_nd(const Tab3& T, const zdc* __restrict__ e, long nd,
                                             int nv, const zdc* x, const zdc* zc, double rscale,
@@ -953,7 +954,7 @@ __device__ __forceinline__ void eval_one_nd(const Tab3& T, const zdc* __restrict
           }
         }
 #pragma unroll
-        for (int r = 0; r < RB; r++)
+        for (int r = 0; r < RBE; r++)
           if (r < nv) {
             zdc c0 = ldz(&row[r]);
             P[r] += c0 * yr;
@@ -979,7 +980,7 @@ __device__ __forceinline__ void eval_one_nd(const Tab3& T, const zdc* __restrict
           DPh = zmul_i((double)m * y * rf);
         }
 #pragma unroll
-        for (int r = 0; r < RB; r++)
+        for (int r = 0; r < RBE; r++)
           if (r < nv) {
             zdc a = ldz(&rowp[r]) * em, bm = ldz(&rown[r]) * emi;
             zdc Sp = a + bm;
@@ -1012,11 +1013,11 @@ __global__ void __launch_bounds__(ENT) k_eval3nd(EvalNdArgs A) {
     const int i = c0 + tid;
     if (i > t1) continue;
     zdc x[3] = {A.ztarg[3 * i], A.ztarg[3 * i + 1], A.ztarg[3 * i + 2]};
-    for (int rb = 0; rb < A.nd; rb += RB) {
-      const int nv = min(RB, A.nd - rb);
-      zdc P[RB], Gx[RB], Gy[RB], Gz[RB];
+    for (int rb = blockIdx.y * RBE; rb < A.nd && rb < (int)(blockIdx.y + 1) * RBE; rb += RBE) {
+      const int nv = min(RBE, A.nd - rb);
+      zdc P[RBE], Gx[RBE], Gy[RBE], Gz[RBE];
 #pragma unroll
-      for (int r = 0; r < RB; r++) P[r] = Gx[r] = Gy[r] = Gz[r] = mkz(0.0);
+      for (int r = 0; r < RBE; r++) P[r] = Gx[r] = Gy[r] = Gz[r] = mkz(0.0);
       for (int e = 0; e < nexp; e++) {
         int eb;
         bool loc;
@@ -1030,14 +1031,14 @@ __global__ void __launch_bounds__(ENT) k_eval3nd(EvalNdArgs A) {
         }
         const zdc* zc = (loc ? A.zct : A.zcs) + 3 * eb;
         const zdc* ex = (loc ? A.loc : A.mp) + (size_t)eb * NC * nd + rb;
-        zdc Gr[RB], Gt[RB], Gp[RB], Pe[RB];
+        zdc Gr[RBE], Gt[RBE], Gp[RBE], Pe[RBE];
 #pragma unroll
-        for (int r = 0; r < RB; r++) Pe[r] = Gr[r] = Gt[r] = Gp[r] = mkz(0.0);
+        for (int r = 0; r < RBE; r++) Pe[r] = Gr[r] = Gt[r] = Gp[r] = mkz(0.0);
         double rscale = A.rsc[A.ilevel[eb]];
         if (loc) eval_one_nd<GRAD, true>(T, ex, nd, nv, x, zc, rscale, Pe, Gr, Gt, Gp);
         else eval_one_nd<GRAD, false>(T, ex, nd, nv, x, zc, rscale, Pe, Gr, Gt, Gp);
 #pragma unroll
-        for (int r = 0; r < RB; r++) P[r] += Pe[r];
+        for (int r = 0; r < RBE; r++) P[r] += Pe[r];
         if (GRAD) {
           Sph s = zcart2sph(x[0], x[1], x[2], zc);
           zdc ir = zinv(s.rz);
@@ -1045,7 +1046,7 @@ __global__ void __launch_bounds__(ENT) k_eval3nd(EvalNdArgs A) {
           zdc et0 = s.ct * s.cp * ir, et1 = s.ct * s.sp * ir, et2 = -(s.st * ir);
           zdc ep0 = -(s.sp * ir), ep1 = s.cp * ir;
 #pragma unroll
-          for (int r = 0; r < RB; r++) {
+          for (int r = 0; r < RBE; r++) {
             Gx[r] += Gr[r] * ezr0 + Gt[r] * et0 + Gp[r] * ep0;
             Gy[r] += Gr[r] * ezr1 + Gt[r] * et1 + Gp[r] * ep1;
             Gz[r] += Gr[r] * ezr2 + Gt[r] * et2;
@@ -1053,7 +1054,7 @@ __global__ void __launch_bounds__(ENT) k_eval3nd(EvalNdArgs A) {
         }
       }
 #pragma unroll
-      for (int r = 0; r < RB; r++)
+      for (int r = 0; r < RBE; r++)
         if (r < nv) {
           A.pot[(long)i * nd + rb + r] += P[r];
           if (GRAD) {
@@ -1103,7 +1104,7 @@ __global__ void __launch_bounds__(ENT) k_p2p3nd(P2PNdArgs A) {
       x[1] = ldz(&A.ztarg[3 * i + 1]);
       x[2] = ldz(&A.ztarg[3 * i + 2]);
     }
-    for (int rb = 0; rb < A.nd; rb += RB) {
+    for (int rb = blockIdx.y * RB; rb < A.nd && rb < (int)(blockIdx.y + 1) * RB; rb += RB) {
       const int nv = min(RB, A.nd - rb);
       zdc P[RB], G0[RB], G1[RB], G2[RB];
 #pragma unroll
@@ -1365,18 +1366,18 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   if (ifpgh > 1) {
     if (dip) {
       ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
-      klaunch(k_p2p3nd<true, true>, nb, ENT, smp, s, Pa);
+      klaunch(k_p2p3nd<true, true>, dim3(nb, div_up(nd, RB)), ENT, smp, s, Pa);
     } else {
       ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
-      klaunch(k_p2p3nd<true, false>, nb, ENT, smp, s, Pa);
+      klaunch(k_p2p3nd<true, false>, dim3(nb, div_up(nd, RB)), ENT, smp, s, Pa);
     }
   } else {
     if (dip) {
       ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
-      klaunch(k_p2p3nd<false, true>, nb, ENT, smp, s, Pa);
+      klaunch(k_p2p3nd<false, true>, dim3(nb, div_up(nd, RB)), ENT, smp, s, Pa);
     } else {
       ZF_CUDA(cudaFuncSetAttribute(k_p2p3nd<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
-      klaunch(k_p2p3nd<false, false>, nb, ENT, smp, s, Pa);
+      klaunch(k_p2p3nd<false, false>, dim3(nb, div_up(nd, RB)), ENT, smp, s, Pa);
     }
   }
   ZF_LAUNCH_CHECK();
@@ -1387,8 +1388,8 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   E.zct = S.zctarg.get(); E.rsc = rsc.get(); E.mp = mp.get(); E.loc = loc.get();
   E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb; E.nd = nd;
   E.pot = potsort.get(); E.grad = gradsort.get();
-  if (ifpgh > 1) klaunch(k_eval3nd<true>, nb, ENT, 0, s, E);
-  else klaunch(k_eval3nd<false>, nb, ENT, 0, s, E);
+  if (ifpgh > 1) klaunch(k_eval3nd<true>, dim3(nb, div_up(nd, RBE)), ENT, 0, s, E);
+  else klaunch(k_eval3nd<false>, dim3(nb, div_up(nd, RBE)), ENT, 0, s, E);
   ZF_LAUNCH_CHECK();
   mark(6);
   unsort3d_nd(nt, nd, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0), mkz(1.0 / S.b0),
