@@ -70,6 +70,9 @@ WORKLOADS = {
                                   cpu_n=30_000, dipoles=False),
     "zlfmm3d_batched_200k_64": dict(kind="lap3d", n=200_000, nrhs=64, eps=1e-9, ifpgh=2,
                                     isep=1, cpu_n=30_000, dipoles=False),
+    # small case of the same distribution for kernel profiles (one 32-right-hand-side pass)
+    "zlfmm3d_batched_30k_32": dict(kind="lap3d", n=30_000, nrhs=32, eps=1e-9, ifpgh=2,
+                                   isep=1, cpu_n=30_000, dipoles=False),
     # zhfmm3d batched uneven instances: 200 independent FMMs, point counts
     # log-uniform in [2,000, 500,000], points on unit spheres displaced by 0.1i
     # times the normal scaled by a degree-4 field, zk = 10+0.2i, charges +
@@ -905,13 +908,13 @@ def run_ours_adjoint(args, wl, ws, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def fwd_bwd(Dx, grads=True):
+    def fwd_bwd(Dx, grads=True, backward=True):
         qq = Dx["q"].clone().requires_grad_(grads)
         dd = Dx["ds"].clone().requires_grad_(grads)
         a = torch.tensor(a0, device=dev, dtype=torch.float64, requires_grad=grads)
         pot = zhfmm2d_curves(eps, zk, Dx["xr"], Dx["disp"], Dx["curve"], a, qq, dd, Dx["dv"])
         Lv = torch.mean(torch.abs(pot - Dx["ref"]) ** 2)
-        if grads:
+        if grads and backward:
             Lv.backward()
             return Lv, qq.grad, dd.grad, a.grad
         return Lv
@@ -953,7 +956,8 @@ def run_ours_adjoint(args, wl, ws, rank, local):
         return e0.elapsed_time(e1) / reps
     plain_ms = timed(lambda: zfmm_b200._fmm2d_torch(eps, zk, n, z, 1, D["q"], 1, D["ds"], D["dv"],
                                                      n, z, 1, 1))
-    fwd_ms = timed(lambda: fwd_bwd(D, grads=False))
+    # the forward as the differentiable call runs it (pot and grad, graph kept)
+    fwd_ms = timed(lambda: fwd_bwd(D, grads=True, backward=False))
     step_ms = tot_ms / args.steps
     # gradient checks at full size: central differences of the FMM loss for both
     # amplitudes, at h = 1e-6 and at h = 1e-3 (at 200,000 points the loss moves
