@@ -7,7 +7,9 @@ solve (itself pinned to the oracle) to 10*eps relative L2, the parity bar of
 the FMMs.  One small case goes straight against the oracle.  The cases cover
 one and many right-hand sides (a ragged last pass of 32), charges and dipoles,
 ifpgh 1 and 2, adaptive trees with lists 3 and 4, plan reuse, and the device
-(torch) entry point.  Helmholtz plan solves run the single-solve passes on
+(torch) entry point.  Fewer than 4 right-hand sides, or orders whose batched
+working set exceeds shared memory (eps below ~3e-10), run the single-solve
+passes per right-hand side on the plan's tree.  Helmholtz plan solves run the single-solve passes on
 the plan's tree for every right-hand side and wavenumber, so they must equal
 the single solves to rounding."""
 import numpy as np
@@ -72,7 +74,7 @@ def test_plan_dipoles_adaptive_tree():
     zs = w["zsrc"]
     n = zs.shape[1]
     rng = np.random.default_rng(5)
-    nd = 3
+    nd = 5
     q, ds = cn(rng, nd, n), cn(rng, nd, n)
     plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
     for ifc, ifd, ifpgh in [(1, 1, 2), (0, 1, 1), (1, 0, 2)]:
@@ -93,7 +95,7 @@ def test_plan_against_oracle():
     zs = w["zsrc"]
     n = zs.shape[1]
     rng = np.random.default_rng(6)
-    nd = 2
+    nd = 4
     q, ds = cn(rng, nd, n), cn(rng, nd, n)
     plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
     p, g = plan.zlfmm3d(nd, 1, q, 1, ds, w["dipvec"], 2)
@@ -160,3 +162,20 @@ def test_helmholtz_plan_matches_single_two_wavenumbers():
                 assert rel(p[r], p1) < 1e-13, (zk, ifc, ifd, r)
                 if ifpgh == 2:
                     assert rel(g[r], g1) < 1e-13, (zk, ifc, ifd, r)
+
+
+def test_plan_small_eps_runs_per_rhs():
+    import zfmm_b200
+    eps = 1e-11  # order 46: beyond the batched translation's shared memory
+    nd = 6
+    w = W.clustered3d(6000, seed=19)
+    zs = w["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(9)
+    q = cn(rng, nd, n)
+    plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
+    p, g = plan.zlfmm3d(nd, 1, q, 0, None, None, 2)
+    for r in (0, nd - 1):
+        p1, g1 = single(eps, zs, q[r], 0, None, None, 2)
+        assert rel(p[r], p1) < 1e-13, r
+        assert rel(g[r], g1) < 1e-13, r

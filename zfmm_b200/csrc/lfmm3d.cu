@@ -950,6 +950,126 @@ void zl3ddirect_device(const Inputs3D& in, zdc* pot, zdc* grad, cudaStream_t s) 
   ZF_LAUNCH_CHECK();
 }
 
+// P2M through L2T/M2T/P2P on a set-up: adds the sorted potentials (and
+// gradients, unscaled) of one right-hand side with sorted, rescaled strengths
+// q, ds, dv to potsort / gradsort; ev[2..5] (optional) get the step boundaries;
+// returns the expansion order
+int lap_core(const Setup3D& S, double eps, const zdc* q, const zdc* ds, const zdc* dv,
+             int ifcharge, int ifdipole, int ifpgh, zdc* potsort, zdc* gradsort, cudaStream_t s,
+             cudaEvent_t* ev) {
+  auto lmark = [&](int i) {
+    if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  int nb = t.nboxes, nlev = t.nlevels;
+  int p = zl3dterms(eps);
+  if (trans_smem(p) > 227 * 1024)
+    throw zf_error(ZF_ERR_ARG, "expansion order " + std::to_string(p) +
+                                   " too large for the 3D translation kernel (eps too small)");
+  Tab3 T = get_tab3(p);
+  const size_t NC = (size_t)T.NC;
+  std::vector<double> rsc_h(nlev + 2, 1.0);
+  for (int l = 0; l <= nlev; l++) rsc_h[l] = S.bsz[l] > 1.0 ? 1.0 : S.bsz[l];
+  DevBuf<double> rsc(rsc_h.size(), s);
+  ZF_CUDA(cudaMemcpyAsync(rsc.get(), rsc_h.data(), rsc_h.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, s));
+  DevBuf<zdc> mp(NC * nb, s), loc(NC * nb, s);
+  mp.zero();
+  loc.zero();
+  // P2M
+  FormArgs F;
+  F.T = T;
+  F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
+  F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
+  F.zsrc = S.zsrcsort.get(); F.charge = q; F.dipstr = ds;
+  F.dipvec = dv; F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get();
+  F.rsc = rsc.get(); F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
+  F.nb = nb; F.ifcharge = ifcharge; F.ifdipole = ifdipole;
+  size_t smf = (FNT / 32) * NC * sizeof(zdc);
+  F.out = mp.get();
+  if (nlev >= 1) {
+    if (ifdipole) {
+      ZF_CUDA(cudaFuncSetAttribute(k_form3<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_form3<false, true>, nb, FNT, smf, s, F);
+    } else {
+      ZF_CUDA(cudaFuncSetAttribute(k_form3<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_form3<false, false>, nb, FNT, smf, s, F);
+    }
+    ZF_LAUNCH_CHECK();
+  }
+  lmark(2);
+  TransArgs A;
+  A.T = T;
+  A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
+  A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
+  A.zcs = S.zcsrc.get(); A.zct = S.zctarg.get(); A.rsc = rsc.get();
+  A.nl2 = L.n[1].get(); A.l2 = L.list[1].get(); A.nl4 = L.n[3].get(); A.mn2 = L.mn[1];
+  // M2M, finest parents first
+  A.in = mp.get();
+  A.out = mp.get();
+  for (int l = nlev - 1; l >= 1; l--) {
+    A.lo = t.laddr[2 * l];
+    A.hi = t.laddr[2 * l + 1];
+    launch_trans<0>(A, s);
+  }
+  lmark(3);
+  // M2L, then P2L (list 4)
+  A.in = mp.get();
+  A.out = loc.get();
+  A.lo = 0;
+  A.hi = nb - 1;
+  launch_trans<1>(A, s);
+  if (L.mn[3] > 0) {
+    F.out = loc.get();
+    if (ifdipole) {
+      ZF_CUDA(cudaFuncSetAttribute(k_form3<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_form3<true, true>, nb, FNT, smf, s, F);
+    } else {
+      ZF_CUDA(cudaFuncSetAttribute(k_form3<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_form3<true, false>, nb, FNT, smf, s, F);
+    }
+    ZF_LAUNCH_CHECK();
+  }
+  lmark(4);
+  // L2L, coarsest first: children at level l+1 of parents at level l >= 1
+  A.in = loc.get();
+  A.out = loc.get();
+  for (int l = 1; l <= nlev - 1; l++) {
+    A.lo = t.laddr[2 * (l + 1)];
+    A.hi = t.laddr[2 * (l + 1) + 1];
+    launch_trans<2>(A, s);
+  }
+  lmark(5);
+  // P2P (list 1), then L2T and M2T (list 3)
+  P2PArgs Pa;
+  Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
+  Pa.zsrc = S.zsrcsort.get(); Pa.charge = q; Pa.dipstr = ds;
+  Pa.dipvec = dv; Pa.ztarg = S.ztargsort.get();
+  Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb;
+  Pa.ifcharge = ifcharge; Pa.ifdipole = ifdipole; Pa.pot = potsort; Pa.grad = gradsort;
+  if (ifpgh > 1) klaunch(k_p2p3<true>, nb, ENT, 0, s, Pa);
+  else klaunch(k_p2p3<false>, nb, ENT, 0, s, Pa);
+  ZF_LAUNCH_CHECK();
+  EvalArgs E;
+  E.T = T;
+  E.ilevel = t.ilevel.get(); E.nchild = t.nchild.get(); E.isrcse = S.isrcse.get();
+  E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
+  E.zct = S.zctarg.get(); E.rsc = rsc.get(); E.mp = mp.get(); E.loc = loc.get();
+  E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb;
+  E.pot = potsort; E.grad = gradsort;
+  size_t sme = NC * sizeof(zdc);
+  if (ifpgh > 1) {
+    ZF_CUDA(cudaFuncSetAttribute(k_eval3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
+    klaunch(k_eval3<true>, nb, ENT, sme, s, E);
+  } else {
+    ZF_CUDA(cudaFuncSetAttribute(k_eval3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
+    klaunch(k_eval3<false>, nb, ENT, sme, s, E);
+  }
+  ZF_LAUNCH_CHECK();
+  return p;
+}
+
 void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
                     cudaStream_t s, StepTimes* times) {
   int ns = in.ns, nt = in.nt;
@@ -971,116 +1091,12 @@ void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* gra
   Setup3D S;
   setup3d(in, tp, S, true, true, s);
   mark(1);
-  const DevTree& t = S.tree;
-  const DevLists& L = S.lists;
-  int nb = t.nboxes, nlev = t.nlevels;
-  int p = zl3dterms(eps);
-  if (trans_smem(p) > 227 * 1024)
-    throw zf_error(ZF_ERR_ARG, "expansion order " + std::to_string(p) +
-                                   " too large for the 3D translation kernel (eps too small)");
-  Tab3 T = get_tab3(p);
-  const size_t NC = (size_t)T.NC;
-  std::vector<double> rsc_h(nlev + 2, 1.0);
-  for (int l = 0; l <= nlev; l++) rsc_h[l] = S.bsz[l] > 1.0 ? 1.0 : S.bsz[l];
-  DevBuf<double> rsc(rsc_h.size(), s);
-  ZF_CUDA(cudaMemcpyAsync(rsc.get(), rsc_h.data(), rsc_h.size() * sizeof(double),
-                          cudaMemcpyHostToDevice, s));
-  DevBuf<zdc> mp(NC * nb, s), loc(NC * nb, s), potsort(nt, s),
-      gradsort(in.ifpgh > 1 ? 3 * (size_t)nt : 1, s);
-  mp.zero();
-  loc.zero();
+  DevBuf<zdc> potsort(nt, s), gradsort(in.ifpgh > 1 ? 3 * (size_t)nt : 1, s);
   potsort.zero();
   gradsort.zero();
-  // P2M
-  FormArgs F;
-  F.T = T;
-  F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
-  F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
-  F.zsrc = S.zsrcsort.get(); F.charge = S.chargesort.get(); F.dipstr = S.dipstrsort.get();
-  F.dipvec = S.dipvecsort.get(); F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get();
-  F.rsc = rsc.get(); F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
-  F.nb = nb; F.ifcharge = in.ifcharge; F.ifdipole = in.ifdipole;
-  size_t smf = (FNT / 32) * NC * sizeof(zdc);
-  F.out = mp.get();
-  if (nlev >= 1) {
-    if (in.ifdipole) {
-      ZF_CUDA(cudaFuncSetAttribute(k_form3<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_form3<false, true>, nb, FNT, smf, s, F);
-    } else {
-      ZF_CUDA(cudaFuncSetAttribute(k_form3<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_form3<false, false>, nb, FNT, smf, s, F);
-    }
-    ZF_LAUNCH_CHECK();
-  }
-  mark(2);
-  TransArgs A;
-  A.T = T;
-  A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
-  A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
-  A.zcs = S.zcsrc.get(); A.zct = S.zctarg.get(); A.rsc = rsc.get();
-  A.nl2 = L.n[1].get(); A.l2 = L.list[1].get(); A.nl4 = L.n[3].get(); A.mn2 = L.mn[1];
-  // M2M, finest parents first
-  A.in = mp.get();
-  A.out = mp.get();
-  for (int l = nlev - 1; l >= 1; l--) {
-    A.lo = t.laddr[2 * l];
-    A.hi = t.laddr[2 * l + 1];
-    launch_trans<0>(A, s);
-  }
-  mark(3);
-  // M2L, then P2L (list 4)
-  A.in = mp.get();
-  A.out = loc.get();
-  A.lo = 0;
-  A.hi = nb - 1;
-  launch_trans<1>(A, s);
-  if (L.mn[3] > 0) {
-    F.out = loc.get();
-    if (in.ifdipole) {
-      ZF_CUDA(cudaFuncSetAttribute(k_form3<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_form3<true, true>, nb, FNT, smf, s, F);
-    } else {
-      ZF_CUDA(cudaFuncSetAttribute(k_form3<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_form3<true, false>, nb, FNT, smf, s, F);
-    }
-    ZF_LAUNCH_CHECK();
-  }
-  mark(4);
-  // L2L, coarsest first: children at level l+1 of parents at level l >= 1
-  A.in = loc.get();
-  A.out = loc.get();
-  for (int l = 1; l <= nlev - 1; l++) {
-    A.lo = t.laddr[2 * (l + 1)];
-    A.hi = t.laddr[2 * (l + 1) + 1];
-    launch_trans<2>(A, s);
-  }
-  mark(5);
-  // P2P (list 1), then L2T and M2T (list 3)
-  P2PArgs Pa;
-  Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
-  Pa.zsrc = S.zsrcsort.get(); Pa.charge = S.chargesort.get(); Pa.dipstr = S.dipstrsort.get();
-  Pa.dipvec = S.dipvecsort.get(); Pa.ztarg = S.ztargsort.get();
-  Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb;
-  Pa.ifcharge = in.ifcharge; Pa.ifdipole = in.ifdipole; Pa.pot = potsort.get(); Pa.grad = gradsort.get();
-  if (in.ifpgh > 1) klaunch(k_p2p3<true>, nb, ENT, 0, s, Pa);
-  else klaunch(k_p2p3<false>, nb, ENT, 0, s, Pa);
-  ZF_LAUNCH_CHECK();
-  EvalArgs E;
-  E.T = T;
-  E.ilevel = t.ilevel.get(); E.nchild = t.nchild.get(); E.isrcse = S.isrcse.get();
-  E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
-  E.zct = S.zctarg.get(); E.rsc = rsc.get(); E.mp = mp.get(); E.loc = loc.get();
-  E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb;
-  E.pot = potsort.get(); E.grad = gradsort.get();
-  size_t sme = NC * sizeof(zdc);
-  if (in.ifpgh > 1) {
-    ZF_CUDA(cudaFuncSetAttribute(k_eval3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
-    klaunch(k_eval3<true>, nb, ENT, sme, s, E);
-  } else {
-    ZF_CUDA(cudaFuncSetAttribute(k_eval3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
-    klaunch(k_eval3<false>, nb, ENT, sme, s, E);
-  }
-  ZF_LAUNCH_CHECK();
+  int p = lap_core(S, eps, S.chargesort.get(), S.dipstrsort.get(), S.dipvecsort.get(),
+                   in.ifcharge, in.ifdipole, in.ifpgh, potsort.get(), gradsort.get(), s,
+                   timing ? ev : nullptr);
   mark(6);
   unsort3d(nt, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0), mkz(1.0 / S.b0), in.ifpgh,
            pot, grad, s);
@@ -1092,13 +1108,13 @@ void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* gra
       ZF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
       times->ms[i] = ms;
     }
-    times->nboxes = nb;
-    times->nlevels = nlev;
+    times->nboxes = S.tree.nboxes;
+    times->nlevels = S.tree.nlevels;
     times->nterms = p;
     for (auto& e : ev) cudaEventDestroy(e);
     times->launches = launch_counter() - launches0;
     if (times->want_counts) {
-      std::vector<int> pl(nlev + 1, p);
+      std::vector<int> pl(S.tree.nlevels + 1, p);
       count_interactions3d(S, pl.data(), 1, 1, 2, times, s);
     }
   }

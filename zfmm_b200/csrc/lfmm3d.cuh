@@ -15,6 +15,14 @@ int lndiv3d(double eps, int ns, int nt);
 void zlfmm3d_device(double eps, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
                     cudaStream_t s, StepTimes* times);
 
+// the passes of zlfmm3d after the set-up, for one right-hand side with sorted,
+// rescaled strengths (q, ds: ns; dv: 3 ns) on a set-up S: ADDS the sorted,
+// unscaled potentials / gradients to potsort / gradsort; ev (optional, 8
+// events) gets the step boundaries 2..5 recorded; returns the order
+int lap_core(const Setup3D& S, double eps, const zdc* q, const zdc* ds, const zdc* dv,
+             int ifcharge, int ifdipole, int ifpgh, zdc* potsort, zdc* gradsort, cudaStream_t s,
+             cudaEvent_t* ev);
+
 // interaction counts of a 3D FMM on this set-up, totals and per level, into
 // times (counts, lvl_counts, lvl_p); p2m_lmin / m2m_lmin / l2l_lmin: the
 // coarsest level with P2M leaves / M2M parents / L2L children

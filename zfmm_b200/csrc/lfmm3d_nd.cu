@@ -1237,8 +1237,75 @@ void plan3d_build(Plan3D& P, double eps, int ns, const zdc* zsrc, int nt, const 
   ZF_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+
+// right-hand sides one at a time through the single-solve passes on the plan's
+// tree: fewer than kMinBatch right-hand sides (the batched kernels fill 32
+// lanes per pass) or orders whose batched working set exceeds shared memory
+void lap_plan_loop(const Plan3D& P, int nd, const StrengthsNd& in, int ifpgh, zdc* pot, zdc* grad,
+                   cudaStream_t s, StepTimes* times) {
+  const Setup3D& S = P.S;
+  const int ns = P.ns, nt = P.nt;
+  long launches0 = launch_counter();
+  const bool timing = times != nullptr;
+  cudaEvent_t ev[8];
+  if (timing)
+    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  float acc[8] = {0};
+  auto mark = [&](int i) {
+    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  DevBuf<zdc> q(ns, s), ds(ns, s), dv(3 * (size_t)ns, s), potsort(nt, s),
+      gradsort(ifpgh > 1 ? 3 * (size_t)nt : 1, s);
+  int p = 0;
+  for (int r = 0; r < nd; r++) {
+    mark(0);
+    gather_strengths_col(S, ns, nd, r, in.ifcharge ? in.charge : nullptr,
+                         in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
+                         true, true, q.get(), ds.get(), dv.get(), s);
+    potsort.zero();
+    gradsort.zero();
+    mark(1);
+    p = lap_core(S, P.eps, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, ifpgh,
+                 potsort.get(), gradsort.get(), s, timing ? ev : nullptr);
+    mark(6);
+    unsort3d_col(nt, nd, r, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0),
+                 mkz(1.0 / S.b0), ifpgh, pot, grad, s);
+    mark(7);
+    if (timing) {
+      ZF_CUDA(cudaEventSynchronize(ev[7]));
+      for (int k = 0; k < 7; k++) {
+        float ms;
+        ZF_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        acc[k] += ms;
+      }
+    }
+  }
+  if (timing) {
+    for (int k = 0; k < 7; k++) times->ms[k] = acc[k];
+    times->nboxes = S.tree.nboxes;
+    times->nlevels = S.tree.nlevels;
+    times->nterms = p;
+    for (auto& e : ev) cudaEventDestroy(e);
+    times->launches = launch_counter() - launches0;
+    if (times->want_counts) {
+      std::vector<int> pl(S.tree.nlevels + 1, p);
+      count_interactions3d(S, pl.data(), 1, 1, 2, times, s);
+    }
+  }
+}
+
+constexpr int kMinBatch = 4;
+
+}  // namespace
+
 void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int ifpgh, zdc* pot,
                           zdc* grad, cudaStream_t s, StepTimes* times) {
+  if (nd < kMinBatch ||
+      xsm_layout(zl3dterms(P.eps), false, nullptr, nullptr) > 227 * 1024) {
+    lap_plan_loop(P, nd, in, ifpgh, pot, grad, s, times);
+    return;
+  }
   const Setup3D& S = P.S;
   const int ns = P.ns, nt = P.nt;
   long launches0 = launch_counter();
@@ -1254,9 +1321,6 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   const DevLists& L = S.lists;
   const int nb = t.nboxes, nlev = t.nlevels;
   const int p = zl3dterms(P.eps);
-  if (xsm_layout(p, false, nullptr, nullptr) > 227 * 1024)
-    throw zf_error(ZF_ERR_ARG, "expansion order " + std::to_string(p) +
-                                   " too large for the batched 3D translation (eps too small)");
   Tab3 T = get_tab3(p);
   RotTab R = get_rottab(p);
   const size_t NC = (size_t)T.NC;
