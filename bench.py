@@ -973,7 +973,7 @@ def run_ours_adjoint(args, wl, ws, rank, local):
         return float(torch.mean(torch.abs(pt - D["ref"]) ** 2))
 
     fd_rel = {}
-    for h in (1e-6, 1e-3):
+    for h in (1e-6, 1e-4, 1e-3):
         errs = []
         for c in range(2):
             ap, am = list(a0), list(a0)
@@ -1004,6 +1004,7 @@ def run_ours_adjoint(args, wl, ws, rank, local):
     # roofline of the forward's dominant step (an instrumented forward solve)
     L.zfmm_set_step_timing(2)
     zfmm_b200._fmm2d_torch(eps, zk, n, z, 1, D["q"], 1, D["ds"], D["dv"], n, z, 2, 1)
+    torch.cuda.synchronize()
     torch.cuda.synchronize()
     counts, _ = zfmm_b200.last_counts()
     st, info = zfmm_b200.last_step_times()

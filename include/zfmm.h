@@ -207,6 +207,33 @@ int zfmm_zhfmm3d_plan_dev(zfmm_plan3d plan, const double *zk, int nd, int ifchar
                           const double *dipvec, int ifpgh, double *pot, double *grad,
                           void *stream);
 
+/* 2D plans, as the 3D ones: the quadtree, sorted points, complex centres and
+ * lists of one geometry (zlfmm2d.f:70-200 / zhfmm2d.f:73-195) built once and
+ * reused by solves of nd right-hand sides at any wavenumber: charge(nd, ns),
+ * dipstr(nd, ns), pot(nd, nt), grad(nd, 2, nt) with the right-hand side
+ * fastest, dipvec(2, ns) shared.  Each right-hand side runs the FMM passes on
+ * the plan's tree, so a solve equals the single call to rounding. */
+typedef struct zfmm_plan2d_s *zfmm_plan2d;
+int zfmm_plan2d_create(double eps, int ns, const double *zsrc, int nt, const double *ztarg,
+                       int isep, zfmm_plan2d *plan);
+int zfmm_plan2d_create_dev(double eps, int ns, const double *zsrc, int nt, const double *ztarg,
+                           int isep, void *stream, zfmm_plan2d *plan);
+int zfmm_plan2d_destroy(zfmm_plan2d plan);
+int zfmm_plan2d_info(zfmm_plan2d plan, int *nboxes, int *nlevels, int *ns, int *nt);
+int zfmm_zlfmm2d_plan(zfmm_plan2d plan, int nd, int ifcharge, const double *charge,
+                      int ifdipole, const double *dipstr, const double *dipvec, int ifpgh,
+                      double *pot, double *grad);
+int zfmm_zlfmm2d_plan_dev(zfmm_plan2d plan, int nd, int ifcharge, const double *charge,
+                          int ifdipole, const double *dipstr, const double *dipvec, int ifpgh,
+                          double *pot, double *grad, void *stream);
+int zfmm_zhfmm2d_plan(zfmm_plan2d plan, const double *zk, int nd, int ifcharge,
+                      const double *charge, int ifdipole, const double *dipstr,
+                      const double *dipvec, int ifpgh, double *pot, double *grad);
+int zfmm_zhfmm2d_plan_dev(zfmm_plan2d plan, const double *zk, int nd, int ifcharge,
+                          const double *charge, int ifdipole, const double *dipstr,
+                          const double *dipvec, int ifpgh, double *pot, double *grad,
+                          void *stream);
+
 /* Many independent 3D FMMs in one call (no counterpart in the reference,
  * where each instance is a separate zlfmm3d / zhfmm3d call): instance i has
  * ns[i] sources zsrc[i](3, ns[i]), strengths charge[i], dipstr[i],

@@ -21,7 +21,7 @@ from ._capi import ZfmmError, check, lib
 
 __all__ = ["zlfmm2d", "zl2devaldirect", "zhfmm2d", "zh2devaldirect", "zlfmm3d", "zl3devaldirect",
            "zhfmm3d", "zh3devaldirect", "zl3dterms", "h3dterms", "tree_dump", "ZfmmError",
-           "set_step_timing", "last_step_times", "last_counts", "version", "Plan3D",
+           "set_step_timing", "last_step_times", "last_counts", "version", "Plan3D", "Plan2D",
            "zlfmm3d_many", "zhfmm3d_many"]
 
 
@@ -281,7 +281,91 @@ def _mat(v, nd, n, name):
     return np.asfortranarray(a)
 
 
-class Plan3D:
+class _Plan:
+    """Geometry of a complex-coordinate FMM built once and reused (base of
+    Plan2D / Plan3D)."""
+
+    D = 3
+    _fn = {}
+
+    def __init__(self, eps, ns, zsrc, nt, ztarg, isep=1):
+        self._h = ctypes.c_void_p()
+        self.ns, self.nt, self.eps = int(ns), int(nt), float(eps)
+        d = self.D
+        if _is_torch(zsrc):
+            import torch
+            zs = _torch_pts(zsrc, d, self.ns, "zsrc")
+            zt = _torch_pts(ztarg, d, self.nt, "ztarg")
+            self.device = zs.device
+            stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
+            check(getattr(lib(), self._fn["create_dev"])(
+                self.eps, self.ns, ctypes.c_void_p(zs.data_ptr()), self.nt,
+                ctypes.c_void_p(zt.data_ptr()), int(isep), stream, ctypes.byref(self._h)))
+        else:
+            self.device = None
+            zs = _pts(zsrc, d, self.ns, "zsrc")
+            zt = _pts(ztarg, d, self.nt, "ztarg")
+            check(getattr(lib(), self._fn["create"])(self.eps, self.ns, _ptr(zs), self.nt,
+                                                     _ptr(zt), int(isep), ctypes.byref(self._h)))
+
+    def info(self):
+        """(nboxes, nlevels) of the plan's tree."""
+        nb, nl, a, b = (ctypes.c_int() for _ in range(4))
+        check(getattr(lib(), self._fn["info"])(self._h, ctypes.byref(nb), ctypes.byref(nl),
+                                               ctypes.byref(a), ctypes.byref(b)))
+        return nb.value, nl.value
+
+    def _solve(self, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh):
+        nd, ns, nt, d = int(nd), self.ns, self.nt, self.D
+        k = None if zk is None else _zk(zk)
+        L = lib()
+        if _is_torch(charge if ifcharge == 1 else dipstr):
+            import torch
+            dev = self.device
+            q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
+            ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
+            dv = _torch_pts(dipvec, d, ns, "dipvec") if ifdipole == 1 else None
+            pot = torch.empty((nt, nd), dtype=torch.complex128, device=dev)
+            grad = torch.empty((nt, d, nd), dtype=torch.complex128, device=dev)
+            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+            p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+            if k is None:
+                check(getattr(L, self._fn["lap_dev"])(self._h, nd, int(ifcharge), p(q),
+                                                      int(ifdipole), p(ds), p(dv), int(ifpgh),
+                                                      p(pot), p(grad), stream))
+            else:
+                check(getattr(L, self._fn["helm_dev"])(self._h, _ptr(k), nd, int(ifcharge), p(q),
+                                                       int(ifdipole), p(ds), p(dv), int(ifpgh),
+                                                       p(pot), p(grad), stream))
+            return pot.t(), grad.permute(2, 1, 0)
+        q = _mat(charge, nd, ns, "charge") if ifcharge == 1 else None
+        ds = _mat(dipstr, nd, ns, "dipstr") if ifdipole == 1 else None
+        dv = _pts(dipvec, d, ns, "dipvec") if ifdipole == 1 else None
+        pot = np.zeros((nd, nt), np.complex128, order="F")
+        grad = np.zeros((nd, d, nt), np.complex128, order="F")
+        if k is None:
+            check(getattr(L, self._fn["lap"])(self._h, nd, int(ifcharge), _ptr(q), int(ifdipole),
+                                              _ptr(ds), _ptr(dv), int(ifpgh), _ptr(pot),
+                                              _ptr(grad)))
+        else:
+            check(getattr(L, self._fn["helm"])(self._h, _ptr(k), nd, int(ifcharge), _ptr(q),
+                                               int(ifdipole), _ptr(ds), _ptr(dv), int(ifpgh),
+                                               _ptr(pot), _ptr(grad)))
+        return pot, grad
+
+    def close(self):
+        if self._h:
+            check(getattr(lib(), self._fn["destroy"])(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan3D(_Plan):
     """Geometry of a 3D complex-coordinate FMM built once and reused.
 
     The octree on the real parts, the sorted and rescaled points, the complex
@@ -298,31 +382,11 @@ class Plan3D:
     views shaped (nd, nt) and (nd, 3, nt) of right-hand-side-fastest storage.
     """
 
-    def __init__(self, eps, ns, zsrc, nt, ztarg, isep=1):
-        self._h = ctypes.c_void_p()
-        self.ns, self.nt, self.eps = int(ns), int(nt), float(eps)
-        if _is_torch(zsrc):
-            import torch
-            zs = _torch_pts(zsrc, 3, self.ns, "zsrc")
-            zt = _torch_pts(ztarg, 3, self.nt, "ztarg")
-            self.device = zs.device
-            stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
-            check(lib().zfmm_plan3d_create_dev(self.eps, self.ns, ctypes.c_void_p(zs.data_ptr()),
-                                               self.nt, ctypes.c_void_p(zt.data_ptr()),
-                                               int(isep), stream, ctypes.byref(self._h)))
-        else:
-            self.device = None
-            zs = _pts(zsrc, 3, self.ns, "zsrc")
-            zt = _pts(ztarg, 3, self.nt, "ztarg")
-            check(lib().zfmm_plan3d_create(self.eps, self.ns, _ptr(zs), self.nt, _ptr(zt),
-                                           int(isep), ctypes.byref(self._h)))
-
-    def info(self):
-        """(nboxes, nlevels) of the plan's tree."""
-        nb, nl, a, b = (ctypes.c_int() for _ in range(4))
-        check(lib().zfmm_plan3d_info(self._h, ctypes.byref(nb), ctypes.byref(nl),
-                                     ctypes.byref(a), ctypes.byref(b)))
-        return nb.value, nl.value
+    D = 3
+    _fn = dict(create="zfmm_plan3d_create", create_dev="zfmm_plan3d_create_dev",
+               info="zfmm_plan3d_info", destroy="zfmm_plan3d_destroy", lap="zfmm_zlfmm3d_plan",
+               lap_dev="zfmm_zlfmm3d_plan_dev", helm="zfmm_zhfmm3d_plan",
+               helm_dev="zfmm_zhfmm3d_plan_dev")
 
     def zlfmm3d(self, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh=1):
         """3D Laplace FMM of nd right-hand sides on the plan's points."""
@@ -332,53 +396,26 @@ class Plan3D:
         """3D Helmholtz FMM (wavenumber zk) of nd right-hand sides on the plan's points."""
         return self._solve(zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh)
 
-    def _solve(self, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh):
-        nd, ns, nt = int(nd), self.ns, self.nt
-        k = None if zk is None else _zk(zk)
-        if _is_torch(charge if ifcharge == 1 else dipstr):
-            import torch
-            dev = self.device
-            q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
-            ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
-            dv = _torch_pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
-            pot = torch.empty((nt, nd), dtype=torch.complex128, device=dev)
-            grad = torch.empty((nt, 3, nd), dtype=torch.complex128, device=dev)
-            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
-            p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
-            if k is None:
-                check(lib().zfmm_zlfmm3d_plan_dev(self._h, nd, int(ifcharge), p(q),
-                                                  int(ifdipole), p(ds), p(dv), int(ifpgh),
-                                                  p(pot), p(grad), stream))
-            else:
-                check(lib().zfmm_zhfmm3d_plan_dev(self._h, _ptr(k), nd, int(ifcharge), p(q),
-                                                  int(ifdipole), p(ds), p(dv), int(ifpgh),
-                                                  p(pot), p(grad), stream))
-            return pot.t(), grad.permute(2, 1, 0)
-        q = _mat(charge, nd, ns, "charge") if ifcharge == 1 else None
-        ds = _mat(dipstr, nd, ns, "dipstr") if ifdipole == 1 else None
-        dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
-        pot = np.zeros((nd, nt), np.complex128, order="F")
-        grad = np.zeros((nd, 3, nt), np.complex128, order="F")
-        if k is None:
-            check(lib().zfmm_zlfmm3d_plan(self._h, nd, int(ifcharge), _ptr(q), int(ifdipole),
-                                          _ptr(ds), _ptr(dv), int(ifpgh), _ptr(pot),
-                                          _ptr(grad)))
-        else:
-            check(lib().zfmm_zhfmm3d_plan(self._h, _ptr(k), nd, int(ifcharge), _ptr(q),
-                                          int(ifdipole), _ptr(ds), _ptr(dv), int(ifpgh),
-                                          _ptr(pot), _ptr(grad)))
-        return pot, grad
 
-    def close(self):
-        if self._h:
-            check(lib().zfmm_plan3d_destroy(self._h))
-            self._h = ctypes.c_void_p()
+class Plan2D(_Plan):
+    """Geometry of a 2D complex-coordinate FMM (quadtree, sorted points,
+    complex centres, lists; zlfmm2d.f:70-200) built once and reused by solves
+    of nd right-hand sides at any wavenumber, as Plan3D with d = 2: charge and
+    dipstr (nd, ns), dipvec (2, ns) shared, pot (nd, nt), grad (nd, 2, nt)."""
 
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
+    D = 2
+    _fn = dict(create="zfmm_plan2d_create", create_dev="zfmm_plan2d_create_dev",
+               info="zfmm_plan2d_info", destroy="zfmm_plan2d_destroy", lap="zfmm_zlfmm2d_plan",
+               lap_dev="zfmm_zlfmm2d_plan_dev", helm="zfmm_zhfmm2d_plan",
+               helm_dev="zfmm_zhfmm2d_plan_dev")
+
+    def zlfmm2d(self, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh=1):
+        """2D Laplace FMM of nd right-hand sides on the plan's points."""
+        return self._solve(None, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh)
+
+    def zhfmm2d(self, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh=1):
+        """2D Helmholtz FMM (wavenumber zk) of nd right-hand sides on the plan's points."""
+        return self._solve(zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh)
 
 
 def _many(eps, zk, instances, ifcharge, ifdipole, ifpgh, isep, nstreams):

@@ -97,6 +97,20 @@ SIGNATURES = {
                                   c_void_p, c_int, c_void_p, c_void_p]),
     "zfmm_zhfmm3d_plan_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
                                       c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "zfmm_plan2d_create": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int,
+                                   ctypes.POINTER(c_void_p)]),
+    "zfmm_plan2d_create_dev": (c_int, [c_double, c_int, c_void_p, c_int, c_void_p, c_int,
+                                       c_void_p, ctypes.POINTER(c_void_p)]),
+    "zfmm_plan2d_destroy": (c_int, [c_void_p]),
+    "zfmm_plan2d_info": (c_int, [c_void_p, c_int_p, c_int_p, c_int_p, c_int_p]),
+    "zfmm_zlfmm2d_plan": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                  c_int, c_void_p, c_void_p]),
+    "zfmm_zlfmm2d_plan_dev": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                      c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "zfmm_zhfmm2d_plan": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                  c_void_p, c_int, c_void_p, c_void_p]),
+    "zfmm_zhfmm2d_plan_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
+                                      c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "zfmm_zlfmm3d_many": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_void_p, c_int,
                                   c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p,
                                   c_void_p, c_int, c_void_p]),

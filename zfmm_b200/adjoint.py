@@ -33,7 +33,8 @@ with zd = dz/da = 1j * disp and zd^T H v = (1/4)[zd- v- D+D+u
 + (zd- v+ + zd+ v-) Du + zd+ v+ D-D-u], x+- = x1 +- i x2, Du = -zk^2 u.  The
 target-motion term uses the forward's gradient, so the forward runs with
 ifpgh = 2 when a requires a gradient.  The backward costs two FMMs with dipole
-sources (about twice a forward solve).
+sources (about twice a forward solve); the forward and both backward solves
+run on one 2D plan (one tree build).
 
 direct=True evaluates every sum above by the FP64 direct sum (zh2devaldirect)
 instead of the FMM: the reference gradient of the tests (small n only).
@@ -41,7 +42,7 @@ instead of the FMM: the reference gradient of the tests (small n only).
 import numpy as np
 import torch
 
-from . import _fmm2d_torch, zh2devaldirect
+from . import Plan2D, zh2devaldirect
 
 __all__ = ["zhfmm2d_curves", "points"]
 
@@ -51,14 +52,16 @@ def points(xr, disp, curve, a):
     return xr.to(torch.complex128) + 1j * (a[curve].unsqueeze(1) * disp).to(torch.complex128)
 
 
-def _eval(eps, zk, src, q, ds, dv, tgt, ifpgh, direct):
+def _eval(plan, zk, src, q, ds, dv, tgt, ifpgh, direct):
     """pot (nt,) and grad (2, nt) of sources src (n, 2) at targets tgt (nt, 2),
-    scaled as zhfmm2d (i/4 included)."""
+    scaled as zhfmm2d (i/4 included); through the plan on src (the forward and
+    both backward solves share one tree) unless direct."""
     n, nt = src.shape[0], tgt.shape[0]
     ifc = 1 if q is not None else 0
     ifd = 1 if ds is not None else 0
     if not direct:
-        return _fmm2d_torch(eps, zk, n, src, ifc, q, ifd, ds, dv, nt, tgt, ifpgh, 1)
+        pot, grad = plan.zhfmm2d(zk, 1, ifc, q, ifd, ds, dv, ifpgh)
+        return pot[0], grad[0]
     c = lambda t: None if t is None else t.detach().cpu().numpy()
     zs = c(src).T
     zt = c(tgt).T
@@ -74,10 +77,12 @@ class _Curves(torch.autograd.Function):
     def forward(ctx, charge, dipstr, a, xr, disp, curve, dipvec, eps, zk, direct):
         z = points(xr, disp, curve, a)
         need_g = a.requires_grad
-        pot, grad = _eval(eps, zk, z, charge, dipstr, dipvec, z, 2 if need_g else 1, direct)
+        plan = None if direct else Plan2D(eps, z.shape[0], z, z.shape[0], z)
+        pot, grad = _eval(plan, zk, z, charge, dipstr, dipvec, z, 2 if need_g else 1, direct)
         ctx.save_for_backward(charge, dipstr, a, xr, disp, curve, dipvec, z,
                               grad if need_g else torch.empty(0))
         ctx.cfg = (eps, zk, direct, charge is not None, dipstr is not None)
+        ctx.plan = plan
         return pot
 
     @staticmethod
@@ -92,8 +97,9 @@ class _Curves(torch.autograd.Function):
         ep[:, 0] = 1.0
         ep[:, 1] = 1j
         em = torch.conj_physical(ep)
-        Fp, Gp = _eval(eps, zk, z, None, w, ep, z, 2, direct)
-        Fm, Gm = _eval(eps, zk, z, None, w, em, z, 2, direct)
+        Fp, Gp = _eval(ctx.plan, zk, z, None, w, ep, z, 2, direct)
+        Fm, Gm = _eval(ctx.plan, zk, z, None, w, em, z, 2, direct)
+        ctx.plan = None
         dpdp = Gp[0] + 1j * Gp[1]
         dmdm = Gm[0] - 1j * Gm[1]
         lap = 0.5 * ((Gp[0] - 1j * Gp[1]) + (Gm[0] + 1j * Gm[1]))

@@ -17,6 +17,7 @@
 #include "lfmm2d.cuh"
 #include "lfmm3d.cuh"
 #include "hfmm3d.cuh"
+#include "plan2d.cuh"
 #include "plan3d.cuh"
 
 using namespace zf;
@@ -1173,6 +1174,189 @@ int zfmm_zhfmm3d_many_dev(int ninst, double eps, const double* zk, const int* ns
   ManyArgs M{ninst, eps, &k, ns, nt, zsrc, charge, dipstr, dipvec, ztarg, pot, grad,
              ifcharge, ifdipole, ifpgh, isep, false};
   return many_impl(M, nstreams, done_ms);
+}
+
+}  // extern "C"
+
+// ---- 2D plans ----------------------------------------------------------------
+struct zfmm_plan2d_s {
+  zf::Plan2D P;
+};
+
+namespace {
+
+int plan2d_create_impl(double eps, int ns, const double* zsrc, int nt, const double* ztarg,
+                       int isep, bool host, cudaStream_t s, zfmm_plan2d_s** out) {
+  return guarded([&] {
+    if (!out) throw zf_error(ZF_ERR_ARG, "null plan output");
+    *out = nullptr;
+    if (ns < 0 || nt < 0) throw zf_error(ZF_ERR_ARG, "ns and nt must be >= 0");
+    if ((ns > 0 && !zsrc) || (nt > 0 && !ztarg))
+      throw zf_error(ZF_ERR_ARG, "null coordinate array");
+    if (isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
+    check_device();
+    auto* pl = new zfmm_plan2d_s();
+    try {
+      HostIn h;
+      const zdc* zs = reinterpret_cast<const zdc*>(zsrc);
+      const zdc* zt = reinterpret_cast<const zdc*>(ztarg);
+      if (host) {
+        upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
+        upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
+        zs = h.zsrc.get();
+        zt = h.ztarg.get();
+      }
+      if (ns > 0 && nt > 0) plan2d_build(pl->P, eps, ns, zs, nt, zt, isep, s);
+      else {
+        pl->P.eps = eps;
+        pl->P.isep = isep;
+        pl->P.ns = ns;
+        pl->P.nt = nt;
+        ZF_CUDA(cudaGetDevice(&pl->P.device));
+      }
+      ZF_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+      delete pl;
+      throw;
+    }
+    *out = pl;
+  });
+}
+
+void check_plan2d_args(zfmm_plan2d_s* plan, int nd, int ifcharge, const double* charge,
+                       int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
+                       double* pot, double* grad) {
+  if (!plan) throw zf_error(ZF_ERR_ARG, "plan is null");
+  if (nd < 1) throw zf_error(ZF_ERR_ARG, "nd must be >= 1");
+  const Plan2D& P = plan->P;
+  if (P.ns > 0 && ifcharge == 1 && !charge) throw zf_error(ZF_ERR_ARG, "ifcharge=1 needs charge");
+  if (P.ns > 0 && ifdipole == 1 && (!dipstr || !dipvec))
+    throw zf_error(ZF_ERR_ARG, "ifdipole=1 needs dipstr and dipvec");
+  if (P.nt > 0 && !pot) throw zf_error(ZF_ERR_ARG, "null pot");
+  if (P.nt > 0 && ifpgh > 1 && !grad) throw zf_error(ZF_ERR_ARG, "ifpgh=2 needs grad");
+  int dev = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  if (dev != P.device) throw zf_error(ZF_ERR_ARG, "plan was built on another device");
+}
+
+void run_plan2d(zfmm_plan2d_s* plan, const zdc* zk, int nd, int ifcharge, const zdc* charge,
+                int ifdipole, const zdc* dipstr, const zdc* dipvec, int ifpgh, zdc* pot,
+                zdc* grad, cudaStream_t s) {
+  const Plan2D& P = plan->P;
+  if (P.nt > 0) {
+    ZF_CUDA(cudaMemsetAsync(pot, 0, sizeof(zdc) * P.nt * (size_t)nd, s));
+    if (ifpgh > 1) ZF_CUDA(cudaMemsetAsync(grad, 0, sizeof(zdc) * 2 * P.nt * (size_t)nd, s));
+  }
+  if (P.ns == 0 || P.nt == 0) return;
+  StepTimes t;
+  t.want_counts = g_timing >= 2;
+  fmm2d_plan_execute(P, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot,
+                     ifpgh > 1 ? grad : nullptr, s, g_timing ? &t : nullptr);
+  if (g_timing) g_times = t;
+}
+
+int plan2d_solve(zfmm_plan2d plan, const double* zk, int nd, int ifcharge, const double* charge,
+                 int ifdipole, const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                 double* grad, bool host, void* stream) {
+  return guarded([&] {
+    clamp_flags(ifcharge, ifdipole, ifpgh);
+    check_plan2d_args(plan, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot, grad);
+    zdc k = zk ? mkz(zk[0], zk[1]) : mkz(0.0);
+    const zdc* kp = zk ? &k : nullptr;
+    if (!host) {
+      cudaStream_t s = (cudaStream_t)stream;
+      run_plan2d(plan, kp, nd, ifcharge, (const zdc*)charge, ifdipole, (const zdc*)dipstr,
+                 (const zdc*)dipvec, ifpgh, (zdc*)pot, (zdc*)grad, s);
+      ZF_CUDA(cudaStreamSynchronize(s));
+      return;
+    }
+    const int ns = plan->P.ns, nt = plan->P.nt;
+    cudaStream_t s = cudaStreamPerThread;
+    HostIn h;
+    if (ifcharge == 1) upload(h.charge, charge, (size_t)nd * ns, s);
+    if (ifdipole == 1) {
+      upload(h.dipstr, dipstr, (size_t)nd * ns, s);
+      upload(h.dipvec, dipvec, 2 * (size_t)ns, s);
+    }
+    DevBuf<zdc> dpot((size_t)nd * nt, s), dgrad(ifpgh > 1 ? 2 * (size_t)nd * nt : 0, s);
+    run_plan2d(plan, kp, nd, ifcharge, h.charge.get(), ifdipole, h.dipstr.get(),
+               h.dipvec.get(), ifpgh, dpot.get(), dgrad.get(), s);
+    if (nt > 0) {
+      ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt * (size_t)nd,
+                              cudaMemcpyDeviceToHost, s));
+      if (grad) {
+        if (ifpgh > 1)
+          ZF_CUDA(cudaMemcpyAsync(grad, dgrad.get(), sizeof(zdc) * 2 * nt * (size_t)nd,
+                                  cudaMemcpyDeviceToHost, s));
+        else
+          memset(grad, 0, sizeof(zdc) * 2 * nt * (size_t)nd);
+      }
+    }
+    ZF_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int zfmm_plan2d_create(double eps, int ns, const double* zsrc, int nt, const double* ztarg,
+                       int isep, zfmm_plan2d* plan) {
+  return plan2d_create_impl(eps, ns, zsrc, nt, ztarg, isep, true, cudaStreamPerThread, plan);
+}
+
+int zfmm_plan2d_create_dev(double eps, int ns, const double* zsrc, int nt, const double* ztarg,
+                           int isep, void* stream, zfmm_plan2d* plan) {
+  return plan2d_create_impl(eps, ns, zsrc, nt, ztarg, isep, false, (cudaStream_t)stream, plan);
+}
+
+int zfmm_plan2d_destroy(zfmm_plan2d plan) {
+  return guarded([&] {
+    if (!plan) return;
+    ZF_CUDA(cudaDeviceSynchronize());
+    delete plan;
+  });
+}
+
+int zfmm_plan2d_info(zfmm_plan2d plan, int* nboxes, int* nlevels, int* ns, int* nt) {
+  return guarded([&] {
+    if (!plan) throw zf_error(ZF_ERR_ARG, "plan is null");
+    if (nboxes) *nboxes = plan->P.S.tree.nboxes;
+    if (nlevels) *nlevels = plan->P.S.tree.nlevels;
+    if (ns) *ns = plan->P.ns;
+    if (nt) *nt = plan->P.nt;
+  });
+}
+
+int zfmm_zlfmm2d_plan(zfmm_plan2d plan, int nd, int ifcharge, const double* charge,
+                      int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
+                      double* pot, double* grad) {
+  return plan2d_solve(plan, nullptr, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot,
+                      grad, true, nullptr);
+}
+
+int zfmm_zlfmm2d_plan_dev(zfmm_plan2d plan, int nd, int ifcharge, const double* charge,
+                          int ifdipole, const double* dipstr, const double* dipvec, int ifpgh,
+                          double* pot, double* grad, void* stream) {
+  return plan2d_solve(plan, nullptr, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot,
+                      grad, false, stream);
+}
+
+int zfmm_zhfmm2d_plan(zfmm_plan2d plan, const double* zk, int nd, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr,
+                      const double* dipvec, int ifpgh, double* pot, double* grad) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  return plan2d_solve(plan, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot, grad,
+                      true, nullptr);
+}
+
+int zfmm_zhfmm2d_plan_dev(zfmm_plan2d plan, const double* zk, int nd, int ifcharge,
+                          const double* charge, int ifdipole, const double* dipstr,
+                          const double* dipvec, int ifpgh, double* pot, double* grad,
+                          void* stream) {
+  if (!zk) return fail(ZF_ERR_ARG, "zk is null");
+  return plan2d_solve(plan, zk, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot, grad,
+                      false, stream);
 }
 
 }  // extern "C"

@@ -110,6 +110,34 @@ __global__ void k_unsort(int nt, const int* __restrict__ perm, const zdc* __rest
   }
 }
 
+// right-hand side r of charge(nd, ns) / dipstr(nd, ns) in tree order; dipvec
+// (2, ns) shared by the right-hand sides
+__global__ void k_gather_col2(int ns, int nd, int r, const int* __restrict__ perm,
+                              const zdc* __restrict__ q, const zdc* __restrict__ ds,
+                              const zdc* __restrict__ dv, zdc* qs, zdc* dss, zdc* dvs) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  long j = perm[i];
+  qs[i] = q ? q[j * nd + r] : mkz(0.0);
+  dss[i] = ds ? ds[j * nd + r] : mkz(0.0);
+  dvs[2 * i] = dv ? dv[2 * j] : mkz(0.0);
+  dvs[2 * i + 1] = dv ? dv[2 * j + 1] : mkz(0.0);
+}
+
+// right-hand side r of pot(nd, nt) / grad(nd, 2, nt)
+__global__ void k_unsort_col2(int nt, int nd, int r, const int* __restrict__ perm,
+                              const zdc* __restrict__ ps, const zdc* __restrict__ gs, zdc scale,
+                              int ifpgh, zdc* pot, zdc* grad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt) return;
+  long j = perm[i];
+  pot[j * nd + r] = ps[i] * scale;
+  if (ifpgh > 1) {
+    grad[(2 * j) * nd + r] = gs[2 * i] * scale;
+    grad[(2 * j + 1) * nd + r] = gs[2 * i + 1] * scale;
+  }
+}
+
 // one thread per box; the same conditions as the eight steps of the drivers
 __global__ void k_count(int nb, const int* ilevel, const int* iparent, const int* nchild,
                         const int* ichild, const int* isrcse, const int* itargse, const int* nl1,
@@ -205,6 +233,42 @@ void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t 
   complex_centres(S.tree, S.isrcse, S.zsrcsort, S.zcsrc, s);
   complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
   build_lists(S.tree, S.lists, s);
+}
+
+void setup2d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
+                  Setup2D& S, cudaStream_t s) {
+  DevBuf<double> srcR(2 * (size_t)ns, s), targR(2 * (size_t)nt, s);
+  klaunch(k_real_parts, div_up(2L * ns, TB), TB, 0, s, zsrc, 2L * ns, srcR.get());
+  klaunch(k_real_parts, div_up(2L * nt, TB), TB, 0, s, ztarg, 2L * nt, targR.get());
+  ZF_LAUNCH_CHECK();
+  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
+  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  S.zsrcsort.alloc(2 * (size_t)ns, s);
+  S.ztargsort.alloc(2 * (size_t)nt, s);
+  klaunch(k_gather_targ, div_up(ns, TB), TB, 0, s, ns, S.isrc.get(), zsrc, S.zsrcsort.get());
+  klaunch(k_gather_targ, div_up(nt, TB), TB, 0, s, nt, S.itarg.get(), ztarg, S.ztargsort.get());
+  ZF_LAUNCH_CHECK();
+  complex_centres(S.tree, S.isrcse, S.zsrcsort, S.zcsrc, s);
+  complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
+  build_lists(S.tree, S.lists, s);
+}
+
+void gather2d_col(const Setup2D& S, int ns, int nd, int r, const zdc* charge, const zdc* dipstr,
+                  const zdc* dipvec, zdc* q, zdc* ds, zdc* dv, cudaStream_t s) {
+  if (ns <= 0) return;
+  klaunch(k_gather_col2, div_up(ns, TB), TB, 0, s, ns, nd, r, S.isrc.get(), charge, dipstr,
+          dipvec, q, ds, dv);
+  ZF_LAUNCH_CHECK();
+}
+
+void unsort2d_col(int nt, int nd, int r, const int* itarg, const zdc* potsort,
+                  const zdc* gradsort, zdc scale, int ifpgh, zdc* pot, zdc* grad,
+                  cudaStream_t s) {
+  if (nt <= 0) return;
+  klaunch(k_unsort_col2, div_up(nt, TB), TB, 0, s, nt, nd, r, itarg, potsort, gradsort, scale,
+          ifpgh, pot, grad);
+  ZF_LAUNCH_CHECK();
 }
 
 void unsort2d(int nt, const int* itarg, const zdc* potsort, const zdc* gradsort, zdc scale,

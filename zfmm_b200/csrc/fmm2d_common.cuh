@@ -35,6 +35,22 @@ struct Setup2D {
 // builds everything above for the given tree parameters (ndiv, idivflag, isep)
 void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t s);
 
+// the geometric part of setup2d only (tree, sort, sorted points, complex
+// centres, lists); the strength arrays of S stay empty
+void setup2d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
+                  Setup2D& S, cudaStream_t s);
+
+// right-hand side r of charge(nd, ns), dipstr(nd, ns) (right-hand side fastest)
+// and the shared dipvec(2, ns) into tree order; null inputs give zeros
+void gather2d_col(const Setup2D& S, int ns, int nd, int r, const zdc* charge, const zdc* dipstr,
+                  const zdc* dipvec, zdc* q, zdc* ds, zdc* dv, cudaStream_t s);
+
+// right-hand side r of pot(nd, nt) / grad(nd, 2, nt) from sorted potsort /
+// gradsort, times `scale`
+void unsort2d_col(int nt, int nd, int r, const int* itarg, const zdc* potsort,
+                  const zdc* gradsort, zdc scale, int ifpgh, zdc* pot, zdc* grad,
+                  cudaStream_t s);
+
 // interaction counts of the FMM on this tree (host array of 16): [P2P pairs,
 // M2T (target, box), L2T targets, M2L box pairs, P2L (box, source), M2M pairs,
 // L2L pairs, P2M sources], then the same weighted by the expansion lengths

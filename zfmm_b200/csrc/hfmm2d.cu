@@ -765,25 +765,16 @@ int h2dterms_host(double bsize, zdc zk, double eps, int isep) {
   return n;
 }
 
-void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
-                    cudaStream_t s, StepTimes* times) {
-  int ns = in.ns, nt = in.nt;
-  long launches0 = launch_counter();
-  cudaEvent_t ev[8];
-  bool timing = times != nullptr;
-  if (timing)
-    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
-  auto mark = [&](int i) {
-    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+// the passes after the set-up for one right-hand side with sorted strengths
+// q, ds, dv on a set-up S: writes the sorted, unscaled potentials / gradients
+// into potsort / gradsort (zeroed by the caller); ev (optional) gets the step
+// boundaries 2..5; *pl (optional) receives the order of every level
+int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, const zdc* ds, const zdc* dv, int ifcharge, int ifdipole, int ifpgh,
+         zdc* potsort, zdc* gradsort, cudaStream_t s, cudaEvent_t* ev,
+         std::vector<int>* pl) {
+  auto cmark = [&](int i) {
+    if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
   };
-  mark(0);
-  TreeParams tp;
-  tp.D = 2;
-  tp.isep = isep;
-  lndiv2d(eps, ns, nt, &tp.ndiv, &tp.idivflag);  // hndiv2d.f: same table
-  Setup2D S;
-  setup2d(in, tp, S, s);
-  mark(1);
   const DevTree& t = S.tree;
   int nb = t.nboxes, nlev = t.nlevels;
   if (nlev + 1 > MAXL) throw zf_error(ZF_ERR_ARG, "too many tree levels");
@@ -805,15 +796,15 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
     tot += (long)(t.laddr[2 * l + 1] - t.laddr[2 * l] + 1) * (2 * A.T.p[l] + 1);
     if (A.T.p[l] > pmax) pmax = A.T.p[l];
   }
-  DevBuf<zdc> mp(tot, s), loc(tot, s), potsort(nt, s), gradsort(in.ifpgh > 1 ? 2 * (size_t)nt : 1, s);
+  DevBuf<zdc> mp(tot, s), loc(tot, s);
   mp.zero();
   loc.zero();
   A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
   A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
-  A.zsrc = S.zsrcsort.get(); A.charge = S.chargesort.get(); A.dipstr = S.dipstrsort.get();
-  A.dipvec = S.dipvecsort.get(); A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
+  A.zsrc = S.zsrcsort.get(); A.charge = q; A.dipstr = ds;
+  A.dipvec = dv; A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
   A.zctarg = S.zctarg.get(); A.mp = mp.get(); A.loc = loc.get();
-  A.ifcharge = in.ifcharge; A.ifdipole = in.ifdipole;
+  A.ifcharge = ifcharge; A.ifdipole = ifdipole;
   const DevLists& L = S.lists;
   int grid_all = div_up(nb, WPB);
   // shared-memory strides (complex elements per warp)
@@ -832,7 +823,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
     klaunch(k_hp2m, div_up(hi - lo + 1, WPB), 32 * WPB, sm_p2m, s, lo, hi, A, pl);
   }
   ZF_LAUNCH_CHECK();
-  mark(2);
+  cmark(2);
   for (int l = nlev - 1; l >= 2; l--) {
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
     int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l + 1]);
@@ -841,7 +832,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
     klaunch(k_hm2m, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, l, A, stride);
   }
   ZF_LAUNCH_CHECK();
-  mark(3);
+  cmark(3);
   // one launch per level (lists 2 and 4 are empty on levels 0 and 1): the
   // shared-memory stride and the register slots follow the level's order, so
   // the many fine-level boxes run at full occupancy
@@ -873,7 +864,7 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
               L.list[3].get(), L.mn[3], stride);
     }
   ZF_LAUNCH_CHECK();
-  mark(4);
+  cmark(4);
   for (int l = 2; l <= nlev - 1; l++) {
     int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
     int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l]);
@@ -883,14 +874,44 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
             L.n[3].get(), stride);
   }
   ZF_LAUNCH_CHECK();
-  mark(5);
-  if (in.ifpgh > 1)
+  cmark(5);
+  if (ifpgh > 1)
     klaunch(k_heval<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-            L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort.get(), gradsort.get());
+            L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort, gradsort);
   else
     klaunch(k_heval<false>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-            L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort.get(), gradsort.get());
+            L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort, gradsort);
   ZF_LAUNCH_CHECK();
+  if (pl) *pl = std::vector<int>(A.T.p, A.T.p + nlev + 1);
+  return pmax;
+}
+
+void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
+                    cudaStream_t s, StepTimes* times) {
+  int ns = in.ns, nt = in.nt;
+  long launches0 = launch_counter();
+  cudaEvent_t ev[8];
+  bool timing = times != nullptr;
+  if (timing)
+    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  auto mark = [&](int i) {
+    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  mark(0);
+  TreeParams tp;
+  tp.D = 2;
+  tp.isep = isep;
+  lndiv2d(eps, ns, nt, &tp.ndiv, &tp.idivflag);  // hndiv2d.f: same table
+  Setup2D S;
+  setup2d(in, tp, S, s);
+  mark(1);
+  std::vector<int> plv;
+  DevBuf<zdc> potsort(nt, s), gradsort(in.ifpgh > 1 ? 2 * (size_t)nt : 1, s);
+  potsort.zero();
+  gradsort.zero();
+  const int pord = helm2d_core(S, eps, zk, isep, S.chargesort.get(), S.dipstrsort.get(),
+      S.dipvecsort.get(), in.ifcharge, in.ifdipole, in.ifpgh, potsort.get(), gradsort.get(), s,
+      timing ? ev : nullptr, &plv);
   mark(6);
   unsort2d(nt, S.itarg.get(), potsort.get(), gradsort.get(), mkz(0.0, 0.25), in.ifpgh, pot, grad,
            s);
@@ -902,15 +923,14 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
       ZF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
       times->ms[i] = ms;
     }
-    times->nboxes = nb;
-    times->nlevels = nlev;
-    times->nterms = pmax;
+    times->nboxes = S.tree.nboxes;
+    times->nlevels = S.tree.nlevels;
+    times->nterms = pord;
     for (auto& e : ev) cudaEventDestroy(e);
     times->launches = launch_counter() - launches0;
   }
   if (timing && times->want_counts) {
-    std::vector<int> pl(A.T.p, A.T.p + nlev + 1);
-    count_interactions2d(S, pl.data(), times->counts, s);
+    count_interactions2d(S, plv.data(), times->counts, s);
   }
 }
 

@@ -12,6 +12,12 @@ int h2dterms_host(double bsize, zdc zk, double eps, int isep);
 void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
                     cudaStream_t s, StepTimes* times);
 
+// the passes of zhfmm2d after the set-up, as lap2d_core (orders from
+// h2dterms for zk on the set-up's tree)
+int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, const zdc* ds,
+                const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* potsort,
+                zdc* gradsort, cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl);
+
 // zh2devaldirect over all pairs: ADDS the unscaled sums (no i/4) into pot/grad
 void zh2ddirect_device(zdc zk, const Inputs2D& in, zdc* pot, zdc* grad, cudaStream_t s);
 

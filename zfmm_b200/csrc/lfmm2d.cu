@@ -473,6 +473,86 @@ void lndiv2d(double eps, int ns, int nt, int* ndiv, int* idivflag) {
   else *ndiv = ns + nt;
 }
 
+// the passes after the set-up for one right-hand side with sorted strengths
+// q, ds, dv on a set-up S: writes the sorted, unscaled potentials / gradients
+// into potsort / gradsort (zeroed by the caller); ev (optional) gets the step
+// boundaries 2..5; *pl (optional) receives the order of every level
+int lap2d_core(const Setup2D& S, double eps, const zdc* q, const zdc* ds, const zdc* dv, int ifcharge, int ifdipole, int ifpgh,
+         zdc* potsort, zdc* gradsort, cudaStream_t s, cudaEvent_t* ev,
+         std::vector<int>* pl) {
+  auto cmark = [&](int i) {
+    if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  const DevTree& t = S.tree;
+  int nb = t.nboxes, nlev = t.nlevels;
+  int p = l2dterms(eps);
+  if (p > 32 * MAXR) throw zf_error(ZF_ERR_ARG, "expansion order too large");
+  int P = 2 * p + 1, ldc = 2 * p;
+  std::vector<double> carr((size_t)(ldc + 1) * (ldc + 1), 0.0);
+  for (int l = 0; l <= ldc; l++) carr[(size_t)l * (ldc + 1)] = 1.0;
+  for (int m = 1; m <= ldc; m++) {
+    carr[(size_t)m * (ldc + 1) + m] = 1.0;
+    for (int l = m + 1; l <= ldc; l++)
+      carr[(size_t)l * (ldc + 1) + m] =
+          carr[(size_t)(l - 1) * (ldc + 1) + m] + carr[(size_t)(l - 1) * (ldc + 1) + m - 1];
+  }
+  DevBuf<double> d_carr(carr.size(), s), d_rsc(nlev + 1, s);
+  ZF_CUDA(cudaMemcpyAsync(d_carr.get(), carr.data(), carr.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaMemcpyAsync(d_rsc.get(), t.boxsize.data(), (nlev + 1) * sizeof(double),
+                          cudaMemcpyHostToDevice, s));
+  DevBuf<zdc> mp((size_t)nb * P, s), loc((size_t)nb * P, s);
+  mp.zero();
+  loc.zero();
+  LapArgs A;
+  A.p = p; A.P = P; A.carray = d_carr.get(); A.ldc1 = ldc + 1; A.rsc = d_rsc.get();
+  A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
+  A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
+  A.zsrc = S.zsrcsort.get(); A.charge = q; A.dipstr = ds;
+  A.dipvec = dv; A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
+  A.zctarg = S.zctarg.get(); A.mp = mp.get(); A.loc = loc.get();
+  A.ifcharge = ifcharge; A.ifdipole = ifdipole;
+  size_t smem = (size_t)WPB * 4 * (p + 1) * sizeof(zdc);
+  int grid_all = div_up(nb, WPB);
+  const DevLists& L = S.lists;
+  // step 1
+  klaunch(k_p2m, grid_all, 32 * WPB, 0, s, nb, A);
+  ZF_LAUNCH_CHECK();
+  cmark(2);
+  // step 2
+  for (int l = nlev - 1; l >= 1; l--) {
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    klaunch(k_m2m, div_up(hi - lo + 1, WPB), 32 * WPB, smem, s, lo, hi, l, A);
+  }
+  ZF_LAUNCH_CHECK();
+  cmark(3);
+  // steps 4 + 6
+  klaunch(k_m2l_p2l, grid_all, 32 * WPB, smem, s, nb, A, L.n[1].get(), L.list[1].get(), L.mn[1],
+                                             L.n[3].get(), L.list[3].get(), L.mn[3]);
+  ZF_LAUNCH_CHECK();
+  cmark(4);
+  // step 7
+  for (int l = 1; l <= nlev - 1; l++) {
+    int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
+    klaunch(k_l2l, div_up(hi - lo + 1, WPB), 32 * WPB, smem, s, lo, hi, l, A, L.n[1].get(),
+                                                           L.n[3].get());
+  }
+  ZF_LAUNCH_CHECK();
+  cmark(5);
+  // steps 3, 5, 8
+  if (ifpgh > 1)
+    klaunch(k_eval<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(), L.mn[0],
+                                               L.n[2].get(), L.list[2].get(), L.mn[2],
+                                               potsort, gradsort);
+  else
+    klaunch(k_eval<false>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(), L.mn[0],
+                                                L.n[2].get(), L.list[2].get(), L.mn[2],
+                                                potsort, gradsort);
+  ZF_LAUNCH_CHECK();
+  if (pl) *pl = std::vector<int>(nlev + 1, p);
+  return p;
+}
+
 void zlfmm2d_device(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
                     cudaStream_t s, StepTimes* times) {
   int ns = in.ns, nt = in.nt;
@@ -492,75 +572,13 @@ void zlfmm2d_device(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* gra
   Setup2D S;
   setup2d(in, tp, S, s);
   mark(1);
-  const DevTree& t = S.tree;
-  int nb = t.nboxes, nlev = t.nlevels;
-  int p = l2dterms(eps);
-  if (p > 32 * MAXR) throw zf_error(ZF_ERR_ARG, "expansion order too large");
-  int P = 2 * p + 1, ldc = 2 * p;
-  std::vector<double> carr((size_t)(ldc + 1) * (ldc + 1), 0.0);
-  for (int l = 0; l <= ldc; l++) carr[(size_t)l * (ldc + 1)] = 1.0;
-  for (int m = 1; m <= ldc; m++) {
-    carr[(size_t)m * (ldc + 1) + m] = 1.0;
-    for (int l = m + 1; l <= ldc; l++)
-      carr[(size_t)l * (ldc + 1) + m] =
-          carr[(size_t)(l - 1) * (ldc + 1) + m] + carr[(size_t)(l - 1) * (ldc + 1) + m - 1];
-  }
-  DevBuf<double> d_carr(carr.size(), s), d_rsc(nlev + 1, s);
-  ZF_CUDA(cudaMemcpyAsync(d_carr.get(), carr.data(), carr.size() * sizeof(double),
-                          cudaMemcpyHostToDevice, s));
-  ZF_CUDA(cudaMemcpyAsync(d_rsc.get(), t.boxsize.data(), (nlev + 1) * sizeof(double),
-                          cudaMemcpyHostToDevice, s));
-  DevBuf<zdc> mp((size_t)nb * P, s), loc((size_t)nb * P, s), potsort(nt, s),
-      gradsort(in.ifpgh > 1 ? 2 * (size_t)nt : 1, s);
-  mp.zero();
-  loc.zero();
+  std::vector<int> plv;
+  DevBuf<zdc> potsort(nt, s), gradsort(in.ifpgh > 1 ? 2 * (size_t)nt : 1, s);
   potsort.zero();
   gradsort.zero();
-  LapArgs A;
-  A.p = p; A.P = P; A.carray = d_carr.get(); A.ldc1 = ldc + 1; A.rsc = d_rsc.get();
-  A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
-  A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
-  A.zsrc = S.zsrcsort.get(); A.charge = S.chargesort.get(); A.dipstr = S.dipstrsort.get();
-  A.dipvec = S.dipvecsort.get(); A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
-  A.zctarg = S.zctarg.get(); A.mp = mp.get(); A.loc = loc.get();
-  A.ifcharge = in.ifcharge; A.ifdipole = in.ifdipole;
-  size_t smem = (size_t)WPB * 4 * (p + 1) * sizeof(zdc);
-  int grid_all = div_up(nb, WPB);
-  const DevLists& L = S.lists;
-  // step 1
-  klaunch(k_p2m, grid_all, 32 * WPB, 0, s, nb, A);
-  ZF_LAUNCH_CHECK();
-  mark(2);
-  // step 2
-  for (int l = nlev - 1; l >= 1; l--) {
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
-    klaunch(k_m2m, div_up(hi - lo + 1, WPB), 32 * WPB, smem, s, lo, hi, l, A);
-  }
-  ZF_LAUNCH_CHECK();
-  mark(3);
-  // steps 4 + 6
-  klaunch(k_m2l_p2l, grid_all, 32 * WPB, smem, s, nb, A, L.n[1].get(), L.list[1].get(), L.mn[1],
-                                             L.n[3].get(), L.list[3].get(), L.mn[3]);
-  ZF_LAUNCH_CHECK();
-  mark(4);
-  // step 7
-  for (int l = 1; l <= nlev - 1; l++) {
-    int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
-    klaunch(k_l2l, div_up(hi - lo + 1, WPB), 32 * WPB, smem, s, lo, hi, l, A, L.n[1].get(),
-                                                           L.n[3].get());
-  }
-  ZF_LAUNCH_CHECK();
-  mark(5);
-  // steps 3, 5, 8
-  if (in.ifpgh > 1)
-    klaunch(k_eval<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(), L.mn[0],
-                                               L.n[2].get(), L.list[2].get(), L.mn[2],
-                                               potsort.get(), gradsort.get());
-  else
-    klaunch(k_eval<false>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(), L.mn[0],
-                                                L.n[2].get(), L.list[2].get(), L.mn[2],
-                                                potsort.get(), gradsort.get());
-  ZF_LAUNCH_CHECK();
+  const int pord = lap2d_core(S, eps, S.chargesort.get(), S.dipstrsort.get(),
+      S.dipvecsort.get(), in.ifcharge, in.ifdipole, in.ifpgh, potsort.get(), gradsort.get(), s,
+      timing ? ev : nullptr, &plv);
   mark(6);
   unsort2d(nt, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0 / (2.0 * M_PI)), in.ifpgh,
            pot, grad, s);
@@ -572,15 +590,14 @@ void zlfmm2d_device(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* gra
       ZF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
       times->ms[i] = ms;
     }
-    times->nboxes = nb;
-    times->nlevels = nlev;
-    times->nterms = p;
+    times->nboxes = S.tree.nboxes;
+    times->nlevels = S.tree.nlevels;
+    times->nterms = pord;
     for (auto& e : ev) cudaEventDestroy(e);
     times->launches = launch_counter() - launches0;
   }
   if (timing && times->want_counts) {
-    std::vector<int> pl(nlev + 1, p);
-    count_interactions2d(S, pl.data(), times->counts, s);
+    count_interactions2d(S, plv.data(), times->counts, s);
   }
 }
 

@@ -28,6 +28,15 @@ void lndiv2d(double eps, int ns, int nt, int* ndiv, int* idivflag);
 void zlfmm2d_device(double eps, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
                     cudaStream_t s, StepTimes* times);
 
+// the passes of zlfmm2d after the set-up for one right-hand side with sorted
+// strengths q, ds, dv(2 ns) on set-up S: writes the sorted, unscaled
+// potentials / gradients into potsort / gradsort (zeroed by the caller); ev
+// (optional, 8 events) gets the step boundaries 2..5; *pl (optional) the
+// order of every level; returns the order
+int lap2d_core(const Setup2D& S, double eps, const zdc* q, const zdc* ds, const zdc* dv,
+               int ifcharge, int ifdipole, int ifpgh, zdc* potsort, zdc* gradsort,
+               cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl);
+
 // zl2devaldirect over all pairs: ADDS the unscaled sums into pot/grad, as the
 // reference routine does.  `scratch` may be null (the routine then takes its
 // own pool memory) or point to at least direct2d_scratch_elems(nt, ifpgh)
