@@ -597,7 +597,17 @@ def run_ours_batched(args, wl, ws, rank, local):
         torch.cuda.synchronize()
     launches = L.zfmm_launch_count() - launches0
     tot_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
-    # the plain single-right-hand-side solve on the same geometry, same run
+    # the plan build alone (tree, lists, centres), and the plain
+    # single-right-hand-side solve on the same geometry, same run
+    pc0, pc1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hh = ctypes.c_void_p()
+    torch.cuda.synchronize()
+    pc0.record(stream)
+    _capi.check(L.zfmm_plan3d_create_dev(eps, n, P(zs), n, P(zs), isep, sp, ctypes.byref(hh)))
+    pc1.record(stream)
+    torch.cuda.synchronize()
+    plan_ms = pc0.elapsed_time(pc1)
+    _capi.check(L.zfmm_plan3d_destroy(hh))
     for _ in range(2):
         solve_plain()
     torch.cuda.synchronize()
@@ -692,6 +702,7 @@ def run_ours_batched(args, wl, ws, rank, local):
                    "nlevels": info["nlevels"], "nterms": p},
         "e2e": {"value": ws * n * nd * args.steps / e2e_tot, "unit": "targets/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "plan_build_ms": plan_ms,
         "plain_single_rhs": {"value": plain_value, "unit": "targets/s", "ms_per_solve": plain_ms,
                              "batched_per_rhs_speedup": value / ws / plain_value},
         "rel_l2_err_vs_direct": max(errs),

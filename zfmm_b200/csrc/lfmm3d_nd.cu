@@ -1142,15 +1142,17 @@ __global__ void __launch_bounds__(ENT) k_p2p3nd(P2PNdArgs A) {
             zdc r1 = ir * PI4I;
             zdc r3 = r1 * (ir * ir);
             if (A.ifcharge) {
+              // the pair's kernel values once, then one complex MAC per output
+              // and right-hand side
+              const zdc w0 = r3 * y0, w1 = r3 * y1, w2 = r3 * y2;
 #pragma unroll
               for (int r = 0; r < RB; r++) {
                 zdc qv = S.q[k][r];
                 P[r] += qv * r1;
                 if (GRAD) {
-                  zdc f = qv * r3;
-                  G0[r] += f * y0;
-                  G1[r] += f * y1;
-                  G2[r] += f * y2;
+                  G0[r] += qv * w0;
+                  G1[r] += qv * w1;
+                  G2[r] += qv * w2;
                 }
               }
             }
