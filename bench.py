@@ -608,18 +608,19 @@ def run_ours_batched(args, wl, ws, rank, local):
     torch.cuda.synchronize()
     plan_ms = pc0.elapsed_time(pc1)
     _capi.check(L.zfmm_plan3d_destroy(hh))
-    for _ in range(2):
+    for _ in range(3):
         solve_plain()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    nplain = 3
-    flush.fill_(1)
-    e0.record(stream)
-    for _ in range(nplain):
+    pl_t = []
+    for k in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(k & 255)
+        e0.record(stream)
         solve_plain()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1) / nplain
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pl_t.append(e0.elapsed_time(e1))
+    plain_ms = statistics.median(pl_t)
     L.zfmm_set_step_timing(0)
     if ws > 1:
         import torch.distributed as dist

@@ -386,35 +386,40 @@ __device__ void rot_nd(const Tab3& T, const RotTab& R, const XSm& S, zdc ca, zdc
   for (int n = 0; n <= p; n++) {
     // samples at angles >= 0: S = F(j) + F(-j), D = F(j) - F(-j); complex
     // [jc x m] x [m x r] products on m8n8k4 tiles (4 real MMAs per k-step)
-    for (int t = w; t < 2 * njt * 4; t += XW) {
-      const int which = t / (njt * 4), rem = t - which * njt * 4, jt = rem >> 2, rt = rem & 3;
+    for (int t = w; t < 4 * njt; t += XW) {
+      const int which = t / (2 * njt), rem = t - which * 2 * njt, jt = rem >> 1, rh = rem & 1;
       const double* Cr = which ? S.Cdr : S.Csr;
       const double* Ci = which ? S.Cdi : S.Csi;
       const double* Ar = which ? S.Adr : S.Asr;
       const double* Ai = which ? S.Adi : S.Asi;
-      double sr[2] = {0.0, 0.0}, si[2] = {0.0, 0.0};
-      const int jc = jt * 8 + g8, r = rt * 8 + g8;
+      double sr[2][2], si[2][2];
+#pragma unroll
+      for (int q = 0; q < 2; q++) sr[q][0] = sr[q][1] = si[q][0] = si[q][1] = 0.0;
+      const int jc = jt * 8 + g8;
       for (int k0 = 0; k0 <= n; k0 += 4) {
         const int m = k0 + t4;
-        double are = 0.0, aim = 0.0, bre = 0.0, bim = 0.0;
-        if (m <= n) {
-          are = Cr[m * CP + jc];
-          aim = Ci[m * CP + jc];
-          bre = Ar[m * RP + r];
-          bim = Ai[m * RP + r];
+        const bool ok = m <= n;
+        const double are = ok ? Cr[m * CP + jc] : 0.0, aim = ok ? Ci[m * CP + jc] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int r = (2 * rh + q) * 8 + g8;
+          const double bre = ok ? Ar[m * RP + r] : 0.0, bim = ok ? Ai[m * RP + r] : 0.0;
+          dmma(sr[q], are, bre);
+          dmma(si[q], are, bim);
+          dmma(sr[q], -aim, bim);
+          dmma(si[q], aim, bre);
         }
-        dmma(sr, are, bre);
-        dmma(sr, -aim, bim);
-        dmma(si, are, bim);
-        dmma(si, aim, bre);
       }
       double* Or = which ? S.Sdr : S.Ssr;
       double* Oi = which ? S.Sdi : S.Ssi;
-      const int ro = (jt * 8 + g8) * RP + rt * 8 + 2 * t4;
-      Or[ro] = sr[0];
-      Or[ro + 1] = sr[1];
-      Oi[ro] = si[0];
-      Oi[ro + 1] = si[1];
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int ro = (jt * 8 + g8) * RP + (2 * rh + q) * 8 + 2 * t4;
+        Or[ro] = sr[q][0];
+        Or[ro + 1] = sr[q][1];
+        Oi[ro] = si[q][0];
+        Oi[ro + 1] = si[q][1];
+      }
     }
     __syncthreads();
     // projection: X = CW (S + [jc = 0] D), Y = SW D on m8n8k4 tiles, then
