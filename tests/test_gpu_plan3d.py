@@ -9,9 +9,11 @@ one and many right-hand sides (a ragged last pass of 32), charges and dipoles,
 ifpgh 1 and 2, adaptive trees with lists 3 and 4, plan reuse, and the device
 (torch) entry point.  Fewer than 4 right-hand sides, or orders whose batched
 working set exceeds shared memory (eps below ~3e-10), run the single-solve
-passes per right-hand side on the plan's tree.  Helmholtz plan solves run the single-solve passes on
-the plan's tree for every right-hand side and wavenumber, so they must equal
-the single solves to rounding."""
+passes per right-hand side on the plan's tree.  Helmholtz plan solves with 4
+or more right-hand sides batch the translations (P2M, P2L, P2P and the
+evaluations run per right-hand side) and must match the single zhfmm3d solves
+to 10*eps; with fewer they run the single-solve passes on the plan's tree and
+equal the single solves to rounding."""
 import numpy as np
 import pytest
 
@@ -179,3 +181,95 @@ def test_plan_small_eps_runs_per_rhs():
         p1, g1 = single(eps, zs, q[r], 0, None, None, 2)
         assert rel(p[r], p1) < 1e-13, r
         assert rel(g[r], g1) < 1e-13, r
+
+
+def hsingle(eps, zk, zs, q, ifd, ds, dv, ifpgh, zt=None):
+    import zfmm_b200
+    n = zs.shape[1]
+    zt = zs if zt is None else zt
+    return zfmm_b200.zhfmm3d(eps, zk, n, zs, 1 if q is not None else 0, q, ifd, ds, dv,
+                             zt.shape[1], zt, ifpgh, 1)
+
+
+def test_helmholtz_batched_matches_single():
+    # 4 or more right-hand sides: the batched translations (one ragged pass of 32)
+    import zfmm_b200
+    eps = 1e-9
+    w = W.sphere3d(15000, seed=21)
+    zs = w["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(21)
+    nd = 37
+    q, ds = cn(rng, nd, n), cn(rng, nd, n)
+    plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
+    zk = 10 + 0.2j
+    p, g = plan.zhfmm3d(zk, nd, 1, q, 1, ds, w["dipvec"], 2)
+    assert p.shape == (nd, n) and g.shape == (nd, 3, n)
+    for r in [0, 13, 31, 32, 36]:
+        p1, g1 = hsingle(eps, zk, zs, q[r], 1, ds[r], w["dipvec"], 2)
+        assert rel(p[r], p1) < 10 * eps, r
+        assert rel(g[r], g1) < 10 * eps, r
+
+
+def test_helmholtz_batched_adaptive_kinds():
+    # adaptive tree (lists 3 and 4), charges only / dipoles only, ifpgh 1 and 2,
+    # two wavenumbers on one plan
+    import zfmm_b200
+    eps = 1e-8
+    w = W.clustered3d(9000, seed=22)
+    zs = w["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(22)
+    nd = 6
+    q, ds = cn(rng, nd, n), cn(rng, nd, n)
+    plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
+    for zk in (6 + 0.1j, 2.5 - 0.05j):
+        for ifc, ifd, ifpgh in [(1, 0, 2), (0, 1, 1)]:
+            p, g = plan.zhfmm3d(zk, nd, ifc, q, ifd, ds, w["dipvec"], ifpgh)
+            for r in (0, nd - 1):
+                p1, g1 = hsingle(eps, zk, zs, q[r] if ifc else None, ifd, ds[r], w["dipvec"],
+                                 ifpgh)
+                assert rel(p[r], p1) < 10 * eps, (zk, ifc, ifd, r)
+                if ifpgh == 2:
+                    assert rel(g[r], g1) < 10 * eps, (zk, ifc, ifd, r)
+
+
+def test_helmholtz_batched_separate_targets_and_oracle():
+    import zfmm_b200
+    eps = 1e-6
+    w = W.clustered3d(2500, seed=23)
+    zs = w["zsrc"]
+    t = W.clustered3d(900, seed=24)["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(23)
+    nd = 4
+    q = cn(rng, nd, n)
+    zk = 3 + 0.1j
+    plan = zfmm_b200.Plan3D(eps, n, zs, t.shape[1], t)
+    p, g = plan.zhfmm3d(zk, nd, 1, q, 0, None, None, 2)
+    for r in range(nd):
+        po, go = O.zhfmm3d(eps, zk, zs.T, q[r], None, None, t.T, ifpgh=2)
+        assert rel(p[r], po) < 10 * eps, r
+        assert rel(g[r], go.T) < 10 * eps, r
+
+
+def test_helmholtz_batched_device_entry_point():
+    import torch
+    import zfmm_b200
+    eps = 1e-9
+    nd = 5
+    w = W.sphere3d(8000, seed=25)
+    zs = w["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(25)
+    q = cn(rng, nd, n)
+    zk = 8 + 0.1j
+    plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
+    p, g = plan.zhfmm3d(zk, nd, 1, q, 0, None, None, 2)
+    zt = torch.from_numpy(np.ascontiguousarray(zs.T)).cuda()
+    qt = torch.from_numpy(np.ascontiguousarray(q.T)).cuda()
+    plan_t = zfmm_b200.Plan3D(eps, n, zt, n, zt)
+    pt, gt = plan_t.zhfmm3d(zk, nd, 1, qt, 0, None, None, 2)
+    torch.cuda.synchronize()
+    assert rel(pt.cpu().numpy(), p) < 1e-13
+    assert rel(gt.cpu().numpy(), g) < 1e-13

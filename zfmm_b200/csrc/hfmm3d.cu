@@ -39,6 +39,7 @@
 #include "helm3d_special.cuh"
 #include "hfmm3d.cuh"
 #include "lfmm3d.cuh"
+#include "helm3d_prep.cuh"
 #include "plan3d.cuh"
 #include "sph3d.cuh"
 
@@ -49,42 +50,8 @@ constexpr int HNT = 256;     // threads of the translation kernel
 constexpr int HFNT = 128;    // threads of the form kernel (at most)
 constexpr int HENT = 128;    // threads of the eval / P2P kernels
 constexpr int HPTILE = 128;  // sources per P2P tile
-constexpr int ML = 52;       // tree levels (nlmax = 51)
-constexpr int PMAXR = 126;   // largest expansion order
 constexpr size_t kSmemMax = 227 * 1024;
 constexpr int kGmemCtas = 2 * 148;  // CTAs of the global-workspace variant
-
-struct HLev {
-  long base[ML];
-  int lo[ML];
-  int p[ML];
-  double rs[ML];
-};
-
-// one quadrature z-shift configuration (per kind and output level)
-struct ShiftTab {
-  int p1, p2, nq;
-  double r, rs1;
-  const double* x;  // nq Gauss-Legendre nodes
-  const double* w;  // nq weights
-  const zdc* cF;    // g_n / ((g_n^2 + g_n'^2) / 2 pi), n <= p2
-  const zdc* cD;    // g_n' / (...)
-};
-
-__device__ __forceinline__ int jdx(int n, int m) { return n * (n + 1) / 2 + m; }
-
-// per-wavenumber state of a solve: orders per level, expansion offsets,
-// tables of the largest order, quadrature z-shift configurations
-struct HelmPrep {
-  HLev lev;
-  int pmax = 0;
-  long tot = 0;
-  Tab3 T;
-  zdc kw;
-  DevBuf<double> dxw;
-  DevBuf<zdc> dcfd;
-  DevBuf<ShiftTab> dst;
-};
 
 // ---- translation kernel ------------------------------------------------------
 struct HTransArgs {
@@ -1145,6 +1112,7 @@ void helm_prep(const Setup3D& S, double eps, zdc zk, int isep, HelmPrep& H, cuda
   }
   DevBuf<ShiftTab>& dst = H.dst;
   dst.alloc(3 * ML, s);
+  H.sth = sth;
   ZF_CUDA(cudaMemcpyAsync(dst.get(), sth.data(), sth.size() * sizeof(ShiftTab),
                           cudaMemcpyHostToDevice, s));
   ZF_CUDA(cudaStreamSynchronize(s));  // the host staging vectors go out of scope below
@@ -1154,6 +1122,89 @@ void helm_prep(const Setup3D& S, double eps, zdc zk, int isep, HelmPrep& H, cuda
 // sorted potentials (and gradients, unscaled) of one right-hand side with
 // sorted strengths q, ds, dv to potsort / gradsort; ev[2..5] (optional) get
 // the step boundaries recorded
+namespace {
+size_t form_smem(int pmax, int* fw_out) {
+  int fw = HFNT / 32;  // warps of the form kernel, one partial expansion each
+  while (fw > 1 && (size_t)fw * (pmax + 1) * (pmax + 1) * sizeof(zdc) > kSmemMax) fw /= 2;
+  size_t smf = (size_t)fw * (pmax + 1) * (pmax + 1) * sizeof(zdc);
+  if (smf > kSmemMax) throw zf_error(ZF_ERR_ARG, "expansion order too large for P2M staging");
+  *fw_out = fw;
+  return smf;
+}
+}  // namespace
+
+void helm_form(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds, const zdc* dv,
+               int ifcharge, int ifdipole, bool local, zdc* out, cudaStream_t s) {
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  const int nb = t.nboxes, nlev = t.nlevels, pmax = H.pmax;
+  if (!local && nlev < 2) return;
+  if (local && L.mn[3] <= 0) return;
+  HFormArgs F;
+  F.r1 = H.T.r1; F.r2 = H.T.r2; F.sq = H.T.sq; F.L = pmax + 1;
+  F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
+  F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
+  F.zsrc = S.zsrcsort.get(); F.charge = q; F.dipstr = ds;
+  F.dipvec = dv; F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get();
+  F.lev = H.lev; F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
+  F.nb = nb; F.ifcharge = ifcharge; F.ifdipole = ifdipole; F.pbuf = pmax; F.zk = H.kw;
+  F.out = out;
+  int fw = 1;
+  size_t smf = form_smem(pmax, &fw);
+  if (local) {
+    if (ifdipole) {
+      ZF_CUDA(cudaFuncSetAttribute(k_hform3<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_hform3<true, true>, nb, 32 * fw, smf, s, F);
+    } else {
+      ZF_CUDA(cudaFuncSetAttribute(k_hform3<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_hform3<true, false>, nb, 32 * fw, smf, s, F);
+    }
+  } else {
+    if (ifdipole) {
+      ZF_CUDA(cudaFuncSetAttribute(k_hform3<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_hform3<false, true>, nb, 32 * fw, smf, s, F);
+    } else {
+      ZF_CUDA(cudaFuncSetAttribute(k_hform3<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+      klaunch(k_hform3<false, false>, nb, 32 * fw, smf, s, F);
+    }
+  }
+  ZF_LAUNCH_CHECK();
+}
+
+void helm_eval(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds, const zdc* dv,
+               int ifcharge, int ifdipole, int ifpgh, const zdc* mp, const zdc* loc,
+               zdc* potsort, zdc* gradsort, cudaStream_t s) {
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  const int nb = t.nboxes, pmax = H.pmax;
+  HP2PArgs Pa;
+  Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
+  Pa.zsrc = S.zsrcsort.get(); Pa.charge = q; Pa.dipstr = ds;
+  Pa.dipvec = dv; Pa.ztarg = S.ztargsort.get();
+  Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb;
+  Pa.ifcharge = ifcharge; Pa.ifdipole = ifdipole; Pa.zk = H.kw;
+  Pa.pot = potsort; Pa.grad = gradsort;
+  if (ifpgh > 1) klaunch(k_hp2p3<true>, nb, HENT, 0, s, Pa);
+  else klaunch(k_hp2p3<false>, nb, HENT, 0, s, Pa);
+  ZF_LAUNCH_CHECK();
+  HEvalArgs E;
+  E.r1 = H.T.r1; E.r2 = H.T.r2; E.sq = H.T.sq; E.L = pmax + 1;
+  E.ilevel = t.ilevel.get(); E.nchild = t.nchild.get(); E.isrcse = S.isrcse.get();
+  E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
+  E.zct = S.zctarg.get(); E.lev = H.lev; E.mp = mp; E.loc = loc;
+  E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb; E.pbuf = pmax;
+  E.zk = H.kw; E.pot = potsort; E.grad = gradsort;
+  size_t sme = (size_t)(pmax + 1) * (pmax + 1) * sizeof(zdc);
+  if (ifpgh > 1) {
+    ZF_CUDA(cudaFuncSetAttribute(k_heval3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
+    klaunch(k_heval3<true>, nb, HENT, sme, s, E);
+  } else {
+    ZF_CUDA(cudaFuncSetAttribute(k_heval3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
+    klaunch(k_heval3<false>, nb, HENT, sme, s, E);
+  }
+  ZF_LAUNCH_CHECK();
+}
+
 void helm_core(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds, const zdc* dv,
                int ifcharge, int ifdipole, int ifpgh, zdc* potsort, zdc* gradsort,
                cudaStream_t s, cudaEvent_t* ev) {
@@ -1172,30 +1223,7 @@ void helm_core(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds,
   DevBuf<zdc> mp(std::max<long>(tot, 1), s), loc(std::max<long>(tot, 1), s);
   mp.zero();
   loc.zero();
-  // P2M
-  HFormArgs F;
-  F.r1 = T.r1; F.r2 = T.r2; F.sq = T.sq; F.L = pmax + 1;
-  F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
-  F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
-  F.zsrc = S.zsrcsort.get(); F.charge = q; F.dipstr = ds;
-  F.dipvec = dv; F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get();
-  F.lev = lev; F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
-  F.nb = nb; F.ifcharge = ifcharge; F.ifdipole = ifdipole; F.pbuf = pmax; F.zk = kw;
-  int fw = HFNT / 32;  // warps of the form kernel, one partial expansion each
-  while (fw > 1 && (size_t)fw * (pmax + 1) * (pmax + 1) * sizeof(zdc) > kSmemMax) fw /= 2;
-  size_t smf = (size_t)fw * (pmax + 1) * (pmax + 1) * sizeof(zdc);
-  if (smf > kSmemMax) throw zf_error(ZF_ERR_ARG, "expansion order too large for P2M staging");
-  F.out = mp.get();
-  if (nlev >= 2) {
-    if (ifdipole) {
-      ZF_CUDA(cudaFuncSetAttribute(k_hform3<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_hform3<false, true>, nb, 32 * fw, smf, s, F);
-    } else {
-      ZF_CUDA(cudaFuncSetAttribute(k_hform3<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_hform3<false, false>, nb, 32 * fw, smf, s, F);
-    }
-    ZF_LAUNCH_CHECK();
-  }
+  helm_form(S, H, q, ds, dv, ifcharge, ifdipole, false, mp.get(), s);
   hmark(2);
   HTransArgs A;
   A.r1 = T.r1; A.r2 = T.r2; A.sq = T.sq; A.dinv = T.dinv; A.L = pmax + 1; A.pT = pmax;
@@ -1231,17 +1259,7 @@ void helm_core(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds,
     A.hi = nb - 1;
     launch_htrans<1>(A, hscratch.get(), s);
   }
-  if (L.mn[3] > 0) {
-    F.out = loc.get();
-    if (ifdipole) {
-      ZF_CUDA(cudaFuncSetAttribute(k_hform3<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_hform3<true, true>, nb, 32 * fw, smf, s, F);
-    } else {
-      ZF_CUDA(cudaFuncSetAttribute(k_hform3<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
-      klaunch(k_hform3<true, false>, nb, 32 * fw, smf, s, F);
-    }
-    ZF_LAUNCH_CHECK();
-  }
+  helm_form(S, H, q, ds, dv, ifcharge, ifdipole, true, loc.get(), s);
   hmark(4);
   // L2L, coarsest first: children at level l+1 of parents at level l >= 2
   A.in = loc.get();
@@ -1253,32 +1271,7 @@ void helm_core(const Setup3D& S, const HelmPrep& H, const zdc* q, const zdc* ds,
     launch_htrans<2>(A, hscratch.get(), s);
   }
   hmark(5);
-  HP2PArgs Pa;
-  Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
-  Pa.zsrc = S.zsrcsort.get(); Pa.charge = q; Pa.dipstr = ds;
-  Pa.dipvec = dv; Pa.ztarg = S.ztargsort.get();
-  Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb;
-  Pa.ifcharge = ifcharge; Pa.ifdipole = ifdipole; Pa.zk = kw;
-  Pa.pot = potsort; Pa.grad = gradsort;
-  if (ifpgh > 1) klaunch(k_hp2p3<true>, nb, HENT, 0, s, Pa);
-  else klaunch(k_hp2p3<false>, nb, HENT, 0, s, Pa);
-  ZF_LAUNCH_CHECK();
-  HEvalArgs E;
-  E.r1 = T.r1; E.r2 = T.r2; E.sq = T.sq; E.L = pmax + 1;
-  E.ilevel = t.ilevel.get(); E.nchild = t.nchild.get(); E.isrcse = S.isrcse.get();
-  E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
-  E.zct = S.zctarg.get(); E.lev = lev; E.mp = mp.get(); E.loc = loc.get();
-  E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb; E.pbuf = pmax;
-  E.zk = kw; E.pot = potsort; E.grad = gradsort;
-  size_t sme = (size_t)(pmax + 1) * (pmax + 1) * sizeof(zdc);
-  if (ifpgh > 1) {
-    ZF_CUDA(cudaFuncSetAttribute(k_heval3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
-    klaunch(k_heval3<true>, nb, HENT, sme, s, E);
-  } else {
-    ZF_CUDA(cudaFuncSetAttribute(k_heval3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sme));
-    klaunch(k_heval3<false>, nb, HENT, sme, s, E);
-  }
-  ZF_LAUNCH_CHECK();
+  helm_eval(S, H, q, ds, dv, ifcharge, ifdipole, ifpgh, mp.get(), loc.get(), potsort, gradsort, s);
 }
 
 void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, zdc* grad,
@@ -1329,8 +1322,8 @@ void zhfmm3d_device(double eps, zdc zk, const Inputs3D& in, int isep, zdc* pot, 
   }
 }
 
-void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in, int ifpgh,
-                          zdc* pot, zdc* grad, cudaStream_t s, StepTimes* times) {
+void helm_plan_loop(const Plan3D& P, const HelmPrep& H, int nd, const StrengthsNd& in, int ifpgh,
+                    zdc* pot, zdc* grad, cudaStream_t s, StepTimes* times, float prep_ms) {
   const Setup3D& S = P.S;
   const int ns = P.ns, nt = P.nt;
   long launches0 = launch_counter();
@@ -1339,6 +1332,7 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   if (timing)
     for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
   float acc[8] = {0};
+  acc[0] = prep_ms;
   auto mark = [&](int i) {
     if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
   };
@@ -1350,8 +1344,6 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
     acc[slot] += ms;
   };
   mark(0);
-  HelmPrep H;
-  helm_prep(S, P.eps, zk, P.isep, H, s);
   DevBuf<zdc> q(ns, s), ds(ns, s), dv(3 * (size_t)ns, s), potsort(nt, s),
       gradsort(ifpgh > 1 ? 3 * (size_t)nt : 1, s);
   mark(1);

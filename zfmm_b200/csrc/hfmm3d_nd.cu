@@ -1,0 +1,596 @@
+// 3D Helmholtz FMM for many right-hand sides on one geometry (a plan).
+//
+// The algorithm of zhfmm3d (zfmm3d/src/helmholtz/zhfmm3d.f:256-600) on the
+// plan's tree, with the translations batched over the right-hand sides: the
+// expansions of every right-hand side live side by side, coefficient (box b of
+// level l, n*n+n+m, r) at (base_l + (b - first box of l) (p_l+1)^2 + n*n+n+m) nd
+// + r, and one pass of the translation kernel moves 32 right-hand sides
+// (one per lane) through the geometry-dependent work of a box pair.
+//
+//   k_htrans3nd  M2M / M2L / L2L (zh3dmpmp / zh3dmploc / zh3dlocloc,
+//                zh3dtrans.f:1-780), one launch per level: z-rotation and
+//                point-and-shoot y-rotation of order p1 (the batched rotation
+//                shared with the Laplace plans: degree-streamed recurrence
+//                states, sample and projection products on FP64 tensor
+//                cores), the quadrature z-shift, and the inverse rotations of
+//                order p2.  The z-shift evaluates the rotated expansion and its
+//                normal derivative at the nq = 2.5 p2 Gauss-Legendre points of a
+//                sphere about the new centre and projects them onto the order-p2
+//                coefficients.  Its geometry-dependent coefficients (radial
+//                functions at every node; per node chunk the value and
+//                derivative Legendre columns and the projection columns) are
+//                tabulated in shared memory once per box pair; the sums over
+//                degrees and nodes then run for the 32 right-hand sides with
+//                the lane as the right-hand-side index.
+//
+// P2M, P2L, P2P, L2T and M2T run per right-hand side through the single-solve
+// passes on the plan's tree; their expansions move in and out of the batched
+// layout by column copies.  Fewer than 4 right-hand sides, or orders whose
+// working set exceeds shared memory, run every pass per right-hand side.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "helm3d_prep.cuh"
+#include "helm3d_special.cuh"
+#include "hfmm3d.cuh"
+#include "lfmm3d.cuh"
+#include "plan3d.cuh"
+#include "rot3nd.cuh"
+#include "sph3d.cuh"
+
+namespace zf {
+
+namespace {
+
+constexpr int QCM = 8;  // nodes per chunk of the z-shift (at most)
+constexpr size_t kHSmemMax = 227 * 1024;
+
+// z-shift tables, aliasing the rotation's work block
+struct HSh {
+  zdc* node;   // nq x 6: cos, sin of the node's polar angle about the old centre,
+               // their ratios to the radius, the node's real sin and cos
+  zdc* rad;    // nq x (p1+2): radial functions of the input kind at k r
+  zdc* drad;   // nq x (p1+2): their k-scaled derivatives
+  zdc* Zc;     // qc x np1: value coefficients of the chunk's nodes, (n, m >= 0) at jdx(n, m)
+  zdc* Dc;     // qc x np1: normal-derivative coefficients
+  double* Yt;  // qc x np2: projection columns (Legendre at the real node x weight)
+};
+
+__host__ __device__ inline size_t hsh_layout(int p1, int p2, int nq, int qc, char* base, HSh* o) {
+  const size_t P2 = p1 + 2, np1 = (size_t)(p1 + 1) * (p1 + 2) / 2,
+               np2 = (size_t)(p2 + 1) * (p2 + 2) / 2;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    void* q = base ? base + off : nullptr;
+    off += (bytes + 15) / 16 * 16;
+    return q;
+  };
+  HSh H;
+  H.node = (zdc*)take((size_t)nq * 6 * 16);
+  H.rad = (zdc*)take((size_t)nq * P2 * 16);
+  H.drad = (zdc*)take((size_t)nq * P2 * 16);
+  H.Zc = (zdc*)take((size_t)qc * np1 * 16);
+  H.Dc = (zdc*)take((size_t)qc * np1 * 16);
+  H.Yt = (double*)take((size_t)qc * np2 * 8);
+  if (o) *o = H;
+  return off;
+}
+
+struct HTransNdArgs {
+  Tab3 T;  // tables of the largest order, row stride LT
+  int LT;
+  RotTab R1, R2;  // DFT tables of the two rotation orders
+  int p1, p2, pmx, nq, qc, rot_smem;
+  double dsc1, dsc2;  // projection-weight rescaling to p1 / p2
+  ShiftTab st;
+  zdc kwave;
+  const int *ilevel, *iparent, *nchild, *ichild, *isrcse, *itargse;
+  const zdc *zcs, *zct;
+  const zdc* in;
+  long base1;  // first coefficient of the input level
+  int lo1;     // its first box
+  zdc* out;
+  long base2;
+  int lo2;
+  zdc* scratch;
+  long scr_per_cta;
+  const int *nl2, *l2, *nl4;
+  int mn2, nd, lo, hi;
+};
+
+// quadrature z-shift of the 32 right-hand sides in X1 (order p1, row stride
+// RC) by zsh into X2 (order p2), zh3dmpmp / zh3dmploc / zh3dlocloc after the
+// rotations (zh3dtrans.f).  KIND 2 (local input) uses the scaled spherical
+// Bessel functions, KIND 0 / 1 (multipole input) the scaled Hankel functions.
+template <int KIND>
+__device__ void hshift_nd(const HTransNdArgs& A, const HSh& H, zdc zsh, const zdc* X1, zdc* X2) {
+  const int p1 = A.p1, p2 = A.p2, nq = A.nq, qc = A.qc, tid = threadIdx.x, lane = tid & 31,
+            w = tid >> 5;
+  const int P2 = p1 + 2, np1 = (p1 + 1) * (p1 + 2) / 2, np2 = (p2 + 1) * (p2 + 2) / 2;
+  const ShiftTab& ST = A.st;
+  const int LT = A.LT;
+  const double* __restrict__ r1 = A.T.r1;
+  const double* __restrict__ r2 = A.T.r2;
+  const double* __restrict__ sq = A.T.sq;
+  const double s4i = 1.0 / sqrt(4 * kPi);
+  if (nq == 0) {  // p2 = 0 configurations have no nodes: the shifted expansion is zero
+    for (int idx = tid; idx < (p2 + 1) * (p2 + 1) * RC; idx += XNT) stcg_z(X2 + idx, mkz(0.0));
+    __syncthreads();
+    return;
+  }
+  // (a) node geometry and radial tables, one thread per node
+  for (int t = tid; t < nq; t += XNT) {
+    const double x = __ldg(&ST.x[t]);
+    const double yi = sqrt(1 - x * x);
+    const zdc zi = zsh + mkz(ST.r * x);
+    const zdc ri = zsqrt_r(mkz((ST.r * yi) * (ST.r * yi)) + zi * zi);
+    const zdc cthi = zi / ri;
+    const zdc sthi = zsqrt_r(mkz(1.0) - cthi * cthi);
+    zdc* nd = H.node + 6 * t;
+    nd[0] = cthi;
+    nd[1] = sthi;
+    nd[2] = cthi / ri;
+    nd[3] = sthi / ri;
+    nd[4] = mkz(yi);
+    nd[5] = mkz(x);
+    const zdc zk = ri * A.kwave;
+    zdc* f = H.rad + (size_t)t * P2;
+    zdc* fd = H.drad + (size_t)t * P2;
+    if (KIND == 2) besseljs3d_z(p1, zk, ST.rs1, f, fd);
+    else h3dall_z(p1, zk, ST.rs1, f, fd);
+    for (int n = 0; n <= p1; n++) fd[n] = A.kwave * fd[n];
+  }
+  __syncthreads();
+  const int ncol = (p1 > p2 ? p1 : p2) + 1;
+  const int ntask = 2 * p2 + 1;
+  for (int q0 = 0; q0 < nq; q0 += qc) {
+    const int nc = min(qc, nq - q0);
+    // (b) one thread per (node, order m >= 0): the value and normal-derivative
+    // coefficients of the expansion's (n, +-m) terms at the node, and the
+    // projection column of order m at the real node
+    for (int item = tid; item < nc * ncol; item += XNT) {
+      const int t = item / ncol, m = item - t * ncol, node = q0 + t;
+      const zdc* nd = H.node + 6 * node;
+      const double x = nd[5].re, yi = nd[4].re;
+      if (m <= p1) {
+        const zdc z = nd[0], sthi = nd[1], cr = nd[2], sr = nd[3];
+        const zdc zz1 = mkz(1.0) - z * z;
+        const zdc u = -zsqrt_r(zz1);
+        const zdc* f = H.rad + (size_t)node * P2;
+        const zdc* fd = H.drad + (size_t)node * P2;
+        zdc* zc = H.Zc + (size_t)t * np1;
+        zdc* dc = H.Dc + (size_t)t * np1;
+        const double sgm = ((m & 1) ? -1.0 : 1.0) * s4i;
+        zdc Ydiag = mkz(1.0);
+        for (int k = 1; k <= m; k++) {
+          const double ckk = __ldg(&r1[k * LT + k]);
+          Ydiag = (k == 1) ? mkz(-ckk) : (Ydiag * u) * ckk;
+        }
+        zdc Yp = Ydiag, Dp = (Ydiag * (double)(-m)) * z, Ypp = mkz(0.0), Dpp = mkz(0.0);
+        for (int n = m; n <= p1; n++) {
+          zdc Y, D;
+          if (n == m) {
+            Y = Yp;
+            D = Dp;
+          } else {
+            if (n == m + 1) {
+              const double cc = __ldg(&r1[n * LT + m]);
+              Y = (z * Yp) * cc;
+              D = (m == 0) ? (z * Dp + Yp) * cc : (z * Dp + zz1 * Yp) * cc;
+            } else {
+              const double c1 = __ldg(&r1[n * LT + m]), c2 = __ldg(&r2[n * LT + m]);
+              Y = (c1 * z) * Yp - c2 * Ypp;
+              D = (m == 0) ? c1 * (z * Dp + Yp) - c2 * Dpp : c1 * (z * Dp + zz1 * Yp) - c2 * Dpp;
+            }
+            Ypp = Yp;
+            Dpp = Dp;
+            Yp = Y;
+            Dp = D;
+          }
+          const double sc = __ldg(&sq[n]) * sgm;
+          const zdc yl = Y * sc, dyl = D * sc;
+          const zdc fn = f[n], fdn = fd[n];
+          zdc df_r, df_th, z1;
+          if (m == 0) {
+            z1 = fn * yl;
+            df_r = fdn * yl;
+            df_th = -(fn * dyl * sthi);
+          } else {
+            z1 = fn * yl * sthi;
+            df_r = fdn * yl * sthi;
+            df_th = -(fn * dyl);
+          }
+          const zdc df_x = df_r * sthi + df_th * cr;
+          const zdc df_y = df_r * z - df_th * sr;
+          zc[jdx(n, m)] = z1;
+          dc[jdx(n, m)] = df_x * yi + df_y * x;
+        }
+      }
+      if (m <= p2) {
+        // zylgndrf at the real node, times (-1)^m / sqrt(4 pi) and the weight
+        const double wq = __ldg(&ST.w[node]) * ((m & 1) ? -1.0 : 1.0) * s4i;
+        const double u = -sqrt(1 - x * x);
+        double yd = 1.0;
+        for (int k = 1; k <= m; k++) yd = (yd * u) * __ldg(&r1[k * LT + k]);
+        double yp = yd, ypp = 0.0;
+        double* yt = H.Yt + (size_t)t * np2;
+        for (int n = m; n <= p2; n++) {
+          double y;
+          if (n == m) {
+            y = yp;
+          } else if (n == m + 1) {
+            y = (x * yp) * __ldg(&r1[n * LT + m]);
+            ypp = yp;
+            yp = y;
+          } else {
+            y = (__ldg(&r1[n * LT + m]) * x) * yp - __ldg(&r2[n * LT + m]) * ypp;
+            ypp = yp;
+            yp = y;
+          }
+          yt[jdx(n, m)] = y * __ldg(&sq[n]) * wq;
+        }
+      }
+    }
+    __syncthreads();
+    // (c) per order m and sign: the node sums of the 32 right-hand sides
+    // (lane = right-hand side), then their projection onto the order-p2
+    // coefficients (n, +-m), accumulated over the node chunks in X2
+    for (int task = w; task < ntask; task += XW) {
+      const int m = (task + 1) >> 1, mm = (task & 1) ? m : -m;
+      zdc F[QCM], D[QCM];
+#pragma unroll
+      for (int t = 0; t < QCM; t++) F[t] = D[t] = mkz(0.0);
+      for (int n = m; n <= p1; n++) {
+        const zdc a = ldcg_z(X1 + ix3(n, mm) * RC + lane);
+        const int j = jdx(n, m);
+#pragma unroll
+        for (int t = 0; t < QCM; t++) {
+          if (t < nc) {
+            F[t] += H.Zc[t * np1 + j] * a;
+            D[t] += H.Dc[t * np1 + j] * a;
+          }
+        }
+      }
+      for (int n = m; n <= p2; n++) {
+        const int j = jdx(n, m);
+        zdc sF = mkz(0.0), sD = mkz(0.0);
+#pragma unroll
+        for (int t = 0; t < QCM; t++) {
+          if (t < nc) {
+            const double y = H.Yt[t * np2 + j];
+            sF += y * F[t];
+            sD += y * D[t];
+          }
+        }
+        const zdc v = ST.cF[n] * sF + ST.cD[n] * sD;
+        zdc* o = X2 + ix3(n, mm) * RC + lane;
+        stcg_z(o, q0 == 0 ? v : ldcg_z(o) + v);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int KIND, int SLOTS>
+__global__ void __launch_bounds__(XNT, 1) k_htrans3nd(HTransNdArgs A) {
+  extern __shared__ zdc sm[];
+  const int tid = threadIdx.x, p1 = A.p1, p2 = A.p2;
+  const int NC1 = (p1 + 1) * (p1 + 1), NC2 = (p2 + 1) * (p2 + 1);
+  XSm S;
+  xsm_layout(A.pmx, A.rot_smem != 0, sm, &S);
+  HSh H;
+  hsh_layout(p1, p2, A.nq, A.qc, (char*)S.Csr, &H);
+  if (S.cw) {
+    // one rotation order in this launch (p1 = p2): its tables staged once
+    const int CP = rot_cp(p1 + 1), TP = rot_tp(p1 + 1);
+    for (int k = tid; k < 2 * CP * TP; k += XNT) S.cw[k] = A.R1.cw[k];
+  }
+  zdc* X1 = A.scratch + (size_t)blockIdx.x * A.scr_per_cta;
+  zdc* X2 = X1 + (size_t)NC1 * RC;
+  const long nd = A.nd;
+  for (int b = A.lo + blockIdx.x; b <= A.hi; b += gridDim.x) {
+    int nin = 0, par = -1;
+    if (KIND == 0) {
+      if (nsrc(A.isrcse, b) <= 0 || A.nchild[b] == 0) continue;
+      nin = A.nchild[b];
+    } else if (KIND == 1) {
+      if (nsrc(A.itargse, b) <= 0 || A.nl2[b] == 0) continue;
+      nin = A.nl2[b];
+    } else {
+      par = A.iparent[b];
+      // zhfmm3d.f:572-576: ((targets and list 2) or list 4) of the parent,
+      // and targets in the child
+      if (par < 0 || nsrc(A.itargse, b) <= 0) continue;
+      if (!((nsrc(A.itargse, par) > 0 && A.nl2[par] > 0) || A.nl4[par] > 0)) continue;
+      nin = 1;
+    }
+    for (int r0 = 0; r0 < A.nd; r0 += RC) {
+      const int nval = min(RC, A.nd - r0);
+      for (int it = 0; it < nin; it++) {
+        int src;
+        const zdc *c0, *c;
+        if (KIND == 0) {
+          src = A.ichild[8 * b + it];
+          if (nsrc(A.isrcse, src) <= 0) continue;
+          c0 = A.zcs + 3 * src;
+          c = A.zcs + 3 * b;
+        } else if (KIND == 1) {
+          src = A.l2[(size_t)b * A.mn2 + it];
+          if (nsrc(A.isrcse, src) <= 0) continue;
+          c0 = A.zcs + 3 * src;
+          c = A.zct + 3 * b;
+        } else {
+          src = par;
+          c0 = A.zct + 3 * par;
+          c = A.zct + 3 * b;
+        }
+        const Geo g = geo3(c0, c);
+        __syncthreads();
+        for (int m = tid; m <= p1; m += XNT) {
+          const zdc ef = zpown(g.cb + zmul_i(g.sb), m);
+          S.Ef[p1 + m] = ef;
+          S.Ef[p1 - m] = zinv(ef);
+        }
+        for (int m = tid; m <= p2; m += XNT) {
+          const zdc eb = zpown(g.cb - zmul_i(g.sb), m);
+          S.Eb[p2 + m] = eb;
+          S.Eb[p2 - m] = zinv(eb);
+        }
+        if (g.yr) rot_zero_pad(S, p1);
+        __syncthreads();
+        const zdc* gin = A.in + (A.base1 + (long)(src - A.lo1) * NC1) * nd + r0;
+        if (g.yr)
+          rot_nd<SLOTS, 0, 3>(A.T, p1, A.LT, A.dsc1, A.R1, S, g.ca, g.sa, g.zr, gin, nd, X1, RC,
+                              nval);
+        else
+          copy_nd<0, 3>(A.T, p1, S, g.zr, gin, nd, X1, RC, nval);
+        __syncthreads();
+        hshift_nd<KIND>(A, H, g.zz, X1, X2);
+        zdc* gout = A.out + (A.base2 + (long)(b - A.lo2) * NC2) * nd + r0;
+        if (g.yr) {
+          rot_zero_pad(S, p2);
+          __syncthreads();
+          rot_nd<SLOTS, 1, 3>(A.T, p2, A.LT, A.dsc2, A.R2, S, g.ca, -g.sa, g.zr, X2, RC, gout, nd,
+                              nval);
+        } else {
+          copy_nd<1, 3>(A.T, p2, S, g.zr, X2, RC, gout, nd, nval);
+        }
+      }
+    }
+  }
+}
+
+// column copies between the single-solve layout and the batched layout
+__global__ void k_put_col(long n, int nd, int r, const zdc* __restrict__ src, zdc* dst) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    dst[i * nd + r] = src[i];
+}
+__global__ void k_get_col(long n, int nd, int r, const zdc* __restrict__ src, zdc* dst) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    dst[i] = src[i * nd + r];
+}
+
+// one translation launch: its orders, node count and shared-memory plan
+struct HLaunch {
+  int p1, p2, nq, qc, slots, rot_smem;
+  size_t smem;
+  bool ok;
+};
+
+HLaunch plan_launch(int p1, int p2, int nq) {
+  HLaunch h{p1, p2, nq, 0, 0, 0, 0, false};
+  const int pmx = std::max(p1, p2);
+  h.slots = div_up((long)(pmx + 1) * (pmx + 1), XNT);
+  if (h.slots > 8) return h;
+  for (int tab = (p1 == p2) ? 1 : 0; tab >= 0; tab--) {
+    const size_t off = xsm_work_offset(pmx, tab != 0);
+    const size_t rot = xsm_layout(pmx, tab != 0, nullptr, nullptr) - off;
+    for (int qc = QCM; qc >= 1; qc /= 2) {
+      const size_t tot = off + std::max(rot, hsh_layout(p1, p2, nq, qc, nullptr, nullptr));
+      if (tot <= kHSmemMax) {
+        h.qc = qc;
+        h.rot_smem = tab;
+        h.smem = tot;
+        h.ok = true;
+        return h;
+      }
+    }
+  }
+  return h;
+}
+
+template <int KIND, int SLOTS>
+void launch_htrans_nd_k(const HTransNdArgs& A, int grid, size_t sm, cudaStream_t s) {
+  ZF_CUDA(cudaFuncSetAttribute(k_htrans3nd<KIND, SLOTS>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  klaunch(k_htrans3nd<KIND, SLOTS>, grid, XNT, sm, s, A);
+}
+
+// boxes lo..hi of output level l2 from input level l1
+template <int KIND>
+void launch_htrans_nd(HTransNdArgs A, const HelmPrep& H, int l1, int l2, int lo, int hi,
+                      int grid, cudaStream_t s) {
+  if (hi < lo) return;
+  const ShiftTab& st = H.sth[KIND * ML + l2];
+  const int p1 = H.lev.p[l1], p2 = H.lev.p[l2];
+  const HLaunch h = plan_launch(p1, p2, st.nq);
+  if (!h.ok) throw zf_error(ZF_ERR_ARG, "expansion order too large for the batched translation");
+  A.p1 = p1;
+  A.p2 = p2;
+  A.pmx = std::max(p1, p2);
+  A.nq = st.nq;
+  A.qc = h.qc;
+  A.rot_smem = h.rot_smem;
+  A.R1 = get_rottab(p1);
+  A.R2 = get_rottab(p2);
+  A.dsc1 = (2.0 * H.pmax + 1.0) / (2.0 * p1 + 1.0);
+  A.dsc2 = (2.0 * H.pmax + 1.0) / (2.0 * p2 + 1.0);
+  A.st = st;
+  A.base1 = H.lev.base[l1];
+  A.lo1 = H.lev.lo[l1];
+  A.base2 = H.lev.base[l2];
+  A.lo2 = H.lev.lo[l2];
+  A.lo = lo;
+  A.hi = hi;
+  grid = std::max(1, std::min(grid, hi - lo + 1));
+  switch (h.slots) {
+    case 1: case 2: case 3: case 4: launch_htrans_nd_k<KIND, 4>(A, grid, h.smem, s); break;
+    case 5: case 6: launch_htrans_nd_k<KIND, 6>(A, grid, h.smem, s); break;
+    default: launch_htrans_nd_k<KIND, 8>(A, grid, h.smem, s); break;
+  }
+  ZF_LAUNCH_CHECK();
+}
+
+constexpr int kMinBatchH = 4;
+
+// every translation launch of the solve fits the batched kernel
+bool batched_fits(const Setup3D& S, const HelmPrep& H) {
+  const int nlev = S.tree.nlevels;
+  for (int l = 2; l <= nlev; l++) {
+    for (int kind = 0; kind < 3; kind++) {
+      int l1;
+      if (kind == 0) {
+        if (l >= nlev) continue;
+        l1 = l + 1;
+      } else if (kind == 1) {
+        l1 = l;
+      } else {
+        if (l < 3) continue;
+        l1 = l - 1;
+      }
+      if (!plan_launch(H.lev.p[l1], H.lev.p[l], H.sth[kind * ML + l].nq).ok) return false;
+    }
+  }
+  return true;
+}
+
+}  // namespace
+
+void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in, int ifpgh,
+                          zdc* pot, zdc* grad, cudaStream_t s, StepTimes* times) {
+  const Setup3D& S = P.S;
+  const int ns = P.ns, nt = P.nt;
+  const bool timing = times != nullptr;
+  cudaEvent_t ev[8];
+  if (timing)
+    for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  auto mark = [&](int i) {
+    if (timing) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  long launches0 = launch_counter();
+  mark(0);
+  HelmPrep H;
+  helm_prep(S, P.eps, zk, P.isep, H, s);
+  mark(1);
+  if (nd < kMinBatchH || !batched_fits(S, H)) {
+    float prep_ms = 0;
+    if (timing) {
+      ZF_CUDA(cudaEventSynchronize(ev[1]));
+      ZF_CUDA(cudaEventElapsedTime(&prep_ms, ev[0], ev[1]));
+      for (auto& e : ev) cudaEventDestroy(e);
+    }
+    helm_plan_loop(P, H, nd, in, ifpgh, pot, grad, s, times, prep_ms);
+    return;
+  }
+  const DevTree& t = S.tree;
+  const DevLists& L = S.lists;
+  const int nb = t.nboxes, nlev = t.nlevels;
+  const long tot = std::max<long>(H.tot, 1);
+  DevBuf<zdc> q(ns, s), ds(ns, s), dv(3 * (size_t)ns, s), mp1(tot, s), loc1(tot, s),
+      mpn((size_t)tot * nd, s), locn((size_t)tot * nd, s), potsort(nt, s),
+      gradsort(ifpgh > 1 ? 3 * (size_t)nt : 1, s);
+  mpn.zero();
+  locn.zero();
+  const int cgrid = std::min(div_up(tot, 256), 148 * 16);
+  auto gather = [&](int r) {
+    gather_strengths_col(S, ns, nd, r, in.ifcharge ? in.charge : nullptr,
+                         in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
+                         true, true, q.get(), ds.get(), dv.get(), s);
+  };
+  // P2M and P2L per right-hand side into the batched expansions (P2L first:
+  // the M2L launches add to it)
+  for (int r = 0; r < nd; r++) {
+    gather(r);
+    if (nlev >= 2) {
+      mp1.zero();
+      helm_form(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, false, mp1.get(), s);
+      klaunch(k_put_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)mp1.get(), mpn.get());
+      ZF_LAUNCH_CHECK();
+    }
+    if (L.mn[3] > 0) {
+      loc1.zero();
+      helm_form(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, true, loc1.get(), s);
+      klaunch(k_put_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)loc1.get(), locn.get());
+      ZF_LAUNCH_CHECK();
+    }
+  }
+  mark(2);
+  int dev = 0, nsm = 148;
+  ZF_CUDA(cudaGetDevice(&dev));
+  ZF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int xgrid = std::max(1, std::min(nsm, nb));
+  const size_t per_cta = 2 * (size_t)(H.pmax + 1) * (H.pmax + 1) * RC;
+  DevBuf<zdc> scratch((size_t)xgrid * per_cta, s);
+  HTransNdArgs A;
+  A.T = H.T;
+  A.LT = H.pmax + 1;
+  A.kwave = H.kw;
+  A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
+  A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
+  A.zcs = S.zcsrc.get(); A.zct = S.zctarg.get();
+  A.nl2 = L.n[1].get(); A.l2 = L.list[1].get(); A.nl4 = L.n[3].get(); A.mn2 = L.mn[1];
+  A.scratch = scratch.get();
+  A.scr_per_cta = (long)per_cta;
+  A.nd = nd;
+  // M2M, finest parents first (parents at levels >= 2)
+  A.in = mpn.get();
+  A.out = mpn.get();
+  for (int l = nlev - 1; l >= 2; l--)
+    launch_htrans_nd<0>(A, H, l + 1, l, t.laddr[2 * l], t.laddr[2 * l + 1], xgrid, s);
+  mark(3);
+  // M2L per level >= 2
+  A.in = mpn.get();
+  A.out = locn.get();
+  for (int l = 2; l <= nlev; l++)
+    launch_htrans_nd<1>(A, H, l, l, t.laddr[2 * l], t.laddr[2 * l + 1], xgrid, s);
+  mark(4);
+  // L2L, coarsest first: children at level l+1 of parents at level l >= 2
+  A.in = locn.get();
+  A.out = locn.get();
+  for (int l = 2; l <= nlev - 1; l++)
+    launch_htrans_nd<2>(A, H, l, l + 1, t.laddr[2 * (l + 1)], t.laddr[2 * (l + 1) + 1], xgrid, s);
+  mark(5);
+  // P2P, L2T and M2T per right-hand side
+  for (int r = 0; r < nd; r++) {
+    gather(r);
+    klaunch(k_get_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)mpn.get(), mp1.get());
+    klaunch(k_get_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)locn.get(), loc1.get());
+    ZF_LAUNCH_CHECK();
+    potsort.zero();
+    gradsort.zero();
+    helm_eval(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, ifpgh, mp1.get(),
+              loc1.get(), potsort.get(), gradsort.get(), s);
+    unsort3d_col(nt, nd, r, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0),
+                 mkz(1.0 / S.b0), ifpgh, pot, grad, s);
+  }
+  mark(6);
+  mark(7);
+  if (timing) {
+    ZF_CUDA(cudaEventSynchronize(ev[7]));
+    float ms;
+    // set-up = the wavenumber tables; P2M column = P2M and P2L of every
+    // right-hand side; eval = P2P, L2T, M2T and the unsort
+    for (int i = 0; i < 7; i++) {
+      ZF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      times->ms[i] = ms;
+    }
+    times->nboxes = nb;
+    times->nlevels = nlev;
+    times->nterms = H.pmax;
+    for (auto& e : ev) cudaEventDestroy(e);
+    times->launches = launch_counter() - launches0;
+    if (times->want_counts) count_interactions3d(S, H.lev.p, 2, 2, 3, times, s);
+  }
+}
+
+}  // namespace zf
