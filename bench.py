@@ -73,6 +73,15 @@ WORKLOADS = {
     # small case of the same distribution for kernel profiles (one 32-right-hand-side pass)
     "zlfmm3d_batched_30k_32": dict(kind="lap3d", n=30_000, nrhs=32, eps=1e-9, ifpgh=2,
                                    isep=1, cpu_n=30_000, dipoles=False),
+    # zhfmm3d batched right-hand sides: one geometry of 200,000 points on the
+    # unit sphere displaced by 0.1i times the normal scaled by a degree-4 field
+    # (the instance distribution below), 64 complex normal charge and dipole
+    # strength vectors with shared complex dipole vectors, zk = 10+0.2i,
+    # pot + grad, eps=1e-9; one step = plan + one 64-right-hand-side solve
+    "zhfmm3d_batched_200k_64": dict(kind="helm3d", n=200_000, nrhs=64, eps=1e-9, zk=10 + 0.2j,
+                                    ifpgh=2, isep=1, cpu_n=30_000, dipoles=True),
+    "zhfmm3d_batched_30k_32": dict(kind="helm3d", n=30_000, nrhs=32, eps=1e-9, zk=10 + 0.2j,
+                                   ifpgh=2, isep=1, cpu_n=30_000, dipoles=True),
     # zhfmm3d batched uneven instances: 200 independent FMMs, point counts
     # log-uniform in [2,000, 500,000], points on unit spheres displaced by 0.1i
     # times the normal scaled by a degree-4 field, zk = 10+0.2i, charges +
@@ -169,6 +178,30 @@ def nd_trans3_flops(p, nd, kind=1):
     return gen + rot + shift
 
 
+def nd_htrans3_flops(p1, p2, nd):
+    """Real flops of one batched 3D Helmholtz translation of nd right-hand
+    sides from order p1 to p2, as implemented: the two batched rotations (as
+    nd_trans3_flops, orders p1 and p2) and the quadrature z-shift over
+    nq = int(2.5 p2) nodes: per 32-right-hand-side pass its node tables (60
+    flops per (node, n, m >= 0) value / derivative coefficient pair, 4 per
+    projection entry); per right-hand side the node sums (two complex MACs per
+    (node, n, +-m)) and the projection (two real-by-complex MACs per
+    (node, n', +-m))."""
+    nq = int(2.5 * p2)
+    passes = -(-nd // 32)
+
+    def rot(p):
+        L = p + 1
+        tri = L * (L + 1) // 2
+        return passes * 100 * L * tri + nd * (L * tri * 8 + L * tri * 4)
+
+    tri1, tri2 = (p1 + 1) * (p1 + 2) // 2, (p2 + 1) * (p2 + 2) // 2
+    tabs = passes * nq * (60 * tri1 + 4 * tri2)
+    sums = sum((1 if m == 0 else 2) * ((p1 + 1 - m) * 16 + (p2 + 1 - m) * 8)
+               for m in range(min(p1, p2) + 1))
+    return rot(p1) + rot(p2) + tabs + nd * nq * sums
+
+
 # Algorithmic work per interaction (real flops; complex add 2, mul 6, div 11;
 # transcendental functions are not counted), per the frozen convention of the
 # project's measurement plan.  P = 2p+1 coefficients of the level.
@@ -196,6 +229,12 @@ def make_inputs(wl, seed, n=None, nrhs=1):
     n = wl["n"] if n is None else n
     if wl["kind"] == "lap3d" and nrhs > 1:
         return W.lap3d_uniform(n, seed=seed, nrhs=nrhs)
+    if wl["kind"] == "helm3d" and nrhs > 1:
+        w = W.sphere3d(n, seed=seed)
+        rng = np.random.default_rng(seed + 7919)
+        cn = lambda: rng.standard_normal((nrhs, n)) + 1j * rng.standard_normal((nrhs, n))
+        w["charge"], w["dipstr"] = cn(), cn()
+        return w
     if wl["kind"] == "lap2d":
         return W.lap2d_uniform(n, seed=seed)
     if wl["kind"] == "helm2d":
@@ -542,31 +581,49 @@ def run_ours_batched(args, wl, ws, rank, local):
     L = _capi.lib()
     n, nd = wl["n"], wl["nrhs"]
     ifpgh, isep, eps = wl["ifpgh"], wl["isep"], wl["eps"]
+    helm = wl["kind"] == "helm3d"
+    ifd = 1 if wl.get("dipoles", False) else 0
+    zk = complex(wl.get("zk", 0))
+    zka = np.array([zk.real, zk.imag])
+    zkp = zka.ctypes.data_as(ctypes.c_void_p)
     inp = make_inputs(wl, seed=rank, nrhs=nd)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     zs = t(inp["zsrc"].T)
     q = t(inp["charge"].T)  # (n, nd): right-hand side fastest
+    ds = t(inp["dipstr"].T) if ifd else None
+    dv = t(inp["dipvec"].T) if ifd else None
     pot = torch.empty((n, nd), dtype=torch.complex128, device=dev)
     grad = torch.empty((n, 3, nd), dtype=torch.complex128, device=dev)
     pot1 = torch.empty(n, dtype=torch.complex128, device=dev)
     grad1 = torch.empty((n, 3), dtype=torch.complex128, device=dev)
     q0 = t(inp["charge"][0])
+    ds0 = t(inp["dipstr"][0]) if ifd else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sp = ctypes.c_void_p(stream.cuda_stream)
     P = lambda x: ctypes.c_void_p(x.data_ptr())
     plan_ms = []
 
+    Po = lambda x: None if x is None else P(x)
+
     def solve():
         h = ctypes.c_void_p()
         _capi.check(L.zfmm_plan3d_create_dev(eps, n, P(zs), n, P(zs), isep, sp, ctypes.byref(h)))
-        _capi.check(L.zfmm_zlfmm3d_plan_dev(h, nd, 1, P(q), 0, None, None, ifpgh, P(pot),
-                                            P(grad), sp))
+        if helm:
+            _capi.check(L.zfmm_zhfmm3d_plan_dev(h, zkp, nd, 1, P(q), ifd, Po(ds), Po(dv), ifpgh,
+                                                P(pot), P(grad), sp))
+        else:
+            _capi.check(L.zfmm_zlfmm3d_plan_dev(h, nd, 1, P(q), ifd, Po(ds), Po(dv), ifpgh,
+                                                P(pot), P(grad), sp))
         _capi.check(L.zfmm_plan3d_destroy(h))
 
     def solve_plain():
-        _capi.check(L.zfmm_zlfmm3d_dev(eps, n, P(zs), 1, P(q0), 0, None, None, P(pot1),
-                                       P(grad1), n, P(zs), ifpgh, isep, sp))
+        if helm:
+            _capi.check(L.zfmm_zhfmm3d_dev(eps, zkp, n, P(zs), 1, P(q0), ifd, Po(ds0), Po(dv),
+                                           P(pot1), P(grad1), n, P(zs), ifpgh, isep, sp))
+        else:
+            _capi.check(L.zfmm_zlfmm3d_dev(eps, n, P(zs), 1, P(q0), ifd, Po(ds0), Po(dv),
+                                           P(pot1), P(grad1), n, P(zs), ifpgh, isep, sp))
 
     for _ in range(max(args.warmup, 3)):
         solve()
@@ -633,15 +690,23 @@ def run_ours_batched(args, wl, ws, rank, local):
     # end to end: host arrays in pinned memory through the host entry points
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     hz, hq = pin(inp["zsrc"].T), pin(inp["charge"].T)
+    hds = pin(inp["dipstr"].T) if ifd else None
+    hdv = pin(inp["dipvec"].T) if ifd else None
     hpot = torch.empty((n, nd), dtype=torch.complex128).pin_memory().numpy()
     hgrad = torch.empty((n, 3, nd), dtype=torch.complex128).pin_memory().numpy()
     hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
 
+    hpo = lambda a: None if a is None else hp(a)
+
     def solve_host():
         h = ctypes.c_void_p()
         _capi.check(L.zfmm_plan3d_create(eps, n, hp(hz), n, hp(hz), isep, ctypes.byref(h)))
-        _capi.check(L.zfmm_zlfmm3d_plan(h, nd, 1, hp(hq), 0, None, None, ifpgh, hp(hpot),
-                                        hp(hgrad)))
+        if helm:
+            _capi.check(L.zfmm_zhfmm3d_plan(h, zkp, nd, 1, hp(hq), ifd, hpo(hds), hpo(hdv),
+                                            ifpgh, hp(hpot), hp(hgrad)))
+        else:
+            _capi.check(L.zfmm_zlfmm3d_plan(h, nd, 1, hp(hq), ifd, hpo(hds), hpo(hdv), ifpgh,
+                                            hp(hpot), hp(hgrad)))
         _capi.check(L.zfmm_plan3d_destroy(h))
 
     solve_host()
@@ -657,7 +722,7 @@ def run_ours_batched(args, wl, ws, rank, local):
         tt = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_tot = float(tt.item())
-    h2d = 2 * hz.nbytes + hq.nbytes
+    h2d = 2 * hz.nbytes + hq.nbytes + (hds.nbytes + hdv.nbytes if ifd else 0)
     d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
     # accuracy: right-hand sides 0 and nd-1 against the FP64 direct sum on a subset
     rng = np.random.default_rng(1234)
@@ -665,8 +730,14 @@ def run_ours_batched(args, wl, ws, rank, local):
     pg = pot.cpu().numpy()
     errs = []
     for r in (0, nd - 1):
-        pd, _ = zfmm_b200.zl3devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
-                                         inp["charge"][r], None, None, 1, 0, 1)
+        dsr = inp["dipstr"][r] if ifd else None
+        dvr = inp["dipvec"] if ifd else None
+        if helm:
+            pd, _ = zfmm_b200.zh3devaldirect(zk, len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                             inp["charge"][r], dsr, dvr, 1, ifd, 1)
+        else:
+            pd, _ = zfmm_b200.zl3devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                             inp["charge"][r], dsr, dvr, 1, ifd, 1)
         errs.append(float(np.linalg.norm(pg[sub, r] - pd) / np.linalg.norm(pd)))
     # plain vs batched agreement on right-hand side 0 (same tree, same algorithm)
     p1 = pot1.cpu().numpy()
@@ -675,7 +746,12 @@ def run_ours_batched(args, wl, ws, rank, local):
     p = info["nterms"]
     avg = {k: v / args.steps for k, v in step_ms.items()}
     m2l_pairs = sum(lvl["m2l_pairs"])
-    flops_m2l = nd_trans3_flops(p, nd, 1) * m2l_pairs
+    if helm:
+        flops_m2l = sum(c * nd_htrans3_flops(o, o, nd) for c, o in zip(lvl["m2l_pairs"], orders))
+        per_trans = {"per_level_order": orders, "m2l_pairs_per_level": lvl["m2l_pairs"]}
+    else:
+        flops_m2l = nd_trans3_flops(p, nd, 1) * m2l_pairs
+        per_trans = {"translation_nd": nd_trans3_flops(p, nd, 1)}
     achieved = flops_m2l / (avg["m2l_p2l"] * 1e-3) / 1e12
     peak = float(L.zfmm_probe_fp64_tflops(20000))
     cpu = None
@@ -696,7 +772,8 @@ def run_ours_batched(args, wl, ws, rank, local):
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": {"workload": args.workload, "n": n, "nrhs": nd, "eps": eps, "ifpgh": ifpgh,
-                   "isep": isep, "charges": True, "dipoles": False,
+                   "isep": isep, "charges": True, "dipoles": bool(ifd),
+                   **({"zk": [zk.real, zk.imag]} if helm else {}),
                    "step": "plan (tree, lists, centres) + one solve of all right-hand sides",
                    "l2": "flushed (256 MiB write) between steps",
                    "parallelism": f"replicas x{ws}", "nboxes": info["nboxes"],
@@ -709,13 +786,14 @@ def run_ours_batched(args, wl, ws, rank, local):
         "rel_l2_err_vs_direct": max(errs),
         "rel_l2_batched_vs_plain_rhs0": agree,
         "step_ms": {k: round(v, 4) for k, v in avg.items()},
-        "roofline": {"bound": "fp64", "kernel": "m2l_p2l (k_trans3nd)", "achieved": achieved,
+        "roofline": {"bound": "fp64",
+                     "kernel": "m2l_p2l (%s)" % ("k_htrans3nd" if helm else "k_trans3nd"),
+                     "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None,
                      "peak_source": "measured FP64 FMA probe (zfmm_probe_fp64_tflops)",
                      "traffic": None, "flops_per_step": flops_m2l,
-                     "flop_model": {"translation_nd": nd_trans3_flops(p, nd, 1),
-                                    "m2l_pairs": m2l_pairs}},
+                     "flop_model": dict(per_trans, m2l_pairs=m2l_pairs)},
         "interactions": counts,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

@@ -23,10 +23,17 @@
 //                degrees and nodes then run for the 32 right-hand sides with
 //                the lane as the right-hand-side index.
 //
-// P2M, P2L, P2P, L2T and M2T run per right-hand side through the single-solve
-// passes on the plan's tree; their expansions move in and out of the batched
-// layout by column copies.  Fewer than 4 right-hand sides, or orders whose
-// working set exceeds shared memory, run every pass per right-hand side.
+//   k_hp2p3nd    list-1 direct interactions: the pair's kernel values (complex
+//                distance, e^{ikR}, the gradient factors) once for HRB
+//                right-hand sides held in registers.
+//   k_heval3nd   L2T / M2T: a thread per target; the radial table and the
+//                Legendre recurrences once per (target, expansion) for HRBE
+//                right-hand sides.
+//
+// P2M and P2L run per right-hand side through the single-solve form kernel on
+// the plan's tree; their expansions move into the batched layout by column
+// copies.  Fewer than 4 right-hand sides, or orders whose working set exceeds
+// shared memory, run every pass per right-hand side.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -43,20 +50,21 @@ namespace zf {
 namespace {
 
 constexpr int QCM = 8;  // nodes per chunk of the z-shift (at most)
+constexpr int PB = 8;   // output rows per read-modify-write block of the z-shift
 constexpr size_t kHSmemMax = 227 * 1024;
 
-// z-shift tables, aliasing the rotation's work block
+// z-shift tables of one node chunk, aliasing the rotation's work block
 struct HSh {
-  zdc* node;   // nq x 6: cos, sin of the node's polar angle about the old centre,
+  zdc* node;   // qc x 6: cos, sin of the node's polar angle about the old centre,
                // their ratios to the radius, the node's real sin and cos
-  zdc* rad;    // nq x (p1+2): radial functions of the input kind at k r
-  zdc* drad;   // nq x (p1+2): their k-scaled derivatives
+  zdc* rad;    // qc x (p1+2): radial functions of the input kind at k r
+  zdc* drad;   // qc x (p1+2): their k-scaled derivatives
   zdc* Zc;     // qc x np1: value coefficients of the chunk's nodes, (n, m >= 0) at jdx(n, m)
   zdc* Dc;     // qc x np1: normal-derivative coefficients
   double* Yt;  // qc x np2: projection columns (Legendre at the real node x weight)
 };
 
-__host__ __device__ inline size_t hsh_layout(int p1, int p2, int nq, int qc, char* base, HSh* o) {
+__host__ __device__ inline size_t hsh_layout(int p1, int p2, int qc, char* base, HSh* o) {
   const size_t P2 = p1 + 2, np1 = (size_t)(p1 + 1) * (p1 + 2) / 2,
                np2 = (size_t)(p2 + 1) * (p2 + 2) / 2;
   size_t off = 0;
@@ -66,9 +74,9 @@ __host__ __device__ inline size_t hsh_layout(int p1, int p2, int nq, int qc, cha
     return q;
   };
   HSh H;
-  H.node = (zdc*)take((size_t)nq * 6 * 16);
-  H.rad = (zdc*)take((size_t)nq * P2 * 16);
-  H.drad = (zdc*)take((size_t)nq * P2 * 16);
+  H.node = (zdc*)take((size_t)qc * 6 * 16);
+  H.rad = (zdc*)take((size_t)qc * P2 * 16);
+  H.drad = (zdc*)take((size_t)qc * P2 * 16);
   H.Zc = (zdc*)take((size_t)qc * np1 * 16);
   H.Dc = (zdc*)take((size_t)qc * np1 * 16);
   H.Yt = (double*)take((size_t)qc * np2 * 8);
@@ -118,46 +126,46 @@ __device__ void hshift_nd(const HTransNdArgs& A, const HSh& H, zdc zsh, const zd
     __syncthreads();
     return;
   }
-  // (a) node geometry and radial tables, one thread per node
-  for (int t = tid; t < nq; t += XNT) {
-    const double x = __ldg(&ST.x[t]);
-    const double yi = sqrt(1 - x * x);
-    const zdc zi = zsh + mkz(ST.r * x);
-    const zdc ri = zsqrt_r(mkz((ST.r * yi) * (ST.r * yi)) + zi * zi);
-    const zdc cthi = zi / ri;
-    const zdc sthi = zsqrt_r(mkz(1.0) - cthi * cthi);
-    zdc* nd = H.node + 6 * t;
-    nd[0] = cthi;
-    nd[1] = sthi;
-    nd[2] = cthi / ri;
-    nd[3] = sthi / ri;
-    nd[4] = mkz(yi);
-    nd[5] = mkz(x);
-    const zdc zk = ri * A.kwave;
-    zdc* f = H.rad + (size_t)t * P2;
-    zdc* fd = H.drad + (size_t)t * P2;
-    if (KIND == 2) besseljs3d_z(p1, zk, ST.rs1, f, fd);
-    else h3dall_z(p1, zk, ST.rs1, f, fd);
-    for (int n = 0; n <= p1; n++) fd[n] = A.kwave * fd[n];
-  }
-  __syncthreads();
   const int ncol = (p1 > p2 ? p1 : p2) + 1;
   const int ntask = 2 * p2 + 1;
   for (int q0 = 0; q0 < nq; q0 += qc) {
     const int nc = min(qc, nq - q0);
+    // (a) node geometry and radial tables, one thread per node of the chunk
+    for (int t = tid; t < nc; t += XNT) {
+      const double x = __ldg(&ST.x[q0 + t]);
+      const double yi = sqrt(1 - x * x);
+      const zdc zi = zsh + mkz(ST.r * x);
+      const zdc ri = zsqrt_r(mkz((ST.r * yi) * (ST.r * yi)) + zi * zi);
+      const zdc cthi = zi / ri;
+      const zdc sthi = zsqrt_r(mkz(1.0) - cthi * cthi);
+      zdc* nd = H.node + 6 * t;
+      nd[0] = cthi;
+      nd[1] = sthi;
+      nd[2] = cthi / ri;
+      nd[3] = sthi / ri;
+      nd[4] = mkz(yi);
+      nd[5] = mkz(x);
+      const zdc zk = ri * A.kwave;
+      zdc* f = H.rad + (size_t)t * P2;
+      zdc* fd = H.drad + (size_t)t * P2;
+      if (KIND == 2) besseljs3d_z(p1, zk, ST.rs1, f, fd);
+      else h3dall_z(p1, zk, ST.rs1, f, fd);
+      for (int n = 0; n <= p1; n++) fd[n] = A.kwave * fd[n];
+    }
+    __syncthreads();
     // (b) one thread per (node, order m >= 0): the value and normal-derivative
     // coefficients of the expansion's (n, +-m) terms at the node, and the
     // projection column of order m at the real node
     for (int item = tid; item < nc * ncol; item += XNT) {
       const int t = item / ncol, m = item - t * ncol, node = q0 + t;
-      const zdc* nd = H.node + 6 * node;
+      const zdc* nd = H.node + 6 * t;
       const double x = nd[5].re, yi = nd[4].re;
       if (m <= p1) {
         const zdc z = nd[0], sthi = nd[1], cr = nd[2], sr = nd[3];
         const zdc zz1 = mkz(1.0) - z * z;
         const zdc u = -zsqrt_r(zz1);
-        const zdc* f = H.rad + (size_t)node * P2;
-        const zdc* fd = H.drad + (size_t)node * P2;
+        const zdc* f = H.rad + (size_t)t * P2;
+        const zdc* fd = H.drad + (size_t)t * P2;
         zdc* zc = H.Zc + (size_t)t * np1;
         zdc* dc = H.Dc + (size_t)t * np1;
         const double sgm = ((m & 1) ? -1.0 : 1.0) * s4i;
@@ -240,6 +248,7 @@ __device__ void hshift_nd(const HTransNdArgs& A, const HSh& H, zdc zsh, const zd
       zdc F[QCM], D[QCM];
 #pragma unroll
       for (int t = 0; t < QCM; t++) F[t] = D[t] = mkz(0.0);
+#pragma unroll 4
       for (int n = m; n <= p1; n++) {
         const zdc a = ldcg_z(X1 + ix3(n, mm) * RC + lane);
         const int j = jdx(n, m);
@@ -251,20 +260,29 @@ __device__ void hshift_nd(const HTransNdArgs& A, const HSh& H, zdc zsh, const zd
           }
         }
       }
-      for (int n = m; n <= p2; n++) {
-        const int j = jdx(n, m);
-        zdc sF = mkz(0.0), sD = mkz(0.0);
+      // output rows in blocks of PB: the previous chunks' partial sums are
+      // fetched together, so their L2 round trips overlap
+      for (int nb = m; nb <= p2; nb += PB) {
+        zdc old[PB];
 #pragma unroll
-        for (int t = 0; t < QCM; t++) {
-          if (t < nc) {
-            const double y = H.Yt[t * np2 + j];
-            sF += y * F[t];
-            sD += y * D[t];
+        for (int k = 0; k < PB; k++)
+          old[k] = (q0 > 0 && nb + k <= p2) ? ldcg_z(X2 + ix3(nb + k, mm) * RC + lane) : mkz(0.0);
+#pragma unroll
+        for (int k = 0; k < PB; k++) {
+          const int n = nb + k;
+          if (n > p2) break;
+          const int j = jdx(n, m);
+          zdc sF = mkz(0.0), sD = mkz(0.0);
+#pragma unroll
+          for (int t = 0; t < QCM; t++) {
+            if (t < nc) {
+              const double y = H.Yt[t * np2 + j];
+              sF += y * F[t];
+              sD += y * D[t];
+            }
           }
+          stcg_z(X2 + ix3(n, mm) * RC + lane, old[k] + ST.cF[n] * sF + ST.cD[n] * sD);
         }
-        const zdc v = ST.cF[n] * sF + ST.cD[n] * sD;
-        zdc* o = X2 + ix3(n, mm) * RC + lane;
-        stcg_z(o, q0 == 0 ? v : ldcg_z(o) + v);
       }
     }
     __syncthreads();
@@ -279,7 +297,7 @@ __global__ void __launch_bounds__(XNT, 1) k_htrans3nd(HTransNdArgs A) {
   XSm S;
   xsm_layout(A.pmx, A.rot_smem != 0, sm, &S);
   HSh H;
-  hsh_layout(p1, p2, A.nq, A.qc, (char*)S.Csr, &H);
+  hsh_layout(p1, p2, A.qc, (char*)S.Csr, &H);
   if (S.cw) {
     // one rotation order in this launch (p1 = p2): its tables staged once
     const int CP = rot_cp(p1 + 1), TP = rot_tp(p1 + 1);
@@ -360,14 +378,328 @@ __global__ void __launch_bounds__(XNT, 1) k_htrans3nd(HTransNdArgs A) {
   }
 }
 
-// column copies between the single-solve layout and the batched layout
+// ---- P2P (list 1), RB right-hand sides per thread pass ---------------------------
+constexpr int HNDT = 128;  // threads of the batched P2P and evaluation kernels
+constexpr int HRB = 8;     // right-hand sides per thread pass of the P2P kernel
+constexpr int HRBE = 4;    // right-hand sides per thread pass of the L2T / M2T kernel
+constexpr int HPT = 64;    // sources per shared-memory tile
+
+struct HP2PNdArgs {
+  const int *nchild, *isrcse, *itargse;
+  const zdc *zsrc, *q, *ds, *dv, *ztarg;
+  const int *nl1, *l1;
+  int mn1, nb, nd, ifcharge;
+  zdc zk;
+  zdc *pot, *grad;
+};
+
+struct HSrcTileNd {
+  zdc y[HPT][3];
+  zdc q[HPT][HRB];
+  zdc ds[HPT][HRB];
+  zdc v[HPT][3];
+};
+
+// the pair interaction of zh3devaldirect (zhfmm3d.f:606-693): the pair's kernel
+// values once, then one complex MAC per output and right-hand side
+template <bool GRAD, bool DIP>
+__global__ void __launch_bounds__(HNDT) k_hp2p3nd(HP2PNdArgs A) {
+  extern __shared__ unsigned char smraw[];
+  HSrcTileNd& S = *reinterpret_cast<HSrcTileNd*>(smraw);
+  constexpr double PI4I = 0.079577471545947667884;
+  const int b = blockIdx.x;
+  if (b >= A.nb) return;
+  const int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
+  if (A.nchild[b] != 0 || t1 < t0 || A.nl1[b] == 0) return;
+  const long nd = A.nd;
+  const zdc zk = A.zk, zk2 = zk * zk;
+  for (int c0 = t0; c0 <= t1; c0 += HNDT) {
+    const int i = c0 + threadIdx.x;
+    const bool valid = i <= t1;
+    zdc x[3] = {mkz(0.0), mkz(0.0), mkz(0.0)};
+    if (valid) {
+      x[0] = ldz(&A.ztarg[3 * i]);
+      x[1] = ldz(&A.ztarg[3 * i + 1]);
+      x[2] = ldz(&A.ztarg[3 * i + 2]);
+    }
+    const int rb = blockIdx.y * HRB;
+    const int nv = min(HRB, A.nd - rb);
+    zdc P[HRB], G0[HRB], G1[HRB], G2[HRB];
+#pragma unroll
+    for (int r = 0; r < HRB; r++) P[r] = G0[r] = G1[r] = G2[r] = mkz(0.0);
+    for (int li = 0; li < A.nl1[b]; li++) {
+      const int jb = A.l1[(size_t)b * A.mn1 + li];
+      const int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
+      for (int j0 = s0; j0 <= s1; j0 += HPT) {
+        const int n = min(HPT, s1 - j0 + 1);
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += HNDT) {
+          const int j = j0 + k;
+          S.y[k][0] = ldz(&A.zsrc[3 * j]);
+          S.y[k][1] = ldz(&A.zsrc[3 * j + 1]);
+          S.y[k][2] = ldz(&A.zsrc[3 * j + 2]);
+          if (DIP) {
+            S.v[k][0] = ldz(&A.dv[3 * j]);
+            S.v[k][1] = ldz(&A.dv[3 * j + 1]);
+            S.v[k][2] = ldz(&A.dv[3 * j + 2]);
+          }
+        }
+        for (int k = threadIdx.x; k < n * HRB; k += HNDT) {
+          const int kk = k / HRB, r = k - kk * HRB;
+          const long off = (long)(j0 + kk) * nd + rb + r;
+          S.q[kk][r] = (r < nv && A.ifcharge) ? ldz(&A.q[off]) : mkz(0.0);
+          if (DIP) S.ds[kk][r] = r < nv ? ldz(&A.ds[off]) : mkz(0.0);
+        }
+        __syncthreads();
+        if (!valid) continue;
+        for (int k = 0; k < n; k++) {
+          const zdc x0 = x[0] - S.y[k][0], x1 = x[1] - S.y[k][1], x2 = x[2] - S.y[k][2];
+          const zdc rz = zsqrt_p(x0 * x0 + x1 * x1 + x2 * x2);
+          if (!(zabs(rz) > (double)1e-16f)) continue;
+          const zdc z = zmul_i(zk * rz);
+          const zdc ez = zexp_p(z);
+          const zdc ir = zinv(rz);
+          const zdc r1 = ir * PI4I;
+          const zdc r3 = r1 * (ir * ir);
+          const zdc t4 = mkz(1.0) - z;
+          if (A.ifcharge) {
+            const zdc kq = ez * r1, hq = ez * t4 * r3;
+            const zdc w0 = -(hq * x0), w1 = -(hq * x1), w2 = -(hq * x2);
+#pragma unroll
+            for (int r = 0; r < HRB; r++) {
+              const zdc qv = S.q[k][r];
+              P[r] += qv * kq;
+              if (GRAD) {
+                G0[r] += qv * w0;
+                G1[r] += qv * w1;
+                G2[r] += qv * w2;
+              }
+            }
+          }
+          if (DIP) {
+            const zdc dot = x0 * S.v[k][0] + x1 * S.v[k][1] + x2 * S.v[k][2];
+            const zdc e3 = ez * r3;
+            const zdc kd = -(e3 * dot * t4);
+            zdc d0 = mkz(0.0), d1 = mkz(0.0), d2 = mkz(0.0);
+            if (GRAD) {
+              const zdc tt1 = dot * e3 * (zk2 - 3.0 * (t4 * (ir * ir)));
+              const zdc tt2 = t4 * e3;
+              d0 = -(S.v[k][0] * tt2 + x0 * tt1);
+              d1 = -(S.v[k][1] * tt2 + x1 * tt1);
+              d2 = -(S.v[k][2] * tt2 + x2 * tt1);
+            }
+#pragma unroll
+            for (int r = 0; r < HRB; r++) {
+              const zdc dsv = S.ds[k][r];
+              P[r] += dsv * kd;
+              if (GRAD) {
+                G0[r] += dsv * d0;
+                G1[r] += dsv * d1;
+                G2[r] += dsv * d2;
+              }
+            }
+          }
+        }
+      }
+    }
+    if (valid)
+#pragma unroll
+      for (int r = 0; r < HRB; r++)
+        if (r < nv) {
+          A.pot[(long)i * nd + rb + r] += P[r];
+          if (GRAD) {
+            A.grad[(3L * i) * nd + rb + r] += G0[r];
+            A.grad[(3L * i + 1) * nd + rb + r] += G1[r];
+            A.grad[(3L * i + 2) * nd + rb + r] += G2[r];
+          }
+        }
+  }
+}
+
+// ---- L2T / M2T, HRBE right-hand sides per thread pass ---------------------------
+struct HEvalNdArgs {
+  const double *r1, *r2, *sq;
+  int L;
+  const int *ilevel, *nchild, *isrcse, *itargse;
+  const zdc *ztarg, *zcs, *zct;
+  HLev lev;
+  const zdc *mp, *loc;
+  const int *nl3, *l3;
+  int mn3, nb, nd;
+  zdc zk;
+  zdc *pot, *grad;
+};
+
+// zh3devalmp (LOCAL = false: h_n) / zh3devalloc (LOCAL = true: j_n) of one
+// target for nv <= HRBE right-hand sides; e: coefficient rows of stride nd.
+// The radial table and the Legendre recurrences are formed once and applied
+// to every right-hand side; the gradient accumulates in spherical components.
+template <bool GRAD, bool LOCAL>
+__device__ __forceinline__ void heval_one_nd(const HEvalNdArgs& A, const zdc* __restrict__ e,
+                                             long nd, int nv, int p, const Sph& s, double rscale,
+                                             zdc* P, zdc* Gr, zdc* Gt, zdc* Gp) {
+  const int L = A.L;
+  zdc f[PMAXR + 2], fd[GRAD ? PMAXR + 2 : 1];
+  const zdc zrk = s.rz * A.zk;
+  if (!LOCAL) h3dall_z(p, zrk, rscale, f, GRAD ? fd : nullptr);
+  else besseljs3d_z(p, zrk, rscale, f, GRAD ? fd : nullptr);
+  const zdc z = s.ct, zz1 = mkz(1.0) - z * z;
+  const zdc u = -zsqrt_r(zz1);
+  zdc Ydiag = mkz(1.0), em = mkz(1.0);
+  for (int m = 0; m <= p; m++) {
+    zdc emi = mkz(1.0);
+    if (m > 0) {
+      const double cmm = __ldg(&A.r1[m * L + m]);
+      if (GRAD) Ydiag = (m == 1) ? mkz(-cmm) : (Ydiag * u) * cmm;
+      else Ydiag = (Ydiag * u) * cmm;
+      em = em * s.eip;
+      emi = zinv(em);
+    }
+    const double sgm = (m & 1) ? -1.0 : 1.0;
+    zdc Yp = Ydiag, Dp = GRAD ? (Ydiag * (double)(-m)) * z : mkz(0.0);
+    zdc Ypp = mkz(0.0), Dpp = mkz(0.0);
+    for (int n = m; n <= p; n++) {
+      zdc Y, D = mkz(0.0);
+      if (n == m) {
+        Y = Yp;
+        D = Dp;
+      } else {
+        if (n == m + 1) {
+          const double c = __ldg(&A.r1[n * L + m]);
+          Y = (z * Yp) * c;
+          if (GRAD) D = (m == 0) ? (z * Dp + Yp) * c : (z * Dp + zz1 * Yp) * c;
+        } else {
+          const double c1 = __ldg(&A.r1[n * L + m]), c2 = __ldg(&A.r2[n * L + m]);
+          Y = (c1 * z) * Yp - c2 * Ypp;
+          if (GRAD)
+            D = (m == 0) ? c1 * (z * Dp + Yp) - c2 * Dpp : c1 * (z * Dp + zz1 * Yp) - c2 * Dpp;
+        }
+        Ypp = Yp;
+        Dpp = Dp;
+        Yp = Y;
+        Dp = D;
+      }
+      const double sc = __ldg(&A.sq[n]) * sgm;
+      const zdc y = Y * sc;
+      if (m == 0) {
+        const zdc* row = e + (long)ix3(n, 0) * nd;
+        const zdc bP = f[n] * y;
+        zdc bR = mkz(0.0), bT = mkz(0.0);
+        if (GRAD) {
+          const zdc dy = D * sc;
+          bR = A.zk * fd[n] * y;
+          bT = -(f[n] * dy * s.st);
+        }
+#pragma unroll
+        for (int r = 0; r < HRBE; r++)
+          if (r < nv) {
+            const zdc a0 = ldz(&row[r]);
+            P[r] += a0 * bP;
+            if (GRAD) {
+              Gr[r] += a0 * bR;
+              Gt[r] += a0 * bT;
+            }
+          }
+      } else {
+        const zdc* rowp = e + (long)ix3(n, m) * nd;
+        const zdc* rown = e + (long)ix3(n, -m) * nd;
+        const zdc bP = GRAD ? f[n] * y * s.st : f[n] * y;
+        zdc bR = mkz(0.0), bT = mkz(0.0), bF = mkz(0.0);
+        if (GRAD) {
+          const zdc dy = D * sc;
+          bR = A.zk * fd[n] * y * s.st;
+          bT = -(f[n] * dy);
+          bF = zmul_i((double)m * f[n] * y);
+        }
+#pragma unroll
+        for (int r = 0; r < HRBE; r++)
+          if (r < nv) {
+            const zdc z1 = ldz(&rowp[r]) * em, z2 = ldz(&rown[r]) * emi;
+            const zdc Sp = z1 + z2;
+            P[r] += bP * Sp;
+            if (GRAD) {
+              Gr[r] += bR * Sp;
+              Gt[r] += bT * Sp;
+              Gp[r] += bF * (z1 - z2);
+            }
+          }
+      }
+    }
+  }
+}
+
+template <bool GRAD>
+__global__ void __launch_bounds__(HNDT) k_heval3nd(HEvalNdArgs A) {
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x;
+  if (b >= A.nb) return;
+  const int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
+  if (A.nchild[b] != 0 || t1 < t0) return;
+  const int lb = A.ilevel[b];
+  const bool own = lb >= 2;  // levels 0 and 1 receive no local expansion
+  const int nexp = (own ? 1 : 0) + A.nl3[b];
+  if (nexp == 0) return;
+  const long nd = A.nd;
+  const int rb = blockIdx.y * HRBE;
+  const int nv = min(HRBE, A.nd - rb);
+  for (int c0 = t0; c0 <= t1; c0 += HNDT) {
+    const int i = c0 + tid;
+    if (i > t1) continue;
+    const zdc x[3] = {A.ztarg[3 * i], A.ztarg[3 * i + 1], A.ztarg[3 * i + 2]};
+    zdc P[HRBE], Gx[HRBE], Gy[HRBE], Gz[HRBE];
+#pragma unroll
+    for (int r = 0; r < HRBE; r++) P[r] = Gx[r] = Gy[r] = Gz[r] = mkz(0.0);
+    for (int ei = 0; ei < nexp; ei++) {
+      int eb;
+      bool loc;
+      if (own && ei == 0) {
+        eb = b;
+        loc = true;
+      } else {
+        eb = A.l3[(size_t)b * A.mn3 + ei - (own ? 1 : 0)];
+        loc = false;
+        if (nsrc(A.isrcse, eb) <= 0) continue;
+      }
+      const int le = A.ilevel[eb], p = A.lev.p[le], NC = (p + 1) * (p + 1);
+      const zdc* zc = (loc ? A.zct : A.zcs) + 3 * eb;
+      const zdc* ex =
+          (loc ? A.loc : A.mp) + (A.lev.base[le] + (long)(eb - A.lev.lo[le]) * NC) * nd + rb;
+      const Sph s = zcart2sph(x[0], x[1], x[2], zc);
+      zdc Gr[HRBE], Gt[HRBE], Gp[HRBE];
+#pragma unroll
+      for (int r = 0; r < HRBE; r++) Gr[r] = Gt[r] = Gp[r] = mkz(0.0);
+      if (loc) heval_one_nd<GRAD, true>(A, ex, nd, nv, p, s, A.lev.rs[le], P, Gr, Gt, Gp);
+      else heval_one_nd<GRAD, false>(A, ex, nd, nv, p, s, A.lev.rs[le], P, Gr, Gt, Gp);
+      if (GRAD) {
+        const zdc ir = zinv(s.rz);
+        const zdc ezr0 = s.st * s.cp, ezr1 = s.st * s.sp, ezr2 = s.ct;
+        const zdc et0 = s.ct * s.cp * ir, et1 = s.ct * s.sp * ir, et2 = -(s.st * ir);
+        const zdc ep0 = -(s.sp * ir), ep1 = s.cp * ir;
+#pragma unroll
+        for (int r = 0; r < HRBE; r++) {
+          Gx[r] += Gr[r] * ezr0 + Gt[r] * et0 + Gp[r] * ep0;
+          Gy[r] += Gr[r] * ezr1 + Gt[r] * et1 + Gp[r] * ep1;
+          Gz[r] += Gr[r] * ezr2 + Gt[r] * et2;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < HRBE; r++)
+      if (r < nv) {
+        A.pot[(long)i * nd + rb + r] += P[r];
+        if (GRAD) {
+          A.grad[(3L * i) * nd + rb + r] += Gx[r];
+          A.grad[(3L * i + 1) * nd + rb + r] += Gy[r];
+          A.grad[(3L * i + 2) * nd + rb + r] += Gz[r];
+        }
+      }
+  }
+}
+
+// column copy from the single-solve layout into the batched layout
 __global__ void k_put_col(long n, int nd, int r, const zdc* __restrict__ src, zdc* dst) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     dst[i * nd + r] = src[i];
-}
-__global__ void k_get_col(long n, int nd, int r, const zdc* __restrict__ src, zdc* dst) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    dst[i] = src[i * nd + r];
 }
 
 // one translation launch: its orders, node count and shared-memory plan
@@ -385,8 +717,8 @@ HLaunch plan_launch(int p1, int p2, int nq) {
   for (int tab = (p1 == p2) ? 1 : 0; tab >= 0; tab--) {
     const size_t off = xsm_work_offset(pmx, tab != 0);
     const size_t rot = xsm_layout(pmx, tab != 0, nullptr, nullptr) - off;
-    for (int qc = QCM; qc >= 1; qc /= 2) {
-      const size_t tot = off + std::max(rot, hsh_layout(p1, p2, nq, qc, nullptr, nullptr));
+    for (int qc = QCM; qc >= 1; qc--) {
+      const size_t tot = off + std::max(rot, hsh_layout(p1, p2, qc, nullptr, nullptr));
       if (tot <= kHSmemMax) {
         h.qc = qc;
         h.rot_smem = tab;
@@ -497,8 +829,7 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   const int nb = t.nboxes, nlev = t.nlevels;
   const long tot = std::max<long>(H.tot, 1);
   DevBuf<zdc> q(ns, s), ds(ns, s), dv(3 * (size_t)ns, s), mp1(tot, s), loc1(tot, s),
-      mpn((size_t)tot * nd, s), locn((size_t)tot * nd, s), potsort(nt, s),
-      gradsort(ifpgh > 1 ? 3 * (size_t)nt : 1, s);
+      mpn((size_t)tot * nd, s), locn((size_t)tot * nd, s);
   mpn.zero();
   locn.zero();
   const int cgrid = std::min(div_up(tot, 256), 148 * 16);
@@ -560,18 +891,58 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   for (int l = 2; l <= nlev - 1; l++)
     launch_htrans_nd<2>(A, H, l, l + 1, t.laddr[2 * (l + 1)], t.laddr[2 * (l + 1) + 1], xgrid, s);
   mark(5);
-  // P2P, L2T and M2T per right-hand side
-  for (int r = 0; r < nd; r++) {
-    gather(r);
-    klaunch(k_get_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)mpn.get(), mp1.get());
-    klaunch(k_get_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)locn.get(), loc1.get());
+  // P2P, L2T and M2T batched over the right-hand sides (tree-order strengths
+  // and outputs with the right-hand side fastest)
+  {
+    // (the gather writes every strength entry, dipole strengths included)
+    DevBuf<zdc> qn((size_t)ns * nd, s), dsn((size_t)ns * nd, s),
+        potn((size_t)nt * nd, s), gradn(ifpgh > 1 ? 3 * (size_t)nt * nd : 1, s);
+    gather_strengths_nd(S, ns, nd, in.ifcharge ? in.charge : nullptr,
+                        in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
+                        true, true, qn.get(), dsn.get(), dv.get(), s);
+    potn.zero();
+    gradn.zero();
+    HP2PNdArgs Pa;
+    Pa.nchild = t.nchild.get(); Pa.isrcse = S.isrcse.get(); Pa.itargse = S.itargse.get();
+    Pa.zsrc = S.zsrcsort.get(); Pa.q = qn.get(); Pa.ds = dsn.get(); Pa.dv = dv.get();
+    Pa.ztarg = S.ztargsort.get();
+    Pa.nl1 = L.n[0].get(); Pa.l1 = L.list[0].get(); Pa.mn1 = L.mn[0]; Pa.nb = nb; Pa.nd = nd;
+    Pa.ifcharge = in.ifcharge; Pa.zk = H.kw;
+    Pa.pot = potn.get(); Pa.grad = gradn.get();
+    const size_t smp = sizeof(HSrcTileNd);
+    const dim3 pgrid(nb, div_up(nd, HRB));
+    const bool dip = in.ifdipole != 0;
+    if (ifpgh > 1) {
+      if (dip) {
+        ZF_CUDA(cudaFuncSetAttribute(k_hp2p3nd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+        klaunch(k_hp2p3nd<true, true>, pgrid, HNDT, smp, s, Pa);
+      } else {
+        ZF_CUDA(cudaFuncSetAttribute(k_hp2p3nd<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+        klaunch(k_hp2p3nd<true, false>, pgrid, HNDT, smp, s, Pa);
+      }
+    } else {
+      if (dip) {
+        ZF_CUDA(cudaFuncSetAttribute(k_hp2p3nd<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+        klaunch(k_hp2p3nd<false, true>, pgrid, HNDT, smp, s, Pa);
+      } else {
+        ZF_CUDA(cudaFuncSetAttribute(k_hp2p3nd<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+        klaunch(k_hp2p3nd<false, false>, pgrid, HNDT, smp, s, Pa);
+      }
+    }
     ZF_LAUNCH_CHECK();
-    potsort.zero();
-    gradsort.zero();
-    helm_eval(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, ifpgh, mp1.get(),
-              loc1.get(), potsort.get(), gradsort.get(), s);
-    unsort3d_col(nt, nd, r, S.itarg.get(), potsort.get(), gradsort.get(), mkz(1.0),
-                 mkz(1.0 / S.b0), ifpgh, pot, grad, s);
+    HEvalNdArgs E;
+    E.r1 = H.T.r1; E.r2 = H.T.r2; E.sq = H.T.sq; E.L = H.pmax + 1;
+    E.ilevel = t.ilevel.get(); E.nchild = t.nchild.get(); E.isrcse = S.isrcse.get();
+    E.itargse = S.itargse.get(); E.ztarg = S.ztargsort.get(); E.zcs = S.zcsrc.get();
+    E.zct = S.zctarg.get(); E.lev = H.lev; E.mp = mpn.get(); E.loc = locn.get();
+    E.nl3 = L.n[2].get(); E.l3 = L.list[2].get(); E.mn3 = L.mn[2]; E.nb = nb; E.nd = nd;
+    E.zk = H.kw; E.pot = potn.get(); E.grad = gradn.get();
+    const dim3 egrid(nb, div_up(nd, HRBE));
+    if (ifpgh > 1) klaunch(k_heval3nd<true>, egrid, HNDT, 0, s, E);
+    else klaunch(k_heval3nd<false>, egrid, HNDT, 0, s, E);
+    ZF_LAUNCH_CHECK();
+    unsort3d_nd(nt, nd, S.itarg.get(), potn.get(), gradn.get(), mkz(1.0), mkz(1.0 / S.b0),
+                ifpgh, pot, grad, s);
   }
   mark(6);
   mark(7);
