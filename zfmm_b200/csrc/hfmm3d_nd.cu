@@ -30,10 +30,13 @@
 //                Legendre recurrences once per (target, expansion) for HRBE
 //                right-hand sides.
 //
-// P2M and P2L run per right-hand side through the single-solve form kernel on
-// the plan's tree; their expansions move into the batched layout by column
-// copies.  Fewer than 4 right-hand sides, or orders whose working set exceeds
-// shared memory, run every pass per right-hand side.
+//   k_hform3nd   P2M / P2L: one warp per (box, 32 right-hand sides); lanes
+//                stream the sources' radial tables and recurrences into a small
+//                shared buffer, then sum it against the staged strengths
+//                (lane = right-hand side).
+//
+// Fewer than 4 right-hand sides, or orders whose working set exceeds shared
+// memory, run every pass per right-hand side.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -696,10 +699,197 @@ __global__ void __launch_bounds__(HNDT) k_heval3nd(HEvalNdArgs A) {
   }
 }
 
-// column copy from the single-solve layout into the batched layout
-__global__ void k_put_col(long n, int nd, int r, const zdc* __restrict__ src, zdc* dst) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    dst[i * nd + r] = src[i];
+// ---- P2M / P2L, one warp per (box, 32 right-hand sides) -------------------------
+constexpr int HFW = 4;  // warps per CTA of the form kernel, one work item each
+constexpr int HKB = 8;  // (n, m) entries buffered per flush
+
+struct HFormNdArgs {
+  const double *r1, *r2, *sq;
+  int L;
+  const int *ilevel, *nchild, *isrcse, *itargse;
+  const zdc *zsrc, *q, *ds, *dv;
+  const zdc *zcs, *zct;
+  HLev lev;
+  zdc* out;
+  const int *nl4, *l4;
+  int mn4, nb, nd, nchunk, ifcharge;
+  zdc zk;
+};
+
+__host__ __device__ inline size_t hform_nd_warp_elems(bool dip) {
+  return (dip ? 2 : 1) * (32 * 32 + HKB * 2 * 32);
+}
+
+// zh3dformmp (LOCAL = false: j_n) / zh3dformloc (LOCAL = true: h_n) of sources
+// s0..s1 about centre zc at order p into the 32 right-hand sides r0.. of `o`
+// (coefficient rows of stride nd).  Lanes stream one source each through the
+// radial table and the Legendre recurrences, buffering the coefficient
+// weights of HKB (n, +-m) entries in shared memory; a flush sums them against
+// the staged strengths with the lane as the right-hand side.
+template <bool LOCAL, bool DIP>
+__device__ void hform_range_nd(const HFormNdArgs& A, int s0, int s1, const zdc* zc, int p,
+                               double rscale, zdc* o, int r0, int nval, zdc* Qt, zdc* Dt,
+                               zdc* Gq, zdc* Gd) {
+  const int L = A.L, lane = threadIdx.x & 31;
+  const long nd = A.nd;
+  const zdc zk = A.zk;
+  const zdc c4 = zmul_i(zk * (1.0 / (4 * kPi)));
+  zdc f[PMAXR + 2], fd[DIP ? PMAXR + 2 : 1];
+  for (int base = s0; base <= s1; base += 32) {
+    const int cnt = min(32, s1 - base + 1);
+    __syncwarp();
+    for (int k = 0; k < 32; k++) {
+      const bool ok = k < cnt && lane < nval;
+      Qt[k * 32 + lane] = (ok && A.ifcharge) ? A.q[(long)(base + k) * nd + r0 + lane] : mkz(0.0);
+      if (DIP) Dt[k * 32 + lane] = ok ? A.ds[(long)(base + k) * nd + r0 + lane] : mkz(0.0);
+    }
+    const bool valid = lane < cnt;
+    const int ii = valid ? base + lane : base;
+    const Sph s = zcart2sph(A.zsrc[3 * ii], A.zsrc[3 * ii + 1], A.zsrc[3 * ii + 2], zc);
+    const zdc zrk = s.rz * zk;
+    if (!LOCAL) besseljs3d_z(p, zrk, rscale, f, DIP ? fd : nullptr);
+    else h3dall_z(p, zrk, rscale, f, DIP ? fd : nullptr);
+    zdc dzr_ = mkz(0.0), dthz = mkz(0.0), dphz = mkz(0.0);
+    if (DIP) {
+      const zdc v0 = A.dv[3 * ii], v1 = A.dv[3 * ii + 1], v2 = A.dv[3 * ii + 2];
+      dzr_ = v0 * (s.st * s.cp) + v1 * (s.st * s.sp) + v2 * s.ct;
+      const zdc dth_ = v0 * (s.ct * s.cp) + v1 * (s.ct * s.sp) - v2 * s.st;
+      const zdc dph_ = -(v0 * s.sp) + v1 * s.cp;
+      dthz = dth_ / s.rz;
+      dphz = dph_ / s.rz;
+    }
+    const zdc z = s.ct, zz1 = mkz(1.0) - z * z;
+    const zdc u = -zsqrt_r(zz1);
+    zdc Ydiag = mkz(1.0), em = mkz(1.0);
+    int e = 0, fm = 0, fn = 0;  // buffered entries and the first (m, n) among them
+    auto flush = [&]() {
+      __syncwarp();
+      int m = fm, n = fn;
+      for (int k = 0; k < e; k++) {
+        zdc ap = mkz(0.0), an = mkz(0.0);
+        const zdc* gq = Gq + k * 64;
+        const zdc* gd = Gd + k * 64;
+        for (int j = 0; j < 32; j++) {
+          const zdc qv = Qt[j * 32 + lane];
+          ap += gq[j] * qv;
+          if (m > 0) an += gq[32 + j] * qv;
+          if (DIP) {
+            const zdc dvv = Dt[j * 32 + lane];
+            ap += gd[j] * dvv;
+            if (m > 0) an += gd[32 + j] * dvv;
+          }
+        }
+        if (lane < nval) {
+          o[(long)ix3(n, m) * nd + lane] += ap;
+          if (m > 0) o[(long)ix3(n, -m) * nd + lane] += an;
+        }
+        if (n < p) n++;
+        else {
+          m++;
+          n = m;
+        }
+      }
+      __syncwarp();
+      e = 0;
+    };
+    for (int m = 0; m <= p; m++) {
+      zdc emi = mkz(1.0);
+      if (m > 0) {
+        const double cmm = __ldg(&A.r1[m * L + m]);
+        if (DIP) Ydiag = (m == 1) ? mkz(-cmm) : (Ydiag * u) * cmm;
+        else Ydiag = (Ydiag * u) * cmm;
+        em = em * s.eip;
+        emi = zinv(em);
+      }
+      const double sgm = (m & 1) ? -1.0 : 1.0;
+      zdc Yp = Ydiag, Dp = DIP ? (Ydiag * (double)(-m)) * z : mkz(0.0);
+      zdc Ypp = mkz(0.0), Dpp = mkz(0.0);
+      for (int n = m; n <= p; n++) {
+        zdc Y, D = mkz(0.0);
+        if (n == m) {
+          Y = Yp;
+          D = Dp;
+        } else {
+          if (n == m + 1) {
+            const double c = __ldg(&A.r1[n * L + m]);
+            Y = (z * Yp) * c;
+            if (DIP) D = (m == 0) ? (z * Dp + Yp) * c : (z * Dp + zz1 * Yp) * c;
+          } else {
+            const double c1 = __ldg(&A.r1[n * L + m]), c2 = __ldg(&A.r2[n * L + m]);
+            Y = (c1 * z) * Yp - c2 * Ypp;
+            if (DIP)
+              D = (m == 0) ? c1 * (z * Dp + Yp) - c2 * Dpp : c1 * (z * Dp + zz1 * Yp) - c2 * Dpp;
+          }
+          Ypp = Yp;
+          Dpp = Dp;
+          Yp = Y;
+          Dp = D;
+        }
+        const zdc sc = c4 * (__ldg(&A.sq[n]) * sgm);
+        const zdc y = Y * sc, dy = D * sc;
+        zdc qp, qn = mkz(0.0), dp = mkz(0.0), dn = mkz(0.0);
+        if (m == 0) {
+          qp = f[n] * y;
+          if (DIP) dp = -(zk * fd[n] * y * dzr_) + f[n] * dy * s.st * dthz;
+        } else {
+          const zdc X = f[n] * (DIP ? y * s.st : y);
+          qp = emi * X;
+          qn = em * X;
+          if (DIP) {
+            const zdc Xd = -(zk * fd[n] * y * s.st * dzr_) + f[n] * dy * dthz;
+            const zdc W = zmul_i((double)m * f[n] * y * dphz);
+            dp = emi * (Xd + W);
+            dn = em * (Xd - W);
+          }
+        }
+        if (!valid) qp = qn = dp = dn = mkz(0.0);
+        if (e == 0) {
+          fm = m;
+          fn = n;
+        }
+        Gq[e * 64 + lane] = qp;
+        Gq[e * 64 + 32 + lane] = qn;
+        if (DIP) {
+          Gd[e * 64 + lane] = dp;
+          Gd[e * 64 + 32 + lane] = dn;
+        }
+        e++;
+        if (e == HKB) flush();
+      }
+    }
+    if (e > 0) flush();
+  }
+}
+
+template <bool LOCAL, bool DIP>
+__global__ void __launch_bounds__(HFW * 32) k_hform3nd(HFormNdArgs A) {
+  extern __shared__ zdc sm[];
+  const int w = threadIdx.x >> 5;
+  const long item = (long)blockIdx.x * HFW + w;
+  if (item >= (long)A.nb * A.nchunk) return;
+  const int b = (int)(item / A.nchunk), r0 = (int)(item % A.nchunk) * 32;
+  const int nval = min(32, A.nd - r0);
+  zdc* Qt = sm + (size_t)w * hform_nd_warp_elems(DIP);
+  zdc* Dt = Qt + 32 * 32;
+  zdc* Gq = Dt + (DIP ? 32 * 32 : 0);
+  zdc* Gd = Gq + HKB * 2 * 32;
+  const int l = A.ilevel[b];
+  const int p = A.lev.p[l], NC = (p + 1) * (p + 1);
+  zdc* o = A.out + (A.lev.base[l] + (long)(b - A.lev.lo[l]) * NC) * A.nd + r0;
+  if (!LOCAL) {
+    // leaves at levels >= 2 (zhfmm3d.f: the multipoles of levels 0 and 1 are never read)
+    if (A.nchild[b] != 0 || nsrc(A.isrcse, b) <= 0 || l < 2) return;
+    hform_range_nd<false, DIP>(A, A.isrcse[2 * b], A.isrcse[2 * b + 1], A.zcs + 3 * b, p,
+                               A.lev.rs[l], o, r0, nval, Qt, Dt, Gq, Gd);
+  } else {
+    if (nsrc(A.itargse, b) <= 0 || A.nl4[b] == 0) return;
+    for (int i = 0; i < A.nl4[b]; i++) {
+      const int jb = A.l4[(size_t)b * A.mn4 + i];
+      if (nsrc(A.isrcse, jb) <= 0) continue;
+      hform_range_nd<true, DIP>(A, A.isrcse[2 * jb], A.isrcse[2 * jb + 1], A.zct + 3 * b, p,
+                                A.lev.rs[l], o, r0, nval, Qt, Dt, Gq, Gd);
+    }
+  }
 }
 
 // one translation launch: its orders, node count and shared-memory plan
@@ -828,31 +1018,53 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   const DevLists& L = S.lists;
   const int nb = t.nboxes, nlev = t.nlevels;
   const long tot = std::max<long>(H.tot, 1);
-  DevBuf<zdc> q(ns, s), ds(ns, s), dv(3 * (size_t)ns, s), mp1(tot, s), loc1(tot, s),
-      mpn((size_t)tot * nd, s), locn((size_t)tot * nd, s);
+  DevBuf<zdc> dv(3 * (size_t)ns, s), mpn((size_t)tot * nd, s), locn((size_t)tot * nd, s);
   mpn.zero();
   locn.zero();
-  const int cgrid = std::min(div_up(tot, 256), 148 * 16);
-  auto gather = [&](int r) {
-    gather_strengths_col(S, ns, nd, r, in.ifcharge ? in.charge : nullptr,
-                         in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
-                         true, true, q.get(), ds.get(), dv.get(), s);
-  };
-  // P2M and P2L per right-hand side into the batched expansions (P2L first:
-  // the M2L launches add to it)
-  for (int r = 0; r < nd; r++) {
-    gather(r);
-    if (nlev >= 2) {
-      mp1.zero();
-      helm_form(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, false, mp1.get(), s);
-      klaunch(k_put_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)mp1.get(), mpn.get());
+  // tree-order strengths with the right-hand side fastest (the gather writes
+  // every strength entry, dipole strengths included)
+  DevBuf<zdc> qn((size_t)ns * nd, s), dsn((size_t)ns * nd, s);
+  gather_strengths_nd(S, ns, nd, in.ifcharge ? in.charge : nullptr,
+                      in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr, true,
+                      true, qn.get(), dsn.get(), dv.get(), s);
+  // P2M, and P2L (list 4) before the M2L launches add to it
+  const bool dip = in.ifdipole != 0;
+  {
+    HFormNdArgs F;
+    F.r1 = H.T.r1; F.r2 = H.T.r2; F.sq = H.T.sq; F.L = H.pmax + 1;
+    F.ilevel = t.ilevel.get(); F.nchild = t.nchild.get();
+    F.isrcse = S.isrcse.get(); F.itargse = S.itargse.get();
+    F.zsrc = S.zsrcsort.get(); F.q = qn.get(); F.ds = dsn.get(); F.dv = dv.get();
+    F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get(); F.lev = H.lev;
+    F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
+    F.nb = nb; F.nd = nd; F.nchunk = div_up(nd, 32); F.ifcharge = in.ifcharge; F.zk = H.kw;
+    const size_t smf = HFW * hform_nd_warp_elems(dip) * sizeof(zdc);
+    const int fgrid = div_up((long)nb * F.nchunk, HFW);
+    auto form = [&](bool local) {
+      if (local) {
+        if (dip) {
+          ZF_CUDA(cudaFuncSetAttribute(k_hform3nd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+          klaunch(k_hform3nd<true, true>, fgrid, HFW * 32, smf, s, F);
+        } else {
+          ZF_CUDA(cudaFuncSetAttribute(k_hform3nd<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+          klaunch(k_hform3nd<true, false>, fgrid, HFW * 32, smf, s, F);
+        }
+      } else {
+        if (dip) {
+          ZF_CUDA(cudaFuncSetAttribute(k_hform3nd<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+          klaunch(k_hform3nd<false, true>, fgrid, HFW * 32, smf, s, F);
+        } else {
+          ZF_CUDA(cudaFuncSetAttribute(k_hform3nd<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+          klaunch(k_hform3nd<false, false>, fgrid, HFW * 32, smf, s, F);
+        }
+      }
       ZF_LAUNCH_CHECK();
-    }
+    };
+    F.out = mpn.get();
+    if (nlev >= 2) form(false);
     if (L.mn[3] > 0) {
-      loc1.zero();
-      helm_form(S, H, q.get(), ds.get(), dv.get(), in.ifcharge, in.ifdipole, true, loc1.get(), s);
-      klaunch(k_put_col, cgrid, 256, 0, s, (long)tot, nd, r, (const zdc*)loc1.get(), locn.get());
-      ZF_LAUNCH_CHECK();
+      F.out = locn.get();
+      form(true);
     }
   }
   mark(2);
@@ -894,12 +1106,7 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   // P2P, L2T and M2T batched over the right-hand sides (tree-order strengths
   // and outputs with the right-hand side fastest)
   {
-    // (the gather writes every strength entry, dipole strengths included)
-    DevBuf<zdc> qn((size_t)ns * nd, s), dsn((size_t)ns * nd, s),
-        potn((size_t)nt * nd, s), gradn(ifpgh > 1 ? 3 * (size_t)nt * nd : 1, s);
-    gather_strengths_nd(S, ns, nd, in.ifcharge ? in.charge : nullptr,
-                        in.ifdipole ? in.dipstr : nullptr, in.ifdipole ? in.dipvec : nullptr,
-                        true, true, qn.get(), dsn.get(), dv.get(), s);
+    DevBuf<zdc> potn((size_t)nt * nd, s), gradn(ifpgh > 1 ? 3 * (size_t)nt * nd : 1, s);
     potn.zero();
     gradn.zero();
     HP2PNdArgs Pa;
@@ -911,7 +1118,6 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
     Pa.pot = potn.get(); Pa.grad = gradn.get();
     const size_t smp = sizeof(HSrcTileNd);
     const dim3 pgrid(nb, div_up(nd, HRB));
-    const bool dip = in.ifdipole != 0;
     if (ifpgh > 1) {
       if (dip) {
         ZF_CUDA(cudaFuncSetAttribute(k_hp2p3nd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
