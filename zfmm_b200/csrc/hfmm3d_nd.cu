@@ -105,6 +105,7 @@ struct HTransNdArgs {
   int lo2;
   zdc* scratch;
   long scr_per_cta;
+  int* queue;  // work-queue counter, zero at launch
   const int *nl2, *l2, *nl4;
   int mn2, nd, lo, hi;
 };
@@ -309,7 +310,19 @@ __global__ void __launch_bounds__(XNT, 1) k_htrans3nd(HTransNdArgs A) {
   zdc* X1 = A.scratch + (size_t)blockIdx.x * A.scr_per_cta;
   zdc* X2 = X1 + (size_t)NC1 * RC;
   const long nd = A.nd;
-  for (int b = A.lo + blockIdx.x; b <= A.hi; b += gridDim.x) {
+  // work items (box, pass of 32 right-hand sides) taken from a queue: the
+  // boxes' list sizes differ widely, and the passes of one box write disjoint
+  // right-hand sides
+  __shared__ int s_item;
+  const int npass = (A.nd + RC - 1) / RC;
+  const int nitems = (A.hi - A.lo + 1) * npass;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_item = atomicAdd(A.queue, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const int b = A.lo + item / npass, r0 = (item % npass) * RC;
     int nin = 0, par = -1;
     if (KIND == 0) {
       if (nsrc(A.isrcse, b) <= 0 || A.nchild[b] == 0) continue;
@@ -325,7 +338,7 @@ __global__ void __launch_bounds__(XNT, 1) k_htrans3nd(HTransNdArgs A) {
       if (!((nsrc(A.itargse, par) > 0 && A.nl2[par] > 0) || A.nl4[par] > 0)) continue;
       nin = 1;
     }
-    for (int r0 = 0; r0 < A.nd; r0 += RC) {
+    {
       const int nval = min(RC, A.nd - r0);
       for (int it = 0; it < nin; it++) {
         int src;
@@ -954,7 +967,8 @@ void launch_htrans_nd(HTransNdArgs A, const HelmPrep& H, int l1, int l2, int lo,
   A.lo2 = H.lev.lo[l2];
   A.lo = lo;
   A.hi = hi;
-  grid = std::max(1, std::min(grid, hi - lo + 1));
+  grid = std::max(1, std::min(grid, (hi - lo + 1) * div_up(A.nd, RC)));
+  ZF_CUDA(cudaMemsetAsync(A.queue, 0, sizeof(int), s));
   switch (h.slots) {
     case 1: case 2: case 3: case 4: launch_htrans_nd_k<KIND, 4>(A, grid, h.smem, s); break;
     case 5: case 6: launch_htrans_nd_k<KIND, 6>(A, grid, h.smem, s); break;
@@ -1071,7 +1085,7 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   int dev = 0, nsm = 148;
   ZF_CUDA(cudaGetDevice(&dev));
   ZF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int xgrid = std::max(1, std::min(nsm, nb));
+  const int xgrid = std::max(1, std::min(nsm, nb * div_up(nd, RC)));
   const size_t per_cta = 2 * (size_t)(H.pmax + 1) * (H.pmax + 1) * RC;
   DevBuf<zdc> scratch((size_t)xgrid * per_cta, s);
   HTransNdArgs A;
@@ -1082,8 +1096,10 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
   A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
   A.zcs = S.zcsrc.get(); A.zct = S.zctarg.get();
   A.nl2 = L.n[1].get(); A.l2 = L.list[1].get(); A.nl4 = L.n[3].get(); A.mn2 = L.mn[1];
+  DevBuf<int> queue(1, s);
   A.scratch = scratch.get();
   A.scr_per_cta = (long)per_cta;
+  A.queue = queue.get();
   A.nd = nd;
   // M2M, finest parents first (parents at levels >= 2)
   A.in = mpn.get();
