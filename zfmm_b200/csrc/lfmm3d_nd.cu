@@ -57,6 +57,7 @@ struct TransNdArgs {
   const zdc* in;
   zdc* out;
   zdc* scratch;  // 2 (p+1)^2 RC per CTA
+  int* queue;    // work-queue counter, zero at launch
   const int *nl2, *l2, *nl4;
   int mn2, nd, lo, hi;
   int rot_smem;  // 1: the cos / sin tables are staged in shared memory
@@ -146,7 +147,19 @@ __global__ void __launch_bounds__(XNT, 1) k_trans3nd(TransNdArgs A) {
   const int nmax = T.nmax, ldA = 2 * nmax + 1;
   const double* __restrict__ am = T.amat;
   const long nd = A.nd;
-  for (int b = A.lo + blockIdx.x; b <= A.hi; b += gridDim.x) {
+  // work items (box, pass of 32 right-hand sides) taken from a queue: the
+  // boxes' list sizes differ widely, and the passes of one box write disjoint
+  // right-hand sides
+  __shared__ int s_item;
+  const int npass = (A.nd + RC - 1) / RC;
+  const int nitems = (A.hi - A.lo + 1) * npass;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_item = atomicAdd(A.queue, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const int b = A.lo + item / npass, r0 = (item % npass) * RC;
     int nin = 0, par = -1;
     if (KIND == 0) {
       if (nsrc(A.isrcse, b) <= 0 || A.nchild[b] == 0) continue;
@@ -162,7 +175,7 @@ __global__ void __launch_bounds__(XNT, 1) k_trans3nd(TransNdArgs A) {
       nin = 1;
     }
     const int lb = A.ilevel[b];
-    for (int r0 = 0; r0 < A.nd; r0 += RC) {
+    {
       const int nval = min(RC, A.nd - r0);
       for (int it = 0; it < nin; it++) {
         int src;
@@ -785,6 +798,8 @@ void launch_trans_nd_k(const TransNdArgs& A, int grid, size_t sm, cudaStream_t s
 template <int KIND>
 void launch_trans_nd(const TransNdArgs& A, int grid, cudaStream_t s) {
   if (A.hi < A.lo) return;
+  grid = std::max(1, std::min(grid, (A.hi - A.lo + 1) * div_up(A.nd, RC)));
+  ZF_CUDA(cudaMemsetAsync(A.queue, 0, sizeof(int), s));
   int L = A.T.p + 1;
   TransNdArgs B = A;
   size_t sm = xsm_layout(A.T.p, true, nullptr, nullptr);
@@ -962,8 +977,9 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   if (nlev >= 1) form(false);
   mark(2);
   // translations: a persistent grid of one CTA per SM, scratch per CTA
-  const int xgrid = std::max(1, std::min(nsm, nb));
+  const int xgrid = std::max(1, std::min(nsm, nb * nchunk));
   DevBuf<zdc> scratch((size_t)xgrid * 2 * NC * RC, s);
+  DevBuf<int> queue(1, s);
   TransNdArgs A;
   A.T = T;
   A.R = R;
@@ -972,13 +988,14 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   A.zcs = S.zcsrc.get(); A.zct = S.zctarg.get(); A.rsc = rsc.get();
   A.nl2 = L.n[1].get(); A.l2 = L.list[1].get(); A.nl4 = L.n[3].get(); A.mn2 = L.mn[1];
   A.scratch = scratch.get();
+  A.queue = queue.get();
   A.nd = nd;
   A.in = mp.get();
   A.out = mp.get();
   for (int l = nlev - 1; l >= 1; l--) {
     A.lo = t.laddr[2 * l];
     A.hi = t.laddr[2 * l + 1];
-    launch_trans_nd<0>(A, std::min(xgrid, A.hi - A.lo + 1), s);
+    launch_trans_nd<0>(A, xgrid, s);
   }
   mark(3);
   A.in = mp.get();
@@ -996,7 +1013,7 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
   for (int l = 1; l <= nlev - 1; l++) {
     A.lo = t.laddr[2 * (l + 1)];
     A.hi = t.laddr[2 * (l + 1) + 1];
-    launch_trans_nd<2>(A, std::min(xgrid, A.hi - A.lo + 1), s);
+    launch_trans_nd<2>(A, xgrid, s);
   }
   mark(5);
   // P2P, then L2T / M2T
