@@ -252,15 +252,24 @@ __device__ void hshift_nd(const HTransNdArgs& A, const HSh& H, zdc zsh, const zd
       zdc F[QCM], D[QCM];
 #pragma unroll
       for (int t = 0; t < QCM; t++) F[t] = D[t] = mkz(0.0);
-#pragma unroll 4
-      for (int n = m; n <= p1; n++) {
-        const zdc a = ldcg_z(X1 + ix3(n, mm) * RC + lane);
-        const int j = jdx(n, m);
+      // the rows of degrees m..p1 in blocks of PB, each block's L2 loads
+      // issued together ahead of its products
+      for (int n0 = m; n0 <= p1; n0 += PB) {
+        zdc a[PB];
 #pragma unroll
-        for (int t = 0; t < QCM; t++) {
-          if (t < nc) {
-            F[t] += H.Zc[t * np1 + j] * a;
-            D[t] += H.Dc[t * np1 + j] * a;
+        for (int k = 0; k < PB; k++)
+          a[k] = (n0 + k <= p1) ? ldcg_z(X1 + ix3(n0 + k, mm) * RC + lane) : mkz(0.0);
+#pragma unroll
+        for (int k = 0; k < PB; k++) {
+          if (n0 + k <= p1) {
+            const int j = jdx(n0 + k, m);
+#pragma unroll
+            for (int t = 0; t < QCM; t++) {
+              if (t < nc) {
+                F[t] += H.Zc[t * np1 + j] * a[k];
+                D[t] += H.Dc[t * np1 + j] * a[k];
+              }
+            }
           }
         }
       }
