@@ -52,7 +52,7 @@ namespace zf {
 
 namespace {
 
-constexpr int QCM = 8;  // nodes per chunk of the z-shift (at most)
+constexpr int QCM = 5;  // nodes per chunk of the z-shift (at most)
 constexpr int PB = 8;   // output rows per read-modify-write block of the z-shift
 constexpr size_t kHSmemMax = 227 * 1024;
 
@@ -247,7 +247,10 @@ __device__ void hshift_nd(const HTransNdArgs& A, const HSh& H, zdc zsh, const zd
     // (c) per order m and sign: the node sums of the 32 right-hand sides
     // (lane = right-hand side), then their projection onto the order-p2
     // coefficients (n, +-m), accumulated over the node chunks in X2
-    for (int task = w; task < ntask; task += XW) {
+    // tasks (m, sign) by decreasing cost, dealt to the warps in snake order
+    for (int rnd = 0;; rnd++) {
+      const int task = rnd * XW + ((rnd & 1) ? XW - 1 - w : w);
+      if (task >= ntask) break;
       const int m = (task + 1) >> 1, mm = (task & 1) ? m : -m;
       zdc F[QCM], D[QCM];
 #pragma unroll
