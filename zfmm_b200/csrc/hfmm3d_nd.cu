@@ -30,7 +30,8 @@
 //                Legendre recurrences once per (target, expansion) for HRBE
 //                right-hand sides.
 //
-//   k_hform3nd   P2M / P2L: one warp per (box, 32 right-hand sides); lanes
+//   k_hform3nd   P2M / P2L: one CTA per (box, 32 right-hand sides), its warps
+//                sharing the staged strengths and splitting the orders m; lanes
 //                stream the sources' radial tables and recurrences into a small
 //                shared buffer, then sum it against the staged strengths
 //                (lane = right-hand side).
@@ -725,7 +726,7 @@ __global__ void __launch_bounds__(HNDT) k_heval3nd(HEvalNdArgs A) {
 }
 
 // ---- P2M / P2L, one warp per (box, 32 right-hand sides) -------------------------
-constexpr int HFW = 4;  // warps per CTA of the form kernel, one work item each
+constexpr int HFW = 4;  // warps per CTA of the form kernel, sharing one work item
 constexpr int HKB = 8;  // (n, m) entries buffered per flush
 
 struct HFormNdArgs {
@@ -741,33 +742,39 @@ struct HFormNdArgs {
   zdc zk;
 };
 
-__host__ __device__ inline size_t hform_nd_warp_elems(bool dip) {
-  return (dip ? 2 : 1) * (32 * 32 + HKB * 2 * 32);
+// shared memory of a form CTA: the staged strengths (32 sources x 32
+// right-hand sides, charges and dipole strengths) and per warp the buffered
+// coefficient weights of HKB (n, +-m) entries
+__host__ __device__ inline size_t hform_nd_elems(bool dip) {
+  return (dip ? 2 : 1) * (32 * 32 + HFW * HKB * 2 * 32);
 }
 
 // zh3dformmp (LOCAL = false: j_n) / zh3dformloc (LOCAL = true: h_n) of sources
 // s0..s1 about centre zc at order p into the 32 right-hand sides r0.. of `o`
-// (coefficient rows of stride nd).  Lanes stream one source each through the
-// radial table and the Legendre recurrences, buffering the coefficient
-// weights of HKB (n, +-m) entries in shared memory; a flush sums them against
-// the staged strengths with the lane as the right-hand side.
+// (coefficient rows of stride nd).  The CTA's warps share each 32-source
+// strength tile; warp w takes the orders m = w, w + HFW, ...: its lanes stream
+// one source each through the radial table and the order-m Legendre column,
+// buffering the coefficient weights of HKB (n, +-m) entries, and a flush sums
+// them against the staged strengths with the lane as the right-hand side.
+// The warps write disjoint coefficient rows.
 template <bool LOCAL, bool DIP>
 __device__ void hform_range_nd(const HFormNdArgs& A, int s0, int s1, const zdc* zc, int p,
                                double rscale, zdc* o, int r0, int nval, zdc* Qt, zdc* Dt,
                                zdc* Gq, zdc* Gd) {
-  const int L = A.L, lane = threadIdx.x & 31;
+  const int L = A.L, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const long nd = A.nd;
   const zdc zk = A.zk;
   const zdc c4 = zmul_i(zk * (1.0 / (4 * kPi)));
   zdc f[PMAXR + 2], fd[DIP ? PMAXR + 2 : 1];
   for (int base = s0; base <= s1; base += 32) {
     const int cnt = min(32, s1 - base + 1);
-    __syncwarp();
-    for (int k = 0; k < 32; k++) {
+    __syncthreads();
+    for (int k = w; k < 32; k += HFW) {
       const bool ok = k < cnt && lane < nval;
       Qt[k * 32 + lane] = (ok && A.ifcharge) ? A.q[(long)(base + k) * nd + r0 + lane] : mkz(0.0);
       if (DIP) Dt[k * 32 + lane] = ok ? A.ds[(long)(base + k) * nd + r0 + lane] : mkz(0.0);
     }
+    __syncthreads();
     const bool valid = lane < cnt;
     const int ii = valid ? base + lane : base;
     const Sph s = zcart2sph(A.zsrc[3 * ii], A.zsrc[3 * ii + 1], A.zsrc[3 * ii + 2], zc);
@@ -785,7 +792,6 @@ __device__ void hform_range_nd(const HFormNdArgs& A, int s0, int s1, const zdc* 
     }
     const zdc z = s.ct, zz1 = mkz(1.0) - z * z;
     const zdc u = -zsqrt_r(zz1);
-    zdc Ydiag = mkz(1.0), em = mkz(1.0);
     int e = 0, fm = 0, fn = 0;  // buffered entries and the first (m, n) among them
     auto flush = [&]() {
       __syncwarp();
@@ -810,22 +816,26 @@ __device__ void hform_range_nd(const HFormNdArgs& A, int s0, int s1, const zdc* 
         }
         if (n < p) n++;
         else {
-          m++;
+          m += HFW;
           n = m;
         }
       }
       __syncwarp();
       e = 0;
     };
-    for (int m = 0; m <= p; m++) {
-      zdc emi = mkz(1.0);
-      if (m > 0) {
-        const double cmm = __ldg(&A.r1[m * L + m]);
-        if (DIP) Ydiag = (m == 1) ? mkz(-cmm) : (Ydiag * u) * cmm;
-        else Ydiag = (Ydiag * u) * cmm;
+    // Ydiag(m) and eip^m as the single-solve kernel forms them (running
+    // products over m), advanced here to this warp's orders
+    zdc Ydiag = mkz(1.0), em = mkz(1.0);
+    int mdone = 0;
+    for (int m = w; m <= p; m += HFW) {
+      for (int k = mdone + 1; k <= m; k++) {
+        const double ckk = __ldg(&A.r1[k * L + k]);
+        if (DIP) Ydiag = (k == 1) ? mkz(-ckk) : (Ydiag * u) * ckk;
+        else Ydiag = (Ydiag * u) * ckk;
         em = em * s.eip;
-        emi = zinv(em);
       }
+      mdone = m;
+      const zdc emi = m > 0 ? zinv(em) : mkz(1.0);
       const double sgm = (m & 1) ? -1.0 : 1.0;
       zdc Yp = Ydiag, Dp = DIP ? (Ydiag * (double)(-m)) * z : mkz(0.0);
       zdc Ypp = mkz(0.0), Dpp = mkz(0.0);
@@ -890,13 +900,13 @@ template <bool LOCAL, bool DIP>
 __global__ void __launch_bounds__(HFW * 32) k_hform3nd(HFormNdArgs A) {
   extern __shared__ zdc sm[];
   const int w = threadIdx.x >> 5;
-  const long item = (long)blockIdx.x * HFW + w;
+  const long item = blockIdx.x;
   if (item >= (long)A.nb * A.nchunk) return;
   const int b = (int)(item / A.nchunk), r0 = (int)(item % A.nchunk) * 32;
   const int nval = min(32, A.nd - r0);
-  zdc* Qt = sm + (size_t)w * hform_nd_warp_elems(DIP);
+  zdc* Qt = sm;
   zdc* Dt = Qt + 32 * 32;
-  zdc* Gq = Dt + (DIP ? 32 * 32 : 0);
+  zdc* Gq = Dt + (DIP ? 32 * 32 : 0) + (size_t)w * HKB * 2 * 32 * (DIP ? 2 : 1);
   zdc* Gd = Gq + HKB * 2 * 32;
   const int l = A.ilevel[b];
   const int p = A.lev.p[l], NC = (p + 1) * (p + 1);
@@ -1064,8 +1074,8 @@ void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in
     F.zcs = S.zcsrc.get(); F.zct = S.zctarg.get(); F.lev = H.lev;
     F.nl4 = L.n[3].get(); F.l4 = L.list[3].get(); F.mn4 = L.mn[3];
     F.nb = nb; F.nd = nd; F.nchunk = div_up(nd, 32); F.ifcharge = in.ifcharge; F.zk = H.kw;
-    const size_t smf = HFW * hform_nd_warp_elems(dip) * sizeof(zdc);
-    const int fgrid = div_up((long)nb * F.nchunk, HFW);
+    const size_t smf = hform_nd_elems(dip) * sizeof(zdc);
+    const int fgrid = nb * F.nchunk;
     auto form = [&](bool local) {
       if (local) {
         if (dip) {
