@@ -432,7 +432,7 @@ struct HSrcTileNd {
 // the pair interaction of zh3devaldirect (zhfmm3d.f:606-693): the pair's kernel
 // values once, then one complex MAC per output and right-hand side
 template <bool GRAD, bool DIP>
-__global__ void __launch_bounds__(HNDT) k_hp2p3nd(HP2PNdArgs A) {
+__global__ void __launch_bounds__(HNDT, 3) k_hp2p3nd(HP2PNdArgs A) {
   extern __shared__ unsigned char smraw[];
   HSrcTileNd& S = *reinterpret_cast<HSrcTileNd*>(smraw);
   constexpr double PI4I = 0.079577471545947667884;
@@ -658,7 +658,7 @@ __device__ __forceinline__ void heval_one_nd(const HEvalNdArgs& A, const zdc* __
 }
 
 template <bool GRAD>
-__global__ void __launch_bounds__(HNDT) k_heval3nd(HEvalNdArgs A) {
+__global__ void __launch_bounds__(HNDT, 3) k_heval3nd(HEvalNdArgs A) {
   const int tid = threadIdx.x;
   const int b = blockIdx.x;
   if (b >= A.nb) return;
