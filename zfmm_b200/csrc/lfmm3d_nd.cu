@@ -589,7 +589,7 @@ __device__ __forceinline__ void eval_one_nd(const Tab3& T, const zdc* __restrict
 }
 
 template <bool GRAD>
-__global__ void __launch_bounds__(ENT) k_eval3nd(EvalNdArgs A) {
+__global__ void __launch_bounds__(ENT, 3) k_eval3nd(EvalNdArgs A) {
   const Tab3& T = A.T;
   const int NC = T.NC, tid = threadIdx.x;
   const int b = blockIdx.x;
@@ -678,7 +678,7 @@ struct SrcTileNd {
 };
 
 template <bool GRAD, bool DIP>
-__global__ void __launch_bounds__(ENT) k_p2p3nd(P2PNdArgs A) {
+__global__ void __launch_bounds__(ENT, 3) k_p2p3nd(P2PNdArgs A) {
   extern __shared__ unsigned char smraw[];
   SrcTileNd& S = *reinterpret_cast<SrcTileNd*>(smraw);
   constexpr double PI4I = 0.079577471545947667884;
