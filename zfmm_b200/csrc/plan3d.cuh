@@ -35,8 +35,9 @@ void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int if
                           zdc* grad, cudaStream_t s, StepTimes* times);
 
 // 3D Helmholtz with wavenumber zk on the plan's points: the orders, tables
-// and shift configurations of zk are built once per call and every
-// right-hand side runs the FMM passes on the plan's tree; same layouts as
+// and shift configurations of zk are built once per call; 4 or more
+// right-hand sides run the batched kernels (hfmm3d_nd.cu), fewer the
+// single-solve passes per right-hand side on the plan's tree; same layouts as
 // zlfmm3d_plan_execute, scaling as zhfmm3d
 void zhfmm3d_plan_execute(const Plan3D& P, zdc zk, int nd, const StrengthsNd& in, int ifpgh,
                           zdc* pot, zdc* grad, cudaStream_t s, StepTimes* times);
