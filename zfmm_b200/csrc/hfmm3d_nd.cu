@@ -658,7 +658,7 @@ __device__ __forceinline__ void heval_one_nd(const HEvalNdArgs& A, const zdc* __
 }
 
 template <bool GRAD>
-__global__ void __launch_bounds__(HNDT, 3) k_heval3nd(HEvalNdArgs A) {
+__global__ void __launch_bounds__(HNDT, 4) k_heval3nd(HEvalNdArgs A) {
   const int tid = threadIdx.x;
   const int b = blockIdx.x;
   if (b >= A.nb) return;
@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(HNDT, 3) k_heval3nd(HEvalNdArgs A) {
 
 // ---- P2M / P2L, one warp per (box, 32 right-hand sides) -------------------------
 constexpr int HFW = 4;  // warps per CTA of the form kernel, sharing one work item
-constexpr int HKB = 8;  // (n, m) entries buffered per flush
+constexpr int HKB = 4;  // (n, m) entries buffered per flush
 
 struct HFormNdArgs {
   const double *r1, *r2, *sq;
