@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(HNDT, 4) k_heval3nd(HEvalNdArgs A) {
 
 // ---- P2M / P2L, one warp per (box, 32 right-hand sides) -------------------------
 constexpr int HFW = 4;  // warps per CTA of the form kernel, sharing one work item
-constexpr int HKB = 4;  // (n, m) entries buffered per flush
+constexpr int HKB = 2;  // (n, m) entries buffered per flush
 
 struct HFormNdArgs {
   const double *r1, *r2, *sq;
