@@ -589,7 +589,7 @@ __device__ __forceinline__ void eval_one_nd(const Tab3& T, const zdc* __restrict
 }
 
 template <bool GRAD>
-__global__ void __launch_bounds__(ENT, 3) k_eval3nd(EvalNdArgs A) {
+__global__ void __launch_bounds__(ENT, 4) k_eval3nd(EvalNdArgs A) {
   const Tab3& T = A.T;
   const int NC = T.NC, tid = threadIdx.x;
   const int b = blockIdx.x;
