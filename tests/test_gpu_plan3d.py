@@ -273,3 +273,25 @@ def test_helmholtz_batched_device_entry_point():
     torch.cuda.synchronize()
     assert rel(pt.cpu().numpy(), p) < 1e-13
     assert rel(gt.cpu().numpy(), g) < 1e-13
+
+
+def test_helmholtz_plan_small_eps_runs_per_rhs():
+    # orders above the batched kernels' shared memory (p > 40): every pass per
+    # right-hand side on the plan's tree, equal to the single solves to rounding
+    import zfmm_b200
+    eps = 1e-12
+    nd = 5
+    w = W.sphere3d(4000, seed=26)
+    zs = w["zsrc"]
+    n = zs.shape[1]
+    rng = np.random.default_rng(26)
+    q = cn(rng, nd, n)
+    zk = 10 + 0.2j
+    # level-2 boxes of the unit sphere's tree: a quarter of the ~2.2 root box
+    assert zfmm_b200.h3dterms(0.25, zk * 2.2, eps) > 40
+    plan = zfmm_b200.Plan3D(eps, n, zs, n, zs)
+    p, g = plan.zhfmm3d(zk, nd, 1, q, 0, None, None, 2)
+    for r in (0, nd - 1):
+        p1, g1 = hsingle(eps, zk, zs, q[r], 0, None, None, 2)
+        assert rel(p[r], p1) < 1e-13, r
+        assert rel(g[r], g1) < 1e-13, r
