@@ -237,7 +237,7 @@ __device__ void form_expansion(const HelmArgs& A, int s0, int s1, zdc c1, zdc c2
 
 constexpr int MAXR = 8;  // coefficient slots per lane: p <= 255
 
-__global__ void __launch_bounds__(32 * WPB) k_hp2m(int lo, int hi, HelmArgs A, int pmax) {
+__global__ void __launch_bounds__(32 * WPB, 4) k_hp2m(int lo, int hi, HelmArgs A, int pmax) {
   extern __shared__ zdc sh[];
   int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b > hi) return;
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
 
 // ---- steps 3, 5, 8: P2P (list1), M2T (list3), L2T per target leaf --------------
 template <bool GRAD>
-__global__ void __launch_bounds__(32 * WPB) k_heval(int nb, HelmArgs A, const int* nl1,
+__global__ void __launch_bounds__(32 * WPB, 4) k_heval(int nb, HelmArgs A, const int* nl1,
                                                    const int* l1, int m1, const int* nl3,
                                                    const int* l3, int m3, zdc* potsort,
                                                    zdc* gradsort) {
