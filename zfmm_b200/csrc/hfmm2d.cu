@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
 }
 
 // P2L (zh2dformloc) over list 4, added to the local expansion
-__global__ void __launch_bounds__(32 * WPB) k_hp2l(int lo, int hi, HelmArgs A, const int* nl4,
+__global__ void __launch_bounds__(32 * WPB, 4) k_hp2l(int lo, int hi, HelmArgs A, const int* nl4,
                                                   const int* l4, int m4, int stride) {
   extern __shared__ zdc sh[];
   int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
