@@ -20,6 +20,12 @@
  *                           host arrays; the *_dev variants take device
  *                           pointers and a cudaStream_t (as void*).
  *
+ * Device pointers (every *_dev, *_plan_dev, *_many_dev and *_noalloc entry
+ * point) must be 16-byte aligned, as cudaMalloc and torch allocations are:
+ * the kernels access complex values as 16-byte pairs.  A misaligned pointer is
+ * refused with status 1 before anything is launched.  Host arrays have no
+ * alignment requirement.
+ *
  * Status codes: 0 ok, 1 bad argument, 2 CUDA error, 3 out of device memory,
  * 4 internal error, 5 the CUDA library is unavailable (no GPU).
  */
@@ -87,7 +93,7 @@ void zhfmm3d_(const double *eps, const double *zk, const int *ns, const double *
               const double *dipvec, double *pot, double *grad, const int *nt,
               const double *ztarg, int *ifpgh, const int *isep, const int *ifprint);
 
-/* Replaces zh3devaldirect (zfmm3d/src/helmholtz/zhfmm3d.f:606-607; MATLAB spec
+/* Replaces zh3devaldirect (zfmm3d/src/helmholtz/zhfmm3d.f:626-627; MATLAB spec
  * zfmm3d/matlab_linux/zh3devaldirect.mw:1).  ADDS the sums (with 1/(4 pi)). */
 void zh3devaldirect_(const double *zk, const int *nt, const double *ztarg, const int *ns,
                      const double *zsrc, const double *charge, const double *dipstr,

@@ -93,7 +93,7 @@ int o_zlfmm3d(double eps, int ns, const double *zsrc, int ifcharge, const double
               int ifdipole, const double *dipstr, const double *dipvec, double *pot,
               double *grad, int nt, const double *ztarg, int ifpgh, int isep, int ifprint);
 
-/* 3D Helmholtz: direct sum (with 1/(4 pi), zhfmm3d.f:606-693) and FMM; zk = (re, im) */
+/* 3D Helmholtz: direct sum (with 1/(4 pi), zhfmm3d.f:626-693) and FMM; zk = (re, im) */
 int o_h3dterms(double size, double zkr, double zki, double eps, int isep);
 void o_gauss_legendre(int n, double *x, double *w);
 void o_zh3devaldirect(const double *zk, int nt, const double *ztarg, int ns, const double *zsrc,

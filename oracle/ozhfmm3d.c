@@ -3,7 +3,7 @@
  *
  * Restates zfmm3d/src/helmholtz/zhfmm3d.f (driver :1-249 with the rescaling by
  * 1/boxsize(0) and zk*boxsize(0), zhfmm3dmain :256-600, zh3devaldirect
- * :606-693, zh3dformmp :699-851, zh3dformloc :857-1009, zh3devalmp
+ * :626-693, zh3dformmp :699-851, zh3dformloc :857-1009, zh3devalmp
  * :1015-1158, zh3devalloc :1164-1309), the translations of
  * zfmm3d/src/helmholtz/zh3dtrans.f (zh3dmploc :1-98, zh3dmpmp :105-200,
  * zh3dlocloc :207-312, and the quadrature z-shifts :319-780), the special

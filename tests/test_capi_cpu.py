@@ -94,3 +94,52 @@ def test_no_gpu_plans_and_batches_are_errors():
     inst = [dict(zsrc=z, charge=np.ones(5))]
     with pytest.raises(zfmm_b200.ZfmmError, match="status 5"):
         zfmm_b200.zhfmm3d_many(1e-6, 1.0, inst, nstreams=2)
+
+
+def test_misaligned_device_pointer_is_refused_before_launch():
+    """Device entry points read complex values as 16-byte pairs: a pointer that
+    is 8-byte but not 16-byte aligned is refused with status 1 (checked before
+    the device is touched, so this runs without a GPU)."""
+    import zfmm_b200
+    L = zfmm_b200.lib()
+    good, bad = ctypes.c_void_p(0x10000), ctypes.c_void_p(0x10008)
+    stream = ctypes.c_void_p(0)
+    rc = L.zfmm_zlfmm2d_dev(1e-6, 4, bad, 1, good, 0, None, None, good, good, 4, good, 1, 1,
+                            stream)
+    assert rc == 1 and b"16-byte aligned" in L.zfmm_last_error()
+    rc = L.zfmm_zhfmm3d_dev(1e-6, np.array([1.0, 0.0]).ctypes.data, 4, good, 1, bad, 0, None,
+                            None, good, good, 4, good, 1, 1, stream)
+    assert rc == 1 and b"16-byte aligned" in L.zfmm_last_error()
+    rc = L.zfmm_zl2devaldirect_dev_noalloc(4, good, 4, good, good, None, None, 1, bad, None, 0,
+                                           1, stream)
+    assert rc == 1 and b"16-byte aligned" in L.zfmm_last_error()
+    # an unused array (flag off) is not checked
+    rc = L.zfmm_zl2devaldirect_dev(4, good, 4, good, good, bad, bad, 1, good, None, 0, 1, stream)
+    assert b"16-byte aligned" not in L.zfmm_last_error()
+
+
+def test_torch_inputs_are_checked_before_any_pointer_is_used():
+    """Strengths passed as torch tensors must be complex128 CUDA tensors of the
+    right length; anything else is a ValueError, never a raw pointer handed to
+    a kernel (checked here with CPU tensors, which no device entry point may
+    receive)."""
+    import torch
+    import zfmm_b200
+    z = torch.zeros((4, 2), dtype=torch.complex128)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        zfmm_b200.zlfmm2d(1e-6, 4, z, 1, torch.ones(4, dtype=torch.complex128), 0, None, None,
+                          4, z, 1, 1)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        zfmm_b200._torch_vec(torch.ones(4, dtype=torch.complex64), 4, "charge",
+                             torch.device("cpu"))
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        zfmm_b200._torch_vec(np.ones(4, np.complex128), 4, "charge", torch.device("cpu"))
+
+
+def test_adjoint_inputs_are_checked():
+    import torch
+    from zfmm_b200.adjoint import zhfmm2d_curves
+    xr = torch.zeros((4, 2), dtype=torch.float64)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        zhfmm2d_curves(1e-6, 1.0, xr, xr, torch.zeros(4, dtype=torch.int64),
+                       torch.zeros(1, dtype=torch.float64), torch.ones(4, dtype=torch.complex128))

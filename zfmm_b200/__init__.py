@@ -50,10 +50,12 @@ def _is_torch(x):
     return type(x).__module__.startswith("torch")
 
 
-def _torch_pts(x, d, n, name):
+def _torch_pts(x, d, n, name, device=None):
     import torch
-    if x.dtype != torch.complex128 or not x.is_cuda:
+    if not isinstance(x, torch.Tensor) or x.dtype != torch.complex128 or not x.is_cuda:
         raise ValueError(f"{name} must be a complex128 CUDA tensor")
+    if device is not None and x.device != device:
+        raise ValueError(f"{name} is on {x.device}, the solve runs on {device}")
     x = x.resolve_conj()  # the C entry points read raw memory: no lazy conjugate views
     if tuple(x.shape) == (n, d):
         x = x.contiguous()
@@ -62,6 +64,20 @@ def _torch_pts(x, d, n, name):
     else:
         raise ValueError(f"{name} must have shape ({n}, {d}) or ({d}, {n})")
     return x
+
+
+def _torch_vec(x, n, name, device):
+    """A complex128 CUDA tensor of n entries on `device`, as contiguous memory
+    (the device entry points read n complex values from its data pointer, so a
+    wrong dtype, device or length must be refused here, not read past)."""
+    import torch
+    if not isinstance(x, torch.Tensor) or x.dtype != torch.complex128 or not x.is_cuda:
+        raise ValueError(f"{name} must be a complex128 CUDA tensor")
+    if x.device != device:
+        raise ValueError(f"{name} is on {x.device}, the solve runs on {device}")
+    if x.numel() != n:
+        raise ValueError(f"{name} must have {n} entries, got {x.numel()}")
+    return x.resolve_conj().contiguous()
 
 
 def _zk(zk):
@@ -120,11 +136,11 @@ def _fmm2d_torch(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, 
                  isep):
     import torch
     zs = _torch_pts(zsrc, 2, ns, "zsrc")
-    zt = _torch_pts(ztarg, 2, nt, "ztarg")
     dev = zs.device
-    q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
-    ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
-    dv = _torch_pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
+    zt = _torch_pts(ztarg, 2, nt, "ztarg", dev)
+    q = _torch_vec(charge, ns, "charge", dev) if ifcharge == 1 else None
+    ds = _torch_vec(dipstr, ns, "dipstr", dev) if ifdipole == 1 else None
+    dv = _torch_pts(dipvec, 2, ns, "dipvec", dev) if ifdipole == 1 else None
     pot = torch.empty(nt, dtype=torch.complex128, device=dev)
     grad = torch.empty((nt, 2), dtype=torch.complex128, device=dev)
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
@@ -177,10 +193,10 @@ def _fmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, zt
     if _is_torch(zsrc):
         import torch
         zs = _torch_pts(zsrc, 3, ns, "zsrc")
-        zt = _torch_pts(ztarg, 3, nt, "ztarg")
-        q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
-        ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
-        dv = _torch_pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
+        zt = _torch_pts(ztarg, 3, nt, "ztarg", zs.device)
+        q = _torch_vec(charge, ns, "charge", zs.device) if ifcharge == 1 else None
+        ds = _torch_vec(dipstr, ns, "dipstr", zs.device) if ifdipole == 1 else None
+        dv = _torch_pts(dipvec, 3, ns, "dipvec", zs.device) if ifdipole == 1 else None
         pot = torch.empty(nt, dtype=torch.complex128, device=zs.device)
         grad = torch.empty((nt, 3), dtype=torch.complex128, device=zs.device)
         stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
@@ -267,7 +283,7 @@ def zl3devaldirect(nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipo
 
 
 def zh3devaldirect(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh=1):
-    """3D Helmholtz direct sum with 1/(4 pi) (reference zhfmm3d.f:606-693)."""
+    """3D Helmholtz direct sum with 1/(4 pi) (reference zhfmm3d.f:626-693)."""
     return _direct3d(zk, nt, ztarg, ns, zsrc, charge, dipstr, dipvec, ifcharge, ifdipole, ifpgh)
 
 
@@ -295,7 +311,7 @@ class _Plan:
         if _is_torch(zsrc):
             import torch
             zs = _torch_pts(zsrc, d, self.ns, "zsrc")
-            zt = _torch_pts(ztarg, d, self.nt, "ztarg")
+            zt = _torch_pts(ztarg, d, self.nt, "ztarg", zs.device)
             self.device = zs.device
             stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
             check(getattr(lib(), self._fn["create_dev"])(
@@ -322,9 +338,11 @@ class _Plan:
         if _is_torch(charge if ifcharge == 1 else dipstr):
             import torch
             dev = self.device
-            q = charge.resolve_conj().contiguous() if ifcharge == 1 else None
-            ds = dipstr.resolve_conj().contiguous() if ifdipole == 1 else None
-            dv = _torch_pts(dipvec, d, ns, "dipvec") if ifdipole == 1 else None
+            if dev is None:
+                raise ValueError("this plan was built from host arrays: pass numpy strengths")
+            q = _torch_vec(charge, ns * nd, "charge", dev) if ifcharge == 1 else None
+            ds = _torch_vec(dipstr, ns * nd, "dipstr", dev) if ifdipole == 1 else None
+            dv = _torch_pts(dipvec, d, ns, "dipvec", dev) if ifdipole == 1 else None
             pot = torch.empty((nt, nd), dtype=torch.complex128, device=dev)
             grad = torch.empty((nt, d, nd), dtype=torch.complex128, device=dev)
             stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)

@@ -97,8 +97,13 @@ class _Curves(torch.autograd.Function):
         ep[:, 0] = 1.0
         ep[:, 1] = 1j
         em = torch.conj_physical(ep)
-        Fp, Gp = _eval(ctx.plan, zk, z, None, w, ep, z, 2, direct)
-        Fm, Gm = _eval(ctx.plan, zk, z, None, w, em, z, 2, direct)
+        plan = ctx.plan
+        if plan is None and not direct:
+            # a second backward over the same graph (retain_graph=True): the
+            # first one released the plan, so the tree is built again
+            plan = Plan2D(eps, n, z, n, z)
+        Fp, Gp = _eval(plan, zk, z, None, w, ep, z, 2, direct)
+        Fm, Gm = _eval(plan, zk, z, None, w, em, z, 2, direct)
         ctx.plan = None
         dpdp = Gp[0] + 1j * Gp[1]
         dmdm = Gm[0] - 1j * Gm[1]
@@ -127,6 +132,41 @@ class _Curves(torch.autograd.Function):
         return gq, gds, ga, None, None, None, None, None, None, None
 
 
+def _check_curves(xr, disp, curve, a, charge, dipstr, dipvec):
+    """Refuse inputs whose dtype, device or shape the device entry points would
+    misread (they take raw data pointers of n complex128 values)."""
+    if not isinstance(xr, torch.Tensor) or not xr.is_cuda:
+        raise ValueError("xr must be a CUDA tensor")
+    dev = xr.device
+    if xr.dim() != 2 or xr.shape[1] != 2:
+        raise ValueError(f"xr must have shape (n, 2), got {tuple(xr.shape)}")
+    n = xr.shape[0]
+
+    def want(t, name, dtype, shape):
+        if not isinstance(t, torch.Tensor):
+            raise ValueError(f"{name} must be a tensor")
+        if t.dtype != dtype:
+            raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+        if t.device != dev:
+            raise ValueError(f"{name} is on {t.device}, xr on {dev}")
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{name} must have shape {shape}, got {tuple(t.shape)}")
+
+    want(xr, "xr", torch.float64, (n, 2))
+    want(disp, "disp", torch.float64, (n, 2))
+    want(curve, "curve", torch.int64, (n,))
+    if not isinstance(a, torch.Tensor) or a.dim() != 1:
+        raise ValueError("a must be a 1-D tensor")
+    want(a, "a", torch.float64, (a.shape[0],))
+    if charge is None and dipstr is None:
+        raise ValueError("charge or dipstr is required")
+    if charge is not None:
+        want(charge, "charge", torch.complex128, (n,))
+    if dipstr is not None:
+        want(dipstr, "dipstr", torch.complex128, (n,))
+        want(dipvec, "dipvec", torch.complex128, (n, 2))
+
+
 def zhfmm2d_curves(eps, zk, xr, disp, curve, a, charge, dipstr=None, dipvec=None,
                    direct=False):
     """pot at the points z = xr + 1j a[curve] disp from charges / dipoles at the
@@ -136,5 +176,6 @@ def zhfmm2d_curves(eps, zk, xr, disp, curve, a, charge, dipstr=None, dipvec=None
     and dipstr (n,) complex128, dipvec (n, 2) complex128."""
     if zk is None or complex(zk) == 0:
         raise ValueError("zk must be nonzero")
+    _check_curves(xr, disp, curve, a, charge, dipstr, dipvec)
     return _Curves.apply(charge, dipstr, a, xr, disp, curve, dipvec, float(eps), complex(zk),
                          bool(direct))

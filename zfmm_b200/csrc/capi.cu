@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdint>
 #include <cstring>
+#include <initializer_list>
 #include <thread>
 #include <mutex>
 #include <string>
@@ -135,6 +137,24 @@ void check_args2d(int ns, int nt, const double* zsrc, const double* ztarg, int i
   if (ns > 0 && ifdipole == 1 && (!dipstr || !dipvec))
     throw zf_error(ZF_ERR_ARG, "ifdipole=1 needs dipstr and dipvec");
   if (nt > 0 && ifpgh > 1 && !grad) throw zf_error(ZF_ERR_ARG, "ifpgh=2 needs grad");
+}
+
+// Device arrays are read and written with 16-byte (double2) accesses: a
+// pointer that is not 16-byte aligned is refused here, before any launch,
+// instead of faulting the kernel.  Arrays a call does not use (flag off) are
+// not checked.
+void check_align16(std::initializer_list<const void*> ptrs) {
+  for (const void* p : ptrs)
+    if (p && (reinterpret_cast<uintptr_t>(p) & 15))
+      throw zf_error(ZF_ERR_ARG, "device arrays must be 16-byte aligned");
+}
+
+void check_align_dev(const double* zsrc, const double* ztarg, int ifcharge, const double* charge,
+                     int ifdipole, const double* dipstr, const double* dipvec, double* pot,
+                     double* grad, int ifpgh) {
+  check_align16({zsrc, ztarg, pot, ifcharge == 1 ? charge : nullptr,
+                 ifdipole == 1 ? dipstr : nullptr, ifdipole == 1 ? dipvec : nullptr,
+                 ifpgh > 1 ? grad : nullptr});
 }
 
 // device path shared by host and device entry points; zk == nullptr selects
@@ -269,6 +289,7 @@ int zfmm_zlfmm2d_dev(double eps, int ns, const double* zsrc, int ifcharge, const
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
     Inputs2D in = make_inputs(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
@@ -336,6 +357,7 @@ int zfmm_zl2devaldirect_dev(int nt, const double* ztarg, int ns, const double* z
   return guarded([&] {
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     if (nt == 0 || ns == 0) return;
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -381,6 +403,7 @@ int zfmm_zhfmm2d_dev(double eps, const double* zk, int ns, const double* zsrc, i
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
     Inputs2D in = make_inputs(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
@@ -416,6 +439,7 @@ int zfmm_zh2devaldirect_dev(const double* zk, int nt, const double* ztarg, int n
     if (!zk) throw zf_error(ZF_ERR_ARG, "zk is null");
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     if (nt == 0 || ns == 0) return;
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -433,6 +457,7 @@ int zfmm_zl2devaldirect_dev_noalloc(int nt, const double* ztarg, int ns, const d
   return guarded([&] {
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     if (nt == 0 || ns == 0) return;
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -655,6 +680,7 @@ int zfmm_zlfmm3d_dev(double eps, int ns, const double* zsrc, int ifcharge, const
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
     Inputs3D in = make_inputs3(ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, ztarg,
@@ -686,6 +712,7 @@ int zfmm_zl3devaldirect_dev(int nt, const double* ztarg, int ns, const double* z
   return guarded([&] {
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     if (nt == 0 || ns == 0) return;
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -732,6 +759,7 @@ int zfmm_zhfmm3d_dev(double eps, const double* zk, int ns, const double* zsrc, i
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
     zdc k = mkz(zk[0], zk[1]);
@@ -767,6 +795,7 @@ int zfmm_zh3devaldirect_dev(const double* zk, int nt, const double* ztarg, int n
     if (!zk) throw zf_error(ZF_ERR_ARG, "zk is null");
     check_args2d(ns, nt, zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad,
                  ifpgh);
+    check_align_dev(zsrc, ztarg, ifcharge, charge, ifdipole, dipstr, dipvec, pot, grad, ifpgh);
     if (nt == 0 || ns == 0) return;
     check_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -852,6 +881,7 @@ int plan3d_create_impl(double eps, int ns, const double* zsrc, int nt, const dou
       HostIn h;
       const zdc* zs = reinterpret_cast<const zdc*>(zsrc);
       const zdc* zt = reinterpret_cast<const zdc*>(ztarg);
+      if (!host) check_align16({zsrc, ztarg});
       if (host) {
         upload(h.zsrc, zsrc, 3 * (size_t)ns, s);
         upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
@@ -953,6 +983,8 @@ int plan_solve_dev(zfmm_plan3d plan, const double* zk, int nd, int ifcharge,
   return guarded([&] {
     clamp_flags(ifcharge, ifdipole, ifpgh);
     check_plan_args(plan, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, pot, grad);
+    check_align16({pot, ifcharge == 1 ? charge : nullptr, ifdipole == 1 ? dipstr : nullptr,
+                   ifdipole == 1 ? dipvec : nullptr, ifpgh > 1 ? grad : nullptr});
     cudaStream_t s = (cudaStream_t)stream;
     zdc k = zk ? mkz(zk[0], zk[1]) : mkz(0.0);
     run_plan3d(plan, zk ? &k : nullptr, nd, ifcharge, (const zdc*)charge, ifdipole,
@@ -1116,11 +1148,17 @@ int many_impl(ManyArgs M, int nworkers, double* done_ms) {
       throw zf_error(ZF_ERR_ARG, "null instance array");
     clamp_flags(M.ifcharge, M.ifdipole, M.ifpgh);
     if (M.isep < 1) throw zf_error(ZF_ERR_ARG, "isep must be >= 1");
-    for (int i = 0; i < M.ninst; i++)
+    for (int i = 0; i < M.ninst; i++) {
       check_args2d(M.ns[i], M.nt[i], M.zsrc[i], M.ztarg[i], M.ifcharge,
                    M.charge ? M.charge[i] : nullptr, M.ifdipole,
                    M.dipstr ? M.dipstr[i] : nullptr, M.dipvec ? M.dipvec[i] : nullptr,
                    M.pot[i], M.grad ? M.grad[i] : nullptr, M.ifpgh);
+      if (!M.host)
+        check_align_dev(M.zsrc[i], M.ztarg[i], M.ifcharge, M.charge ? M.charge[i] : nullptr,
+                        M.ifdipole, M.dipstr ? M.dipstr[i] : nullptr,
+                        M.dipvec ? M.dipvec[i] : nullptr, M.pot[i],
+                        M.grad ? M.grad[i] : nullptr, M.ifpgh);
+    }
     check_device();
     run_many(M, std::max(1, std::min(nworkers, 64)), done_ms);
   });
@@ -1200,6 +1238,7 @@ int plan2d_create_impl(double eps, int ns, const double* zsrc, int nt, const dou
       HostIn h;
       const zdc* zs = reinterpret_cast<const zdc*>(zsrc);
       const zdc* zt = reinterpret_cast<const zdc*>(ztarg);
+      if (!host) check_align16({zsrc, ztarg});
       if (host) {
         upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
         upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
@@ -1264,6 +1303,8 @@ int plan2d_solve(zfmm_plan2d plan, const double* zk, int nd, int ifcharge, const
     zdc k = zk ? mkz(zk[0], zk[1]) : mkz(0.0);
     const zdc* kp = zk ? &k : nullptr;
     if (!host) {
+      check_align16({pot, ifcharge == 1 ? charge : nullptr, ifdipole == 1 ? dipstr : nullptr,
+                     ifdipole == 1 ? dipvec : nullptr, ifpgh > 1 ? grad : nullptr});
       cudaStream_t s = (cudaStream_t)stream;
       run_plan2d(plan, kp, nd, ifcharge, (const zdc*)charge, ifdipole, (const zdc*)dipstr,
                  (const zdc*)dipvec, ifpgh, (zdc*)pot, (zdc*)grad, s);

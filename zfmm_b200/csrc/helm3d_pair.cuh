@@ -1,5 +1,5 @@
 // One source-target interaction of zh3devaldirect
-// (zfmm3d/src/helmholtz/zhfmm3d.f:606-693), x = target - source, R = sqrt(x . x)
+// (zfmm3d/src/helmholtz/zhfmm3d.f:626-693), x = target - source, R = sqrt(x . x)
 // on the principal branch, z = i k R:
 //   pot  += q e^z / (4 pi R) - ds (x . v) e^z (1 - z) / (4 pi R^3)
 //   grad += -q x e^z (1 - z) / (4 pi R^3)

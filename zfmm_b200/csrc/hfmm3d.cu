@@ -1,7 +1,7 @@
 // 3D Helmholtz complex-coordinate FMM (zhfmm3d) on the device.
 //
 // Reference: zfmm3d/src/helmholtz/zhfmm3d.f (driver :1-249, zhfmm3dmain
-// :256-600, direct sum :606-693, form/eval :699-1309), the translations of
+// :256-600, direct sum :626-693, form/eval :699-1309), the translations of
 // zfmm3d/src/helmholtz/zh3dtrans.f:1-780, h3dcommon.f, besseljs3d.f,
 // h3dterms.f and hndiv_fast.f.
 //

@@ -429,7 +429,7 @@ struct HSrcTileNd {
   zdc v[HPT][3];
 };
 
-// the pair interaction of zh3devaldirect (zhfmm3d.f:606-693): the pair's kernel
+// the pair interaction of zh3devaldirect (zhfmm3d.f:626-693): the pair's kernel
 // values once, then one complex MAC per output and right-hand side
 template <bool GRAD, bool DIP>
 __global__ void __launch_bounds__(HNDT, 3) k_hp2p3nd(HP2PNdArgs A) {

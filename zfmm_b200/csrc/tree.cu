@@ -23,6 +23,7 @@
 //     child order.  cub's radix sort is stable.
 // This file is compiled with --fmad=false so that the distance tests see the
 // same roundings as the reference (no contracted multiply-adds).
+#include <cmath>
 #include <cub/cub.cuh>
 #include <vector>
 #include "tree.cuh"
@@ -51,6 +52,15 @@ __device__ __forceinline__ int child_index(const double* p, const double* c) {
 }
 
 // ---- bounding box ------------------------------------------------------------
+// min / max that keep a NaN once one is seen (fmin / fmax drop it), so a NaN
+// coordinate reaches the root box size, where the host refuses it
+__device__ __forceinline__ double nan_min(double a, double b) {
+  return (a != a || b != b) ? a + b : fmin(a, b);
+}
+__device__ __forceinline__ double nan_max(double a, double b) {
+  return (a != a || b != b) ? a + b : fmax(a, b);
+}
+
 template <int D>
 __global__ void k_bbox_partial(const double* __restrict__ a, int na, const double* __restrict__ b,
                                int nb, double* __restrict__ part) {
@@ -63,8 +73,8 @@ __global__ void k_bbox_partial(const double* __restrict__ a, int na, const doubl
 #pragma unroll
     for (int d = 0; d < D; d++) {
       double v = p[d];
-      mn[d] = fmin(mn[d], v);
-      mx[d] = fmax(mx[d], v);
+      mn[d] = nan_min(mn[d], v);
+      mx[d] = nan_max(mx[d], v);
     }
   }
   __shared__ double smn[D][TB], smx[D][TB];
@@ -75,8 +85,8 @@ __global__ void k_bbox_partial(const double* __restrict__ a, int na, const doubl
     if (threadIdx.x < o)
 #pragma unroll
       for (int d = 0; d < D; d++) {
-        smn[d][threadIdx.x] = fmin(smn[d][threadIdx.x], smn[d][threadIdx.x + o]);
-        smx[d][threadIdx.x] = fmax(smx[d][threadIdx.x], smx[d][threadIdx.x + o]);
+        smn[d][threadIdx.x] = nan_min(smn[d][threadIdx.x], smn[d][threadIdx.x + o]);
+        smx[d][threadIdx.x] = nan_max(smx[d][threadIdx.x], smx[d][threadIdx.x + o]);
       }
     __syncthreads();
   }
@@ -97,12 +107,12 @@ __global__ void k_root(const double* part, int nparts, double* centers, double* 
   for (int d = 0; d < D; d++) { mn[d] = INFINITY; mx[d] = -INFINITY; }
   for (int i = 0; i < nparts; i++)
     for (int d = 0; d < D; d++) {
-      mn[d] = fmin(mn[d], part[i * 2 * D + d]);
-      mx[d] = fmax(mx[d], part[i * 2 * D + D + d]);
+      mn[d] = nan_min(mn[d], part[i * 2 * D + d]);
+      mx[d] = nan_max(mx[d], part[i * 2 * D + D + d]);
     }
   double b = mx[0] - mn[0];
   for (int d = 1; d < D; d++)
-    if (mx[d] - mn[d] > b) b = mx[d] - mn[d];
+    if (mx[d] - mn[d] > b || mx[d] - mn[d] != mx[d] - mn[d]) b = mx[d] - mn[d];
   *bs0 = b;
   for (int d = 0; d < D; d++) centers[d] = (mn[d] + mx[d]) / 2;
   ilevel[0] = 0;
@@ -188,7 +198,11 @@ __global__ void k_assign(const double* __restrict__ pts, int n, int* __restrict_
   int c = child_index<D>(p, centers + b * D);
   int j = ichild[b * NC + c];
   pbox[i] = j;
-  atomicAdd(&cnt[j], 1);
+  // points of one warp mostly fall in the same few boxes (at the coarse levels
+  // all of them do): one atomic per distinct box and warp instead of one per
+  // point, so the counters of the few coarse boxes are not serialised
+  unsigned grp = __match_any_sync(__activemask(), j);
+  if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&cnt[j], __popc(grp));
 }
 
 // ---- colleagues --------------------------------------------------------------
@@ -456,10 +470,12 @@ __global__ void k_lists(int nb, int fill, const int* __restrict__ ilevel,
   n4[b] = c4;
 }
 
+// maxima of four count arrays: grid-stride, one atomicMax per block and array
+// (out zeroed by the caller)
 __global__ void k_max4(int nb, const int* a, const int* b, const int* c, const int* d, int* out) {
   __shared__ int s[4][TB];
   int m0 = 0, m1 = 0, m2 = 0, m3 = 0;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
     m0 = max(m0, a[i]); m1 = max(m1, b[i]); m2 = max(m2, c[i]); m3 = max(m3, d[i]);
   }
   s[0][threadIdx.x] = m0; s[1][threadIdx.x] = m1; s[2][threadIdx.x] = m2; s[3][threadIdx.x] = m3;
@@ -469,7 +485,7 @@ __global__ void k_max4(int nb, const int* a, const int* b, const int* c, const i
       for (int k = 0; k < 4; k++) s[k][threadIdx.x] = max(s[k][threadIdx.x], s[k][threadIdx.x + o]);
     __syncthreads();
   }
-  if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
+  if (threadIdx.x < 4) atomicMax(&out[threadIdx.x], s[threadIdx.x][0]);
 }
 
 // ---- host helpers -----------------------------------------------------------
@@ -627,6 +643,10 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
   pbs.zero();
   pbt.zero();
   ZF_CUDA(cudaStreamSynchronize(s));
+  // a NaN or infinite real part makes the root size non-finite: no tree can be
+  // built (the reference would loop or divide by it), so the call is refused
+  if (!std::isfinite(bsz[0]))
+    throw zf_error(ZF_ERR_ARG, "coordinates must be finite (NaN or Inf in a real part)");
 
   std::vector<int> laddr(2 * (p.nlmax + 1), 0);
   laddr[0] = 0;
@@ -799,7 +819,9 @@ void build_lists_t(const DevTree& t, DevLists& L, cudaStream_t s) {
       t.ncoll.get(), t.coll.get(), t.mnbors, t.bsz.get(), t.isep, L.n[0].get(), L.n[1].get(),
       L.n[2].get(), L.n[3].get(), nullptr, nullptr, nullptr, nullptr, dummy_m, dummy_m, dummy_m,
       dummy_m);
-  klaunch(k_max4, 1, TB, 0, s, nb, L.n[0].get(), L.n[1].get(), L.n[2].get(), L.n[3].get(), mx.get());
+  mx.zero();
+  klaunch(k_max4, std::min(div_up(nb, TB), 1184), TB, 0, s, nb, L.n[0].get(), L.n[1].get(),
+          L.n[2].get(), L.n[3].get(), mx.get());
   ZF_LAUNCH_CHECK();
   ZF_CUDA(cudaMemcpyAsync(L.mn, mx.get(), 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   ZF_CUDA(cudaStreamSynchronize(s));
