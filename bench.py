@@ -78,6 +78,14 @@ WORKLOADS = {
     # (the instance distribution below), 64 complex normal charge and dipole
     # strength vectors with shared complex dipole vectors, zk = 10+0.2i,
     # pot + grad, eps=1e-9; one step = plan + one 64-right-hand-side solve
+    # zhfmm3d batched right-hand sides on the batched zlfmm3d geometry (1,000,000
+    # points U[-1,1]^3 with imaginary parts 0.05 sin(2 pi .)), zk = 10+0.2i, 64
+    # complex normal charge vectors, charges only, pot + grad, eps=1e-9: the
+    # batched-vs-plain per-right-hand-side speed-up of this case is the
+    # north-star target line (also carried by the default line)
+    "zhfmm3d_batched_1m_64": dict(kind="helm3d", geometry="cube", n=1_000_000, nrhs=64,
+                                  eps=1e-9, zk=10 + 0.2j, ifpgh=2, isep=1, cpu_n=30_000,
+                                  dipoles=False),
     "zhfmm3d_batched_200k_64": dict(kind="helm3d", n=200_000, nrhs=64, eps=1e-9, zk=10 + 0.2j,
                                     ifpgh=2, isep=1, cpu_n=30_000, dipoles=True),
     "zhfmm3d_batched_30k_32": dict(kind="helm3d", n=30_000, nrhs=32, eps=1e-9, zk=10 + 0.2j,
@@ -99,7 +107,13 @@ WORKLOADS = {
                                   n=500_000, eps=1e-9, zk=10 + 0.2j, ifpgh=2, isep=1,
                                   cpu_n=30_000, nstreams=8),
 }
+for _k, _v in WORKLOADS.items():
+    _v["name"] = _k
 DEFAULT_WORKLOAD = "zhfmm2d_curve_2m"
+# the batched case reported beside the default line (batched_rhs key)
+BATCHED_KEY_WORKLOAD = "zhfmm3d_batched_1m_64"
+# wall-clock bound of the reference arm's timed solves at full size
+REF_BUDGET_S = 600.0
 
 def m2l3d_flops(p):
     """Real flops of one point-and-shoot 3D Laplace translation at order p, as
@@ -229,6 +243,8 @@ def make_inputs(wl, seed, n=None, nrhs=1):
     n = wl["n"] if n is None else n
     if wl["kind"] == "lap3d" and nrhs > 1:
         return W.lap3d_uniform(n, seed=seed, nrhs=nrhs)
+    if wl["kind"] == "helm3d" and nrhs > 1 and wl.get("geometry") == "cube":
+        return W.lap3d_uniform(n, seed=seed, nrhs=nrhs)
     if wl["kind"] == "helm3d" and nrhs > 1:
         w = W.sphere3d(n, seed=seed)
         rng = np.random.default_rng(seed + 7919)
@@ -312,11 +328,30 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def host_cores():
+    """(physical cores, logical CPUs) of this host."""
+    logical = os.cpu_count() or 1
+    try:
+        import psutil
+        phys = psutil.cpu_count(logical=False) or logical
+    except Exception:
+        phys = logical
+    return phys, logical
+
+
+def set_omp_threads():
+    """OpenMP threads of the CPU oracle = the physical core count (set before the
+    oracle library is loaded, which reads it once)."""
+    phys, _ = host_cores()
+    os.environ["OMP_NUM_THREADS"] = str(phys)
+    return phys
+
+
 def cpu_time_oracle(wl, inp, reps_min=1, budget_s=15.0):
     """Oracle (C restatement, OpenMP) on the host cores; returns (sec per solve, cores)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
-    cores = os.cpu_count() or 1
+    cores = int(os.environ.get("OMP_NUM_THREADS", host_cores()[0]))
     z = inp["zsrc"].T
     times = []
     t_end = time.perf_counter() + budget_s
@@ -342,12 +377,22 @@ def cpu_time_oracle(wl, inp, reps_min=1, budget_s=15.0):
 
 
 def run_reference(args, wl, ws, rank):
+    """The reference algorithm on the host cores (the C restatement in oracle/,
+    OpenMP on every physical core), on the full workload: each step is one
+    whole solve of the same points as the GPU arm.  Only if one solve is so
+    slow that K steps would run past REF_BUDGET_S does it fall back to a
+    sample of the workload's distribution (and says so in the line)."""
     if rank != 0:
         return
-    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    nt = wl["cpu_n"]
+    phys = set_omp_threads()
+    logical = host_cores()[1]
+    nfull = wl["n"] * wl.get("nrhs", 1)
+    nt = wl["n"]
     inp = make_inputs(wl, seed=0, n=nt)
-    for _ in range(min(args.warmup, 1)):
+    t1, cores, _n = cpu_time_oracle(wl, inp, reps_min=1, budget_s=0.0)  # warm-up solve
+    if t1 * args.steps > REF_BUDGET_S:
+        nt = wl["cpu_n"]
+        inp = make_inputs(wl, seed=0, n=nt)
         cpu_time_oracle(wl, inp, reps_min=1, budget_s=0.0)
     per = []
     for _ in range(args.steps):
@@ -355,17 +400,24 @@ def run_reference(args, wl, ws, rank):
         per.append(t)
     tot = sum(per)
     value = nt * args.steps / tot
+    full = nt == wl["n"]
     line = {
         "impl": "reference", "metric": "targets/sec at eps=1e-9", "value": value,
         "unit": "targets/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "n": wl["n"], "n_timed_sample": nt,
-                   "eps": wl["eps"], "zk": str(wl.get("zk")), "ifpgh": wl["ifpgh"],
-                   "isep": wl["isep"], "l2": "n/a (host)"},
+        "config": {"workload": args.workload, "n": wl["n"], "n_timed": nt,
+                   "same_config": full, "eps": wl["eps"], "zk": str(wl.get("zk")),
+                   "ifpgh": wl["ifpgh"], "isep": wl["isep"], "l2": "n/a (host)",
+                   "omp_threads": phys, "physical_cores": phys, "logical_cpus": logical},
         "cpu_baseline": {"value": value, "unit": "targets/s", "cores": cores, "kind": "port",
-                         "sample": (f"{nt} points of the workload's distribution "
-                                    f"(full workload: {wl['n']}), {args.steps} solves")},
+                         "sample": ((f"the full workload ({nt} points, seed 0), one solve per "
+                                     f"step, {args.steps} steps after one warm-up solve")
+                                    if full else
+                                    (f"{nt} points of the workload's distribution (full "
+                                     f"workload: {wl['n']}: one full solve took {t1:.1f} s, "
+                                     f"{args.steps} would exceed {REF_BUDGET_S:.0f} s), "
+                                     f"{args.steps} solves"))},
         "e2e": {"value": value, "unit": "targets/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -531,13 +583,22 @@ def run_ours(args, wl, ws, rank, local):
         traffic = json.load(open(tpath)).get(top)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        set_omp_threads()
         ncpu = wl["cpu_n"]
         cinp = inp if ncpu == n else make_inputs(wl, seed=0, n=ncpu)
         t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
         cpu = {"value": ncpu / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
                "sample": (f"{ncpu} points of the workload's distribution (full workload: {n}), "
                           f"median of {nrep} solves")}
+    # the batched-right-hand-side target case, measured in the same run (one
+    # GPU only: it is not part of the replicated step)
+    batched = None
+    if ws == 1 and args.workload == DEFAULT_WORKLOAD and not args.no_batched:
+        import types
+        bargs = types.SimpleNamespace(steps=1, warmup=1, no_cpu=True,
+                                      workload=BATCHED_KEY_WORKLOAD)
+        batched = run_ours_batched(bargs, WORKLOADS[BATCHED_KEY_WORKLOAD], ws, rank, local,
+                                   summary=True)
     if rank != 0:
         return
     line = {
@@ -564,12 +625,18 @@ def run_ours(args, wl, ws, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "batched_rhs": batched,
     }
     print(json.dumps(line), flush=True)
 
 
-def run_ours_batched(args, wl, ws, rank, local):
-    """One step = plan (tree, lists, centres) + one nd-right-hand-side solve."""
+def run_ours_batched(args, wl, ws, rank, local, summary=False):
+    """One step = plan (tree, lists, centres) + one nd-right-hand-side solve.
+
+    summary=True (the default line's batched key): one warm-up and one timed
+    step, the plain single solve on the same geometry, the accuracy against the
+    direct sum; no end-to-end pass, no CPU leg; returns a dict instead of
+    printing a line."""
     import ctypes
 
     import torch
@@ -586,7 +653,18 @@ def run_ours_batched(args, wl, ws, rank, local):
     zk = complex(wl.get("zk", 0))
     zka = np.array([zk.real, zk.imag])
     zkp = zka.ctypes.data_as(ctypes.c_void_p)
-    inp = make_inputs(wl, seed=rank, nrhs=nd)
+    # one geometry and nd right-hand sides for the whole job; with N ranks each
+    # solves a contiguous block of the right-hand sides (zfmm_b200.shard: no
+    # collective on the data path; every rank builds the geometry's plan)
+    from zfmm_b200 import shard
+    nd_total = nd
+    r0, r1 = shard.rhs_block(nd_total, rank, ws)
+    nd = r1 - r0
+    if nd < 1:
+        raise SystemExit("more ranks than right-hand sides")
+    inp = make_inputs(wl, seed=0, nrhs=nd_total)
+    inp["charge"] = inp["charge"][r0:r1]
+    inp["dipstr"] = inp["dipstr"][r0:r1]
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     zs = t(inp["zsrc"].T)
     q = t(inp["charge"].T)  # (n, nd): right-hand side fastest
@@ -625,7 +703,7 @@ def run_ours_batched(args, wl, ws, rank, local):
             _capi.check(L.zfmm_zlfmm3d_dev(eps, n, P(zs), 1, P(q0), ifd, Po(ds0), Po(dv),
                                            P(pot1), P(grad1), n, P(zs), ifpgh, isep, sp))
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(1 if summary else max(args.warmup, 3)):
         solve()
     torch.cuda.synchronize()
     L.zfmm_set_step_timing(2)
@@ -665,11 +743,11 @@ def run_ours_batched(args, wl, ws, rank, local):
     torch.cuda.synchronize()
     plan_ms = pc0.elapsed_time(pc1)
     _capi.check(L.zfmm_plan3d_destroy(hh))
-    for _ in range(3):
+    for _ in range(1 if summary else 3):
         solve_plain()
     torch.cuda.synchronize()
     pl_t = []
-    for k in range(5):
+    for k in range(2 if summary else 5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.fill_(k & 255)
         e0.record(stream)
@@ -684,8 +762,36 @@ def run_ours_batched(args, wl, ws, rank, local):
         tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         tot_ms = float(tt.item())
-    value = ws * n * nd * args.steps / (tot_ms * 1e-3)
+    value = n * nd_total * args.steps / (tot_ms * 1e-3)
     plain_value = n / (plain_ms * 1e-3)
+    if summary:
+        pg = pot.cpu().numpy()
+        p1 = pot1.cpu().numpy()
+        rng = np.random.default_rng(1234)
+        sub = np.sort(rng.choice(n, size=min(n, 1024), replace=False))
+        errs = []
+        for r in (0, nd - 1):
+            dsr = inp["dipstr"][r] if ifd else None
+            dvr = inp["dipvec"] if ifd else None
+            if helm:
+                pd, _ = zfmm_b200.zh3devaldirect(zk, len(sub), inp["zsrc"][:, sub], n,
+                                                 inp["zsrc"], inp["charge"][r], dsr, dvr, 1, ifd,
+                                                 1)
+            else:
+                pd, _ = zfmm_b200.zl3devaldirect(len(sub), inp["zsrc"][:, sub], n, inp["zsrc"],
+                                                 inp["charge"][r], dsr, dvr, 1, ifd, 1)
+            errs.append(float(np.linalg.norm(pg[sub, r] - pd) / np.linalg.norm(pd)))
+        L.zfmm_set_step_timing(0)
+        return {"workload": wl["name"], "n": n, "nrhs": nd, "eps": eps,
+                "zk": [zk.real, zk.imag] if helm else None, "ms_per_step": tot_ms / args.steps,
+                "value": value, "unit": "targets/s",
+                "step": "plan (tree, lists, centres) + one solve of all right-hand sides",
+                "plain_single_rhs_ms": plain_ms,
+                "batched_per_rhs_speedup": value / ws / plain_value,
+                "rel_l2_err_vs_direct": max(errs),
+                "rel_l2_batched_vs_plain_rhs0": float(np.linalg.norm(pg[:, 0] - p1)
+                                                      / np.linalg.norm(p1)),
+                "plan_build_ms": plan_ms}
 
     # end to end: host arrays in pinned memory through the host entry points
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -756,7 +862,7 @@ def run_ours_batched(args, wl, ws, rank, local):
     peak = float(L.zfmm_probe_fp64_tflops(20000))
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        set_omp_threads()
         ncpu = wl["cpu_n"]
         cinp = make_inputs(wl, seed=0, n=ncpu)
         t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
@@ -769,16 +875,18 @@ def run_ours_batched(args, wl, ws, rank, local):
     line = {
         "metric": "targets/sec at eps=1e-9", "value": value, "unit": "targets/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if ws > 1 else "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "n": n, "nrhs": nd, "eps": eps, "ifpgh": ifpgh,
+        "config": {"workload": args.workload, "n": n, "nrhs": nd_total, "eps": eps, "ifpgh": ifpgh,
                    "isep": isep, "charges": True, "dipoles": bool(ifd),
                    **({"zk": [zk.real, zk.imag]} if helm else {}),
                    "step": "plan (tree, lists, centres) + one solve of all right-hand sides",
                    "l2": "flushed (256 MiB write) between steps",
-                   "parallelism": f"replicas x{ws}", "nboxes": info["nboxes"],
-                   "nlevels": info["nlevels"], "nterms": p},
-        "e2e": {"value": ws * n * nd * args.steps / e2e_tot, "unit": "targets/s",
+                   "parallelism": (f"right-hand sides sharded over {ws} ranks ({nd} on rank 0)"
+                                   if ws > 1 else "one GPU"),
+                   "nboxes": info["nboxes"], "nlevels": info["nlevels"], "nterms": p},
+        "e2e": {"value": n * nd_total * args.steps / e2e_tot, "unit": "targets/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "plan_build_ms": plan_ms,
         "plain_single_rhs": {"value": plain_value, "unit": "targets/s", "ms_per_solve": plain_ms,
@@ -814,11 +922,19 @@ def run_ours_many(args, wl, ws, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     L = _capi.lib()
-    rng = np.random.default_rng(2024 + rank)
-    ni = wl["instances"]
-    sizes = np.exp(rng.uniform(np.log(wl["nmin"]), np.log(wl["nmax"]), ni)).astype(np.int64)
+    from zfmm_b200 import shard
+    # one set of instances for the whole job; with N ranks each solves the
+    # share zfmm_b200.shard assigns it by size (independent units, no
+    # collective on the data path)
+    rng = np.random.default_rng(2024)
+    ni_all = wl["instances"]
+    all_sizes = np.exp(rng.uniform(np.log(wl["nmin"]), np.log(wl["nmax"]),
+                                   ni_all)).astype(np.int64)
+    mine = shard.partition_by_size(all_sizes, ws)[rank]
+    sizes = all_sizes[mine]
+    ni = len(mine)
     eps, zk, ifpgh, isep = wl["eps"], wl["zk"], wl["ifpgh"], wl["isep"]
-    inst = [W.sphere3d(int(n), seed=1000 * rank + i) for i, n in enumerate(sizes)]
+    inst = [W.sphere3d(int(all_sizes[i]), seed=i) for i in mine]
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     dz = [t(w["zsrc"].T) for w in inst]
     dq = [t(w["charge"]) for w in inst]
@@ -865,8 +981,8 @@ def run_ours_many(args, wl, ws, rank, local):
         tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         tot_ms = float(tt.item())
-    npts = int(sizes.sum())
-    value = ws * npts * args.steps / (tot_ms * 1e-3)
+    npts = int(all_sizes.sum())
+    value = npts * args.steps / (tot_ms * 1e-3)
     lat_all = np.concatenate(lat)
     # the same instances one after another on one stream (the plain calls)
     torch.cuda.synchronize()
@@ -917,7 +1033,7 @@ def run_ours_many(args, wl, ws, rank, local):
     peak = float(L.zfmm_probe_fp64_tflops(20000))
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        set_omp_threads()
         cinp = make_inputs(wl, seed=0, n=wl["cpu_n"])
         t_cpu, cores, nrep = cpu_time_oracle(wl, cinp, reps_min=1, budget_s=12.0)
         cpu = {"value": wl["cpu_n"] / t_cpu, "unit": "targets/s", "cores": cores, "kind": "port",
@@ -929,16 +1045,18 @@ def run_ours_many(args, wl, ws, rank, local):
     line = {
         "metric": "targets/sec at eps=1e-9", "value": value, "unit": "targets/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "instances": ni, "points_total": npts,
-                   "n_min": int(sizes.min()), "n_max": int(sizes.max()), "eps": eps,
+        "config": {"workload": args.workload, "instances": ni_all, "points_total": npts,
+                   "instances_rank0": ni,
+                   "n_min": int(all_sizes.min()), "n_max": int(all_sizes.max()), "eps": eps,
                    "zk": str(zk), "ifpgh": ifpgh, "isep": isep, "charges": True,
                    "dipoles": True, "nstreams": nst,
                    "timing": ("CUDA events on the current stream bracketing the call, which "
                               "returns after every worker stream has finished"),
                    "l2": "flushed (256 MiB write) between steps",
-                   "parallelism": f"replicas x{ws}"},
+                   "parallelism": (f"instances sharded by size over {ws} ranks"
+                                   if ws > 1 else "one GPU")},
         "latency_ms": {"p50": float(np.percentile(lat_all, 50)),
                        "p99": float(np.percentile(lat_all, 99)),
                        "max": float(lat_all.max())},
@@ -1105,7 +1223,7 @@ def run_ours_adjoint(args, wl, ws, rank, local):
     peak = float(L.zfmm_probe_fp64_tflops(20000))
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        set_omp_threads()
         ncpu = wl["cpu_n"]
         zc = points(*(torch.tensor(x) for x in (xr[:ncpu], disp[:ncpu], curve[:ncpu])),
                     torch.tensor(a0, dtype=torch.float64)).numpy()
@@ -1154,6 +1272,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-right-hand-side key of the default line")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_init()

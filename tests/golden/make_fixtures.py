@@ -1,7 +1,7 @@
 """Generate the golden fixtures used by the parity tests.
 
-Run once, in a checkout that can see the reference tree (its path is given by
---ref, default /root/reference); the outputs are committed, so the tests never
+Run once, in a checkout that can see the reference tree (its root is given by
+the required --ref argument); the outputs are committed, so the tests never
 read the reference at run time.
 
 Inputs (reference test data and logs):
@@ -68,7 +68,8 @@ def parse_log(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True,
+                    help="root of a checkout of the reference (wangyuguan/zfmm)")
     args = ap.parse_args()
     ref = args.ref
 

@@ -33,6 +33,7 @@ __global__ void __launch_bounds__(DTB) k_direct2d(Inputs2D in, zdc zk, int chunk
     x2 = ldz(&in.ztarg[2 * i + 1]);
   }
   zdc p = mkz(0.0), g1 = mkz(0.0), g2 = mkz(0.0);
+  const HelmK K = helm_k(zk);
   for (int t = j0; t < j1; t += TILE) {
     int n = min(TILE, j1 - t);
     __syncthreads();
@@ -53,7 +54,7 @@ __global__ void __launch_bounds__(DTB) k_direct2d(Inputs2D in, zdc zk, int chunk
     if (valid)
       for (int k = 0; k < n; k++) {
         if (HELM)
-          helm_pair<GRAD>(zk, x1, x2, sy[k][0], sy[k][1], sy[k][2], sy[k][3], sy[k][4], sy[k][5],
+          helm_pair<GRAD>(K, x1, x2, sy[k][0], sy[k][1], sy[k][2], sy[k][3], sy[k][4], sy[k][5],
                           in.ifcharge, in.ifdipole, p, g1, g2);
         else
           lap2d_pair<GRAD>(x1, x2, sy[k][0], sy[k][1], sy[k][2], sy[k][3], sy[k][4], sy[k][5],

@@ -22,6 +22,8 @@
 //               accumulating pot and grad without storing the function table;
 //   P2P:        group of lanes per target over the list-1 sources, shuffle
 //               reduction.
+#include <cmath>
+#include <cub/cub.cuh>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -80,180 +82,415 @@ __device__ __forceinline__ void polar(zdc a1, zdc a2, zdc& rz, zdc& ez) {
   ez = a1 / rz + zmul_i(a2 / rz);
 }
 
-// H0, H1 for a warp-uniform argument: the quadrature nodes of hank01_integral
-// are spread over the lanes; the other regions are evaluated by every lane.
-__device__ void hank01_warp(zdc z, zdc& h0, zdc& h1) {
-  if (z.im == 0.0) z.im = 0.0;
-  if (zabs(z) < 2.0 || z.im < 0.0) {
-    hank01(z, h0, h1);
-    return;
-  }
-  int lane = threadIdx.x & 31;
-  zdc c = zmul_i(zinv(2.0 * z));
-  double s = ZF_HQ_STEP * lane, s2 = s * s;
-  double w = ZF_HQ_STEP * exp(-s2) * (lane == 0 ? 0.5 : 1.0);
-  zdc r = zsqrt_p(mkz(1.0) + s2 * c);
-  zdc f0 = w * zinv(r), f1 = (w * s2) * r;
-  for (int o = 16; o; o >>= 1) {
-    f0 += shfl_xor_z(f0, o);
-    f1 += shfl_xor_z(f1, o);
-  }
-  zdc pre = ZF_SQRT_2_PI * zinv(zsqrt_p(z));
-  zdc e = zexp_p(zmul_i(z));
-  const double r2 = 0.70710678118654752440;
-  h0 = (2.0 * ZF_INV_SQRT_PI) * ((pre * (e * zdc{r2, -r2})) * f0);
-  h1 = (4.0 * ZF_INV_SQRT_PI) * ((pre * (e * zdc{-r2, -r2})) * f1);
-}
+constexpr int MAXR = 8;  // M2M / M2L / L2L coefficient slots per lane: p <= 255
 
-// scaled Hankel table hv[0..n] of a warp-uniform argument into shared memory
-__device__ void h2dall_warp(int n, zdc z, double rscale, zdc* hv) {
-  int lane = threadIdx.x & 31;
+// ---- translation tables --------------------------------------------------------
+// Every M2L, M2M and L2L translation of the reference (zh2dmploc, zh2dmpmp,
+// zh2dlocloc) uses, per box pair, one table of scaled Bessel or Hankel
+// functions of z = zk |c1 - c2| and the powers of the pair's angle factor
+// e = (d1 + i d2)/|d| (zcart2polar; the reference's ezs(m) = ez^m).  The
+// tables depend on the geometry and zk only, so they are built once per
+// solve (or per plan and wavenumber) for all pairs, one thread per pair, and
+// read by the translation kernels.  Entry k of a table is the pair
+//   tab[k] = ( F_k e^k , (-1)^k F_k e^-k ),   k = 0..n,
+// with F_k = H_k rs^k (h2dall, M2L) or F_k = J_k / rs^k (jbessel2d, M2M and
+// L2L); a Bessel table carries Miller's normalisation factor in tab[n+1].
+
+__device__ __forceinline__ double4 tab_entry(zdc u, zdc v) { return make_double4(u.re, u.im, v.re, v.im); }
+
+// Scaled Hankel functions h2dall(n, z, rs) (h2dcommon.f:71-173: H0/H1, then the
+// forward recurrence H_{k+1} = (2k/z) H_k - H_{k-1}; zero table for |z| < 1e-200)
+// times the angle powers, running products of e and 1/e.
+__device__ void hank_table(zdc z, zdc e, double rs, int n, double4* out) {
   if (zabs(z) < 1e-200) {
-    for (int i = lane; i <= n; i += 32) hv[i] = mkz(0.0);
-    __syncwarp();
+    for (int k = 0; k <= n; k++) out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
     return;
   }
   zdc h0, h1;
-  hank01_warp(z, h0, h1);
-  if (lane == 0) {
-    hv[0] = h0;
-    if (n >= 1) hv[1] = h1 * rscale;
-    double sc2 = rscale * rscale;
-    zdc zi = rscale * zinv(z);
-    for (int i = 1; i < n; i++) hv[i + 1] = ((2.0 * i) * zi) * hv[i] - sc2 * hv[i - 1];
+  hank01(z, h0, h1);
+  zdc ie = zinv(e), E = mkz(1.0), IE = mkz(1.0);
+  zdc zi = rs * zinv(z);
+  double sc2 = rs * rs;
+  zdc hm = h0, h = h1 * rs;
+  out[0] = tab_entry(h0, h0);
+  for (int k = 1; k <= n; k++) {
+    E = E * e;
+    IE = IE * ie;
+    out[k] = tab_entry(h * E, sgn(k) * (h * IE));
+    zdc hn = ((2.0 * k) * zi) * h - sc2 * hm;
+    hm = h;
+    h = hn;
   }
-  __syncwarp();
 }
 
-// Scaled Bessel table out[0..nterms+1] = J_n(z)/rscale^n by Miller's backward
-// recurrence from the reference's start index, keeping only the entries that
-// are returned (the normalisation sum is accumulated during the sweep).
-__device__ void jbessel_stream(int nterms, zdc z, double rscale, zdc* out) {
-  int top = nterms + 1;
+// Scaled Bessel functions J_k/rs^k, k = 0..n, by the backward recurrence of
+// jbessel2d (cdjseval2d.f:23-221) from the reference's start index, with the
+// normalisation sum psi (e^{-+iz} = J0 + 2 sum (-+i)^k J_k) accumulated on the
+// way down.  The entries are written unnormalised times the angle powers
+// (e^k from e^n downwards); tab[n+1] = (e^{-+iz}/psi, 0) is applied by the
+// reader.  On overflow the values written so far are rescaled, as the
+// reference does.
+__device__ void bessel_table(zdc z, zdc e, double rs, int n, double4* out) {
   if (zabs(z) < 1e-200) {
-    out[0] = mkz(1.0);
-    for (int i = 1; i <= top; i++) out[i] = mkz(0.0);
+    out[0] = make_double4(1.0, 0.0, 1.0, 0.0);
+    for (int k = 1; k <= n; k++) out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+    out[n + 1] = make_double4(1.0, 0.0, 0.0, 0.0);
     return;
   }
-  int ntop = jbessel_top(nterms, z);
-  zdc zr = rscale * zinv(z);
-  double sc2 = rscale * rscale;
+  const int top = n + 1;  // jbessel2d's table runs to nterms + 1
+  int ntop = jbessel_top(n, z);
+  zdc zr = rs * zinv(z);
+  double sc2 = rs * rs;
   zdc zmul = z.im < 0.0 ? mkz(0.0, 1.0) : mkz(0.0, -1.0);
-  // g_{ntop} = 0, g_{ntop-1} = 1
-  zdc gp1 = mkz(0.0), g = mkz(1.0), psi = mkz(0.0);
-  for (int i = 0; i <= top; i++) out[i] = mkz(0.0);
-  // psi accumulates sum_{n>=1} zmul^n rscale^(n-1) g_n in Horner form from the top
-  for (int n = ntop - 1; n >= 0; n--) {
-    // g holds g_n
-    if (n <= top) out[n] = g;
-    if (n >= 1) {
-      int r = n & 3;
+  zdc ie = zinv(e);
+  zdc E = zpown(e, n), IE = zpown(ie, n);
+  zdc gp1 = mkz(0.0), g = mkz(1.0), psi = mkz(0.0), g0 = mkz(0.0);
+  for (int k = ntop - 1; k >= 0; k--) {
+    if (k <= n) {
+      out[k] = tab_entry(g * E, sgn(k) * (g * IE));
+      E = E * ie;
+      IE = IE * e;
+    }
+    if (k == 0) g0 = g;
+    if (k >= 1) {
+      int r = k & 3;
       zdc zn = r == 0 ? mkz(1.0) : (r == 1 ? zmul : (r == 2 ? mkz(-1.0) : -zmul));
-      psi = rscale * psi + zn * g;
-      zdc gm1 = ((2.0 * n) * zr) * g - sc2 * gp1;
+      psi = rs * psi + zn * g;
+      zdc gm1 = ((2.0 * k) * zr) * g - sc2 * gp1;
       gp1 = g;
       g = gm1;
       if (zabs(g) > 1e200) {
         g = 1e-200 * g;
         gp1 = 1e-200 * gp1;
         psi = 1e-200 * psi;
-        for (int k = n; k <= top; k++) out[k] = 1e-200 * out[k];
+        for (int j = k; j <= n; j++) {
+          double4 v = out[j];
+          out[j] = make_double4(1e-200 * v.x, 1e-200 * v.y, 1e-200 * v.z, 1e-200 * v.w);
+        }
       }
     }
   }
-  // g_{ntop}=0 contributes nothing; psi misses the factor for the top zero
-  psi = 2.0 * rscale * psi + out[0];
-  zdc e = z.im < 0.0 ? zexp_p(zmul_i(z)) : zexp_p(-zmul_i(z));
-  zdc sc = e / psi;
-  for (int i = 0; i <= top; i++) out[i] = out[i] * sc;
+  (void)top;
+  psi = 2.0 * rs * psi + g0;
+  zdc ex = z.im < 0.0 ? zexp_p(zmul_i(z)) : zexp_p(-zmul_i(z));
+  zdc sc = ex / psi;
+  out[n + 1] = make_double4(sc.re, sc.im, 0.0, 0.0);
+}
+
+struct TabArgs {
+  double4* tab;
+  // per-level real power tables (host-computed): rs^k for the M2L weights,
+  // (rs1 rs2)^k and (rs2/rs1)^k for M2M, rs1^(2k) and (rs1/rs2)^k for L2L
+  const double* pw;
+  long pw_m2l[MAXL], pw_m2m[MAXL], pw_l2l[MAXL];
+  long m2l_base[MAXL];   // first entry of the level's M2L tables
+  long m2l_pair0[MAXL];  // first list-2 pair (index into pairoff order) of the level
+  long ml_base[MAXL];    // first entry of the M2M / L2L tables of the children of level l
+};
+
+// first box of the level range [lo, hi] whose pair range contains pair q
+__device__ __forceinline__ int pair_box(const int* pairoff, int lo, int hi, long q) {
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (pairoff[mid] <= q) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// M2L tables of every list-2 pair of levels >= 2 (one thread per pair)
+__global__ void __launch_bounds__(128) k_tab_m2l(long q0, long q1, int b0, int b1, HelmArgs A,
+                                                 TabArgs TA, const int* pairoff, const int* nl2,
+                                                 const int* l2, int m2) {
+  long q = q0 + blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (q >= q1) return;
+  int b = pair_box(pairoff, b0, b1, q);
+  int il = (int)(q - pairoff[b]);
+  if (il >= nl2[b] || A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
+  int jb = l2[(size_t)b * m2 + il];
+  if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) return;
+  int l = A.ilevel[b], p = A.T.p[l];
+  zdc rz, e;
+  polar(A.zctarg[2 * b] - A.zcsrc[2 * jb], A.zctarg[2 * b + 1] - A.zcsrc[2 * jb + 1], rz, e);
+  hank_table(rz * A.zk, e, A.T.rs[l], 2 * p,
+             TA.tab + TA.m2l_base[l] + (q - TA.m2l_pair0[l]) * (2 * p + 1));
+}
+
+// M2M and L2L tables of every box of levels >= 3 with its parent (one thread
+// per child): M2M (zh2dmpmp, child multipole -> parent at the source centres,
+// scale of the parent) if both hold sources; L2L (zh2dlocloc, parent local ->
+// child at the target centres, scale of the child) if both hold targets and
+// the parent has list-2 or list-4 boxes (the reference's step-7 test).
+__global__ void __launch_bounds__(128) k_tab_m2m_l2l(int c0, int c1, HelmArgs A, TabArgs TA,
+                                                     const int* nl2, const int* nl4) {
+  int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > c1) return;
+  int lc = A.ilevel[c];
+  if (lc < 3) return;
+  int b = A.iparent[c], l = lc - 1;
+  int nt = A.T.p[l] + A.T.p[lc];
+  double4* t = TA.tab + TA.ml_base[l] + (long)(c - A.T.lo[lc]) * 2 * (nt + 2);
+  if (A.isrcse[2 * b + 1] >= A.isrcse[2 * b] && A.isrcse[2 * c + 1] >= A.isrcse[2 * c]) {
+    zdc rz, e;
+    polar(A.zcsrc[2 * b] - A.zcsrc[2 * c], A.zcsrc[2 * b + 1] - A.zcsrc[2 * c + 1], rz, e);
+    bessel_table(rz * A.zk, e, A.T.rs[l], nt, t);
+  }
+  if (A.itargse[2 * b + 1] >= A.itargse[2 * b] && (nl2[b] > 0 || nl4[b] > 0) &&
+      A.itargse[2 * c + 1] >= A.itargse[2 * c]) {
+    zdc rz, e;
+    polar(A.zctarg[2 * c] - A.zctarg[2 * b], A.zctarg[2 * c + 1] - A.zctarg[2 * b + 1], rz, e);
+    bessel_table(rz * A.zk, e, A.T.rs[lc], nt, t + (nt + 2));
+  }
 }
 
 // ---- step 1 / 6: P2M (zh2dformmp) and P2L (zh2dformloc) ------------------------
-constexpr int FCH = 8;  // sources whose function tables are built at once
+// One warp per expansion centre.  Sources are taken fch at a time: lane k < fch
+// computes the whole coefficient vector of one source (its Bessel or Hankel
+// functions by the same recurrences as above, the powers ez^(+-m) as running
+// products) into a shared column; then every lane sums its coefficients over
+// the fch columns in registers.  Coefficient i of the register slots is
+// m = i - p (i = lane + 32 r).  fch = FCH unless the columns of a high order
+// would not fit in shared memory.
+constexpr int FCH = 16;
 
-// Accumulate the expansion about centre (c1, c2) with scale rs and p terms
-// from sources [s0, s1].  `tab` is per-warp shared scratch of FCH*(p+2)
-// complex; `local` selects Hankel (P2L) or Bessel (P2M) functions.  Lane k
-// (< FCH) builds the table of one source, then lane = coefficient m adds the
-// contributions of the FCH sources.
-__device__ void form_expansion(const HelmArgs& A, int s0, int s1, zdc c1, zdc c2, double rs, int p,
-                               bool local, zdc* tab, zdc* accp, zdc* accm, zdc& acc0) {
-  int lane = threadIdx.x & 31;
-  int P2 = p + 2;
-  for (int j0 = s0; j0 <= s1; j0 += FCH) {
-    int j = j0 + lane;
-    if (lane < FCH && j <= s1) {
-      zdc* col = tab + lane * P2;
-      zdc rz, ez;
-      polar(ldz(&A.zsrc[2 * j]) - c1, ldz(&A.zsrc[2 * j + 1]) - c2, rz, ez);
-      zdc z = rz * A.zk;
-      if (local) h2dall(p + 1, z, rs, col, 0, nullptr);
-      else jbessel_stream(p, z, rs, col);
-    }
-    __syncwarp();
-    int nsrc = min(FCH, s1 - j0 + 1);
-    for (int k = 0; k < nsrc; k++) {
-      int jj = j0 + k;
-      const zdc* f = tab + k * P2;
-      zdc a1 = ldz(&A.zsrc[2 * jj]) - c1, a2 = ldz(&A.zsrc[2 * jj + 1]) - c2;
-      zdc rzk, ezk;
-      polar(a1, a2, rzk, ezk);
-      zdc iez = zinv(ezk);
-      zdc q = A.ifcharge ? ldz(&A.charge[jj]) : mkz(0.0);
-      zdc ds = mkz(0.0), pr = mkz(0.0), pe = mkz(0.0);
-      if (A.ifdipole) {
-        ds = ldz(&A.dipstr[jj]);
-        zdc d1 = ldz(&A.dipvec[2 * jj]), d2 = ldz(&A.dipvec[2 * jj + 1]);
-        zdc vr1 = a1 / rzk, vr2 = a2 / rzk;
-        pr = vr1 * d1 + vr2 * d2;
-        pe = -vr2 * d1 + vr1 * d2;
-      }
-      zdc pe_rz = pe / rzk, izk = zinv(rzk * A.zk);
-      // coefficients m = lane, lane+32, ... (0..p); ezs(-m) = ez^-m, ezs(m) = ez^m
-      for (int m = lane, r = 0; m <= p; m += 32, r++) {
-        zdc em = zpown(iez, m), ep = zpown(ezk, m);
-        zdc fm = f[m];
-        zdc fder;  // derivative of the scaled function (h2dall / jbessel2d conventions)
-        if (local) fder = (m == 0) ? -f[1] / rs : rs * f[m - 1] - ((double)m * izk) * fm;
-        else fder = (m == 0) ? -f[1] * rs : (0.5 / rs) * f[m - 1] - (0.5 * rs) * f[m + 1];
-        zdc cm = fm * em * q, cneg = sgn(m) * (fm * ep * q);
-        if (A.ifdipole) {
-          zdc dr = em * fder * A.zk, dth = fm * zdc{0.0, -(double)m} * em;
-          cm -= ds * (dr * pr + dth * pe_rz);
-          zdc drn = ep * fder * A.zk, dthn = fm * zdc{0.0, (double)m} * ep;
-          cneg -= ds * sgn(m) * (drn * pr + dthn * pe_rz);
-        }
-        if (m == 0) {
-          acc0 += cm;
-        } else {
-          accp[r] += cm;
-          accm[r] += cneg;
-        }
-      }
-    }
-    __syncwarp();
+struct SrcTerm {  // per-source factors of the P2M / P2L coefficients
+  zdc q, ds, pr, pe_rz, izk;
+};
+
+__device__ __forceinline__ SrcTerm src_term(const HelmArgs& A, int j, zdc a1, zdc a2, zdc rzk) {
+  SrcTerm t;
+  t.q = A.ifcharge ? ldz(&A.charge[j]) : mkz(0.0);
+  t.ds = mkz(0.0);
+  t.pr = t.pe_rz = mkz(0.0);
+  if (A.ifdipole) {
+    t.ds = ldz(&A.dipstr[j]);
+    zdc d1 = ldz(&A.dipvec[2 * j]), d2 = ldz(&A.dipvec[2 * j + 1]);
+    zdc vr1 = a1 / rzk, vr2 = a2 / rzk;
+    t.pr = vr1 * d1 + vr2 * d2;
+    t.pe_rz = (-vr2 * d1 + vr1 * d2) / rzk;
+  }
+  t.izk = zinv(rzk * A.zk);
+  return t;
+}
+
+// coefficients +m and -m of one source from f = F_m, its derivative fder and
+// the powers em = ez^-m, ep = ez^m (zh2dformmp / zh2dformloc)
+__device__ __forceinline__ void src_coeffs(const HelmArgs& A, const SrcTerm& t, int m, zdc fm,
+                                           zdc fder, zdc em, zdc ep, zdc& cpos, zdc& cneg) {
+  cpos = fm * em * t.q;
+  cneg = sgn(m) * (fm * ep * t.q);
+  if (A.ifdipole) {
+    zdc dr = em * fder * A.zk, dth = fm * zdc{0.0, -(double)m} * em;
+    cpos -= t.ds * (dr * t.pr + dth * t.pe_rz);
+    zdc drn = ep * fder * A.zk, dthn = fm * zdc{0.0, (double)m} * ep;
+    cneg -= t.ds * sgn(m) * (drn * t.pr + dthn * t.pe_rz);
   }
 }
 
-constexpr int MAXR = 8;  // coefficient slots per lane: p <= 255
+// P2M column of source j about centre (c1, c2): Bessel functions by the
+// backward recurrence (coefficients emitted from m = p down to 0, scaled by
+// the normalisation at the end)
+__device__ void p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col) {
+  zdc a1 = ldz(&A.zsrc[2 * j]) - c1, a2 = ldz(&A.zsrc[2 * j + 1]) - c2;
+  zdc rzk, ez;
+  polar(a1, a2, rzk, ez);
+  SrcTerm t = src_term(A, j, a1, a2, rzk);
+  zdc z = rzk * A.zk;
+  const int P2 = 2 * p + 1;
+  if (zabs(z) < 1e-200) {  // jbessel2d's table for z = 0: J_0 = 1, the rest 0
+    for (int m = 0; m <= p; m++) {
+      zdc fm = m == 0 ? mkz(1.0) : mkz(0.0);
+      zdc fder = m == 1 ? mkz(0.5 / rs) : mkz(0.0);
+      zdc cp, cn;
+      src_coeffs(A, t, m, fm, fder, mkz(1.0), mkz(1.0), cp, cn);
+      col[p + m] = cp;
+      if (m) col[p - m] = cn;
+    }
+    return;
+  }
+  int ntop = jbessel_top(p, z);
+  zdc zr = rs * zinv(z);
+  double sc2 = rs * rs;
+  zdc zmul = z.im < 0.0 ? mkz(0.0, 1.0) : mkz(0.0, -1.0);
+  zdc iez = zinv(ez);
+  zdc ep = zpown(ez, p), em = zpown(iez, p);
+  zdc gp1 = mkz(0.0), g = mkz(1.0), psi = mkz(0.0), g0 = mkz(0.0);
+  for (int n = ntop - 1; n >= 0; n--) {
+    zdc gm1 = n >= 1 ? ((2.0 * n) * zr) * g - sc2 * gp1 : mkz(0.0);
+    if (n <= p) {
+      // F_{n-1}, F_n, F_{n+1} = gm1, g, gp1 (unnormalised); jbessel2d's
+      // derivative: (F_{n-1}/rs - rs F_{n+1})/2, and -rs F_1 at n = 0
+      zdc fder = n == 0 ? (-rs) * gp1 : (0.5 / rs) * gm1 - (0.5 * rs) * gp1;
+      zdc cp, cn;
+      src_coeffs(A, t, n, g, fder, em, ep, cp, cn);
+      col[p + n] = cp;
+      if (n) col[p - n] = cn;
+      ep = ep * iez;
+      em = em * ez;
+    }
+    if (n == 0) g0 = g;
+    if (n >= 1) {
+      int r = n & 3;
+      zdc zn = r == 0 ? mkz(1.0) : (r == 1 ? zmul : (r == 2 ? mkz(-1.0) : -zmul));
+      psi = rs * psi + zn * g;
+      gp1 = g;
+      g = gm1;
+      if (zabs(g) > 1e200) {
+        g = 1e-200 * g;
+        gp1 = 1e-200 * gp1;
+        psi = 1e-200 * psi;
+        for (int m = n; m <= p; m++) {
+          col[p + m] = 1e-200 * col[p + m];
+          if (m) col[p - m] = 1e-200 * col[p - m];
+        }
+      }
+    }
+  }
+  psi = 2.0 * rs * psi + g0;
+  zdc ex = z.im < 0.0 ? zexp_p(zmul_i(z)) : zexp_p(-zmul_i(z));
+  zdc sc = ex / psi;
+  for (int i = 0; i < P2; i++) col[i] = col[i] * sc;
+}
 
-__global__ void __launch_bounds__(32 * WPB, 4) k_hp2m(int lo, int hi, HelmArgs A, int pmax) {
+// P2L column of source j about centre (c1, c2): Hankel functions by the
+// forward recurrence (h2dall), coefficients emitted from m = 0 up to p
+__device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col) {
+  zdc a1 = ldz(&A.zsrc[2 * j]) - c1, a2 = ldz(&A.zsrc[2 * j + 1]) - c2;
+  zdc rzk, ez;
+  polar(a1, a2, rzk, ez);
+  SrcTerm t = src_term(A, j, a1, a2, rzk);
+  zdc z = rzk * A.zk;
+  if (zabs(z) < 1e-200) {  // h2dall's zero table
+    for (int i = 0; i <= 2 * p; i++) col[i] = mkz(0.0);
+    return;
+  }
+  zdc h0, h1;
+  hank01(z, h0, h1);
+  zdc zi = rs * zinv(z);
+  double sc2 = rs * rs;
+  zdc iez = zinv(ez), ep = mkz(1.0), em = mkz(1.0);
+  zdc fm1 = mkz(0.0), f = h0, fp1 = h1 * rs;  // F_{m-1}, F_m, F_{m+1}
+  for (int m = 0; m <= p; m++) {
+    zdc fder = m == 0 ? -fp1 / rs : rs * fm1 - ((double)m * t.izk) * f;
+    zdc cp, cn;
+    src_coeffs(A, t, m, f, fder, em, ep, cp, cn);
+    col[p + m] = cp;
+    if (m) col[p - m] = cn;
+    zdc fn = ((2.0 * (m + 1)) * zi) * fp1 - sc2 * f;
+    fm1 = f;
+    f = fp1;
+    fp1 = fn;
+    ep = ep * ez;
+    em = em * iez;
+  }
+}
+
+// P2M over the leaves of one level (lo..hi), R register slots per lane
+// (2p+1 <= 32 R)
+template <int R>
+__global__ void __launch_bounds__(32 * WPB) k_hp2m(int lo, int hi, HelmArgs A, int fch) {
   extern __shared__ zdc sh[];
-  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int b = lo + blockIdx.x * WPB + w;
   if (b > hi) return;
   int s0 = A.isrcse[2 * b], s1 = A.isrcse[2 * b + 1];
   if (A.nchild[b] > 0 || s1 < s0 || A.ilevel[b] < 2) return;
-  int l = A.ilevel[b], p = A.T.p[l];
-  zdc* tab = sh + (threadIdx.x >> 5) * FCH * (pmax + 2);
-  zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
+  int l = A.ilevel[b], p = A.T.p[l], P2 = 2 * p + 1;
+  double rs = A.T.rs[l];
+  zdc* cols = sh + (size_t)w * fch * P2;
+  zdc c1 = A.zcsrc[2 * b], c2 = A.zcsrc[2 * b + 1];
+  zdc acc[R];
 #pragma unroll
-  for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
-  form_expansion(A, s0, s1, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, false, tab, accp,
-                 accm, acc0);
-  zdc* M = expo(A, A.mp, b);
-  for (int m = lane, r = 0; m <= p; m += 32, r++) {
-    if (m == 0) M[0] = acc0;
-    else { M[m] = accp[r]; M[-m] = accm[r]; }
+  for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
+  for (int j0 = s0; j0 <= s1; j0 += fch) {
+    int nsrc = min(fch, s1 - j0 + 1);
+    if (lane < nsrc) p2m_column(A, j0 + lane, c1, c2, rs, p, cols + lane * P2);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int i = lane + 32 * r;
+      if (i < P2)
+        for (int k = 0; k < nsrc; k++) acc[r] += cols[k * P2 + i];
+    }
+    __syncwarp();
+  }
+  zdc* M = expo(A, A.mp, b) - p;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    int i = lane + 32 * r;
+    if (i < P2) M[i] = acc[r];
+  }
+}
+
+// P2L over list 4 of the target boxes of one level, added to their local
+// expansions: the sources of all list-4 boxes of a target box are taken fch at
+// a time in list order.
+template <int R>
+__global__ void __launch_bounds__(32 * WPB) k_hp2l(int lo, int hi, HelmArgs A, const int* nl4,
+                                                   const int* l4, int m4, int fch) {
+  extern __shared__ zdc sh[];
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int b = lo + blockIdx.x * WPB + w;
+  if (b > hi) return;
+  if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
+  int n4c = nl4[b];
+  if (n4c == 0) return;
+  int l = A.ilevel[b], p = A.T.p[l], P2 = 2 * p + 1;
+  double rs = A.T.rs[l];
+  zdc* cols = sh + (size_t)w * fch * P2;
+  zdc c1 = A.zctarg[2 * b], c2 = A.zctarg[2 * b + 1];
+  zdc acc[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
+  // walk the concatenated source ranges of the list-4 boxes; lane < fch takes
+  // the (lane)th source of each batch
+  int il = 0, off = 0;  // current list entry and the number of its sources already taken
+  while (il < n4c) {
+    // the batch: lane k finds its source by stepping through the list from (il, off)
+    int my = -1;
+    {
+      int jl = il, o = off, k = 0;
+      while (jl < n4c && k <= lane && lane < fch) {
+        int jb = l4[(size_t)b * m4 + jl];
+        int s0 = A.isrcse[2 * jb], cnt = A.isrcse[2 * jb + 1] - s0 + 1;
+        int take = max(cnt - o, 0);
+        if (lane - k < take) {
+          my = s0 + o + (lane - k);
+          break;
+        }
+        k += take;
+        jl++;
+        o = 0;
+      }
+    }
+    // advance the warp's position by fch sources
+    int taken = 0;
+    while (il < n4c && taken < fch) {
+      int jb = l4[(size_t)b * m4 + il];
+      int cnt = A.isrcse[2 * jb + 1] - A.isrcse[2 * jb] + 1;
+      int take = min(max(cnt - off, 0), fch - taken);
+      taken += take;
+      off += take;
+      if (off >= cnt) {
+        il++;
+        off = 0;
+      }
+    }
+    if (my >= 0) p2l_column(A, my, c1, c2, rs, p, cols + lane * P2);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int i = lane + 32 * r;
+      if (i < P2)
+        for (int k = 0; k < taken; k++) acc[r] += cols[k * P2 + i];
+    }
+    __syncwarp();
+  }
+  zdc* L = expo(A, A.loc, b) - p;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    int i = lane + 32 * r;
+    if (i < P2) L[i] += acc[r];
   }
 }
 
@@ -265,44 +502,44 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hp2m(int lo, int hi, HelmArgs A
 // is a Toeplitz product in k = m - n once w is split by the signs of m, n:
 // opposite signs (or n = 0): (rs1 rs2)^|n|; same sign, |n| <= |m|:
 // (rs2/rs1)^|n|; same sign, |n| > |m|: (rs2/rs1)^|m| (rs1 rs2)^|k|.
+// The symbol S1[k] = (-1)^k J_k e^{-ik theta} comes from the pair's table.
+template <int R>
 __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, HelmArgs A,
-                                                  int stride) {
+                                                   TabArgs TA, int stride) {
   extern __shared__ zdc sh[];
   int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b > hi) return;
   if (A.nchild[b] == 0 || A.isrcse[2 * b + 1] < A.isrcse[2 * b]) return;
   int n1 = A.T.p[lev], n2 = A.T.p[lev + 1], nt = n1 + n2;
   double rs1 = A.T.rs[lev], rs2 = A.T.rs[lev + 1];
-  zdc* fj = sh + (threadIdx.x >> 5) * stride;   // [nt+2]
-  zdc* S1 = fj + (nt + 2) + nt;                  // S1[k], k = -nt..nt
-  zdc* S2 = S1 + nt + 1 + nt;                    // S1[k] (rs1 rs2)^|k|
-  zdc* uu = S2 + nt + 1 + n2;                    // (rs2/rs1)^|n| mp_child(n), n = -n2..n2
-  zdc* ww = uu + n2 + 1 + n2;                    // (rs1 rs2)^|n| mp_child(n)
-  double* qa = (double*)(ww + n2 + 1);           // (rs1 rs2)^k, k = 0..nt
-  double* qb = qa + nt + 1;                      // (rs2/rs1)^k, k = 0..nt
-  zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
+  zdc* S1 = sh + (threadIdx.x >> 5) * stride + nt;  // S1[k], k = -nt..nt
+  zdc* S2 = S1 + nt + 1 + nt;                       // S1[k] (rs1 rs2)^|k|
+  zdc* uu = S2 + nt + 1 + n2;                       // (rs2/rs1)^|n| mp_child(n), n = -n2..n2
+  zdc* ww = uu + n2 + 1 + n2;                       // (rs1 rs2)^|n| mp_child(n)
+  double* qa = (double*)(ww + n2 + 1);              // (rs1 rs2)^k, k = 0..nt
+  double* qb = qa + nt + 1;                         // (rs2/rs1)^k, k = 0..nt
+  zdc accp[R], accm[R], acc0 = mkz(0.0);
 #pragma unroll
-  for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
+  for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
   for (int k = lane; k <= nt; k += 32) {
-    qa[k] = pow(rs1 * rs2, (double)k);
-    qb[k] = pow(rs2 / rs1, (double)k);
+    qa[k] = TA.pw[TA.pw_m2m[lev] + k];
+    qb[k] = TA.pw[TA.pw_m2m[lev] + nt + 1 + k];
   }
+  const int lc = lev + 1;
   for (int jc = 0; jc < 4; jc++) {
     int jb = A.ichild[4 * b + jc];
     if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-    zdc rz, e;
-    polar(A.zcsrc[2 * b] - A.zcsrc[2 * jb], A.zcsrc[2 * b + 1] - A.zcsrc[2 * jb + 1], rz, e);
+    const double4* t = TA.tab + TA.ml_base[lev] + (long)(jb - A.T.lo[lc]) * 2 * (nt + 2);
+    double4 nv = t[nt + 1];
+    zdc nrm = mkz(nv.x, nv.y);
     __syncwarp();
-    if (lane == 0) jbessel_stream(nt, rz * A.zk, rs1, fj);
-    __syncwarp();
-    zdc ie = zinv(e);
-    // S1[k] = (-1)^k t(k) e^{-ik theta}, t(k) = J_k (k >= 0), (-1)^k J_-k (k < 0)
     for (int k = lane; k <= nt; k += 32) {
-      zdc f = fj[k];
-      S1[k] = (sgn(k) * f) * zpown(ie, k);
-      S1[-k] = f * zpown(e, k);
-      S2[k] = S1[k] * qa[k];
-      S2[-k] = S1[-k] * qa[k];
+      double4 v = t[k];
+      zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
+      S1[k] = vv;   // (-1)^k J_k e^{-ik theta}
+      S1[-k] = u;   // J_k e^{ik theta}
+      S2[k] = vv * qa[k];
+      S2[-k] = u * qa[k];
     }
     const zdc* M2 = expo(A, A.mp, jb);
     for (int n = lane - n2; n <= n2; n += 32) {
@@ -312,7 +549,10 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
       ww[n] = qa[an] * v;
     }
     __syncwarp();
-    for (int m = lane, r = 0; m <= n1; m += 32, r++) {
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int m = lane + 32 * r;
+      if (m > n1) break;
       zdc a1 = mkz(0.0), a2 = mkz(0.0);
       for (int n = -n2; n <= n2; n++) {
         int k = m - n;
@@ -338,17 +578,24 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
     }
   }
   zdc* M = expo(A, A.mp, b);
-  for (int m = lane, r = 0; m <= n1; m += 32, r++) {
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    int m = lane + 32 * r;
+    if (m > n1) break;
     if (m == 0) M[0] = acc0;
-    else { M[m] = accp[r]; M[-m] = accm[r]; }
+    else {
+      M[m] = accp[r];
+      M[-m] = accm[r];
+    }
   }
 }
 
 // M2L (zh2dmploc) over list 2; R coefficient slots per lane (p < 32 R).  The
 // local expansion is written here; P2L (k_hp2l) adds to it afterwards.
 template <int R>
-__global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A, const int* nl2,
-                                                  const int* l2, int m2, int stride) {
+__global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A, TabArgs TA,
+                                                      const int* pairoff, const int* nl2,
+                                                      const int* l2, int m2, int stride) {
   extern __shared__ zdc sh[];
   int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b > hi) return;
@@ -357,34 +604,31 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
   if (n2c == 0) return;
   int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
   double rs = A.T.rs[l];
-  zdc* fh = sh + (threadIdx.x >> 5) * stride;  // [n2+2]
-  zdc* T = fh + (n2 + 2);                       // [2*n2+1]
-  double* rp = (double*)(T + 2 * n2 + 1);       // rs^k, k = 0..n2
-  zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;      // b(n), n = -p..p
-  zdc* cc = bb + 2 * p + 1;                     // c(n)
+  zdc* T = sh + (threadIdx.x >> 5) * stride;  // [2*n2+1]
+  double* rp = (double*)(T + 2 * n2 + 1);     // rs^k, k = 0..n2
+  zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;    // b(n), n = -p..p
+  zdc* cc = bb + 2 * p + 1;                   // c(n)
   zdc accp[R], accm[R], acc0 = mkz(0.0);
 #pragma unroll
   for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
-  for (int k = lane; k <= n2; k += 32) rp[k] = pow(rs, (double)k);
-  zdc c1 = A.zctarg[2 * b], c2 = A.zctarg[2 * b + 1];
+  for (int k = lane; k <= n2; k += 32) rp[k] = TA.pw[TA.pw_m2l[l] + k];
+  const double4* tl = TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
   for (int il = 0; il < n2c; il++) {
     int jb = l2[(size_t)b * m2 + il];
     if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-    zdc rz, e;
-    polar(c1 - A.zcsrc[2 * jb], c2 - A.zcsrc[2 * jb + 1], rz, e);
     __syncwarp();
-    h2dall_warp(n2, rz * A.zk, rs, fh);
-    zdc ie = zinv(e);
     // Toeplitz symbol T[k] = H_k e^{ik theta} (k = -2p..2p, H_-k = (-1)^k H_k,
-    // scaled) and the source coefficients without (b) and with (c) the factor
-    // rs^(2|n|): the reference's weight rs^|m| rs^|n| / rs^|n-m| is 1 for n, m
-    // of opposite signs and rs^(2 min(|m|,|n|)) otherwise, so
+    // scaled) from the pair's table, and the source coefficients without (b)
+    // and with (c) the factor rs^(2|n|): the reference's weight
+    // rs^|m| rs^|n| / rs^|n-m| is 1 for n, m of opposite signs and
+    // rs^(2 min(|m|,|n|)) otherwise, so
     //   loc(m) = sum_{n<0} T[n-m] b(n) + sum_{0<=n<=m} T[n-m] c(n)
     //          + rs^(2m) sum_{n>m} T[n-m] b(n)        (m >= 0, mirrored for m < 0)
+    const double4* t = tl + (long)il * (n2 + 1);
     for (int k = lane; k <= n2; k += 32) {
-      zdc f = fh[k];
-      T[n2 + k] = f * zpown(e, k);
-      T[n2 - k] = (sgn(k) * f) * zpown(ie, k);
+      double4 v = t[k];
+      T[n2 + k] = mkz(v.x, v.y);
+      T[n2 - k] = mkz(v.z, v.w);
     }
     const zdc* M = expo(A, A.mp, jb);
     for (int n = lane - p; n <= p; n += 32) {
@@ -420,7 +664,6 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
       accp[r] += sp;
       accm[r] += a1 + rp[2 * m] * a2;
     }
-    __syncwarp();
   }
   zdc* L = expo(A, A.loc, b);
 #pragma unroll
@@ -435,46 +678,16 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
   }
 }
 
-// P2L (zh2dformloc) over list 4, added to the local expansion
-__global__ void __launch_bounds__(32 * WPB, 4) k_hp2l(int lo, int hi, HelmArgs A, const int* nl4,
-                                                  const int* l4, int m4, int stride) {
-  extern __shared__ zdc sh[];
-  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b > hi) return;
-  if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
-  int n4c = nl4[b];
-  if (n4c == 0) return;
-  int l = A.ilevel[b], p = A.T.p[l];
-  double rs = A.T.rs[l];
-  zdc* tab = sh + (threadIdx.x >> 5) * stride;  // FCH*(p+2)
-  zdc accp[MAXR], accm[MAXR], acc0 = mkz(0.0);
-#pragma unroll
-  for (int r = 0; r < MAXR; r++) accp[r] = accm[r] = mkz(0.0);
-  zdc c1 = A.zctarg[2 * b], c2 = A.zctarg[2 * b + 1];
-  for (int il = 0; il < n4c; il++) {
-    int jb = l4[(size_t)b * m4 + il];
-    int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
-    if (s1 < s0) continue;
-    __syncwarp();
-    form_expansion(A, s0, s1, c1, c2, rs, p, true, tab, accp, accm, acc0);
-  }
-  zdc* L = expo(A, A.loc, b);
-  for (int m = lane, r = 0; m <= p; m += 32, r++) {
-    if (m == 0) L[0] += acc0;
-    else {
-      L[m] += accp[r];
-      L[-m] += accm[r];
-    }
-  }
-}
-
 // L2L (zh2dlocloc) into the children at level lev+1
 // L2L (zh2dlocloc): loc_child(m) += sum_n t(n-m) e^{i(n-m) theta} loc(n)
 //   rs1^|m| rs1^|n-m| / rs2^|n|   (rs1 child, rs2 parent scale, rs1 <= rs2)
 // split by signs: same sign with |n| >= |m|: (rs1/rs2)^|n|; same sign with
 // |n| < |m| (and n = 0): (rs1/rs2)^|n| rs1^(2|k|); opposite: (rs1/rs2)^|n| rs1^(2|m|).
+// The symbol S1[k] = J_k e^{ik theta} comes from the pair's table.
+template <int R>
 __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, HelmArgs A,
-                                                  const int* nl2, const int* nl4, int stride) {
+                                                   TabArgs TA, const int* nl2, const int* nl4,
+                                                   int stride) {
   extern __shared__ zdc sh[];
   int jb = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (jb > hi) return;
@@ -483,33 +696,36 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
   if (A.itargse[2 * jb + 1] < A.itargse[2 * jb]) return;
   int n1 = A.T.p[lev + 1], n2 = A.T.p[lev], nt = n1 + n2;
   double rs1 = A.T.rs[lev + 1], rs2 = A.T.rs[lev];
-  zdc* fj = sh + (threadIdx.x >> 5) * stride;   // [nt+2]
-  zdc* S1 = fj + (nt + 2) + nt;                  // S1[k] = t(k) e^{ik theta}, k = -nt..nt
-  zdc* S3 = S1 + nt + 1 + nt;                    // S1[k] rs1^(2|k|)
-  zdc* uu = S3 + nt + 1 + n2;                    // (rs1/rs2)^|n| loc_parent(n)
-  double* qa = (double*)(uu + n2 + 1);           // rs1^(2k), k = 0..nt
-  double* qb = qa + nt + 1;                      // (rs1/rs2)^k, k = 0..nt
+  zdc* S1 = sh + (threadIdx.x >> 5) * stride + nt;  // S1[k] = t(k) e^{ik theta}, k = -nt..nt
+  zdc* S3 = S1 + nt + 1 + nt;                       // S1[k] rs1^(2|k|)
+  zdc* uu = S3 + nt + 1 + n2;                       // (rs1/rs2)^|n| loc_parent(n)
+  double* qa = (double*)(uu + n2 + 1);              // rs1^(2k), k = 0..nt
+  double* qb = qa + nt + 1;                         // (rs1/rs2)^k, k = 0..nt
   for (int k = lane; k <= nt; k += 32) {
-    qa[k] = pow(rs1, 2.0 * k);
-    qb[k] = pow(rs1 / rs2, (double)k);
+    qa[k] = TA.pw[TA.pw_l2l[lev] + k];
+    qb[k] = TA.pw[TA.pw_l2l[lev] + nt + 1 + k];
   }
-  zdc rz, e;
-  polar(A.zctarg[2 * jb] - A.zctarg[2 * b], A.zctarg[2 * jb + 1] - A.zctarg[2 * b + 1], rz, e);
-  if (lane == 0) jbessel_stream(nt, rz * A.zk, rs1, fj);
+  const double4* t =
+      TA.tab + TA.ml_base[lev] + (long)(jb - A.T.lo[lev + 1]) * 2 * (nt + 2) + (nt + 2);
+  double4 nv = t[nt + 1];
+  zdc nrm = mkz(nv.x, nv.y);
   __syncwarp();
-  zdc ie = zinv(e);
   for (int k = lane; k <= nt; k += 32) {
-    zdc f = fj[k];
-    S1[k] = f * zpown(e, k);
-    S1[-k] = (sgn(k) * f) * zpown(ie, k);
-    S3[k] = S1[k] * qa[k];
-    S3[-k] = S1[-k] * qa[k];
+    double4 v = t[k];
+    zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
+    S1[k] = u;    // J_k e^{ik theta}
+    S1[-k] = vv;  // (-1)^k J_k e^{-ik theta}
+    S3[k] = u * qa[k];
+    S3[-k] = vv * qa[k];
   }
   const zdc* L2 = expo(A, A.loc, b);
   for (int n = lane - n2; n <= n2; n += 32) uu[n] = qb[abs(n)] * L2[n];
   __syncwarp();
   zdc* L1 = expo(A, A.loc, jb);
-  for (int m = lane; m <= n1; m += 32) {
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    int m = lane + 32 * r;
+    if (m > n1) break;
     zdc a1 = mkz(0.0), a2 = mkz(0.0);
     for (int n = -n2; n <= n2; n++) {
       int k = n - m;
@@ -666,6 +882,7 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_heval(int nb, HelmArgs A, const
   while (pw < ntb && pw < 32) pw <<= 1;
   int G = 32 / pw, T = 32 / G, tl = lane / G, r = lane % G;
   int n1 = nl1[b];
+  const HelmK K = helm_k(A.zk);
   for (int base = 0; base < ntb; base += T) {
     int ti = t0 + base + tl;
     bool valid = base + tl < ntb;
@@ -683,7 +900,7 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_heval(int nb, HelmArgs A, const
             d1 = ldz(&A.dipvec[2 * j]);
             d2 = ldz(&A.dipvec[2 * j + 1]);
           }
-          helm_pair<GRAD>(A.zk, x1, x2, ldz(&A.zsrc[2 * j]), ldz(&A.zsrc[2 * j + 1]), q, ds, d1, d2,
+          helm_pair<GRAD>(K, x1, x2, ldz(&A.zsrc[2 * j]), ldz(&A.zsrc[2 * j + 1]), q, ds, d1, d2,
                           A.ifcharge, A.ifdipole, pot, g1, g2);
         }
       }
@@ -769,16 +986,38 @@ int h2dterms_host(double bsize, zdc zk, double eps, int isep) {
 // q, ds, dv on a set-up S: writes the sorted, unscaled potentials / gradients
 // into potsort / gradsort (zeroed by the caller); ev (optional) gets the step
 // boundaries 2..5; *pl (optional) receives the order of every level
-int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, const zdc* ds, const zdc* dv, int ifcharge, int ifdipole, int ifpgh,
-         zdc* potsort, zdc* gradsort, cudaStream_t s, cudaEvent_t* ev,
-         std::vector<int>* pl) {
-  auto cmark = [&](int i) {
-    if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
-  };
+// Orders, scales and translation tables of the 2D Helmholtz passes for one
+// tree and wavenumber (independent of the strengths: built once per solve,
+// or once per plan solve for all its right-hand sides).
+struct Helm2DPrep {
+  HelmArgs A0;  // level table and geometry pointers (strength pointers unset)
+  TabArgs TA;
+  DevBuf<int> pairoff;
+  DevBuf<double4> tab;
+  DevBuf<double> pw;
+  long tot = 0;
+  int pmax = 0;
+};
+
+void Helm2DPrepDeleter::operator()(Helm2DPrep* p) const { delete p; }
+
+namespace {
+__global__ void k_pairoff_at(const int* pairoff, const int* idx, int n, int* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = pairoff[idx[i]];
+}
+
+__global__ void k_last_plus(const int* off, const int* cnt, int nb, int* out) {
+  *out = off[nb - 1] + cnt[nb - 1];
+}
+}  // namespace
+
+Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cudaStream_t s) {
   const DevTree& t = S.tree;
   int nb = t.nboxes, nlev = t.nlevels;
   if (nlev + 1 > MAXL) throw zf_error(ZF_ERR_ARG, "too many tree levels");
-  HelmArgs A;
+  Helm2DPrepPtr H(new Helm2DPrep());
+  HelmArgs& A = H->A0;
   A.zk = zk;
   long tot = 0;
   int pmax = 0;
@@ -796,82 +1035,221 @@ int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, co
     tot += (long)(t.laddr[2 * l + 1] - t.laddr[2 * l] + 1) * (2 * A.T.p[l] + 1);
     if (A.T.p[l] > pmax) pmax = A.T.p[l];
   }
-  DevBuf<zdc> mp(tot, s), loc(tot, s);
-  mp.zero();
-  loc.zero();
+  H->tot = tot;
+  H->pmax = pmax;
   A.ilevel = t.ilevel.get(); A.iparent = t.iparent.get(); A.nchild = t.nchild.get();
   A.ichild = t.ichild.get(); A.isrcse = S.isrcse.get(); A.itargse = S.itargse.get();
-  A.zsrc = S.zsrcsort.get(); A.charge = q; A.dipstr = ds;
-  A.dipvec = dv; A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
-  A.zctarg = S.zctarg.get(); A.mp = mp.get(); A.loc = loc.get();
-  A.ifcharge = ifcharge; A.ifdipole = ifdipole;
+  A.zsrc = S.zsrcsort.get(); A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
+  A.zctarg = S.zctarg.get();
+  const DevLists& L = S.lists;
+  // list-2 pair offsets of every box, and the first pair of every level
+  H->pairoff.alloc(nb + 1, s);
+  {
+    size_t bytes = 0;
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, L.n[1].get(), H->pairoff.get(), nb, s));
+    DevBuf<char> tmp(bytes, s);
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, L.n[1].get(), H->pairoff.get(), nb,
+                                          s));
+    klaunch(k_last_plus, 1, 1, 0, s, H->pairoff.get(), L.n[1].get(), nb, H->pairoff.get() + nb);
+  }
+  std::vector<int> idx(nlev + 2);
+  for (int l = 0; l <= nlev; l++) idx[l] = t.laddr[2 * l];
+  idx[nlev + 1] = nb;
+  DevBuf<int> didx(nlev + 2, s), dout(nlev + 2, s);
+  ZF_CUDA(cudaMemcpyAsync(didx.get(), idx.data(), idx.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, s));
+  klaunch(k_pairoff_at, 1, 64, 0, s, H->pairoff.get(), didx.get(), nlev + 2, dout.get());
+  std::vector<int> p0(nlev + 2);
+  ZF_CUDA(cudaMemcpyAsync(p0.data(), dout.get(), p0.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                          s));
+  ZF_CUDA(cudaStreamSynchronize(s));
+  // table layout: M2L tables of levels 2..nlev, then the M2M / L2L tables of
+  // the children of levels 2..nlev-1
+  TabArgs& TA = H->TA;
+  long ntab = 0;
+  for (int l = 0; l <= nlev; l++) {
+    TA.m2l_pair0[l] = p0[l];
+    TA.m2l_base[l] = ntab;
+    if (l >= 2) ntab += (long)(p0[l + 1] - p0[l]) * (2 * A.T.p[l] + 1);
+  }
+  for (int l = 0; l <= nlev; l++) {
+    TA.ml_base[l] = ntab;
+    if (l >= 2 && l < nlev) {
+      int nch = t.laddr[2 * (l + 1) + 1] - t.laddr[2 * (l + 1)] + 1;
+      ntab += (long)nch * 2 * (A.T.p[l] + A.T.p[l + 1] + 2);
+    }
+  }
+  H->tab.alloc(ntab > 0 ? ntab : 1, s);
+  TA.tab = H->tab.get();
+  // real power tables of the translation weights, one block per level
+  std::vector<double> pw;
+  for (int l = 0; l <= nlev; l++) {
+    TA.pw_m2l[l] = (long)pw.size();
+    if (l >= 2)
+      for (int k = 0; k <= 2 * A.T.p[l]; k++) pw.push_back(std::pow(A.T.rs[l], (double)k));
+    TA.pw_m2m[l] = TA.pw_l2l[l] = (long)pw.size();
+    if (l >= 2 && l < nlev) {
+      int nt = A.T.p[l] + A.T.p[l + 1];
+      double rp = A.T.rs[l], rc = A.T.rs[l + 1];  // parent, child scales
+      for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rp * rc, (double)k));
+      for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rc / rp, (double)k));
+      TA.pw_l2l[l] = (long)pw.size();
+      for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rc, 2.0 * k));
+      for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rc / rp, (double)k));
+    }
+  }
+  H->pw.alloc(pw.size() > 0 ? pw.size() : 1, s);
+  if (!pw.empty())
+    ZF_CUDA(cudaMemcpyAsync(H->pw.get(), pw.data(), pw.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, s));
+  TA.pw = H->pw.get();
+  if (nlev >= 2) {
+    long q0 = p0[2], q1 = p0[nlev + 1];
+    if (q1 > q0)
+      klaunch(k_tab_m2l, div_up(q1 - q0, 128), 128, 0, s, q0, q1, t.laddr[4], nb - 1, A, TA,
+              H->pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1]);
+  }
+  if (nlev >= 3) {
+    int c0 = t.laddr[6], c1 = nb - 1;
+    klaunch(k_tab_m2m_l2l, div_up(c1 - c0 + 1, 128), 128, 0, s, c0, c1, A, TA, L.n[1].get(),
+            L.n[3].get());
+  }
+  ZF_LAUNCH_CHECK();
+  return H;
+}
+
+// the passes after the set-up for one right-hand side with sorted strengths
+// q, ds, dv on a set-up S and its prepared tables H: writes the sorted,
+// unscaled potentials / gradients into potsort / gradsort (zeroed by the
+// caller); ev (optional) gets the step boundaries 2..5; *pl (optional)
+// receives the order of every level
+int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc* ds,
+                  const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* potsort,
+                  zdc* gradsort, cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl) {
+  auto cmark = [&](int i) {
+    if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
+  };
+  const DevTree& t = S.tree;
+  int nb = t.nboxes, nlev = t.nlevels;
+  HelmArgs A = H.A0;
+  const TabArgs& TA = H.TA;
+  DevBuf<zdc> mp(H.tot, s), loc(H.tot, s);
+  mp.zero();
+  loc.zero();
+  A.charge = q;
+  A.dipstr = ds;
+  A.dipvec = dv;
+  A.mp = mp.get();
+  A.loc = loc.get();
+  A.ifcharge = ifcharge;
+  A.ifdipole = ifdipole;
   const DevLists& L = S.lists;
   int grid_all = div_up(nb, WPB);
-  // shared-memory strides (complex elements per warp)
-  auto dense_stride = [](int ntt) { return (ntt + 2) + (2 * ntt + 1) + (ntt + 1 + 1); };
-  // M2M / L2L: J table, two Toeplitz symbols, two weighted input vectors and
-  // two real power tables
+  // shared memory per warp (complex elements) of the M2M / L2L products: two
+  // Toeplitz symbols of 2 nt + 1, two weighted input vectors and two real
+  // power tables
   auto trans_stride = [](int ntt, int nin) {
-    return (ntt + 2) + 2 * (2 * ntt + 1) + 2 * (2 * nin + 1) + (ntt + 1);
+    return 2 * (2 * ntt + 1) + 2 * (2 * nin + 1) + (ntt + 1);
   };
-  // P2M per level (leaves of levels >= 2), shared memory sized by the level's order
+  auto slots = [](int ncoef) { return (ncoef + 31) / 32; };  // register slots per lane
+  // a templated launch choosing R from {1, 2, 4, 8, 16} >= need
+  auto pickR = [](int need) { return need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : need <= 8 ? 8 : 16; };
+  // sources per batch of the P2M / P2L kernels: FCH, fewer when the columns of
+  // order p would exceed the shared memory of a block
+  auto form_fch = [](int P2) {
+    int f = (int)((227 * 1024) / ((size_t)WPB * P2 * sizeof(zdc)));
+    return f < 1 ? 1 : (f > FCH ? FCH : f);
+  };
+  // P2M per level (leaves of levels >= 2)
   for (int l = 2; l <= nlev; l++) {
-    int pl = A.T.p[l];
-    size_t sm_p2m = (size_t)WPB * FCH * (pl + 2) * sizeof(zdc);
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
-    ZF_CUDA(cudaFuncSetAttribute(k_hp2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
-    klaunch(k_hp2m, div_up(hi - lo + 1, WPB), 32 * WPB, sm_p2m, s, lo, hi, A, pl);
+    int pl_ = A.T.p[l], P2 = 2 * pl_ + 1, fch = form_fch(P2);
+    size_t sm = (size_t)WPB * fch * P2 * sizeof(zdc);
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+    auto go = [&](auto kern) {
+      ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, fch);
+    };
+    switch (pickR(slots(P2))) {
+      case 1: go(k_hp2m<1>); break;
+      case 2: go(k_hp2m<2>); break;
+      case 4: go(k_hp2m<4>); break;
+      case 8: go(k_hp2m<8>); break;
+      default: go(k_hp2m<16>); break;
+    }
   }
   ZF_LAUNCH_CHECK();
   cmark(2);
   for (int l = nlev - 1; l >= 2; l--) {
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
     int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l + 1]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
-    ZF_CUDA(cudaFuncSetAttribute(k_hm2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    klaunch(k_hm2m, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, l, A, stride);
+    auto go = [&](auto kern) {
+      ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, l, A, TA, stride);
+    };
+    switch (pickR(slots(A.T.p[l] + 1))) {
+      case 1: go(k_hm2m<1>); break;
+      case 2: go(k_hm2m<2>); break;
+      case 4: go(k_hm2m<4>); break;
+      default: go(k_hm2m<MAXR>); break;
+    }
   }
   ZF_LAUNCH_CHECK();
   cmark(3);
   // one launch per level (lists 2 and 4 are empty on levels 0 and 1): the
-  // shared-memory stride and the register slots follow the level's order, so
-  // the many fine-level boxes run at full occupancy
+  // shared-memory stride and the register slots follow the level's order
   for (int l = 2; l <= nlev; l++) {
-    int pl = A.T.p[l];
-    int stride = dense_stride(2 * pl) + 2 * (2 * pl + 1);
+    int pl_ = A.T.p[l], n2 = 2 * pl_;
+    int stride = (2 * n2 + 1) + (n2 + 2) + 2 * (2 * pl_ + 1);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
     auto go = [&](auto kern) {
       ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, L.n[1].get(), L.list[1].get(), L.mn[1],
-              stride);
+      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, TA, H.pairoff.get(), L.n[1].get(),
+              L.list[1].get(), L.mn[1], stride);
     };
-    int R = (pl + 32) / 32;
-    if (R <= 1) go(k_hm2l<1>);
-    else if (R <= 2) go(k_hm2l<2>);
-    else if (R <= 4) go(k_hm2l<4>);
-    else go(k_hm2l<MAXR>);
+    switch (pickR(slots(pl_ + 1))) {
+      case 1: go(k_hm2l<1>); break;
+      case 2: go(k_hm2l<2>); break;
+      case 4: go(k_hm2l<4>); break;
+      default: go(k_hm2l<MAXR>); break;
+    }
   }
   ZF_LAUNCH_CHECK();
   if (L.mn[3] > 0)
     for (int l = 2; l <= nlev; l++) {
-      int pl = A.T.p[l];
-      int stride = FCH * (pl + 2);
-      size_t sm = (size_t)WPB * stride * sizeof(zdc);
-      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
-      ZF_CUDA(cudaFuncSetAttribute(k_hp2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      klaunch(k_hp2l, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, A, L.n[3].get(),
-              L.list[3].get(), L.mn[3], stride);
+      int pl_ = A.T.p[l], P2 = 2 * pl_ + 1, fch = form_fch(P2);
+      size_t sm = (size_t)WPB * fch * P2 * sizeof(zdc);
+      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+      auto go = [&](auto kern) {
+        ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, L.n[3].get(), L.list[3].get(), L.mn[3],
+                fch);
+      };
+      switch (pickR(slots(P2))) {
+        case 1: go(k_hp2l<1>); break;
+        case 2: go(k_hp2l<2>); break;
+        case 4: go(k_hp2l<4>); break;
+        case 8: go(k_hp2l<8>); break;
+        default: go(k_hp2l<16>); break;
+      }
     }
   ZF_LAUNCH_CHECK();
   cmark(4);
   for (int l = 2; l <= nlev - 1; l++) {
-    int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
+    int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1], grid = div_up(hi - lo + 1, WPB);
     int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
-    ZF_CUDA(cudaFuncSetAttribute(k_hl2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    klaunch(k_hl2l, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, l, A, L.n[1].get(),
-            L.n[3].get(), stride);
+    auto go = [&](auto kern) {
+      ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, l, A, TA, L.n[1].get(), L.n[3].get(), stride);
+    };
+    switch (pickR(slots(A.T.p[l + 1] + 1))) {
+      case 1: go(k_hl2l<1>); break;
+      case 2: go(k_hl2l<2>); break;
+      case 4: go(k_hl2l<4>); break;
+      default: go(k_hl2l<MAXR>); break;
+    }
   }
   ZF_LAUNCH_CHECK();
   cmark(5);
@@ -883,7 +1261,14 @@ int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, co
             L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort, gradsort);
   ZF_LAUNCH_CHECK();
   if (pl) *pl = std::vector<int>(A.T.p, A.T.p + nlev + 1);
-  return pmax;
+  return H.pmax;
+}
+
+int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, const zdc* ds,
+                const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* potsort,
+                zdc* gradsort, cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl) {
+  Helm2DPrepPtr H = helm2d_prepare(S, eps, zk, isep, s);
+  return helm2d_passes(S, *H, q, ds, dv, ifcharge, ifdipole, ifpgh, potsort, gradsort, s, ev, pl);
 }
 
 void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, zdc* grad,
@@ -904,14 +1289,17 @@ void zhfmm2d_device(double eps, zdc zk, const Inputs2D& in, int isep, zdc* pot, 
   lndiv2d(eps, ns, nt, &tp.ndiv, &tp.idivflag);  // hndiv2d.f: same table
   Setup2D S;
   setup2d(in, tp, S, s);
+  // the translation tables belong to the set-up: they depend on the tree and
+  // zk only
+  Helm2DPrepPtr H = helm2d_prepare(S, eps, zk, isep, s);
   mark(1);
   std::vector<int> plv;
   DevBuf<zdc> potsort(nt, s), gradsort(in.ifpgh > 1 ? 2 * (size_t)nt : 1, s);
   potsort.zero();
   gradsort.zero();
-  const int pord = helm2d_core(S, eps, zk, isep, S.chargesort.get(), S.dipstrsort.get(),
-      S.dipvecsort.get(), in.ifcharge, in.ifdipole, in.ifpgh, potsort.get(), gradsort.get(), s,
-      timing ? ev : nullptr, &plv);
+  const int pord = helm2d_passes(S, *H, S.chargesort.get(), S.dipstrsort.get(),
+                                 S.dipvecsort.get(), in.ifcharge, in.ifdipole, in.ifpgh,
+                                 potsort.get(), gradsort.get(), s, timing ? ev : nullptr, &plv);
   mark(6);
   unsort2d(nt, S.itarg.get(), potsort.get(), gradsort.get(), mkz(0.0, 0.25), in.ifpgh, pot, grad,
            s);

@@ -43,6 +43,10 @@ void fmm2d_plan_execute(const Plan2D& P, const zdc* zk, int nd, int ifcharge, co
   const zdc scale = zk ? mkz(0.0, 0.25) : mkz(1.0 / (2.0 * M_PI));
   std::vector<int> pl;
   int pord = 0;
+  // the Helmholtz orders and translation tables depend on the tree and zk
+  // only: built once for all right-hand sides
+  Helm2DPrepPtr H;
+  if (zk) H = helm2d_prepare(S, P.eps, *zk, P.isep, s);
   for (int r = 0; r < nd; r++) {
     mark(0);
     gather2d_col(S, ns, nd, r, ifcharge ? charge : nullptr, ifdipole ? dipstr : nullptr,
@@ -51,8 +55,8 @@ void fmm2d_plan_execute(const Plan2D& P, const zdc* zk, int nd, int ifcharge, co
     gradsort.zero();
     mark(1);
     if (zk)
-      pord = helm2d_core(S, P.eps, *zk, P.isep, q.get(), ds.get(), dv.get(), ifcharge, ifdipole,
-                         ifpgh, potsort.get(), gradsort.get(), s, timing ? ev : nullptr, &pl);
+      pord = helm2d_passes(S, *H, q.get(), ds.get(), dv.get(), ifcharge, ifdipole, ifpgh,
+                           potsort.get(), gradsort.get(), s, timing ? ev : nullptr, &pl);
     else
       pord = lap2d_core(S, P.eps, q.get(), ds.get(), dv.get(), ifcharge, ifdipole, ifpgh,
                         potsort.get(), gradsort.get(), s, timing ? ev : nullptr, &pl);
