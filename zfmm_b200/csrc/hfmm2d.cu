@@ -244,14 +244,12 @@ __global__ void __launch_bounds__(128) k_tab_m2m_l2l(int c0, int c1, HelmArgs A,
 }
 
 // ---- step 1 / 6: P2M (zh2dformmp) and P2L (zh2dformloc) ------------------------
-// One warp per expansion centre.  Sources are taken fch at a time: lane k < fch
-// computes the whole coefficient vector of one source (its Bessel or Hankel
-// functions by the same recurrences as above, the powers ez^(+-m) as running
-// products) into a shared column; then every lane sums its coefficients over
-// the fch columns in registers.  Coefficient i of the register slots is
-// m = i - p (i = lane + 32 r).  fch = FCH unless the columns of a high order
-// would not fit in shared memory.
-constexpr int FCH = 16;
+// One thread per (centre, source) computes the whole coefficient vector of the
+// source about the centre (its Bessel or Hankel functions by the same
+// recurrences as above, the powers ez^(+-m) as running products) into a
+// column of global scratch; then one warp per centre sums its columns, lane i
+// holding coefficients m = i - p (i = lane + 32 r).  Every lane of the column
+// pass does work, whatever the number of sources per box.
 
 struct SrcTerm {  // per-source factors of the P2M / P2L coefficients
   zdc q, ds, pr, pe_rz, izk;
@@ -385,112 +383,126 @@ __device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
   }
 }
 
-// P2M over the leaves of one level (lo..hi), R register slots per lane
-// (2p+1 <= 32 R)
-template <int R>
-__global__ void __launch_bounds__(32 * WPB) k_hp2m(int lo, int hi, HelmArgs A, int fch) {
-  extern __shared__ zdc sh[];
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int b = lo + blockIdx.x * WPB + w;
-  if (b > hi) return;
+// The columns of a pass live in global scratch: colbase[b] is the first
+// column entry of box b (P2M: the box's own sources; P2L: the sources of its
+// list-4 boxes in list order), (2p+1) entries per source.
+
+// leaf box of every source of a leaf of level >= 2 (-1 otherwise): the P2M
+// centres, one thread per box
+__global__ void k_src_leaf(int nb, HelmArgs A, int* srcleaf) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
   int s0 = A.isrcse[2 * b], s1 = A.isrcse[2 * b + 1];
-  if (A.nchild[b] > 0 || s1 < s0 || A.ilevel[b] < 2) return;
-  int l = A.ilevel[b], p = A.T.p[l], P2 = 2 * p + 1;
-  double rs = A.T.rs[l];
-  zdc* cols = sh + (size_t)w * fch * P2;
-  zdc c1 = A.zcsrc[2 * b], c2 = A.zcsrc[2 * b + 1];
-  zdc acc[R];
-#pragma unroll
-  for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
-  for (int j0 = s0; j0 <= s1; j0 += fch) {
-    int nsrc = min(fch, s1 - j0 + 1);
-    if (lane < nsrc) p2m_column(A, j0 + lane, c1, c2, rs, p, cols + lane * P2);
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      int i = lane + 32 * r;
-      if (i < P2)
-        for (int k = 0; k < nsrc; k++) acc[r] += cols[k * P2 + i];
-    }
-    __syncwarp();
-  }
-  zdc* M = expo(A, A.mp, b) - p;
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    int i = lane + 32 * r;
-    if (i < P2) M[i] = acc[r];
-  }
+  if (A.nchild[b] > 0 || s1 < s0) return;
+  int v = A.ilevel[b] >= 2 ? b : -1;
+  for (int j = s0; j <= s1; j++) srcleaf[j] = v;
 }
 
-// P2L over list 4 of the target boxes of one level, added to their local
-// expansions: the sources of all list-4 boxes of a target box are taken fch at
-// a time in list order.
-template <int R>
-__global__ void __launch_bounds__(32 * WPB) k_hp2l(int lo, int hi, HelmArgs A, const int* nl4,
-                                                   const int* l4, int m4, int fch) {
-  extern __shared__ zdc sh[];
+// per-box column counts: P2M sources of leaves of level >= 2 (w1 = sources,
+// w2 = sources x (2p+1)); P2L sources of the list-4 boxes of target boxes
+// (w3 = sources, w4 = sources x (2p+1))
+__global__ void k_form_counts(int nb, HelmArgs A, const int* nl4, const int* l4, int m4,
+                              long long* w1, long long* w2, long long* w3, long long* w4) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int l = A.ilevel[b], P2 = 2 * A.T.p[l] + 1;
+  long long c = 0;
+  int s0 = A.isrcse[2 * b], s1 = A.isrcse[2 * b + 1];
+  if (A.nchild[b] == 0 && s1 >= s0 && l >= 2) c = s1 - s0 + 1;
+  w1[b] = c;
+  w2[b] = c * P2;
+  long long c4 = 0;
+  if (A.itargse[2 * b + 1] >= A.itargse[2 * b] && l >= 2)
+    for (int il = 0; il < nl4[b]; il++) {
+      int jb = l4[(size_t)b * m4 + il];
+      int n = A.isrcse[2 * jb + 1] - A.isrcse[2 * jb] + 1;
+      if (n > 0) c4 += n;
+    }
+  w3[b] = c4;
+  w4[b] = c4 * P2;
+}
+
+// P2M columns, one thread per source
+__global__ void __launch_bounds__(128) k_p2m_cols(int ns, HelmArgs A, const int* srcleaf,
+                                                  const long long* colbase, zdc* cols) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  int b = srcleaf[j];
+  if (b < 0) return;
+  int l = A.ilevel[b], p = A.T.p[l];
+  zdc* col = cols + colbase[b] + (long long)(j - A.isrcse[2 * b]) * (2 * p + 1);
+  p2m_column(A, j, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, col);
+}
+
+// box of flattened index q: the last box in [lo, hi] with off[box] <= q
+__device__ __forceinline__ int search_box(const long long* off, int lo, int hi, long long q) {
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= q) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// P2L columns, one thread per (target box, list-4 source) in list order
+__global__ void __launch_bounds__(128) k_p2l_cols(long long nq, int b0, int b1, HelmArgs A,
+                                                  const long long* off4, const int* nl4,
+                                                  const int* l4, int m4,
+                                                  const long long* colbase, zdc* cols) {
+  long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  int b = search_box(off4, b0, b1, q);
+  long long r = q - off4[b];
+  int j = -1;
+  for (int il = 0; il < nl4[b]; il++) {
+    int jb = l4[(size_t)b * m4 + il];
+    int s0 = A.isrcse[2 * jb], n = A.isrcse[2 * jb + 1] - s0 + 1;
+    if (n <= 0) continue;
+    if (r < n) {
+      j = s0 + (int)r;
+      break;
+    }
+    r -= n;
+  }
+  if (j < 0) return;
+  int l = A.ilevel[b], p = A.T.p[l];
+  zdc* col = cols + colbase[b] + (q - off4[b]) * (2 * p + 1);
+  p2l_column(A, j, A.zctarg[2 * b], A.zctarg[2 * b + 1], A.T.rs[l], p, col);
+}
+
+// sums of the columns of every box of one level: one warp per box, R register
+// slots per lane (2p+1 <= 32 R); P2M writes the multipole expansion, P2L adds
+// to the local expansion
+template <int R, bool LOCAL>
+__global__ void __launch_bounds__(32 * WPB) k_form_sum(int lo, int hi, HelmArgs A,
+                                                       const long long* cnt,
+                                                       const long long* colbase,
+                                                       const zdc* cols) {
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int b = lo + blockIdx.x * WPB + w;
   if (b > hi) return;
-  if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
-  int n4c = nl4[b];
-  if (n4c == 0) return;
+  long long n = cnt[b];
+  if (n == 0) return;
   int l = A.ilevel[b], p = A.T.p[l], P2 = 2 * p + 1;
-  double rs = A.T.rs[l];
-  zdc* cols = sh + (size_t)w * fch * P2;
-  zdc c1 = A.zctarg[2 * b], c2 = A.zctarg[2 * b + 1];
+  const zdc* c = cols + colbase[b];
   zdc acc[R];
 #pragma unroll
   for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
-  // walk the concatenated source ranges of the list-4 boxes; lane < fch takes
-  // the (lane)th source of each batch
-  int il = 0, off = 0;  // current list entry and the number of its sources already taken
-  while (il < n4c) {
-    // the batch: lane k finds its source by stepping through the list from (il, off)
-    int my = -1;
-    {
-      int jl = il, o = off, k = 0;
-      while (jl < n4c && k <= lane && lane < fch) {
-        int jb = l4[(size_t)b * m4 + jl];
-        int s0 = A.isrcse[2 * jb], cnt = A.isrcse[2 * jb + 1] - s0 + 1;
-        int take = max(cnt - o, 0);
-        if (lane - k < take) {
-          my = s0 + o + (lane - k);
-          break;
-        }
-        k += take;
-        jl++;
-        o = 0;
-      }
-    }
-    // advance the warp's position by fch sources
-    int taken = 0;
-    while (il < n4c && taken < fch) {
-      int jb = l4[(size_t)b * m4 + il];
-      int cnt = A.isrcse[2 * jb + 1] - A.isrcse[2 * jb] + 1;
-      int take = min(max(cnt - off, 0), fch - taken);
-      taken += take;
-      off += take;
-      if (off >= cnt) {
-        il++;
-        off = 0;
-      }
-    }
-    if (my >= 0) p2l_column(A, my, c1, c2, rs, p, cols + lane * P2);
-    __syncwarp();
+  for (long long k = 0; k < n; k++) {
 #pragma unroll
     for (int r = 0; r < R; r++) {
       int i = lane + 32 * r;
-      if (i < P2)
-        for (int k = 0; k < taken; k++) acc[r] += cols[k * P2 + i];
+      if (i < P2) acc[r] += ldz(&c[k * P2 + i]);
     }
-    __syncwarp();
   }
-  zdc* L = expo(A, A.loc, b) - p;
+  zdc* E = expo(A, LOCAL ? A.loc : A.mp, b) - p;
 #pragma unroll
   for (int r = 0; r < R; r++) {
     int i = lane + 32 * r;
-    if (i < P2) L[i] += acc[r];
+    if (i < P2) {
+      if (LOCAL) E[i] += acc[r];
+      else E[i] = acc[r];
+    }
   }
 }
 
@@ -503,6 +515,14 @@ __global__ void __launch_bounds__(32 * WPB) k_hp2l(int lo, int hi, HelmArgs A, c
 // opposite signs (or n = 0): (rs1 rs2)^|n|; same sign, |n| <= |m|:
 // (rs2/rs1)^|n|; same sign, |n| > |m|: (rs2/rs1)^|m| (rs1 rs2)^|k|.
 // The symbol S1[k] = (-1)^k J_k e^{-ik theta} comes from the pair's table.
+// With g(d) = (rs1 rs2)^d for d > 0 and (rs1/rs2)^-d for d <= 0, the weight
+// of every term with n of the sign of m (n != 0) is (rs2/rs1)^|m| g(|n|-|m|),
+// and (rs1 rs2)^|n| for the others, so with the symbols S3[j] = S1[j] g(-j)
+// and S4[k] = S1[k] g(k) the translation is branch-free:
+//   mp(m)  = sum_{n<=0} S1[m-n] w(n) + (rs2/rs1)^m sum_{n>0} S3[m-n] mp_c(n)
+//   mp(-m) = sum_{n>=0} S1[-m-n] w(n) + (rs2/rs1)^m sum_{n<0} S4[-m-n] mp_c(n)
+// (w(n) = (rs1 rs2)^|n| mp_c(n)); rs1/rs2 is at most the box-size ratio, so
+// the factors stay within the double range.
 template <int R>
 __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, HelmArgs A,
                                                    TabArgs TA, int stride) {
@@ -511,20 +531,17 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
   if (b > hi) return;
   if (A.nchild[b] == 0 || A.isrcse[2 * b + 1] < A.isrcse[2 * b]) return;
   int n1 = A.T.p[lev], n2 = A.T.p[lev + 1], nt = n1 + n2;
-  double rs1 = A.T.rs[lev], rs2 = A.T.rs[lev + 1];
   zdc* S1 = sh + (threadIdx.x >> 5) * stride + nt;  // S1[k], k = -nt..nt
-  zdc* S2 = S1 + nt + 1 + nt;                       // S1[k] (rs1 rs2)^|k|
-  zdc* uu = S2 + nt + 1 + n2;                       // (rs2/rs1)^|n| mp_child(n), n = -n2..n2
-  zdc* ww = uu + n2 + 1 + n2;                       // (rs1 rs2)^|n| mp_child(n)
-  double* qa = (double*)(ww + n2 + 1);              // (rs1 rs2)^k, k = 0..nt
-  double* qb = qa + nt + 1;                         // (rs2/rs1)^k, k = 0..nt
+  zdc* S3 = S1 + nt + 1 + nt;                       // S1[j] g(-j)
+  zdc* S4 = S3 + nt + 1 + nt;                       // S1[k] g(k)
+  zdc* ww = S4 + nt + 1 + n2;                       // (rs1 rs2)^|n| mp_child(n), n = -n2..n2
+  zdc* mc = ww + n2 + 1 + n2;                       // mp_child(n)
+  const double* qa = TA.pw + TA.pw_m2m[lev];        // (rs1 rs2)^k, k = 0..nt
+  const double* qb = qa + nt + 1;                   // (rs2/rs1)^k
+  const double* qi = qb + nt + 1;                   // (rs1/rs2)^k
   zdc accp[R], accm[R], acc0 = mkz(0.0);
 #pragma unroll
   for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
-  for (int k = lane; k <= nt; k += 32) {
-    qa[k] = TA.pw[TA.pw_m2m[lev] + k];
-    qb[k] = TA.pw[TA.pw_m2m[lev] + nt + 1 + k];
-  }
   const int lc = lev + 1;
   for (int jc = 0; jc < 4; jc++) {
     int jb = A.ichild[4 * b + jc];
@@ -538,15 +555,17 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
       zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
       S1[k] = vv;   // (-1)^k J_k e^{-ik theta}
       S1[-k] = u;   // J_k e^{ik theta}
-      S2[k] = vv * qa[k];
-      S2[-k] = u * qa[k];
+      double gp = k > 0 ? qa[k] : 1.0, gm = qi[k];  // g(k), g(-k)
+      S3[k] = vv * gm;
+      S3[-k] = u * gp;
+      S4[k] = vv * gp;
+      S4[-k] = u * gm;
     }
     const zdc* M2 = expo(A, A.mp, jb);
     for (int n = lane - n2; n <= n2; n += 32) {
       zdc v = M2[n];
-      int an = abs(n);
-      uu[n] = qb[an] * v;
-      ww[n] = qa[an] * v;
+      mc[n] = v;
+      ww[n] = qa[abs(n)] * v;
     }
     __syncwarp();
 #pragma unroll
@@ -554,12 +573,8 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
       int m = lane + 32 * r;
       if (m > n1) break;
       zdc a1 = mkz(0.0), a2 = mkz(0.0);
-      for (int n = -n2; n <= n2; n++) {
-        int k = m - n;
-        if (n <= 0) a1 += S1[k] * ww[n];
-        else if (n <= m) a1 += S1[k] * uu[n];
-        else a2 += S2[k] * M2[n];
-      }
+      for (int n = -n2; n <= 0; n++) a1 += S1[m - n] * ww[n];
+      for (int n = 1; n <= n2; n++) a2 += S3[m - n] * mc[n];
       zdc sp = a1 + qb[m] * a2;
       if (m == 0) {
         acc0 += sp;
@@ -567,12 +582,8 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
       }
       a1 = mkz(0.0);
       a2 = mkz(0.0);
-      for (int n = -n2; n <= n2; n++) {
-        int k = -m - n;
-        if (n >= 0) a1 += S1[k] * ww[n];
-        else if (n >= -m) a1 += S1[k] * uu[n];
-        else a2 += S2[k] * M2[n];
-      }
+      for (int n = 0; n <= n2; n++) a1 += S1[-m - n] * ww[n];
+      for (int n = -n2; n < 0; n++) a2 += S4[-m - n] * mc[n];
       accp[r] += sp;
       accm[r] += a1 + qb[m] * a2;
     }
@@ -607,7 +618,6 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
   zdc* T = sh + (threadIdx.x >> 5) * stride;  // [2*n2+1]
   double* rp = (double*)(T + 2 * n2 + 1);     // rs^k, k = 0..n2
   zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;    // b(n), n = -p..p
-  zdc* cc = bb + 2 * p + 1;                   // c(n)
   zdc accp[R], accm[R], acc0 = mkz(0.0);
 #pragma unroll
   for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
@@ -618,12 +628,11 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
     if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
     __syncwarp();
     // Toeplitz symbol T[k] = H_k e^{ik theta} (k = -2p..2p, H_-k = (-1)^k H_k,
-    // scaled) from the pair's table, and the source coefficients without (b)
-    // and with (c) the factor rs^(2|n|): the reference's weight
-    // rs^|m| rs^|n| / rs^|n-m| is 1 for n, m of opposite signs and
-    // rs^(2 min(|m|,|n|)) otherwise, so
-    //   loc(m) = sum_{n<0} T[n-m] b(n) + sum_{0<=n<=m} T[n-m] c(n)
-    //          + rs^(2m) sum_{n>m} T[n-m] b(n)        (m >= 0, mirrored for m < 0)
+    // scaled) from the pair's table and the source coefficients b(n): the
+    // reference's weight rs^|m| rs^|n| / rs^|n-m| is 1 for n, m of opposite
+    // signs and rs^(2 min(|m|,|n|)) otherwise, so
+    //   loc(m) = sum_{n<0} T[n-m] b(n) + sum_{n>=0} rs^(2 min(n,m)) T[n-m] b(n)
+    //   (m >= 0, mirrored for m < 0)
     const double4* t = tl + (long)il * (n2 + 1);
     for (int k = lane; k <= n2; k += 32) {
       double4 v = t[k];
@@ -631,38 +640,37 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
       T[n2 - k] = mkz(v.z, v.w);
     }
     const zdc* M = expo(A, A.mp, jb);
-    for (int n = lane - p; n <= p; n += 32) {
-      zdc v = M[n];
-      bb[n] = v;
-      cc[n] = rp[2 * abs(n)] * v;
-    }
+    for (int n = lane - p; n <= p; n += 32) bb[n] = M[n];
     __syncwarp();
+    // per output the weight is rs^(2 min(|n|, |m|)) for n of the sign of m
+    // (n = 0 included) and 1 otherwise; it is applied to b(n) as the scale
+    // rp[2|n|] (|n| <= |m|) or rp[2|m|] (|n| > |m|), selected per lane, so
+    // the inner loops have no branches
 #pragma unroll
     for (int r = 0; r < R; r++) {
       int m = lane + 32 * r;
       if (m > p) break;
-      zdc a1 = mkz(0.0), a2 = mkz(0.0);
+      const double rpm = rp[2 * m];
+      zdc a = mkz(0.0);
       const zdc* Tm = T + n2 - m;  // Tm[n] = T[n - m]
-      for (int n = -p; n <= p; n++) {
-        zdc t = Tm[n];
-        if (n > m) a2 += t * bb[n];
-        else a1 += t * (n < 0 ? bb[n] : cc[n]);
+      for (int n = -p; n < 0; n++) a += Tm[n] * bb[n];
+      for (int n = 0; n <= p; n++) {
+        double sc = n <= m ? rp[2 * n] : rpm;
+        a += Tm[n] * (sc * bb[n]);
       }
-      zdc sp = a1 + rp[2 * m] * a2;
       if (m == 0) {
-        acc0 += sp;
+        acc0 += a;
         continue;
       }
-      a1 = mkz(0.0);
-      a2 = mkz(0.0);
+      zdc c = mkz(0.0);
       const zdc* Tq = T + n2 + m;  // Tq[n] = T[n + m]
-      for (int n = -p; n <= p; n++) {
-        zdc t = Tq[n];
-        if (n < -m) a2 += t * bb[n];
-        else a1 += t * (n > 0 ? bb[n] : cc[n]);
+      for (int n = 1; n <= p; n++) c += Tq[n] * bb[n];
+      for (int n = -p; n <= 0; n++) {
+        double sc = -n <= m ? rp[-2 * n] : rpm;
+        c += Tq[n] * (sc * bb[n]);
       }
-      accp[r] += sp;
-      accm[r] += a1 + rp[2 * m] * a2;
+      accp[r] += a;
+      accm[r] += c;
     }
   }
   zdc* L = expo(A, A.loc, b);
@@ -722,161 +730,171 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
   for (int n = lane - n2; n <= n2; n += 32) uu[n] = qb[abs(n)] * L2[n];
   __syncwarp();
   zdc* L1 = expo(A, A.loc, jb);
+  // per output the terms with n of the other sign form a plain Toeplitz sum
+  // (times rs1^(2|m|)); for the others the symbol S1 or S3 is selected per
+  // lane, so the loops have no branches
 #pragma unroll
   for (int r = 0; r < R; r++) {
     int m = lane + 32 * r;
     if (m > n1) break;
     zdc a1 = mkz(0.0), a2 = mkz(0.0);
-    for (int n = -n2; n <= n2; n++) {
-      int k = n - m;
-      if (n >= m) a1 += S1[k] * uu[n];
-      else if (n >= 0) a1 += S3[k] * uu[n];
-      else a2 += S1[k] * uu[n];
-    }
+    for (int n = -n2; n < 0; n++) a2 += S1[n - m] * uu[n];
+    for (int n = 0; n <= n2; n++) a1 += (n >= m ? S1[n - m] : S3[n - m]) * uu[n];
     L1[m] += a1 + qa[m] * a2;
     if (m == 0) continue;
     a1 = mkz(0.0);
     a2 = mkz(0.0);
-    for (int n = -n2; n <= n2; n++) {
-      int k = n + m;
-      if (n <= -m) a1 += S1[k] * uu[n];
-      else if (n <= 0) a1 += S3[k] * uu[n];
-      else a2 += S1[k] * uu[n];
-    }
+    for (int n = 1; n <= n2; n++) a2 += S1[n + m] * uu[n];
+    for (int n = -n2; n <= 0; n++) a1 += (n <= -m ? S1[n + m] : S3[n + m]) * uu[n];
     L1[-m] += a1 + qa[m] * a2;
   }
 }
 
-// ---- steps 3, 5, 8: P2P (list1), M2T (list3), L2T per target leaf --------------
+// ---- steps 5, 8: M2T (list 3) and L2T, one thread per target -------------------
+// Every target of a leaf box runs its own L2T sweep and its M2T sums, so all
+// lanes of a warp work whatever the number of targets per leaf.
+
+// leaf box of every target (-1 for targets of no leaf: none)
+__global__ void k_tgt_leaf(int nb, HelmArgs A, int* tgtleaf) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
+  if (A.nchild[b] > 0 || t1 < t0) return;
+  for (int t = t0; t <= t1; t++) tgtleaf[t] = b;
+}
+
 template <bool GRAD>
-__global__ void __launch_bounds__(32 * WPB, 4) k_heval(int nb, HelmArgs A, const int* nl1,
-                                                   const int* l1, int m1, const int* nl3,
-                                                   const int* l3, int m3, zdc* potsort,
-                                                   zdc* gradsort) {
+__global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgtleaf,
+                                              const int* nl3, const int* l3, int m3,
+                                              zdc* potsort, zdc* gradsort) {
+  int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= nt) return;
+  int b = tgtleaf[ti];
+  if (b < 0) return;
+  int lb = A.ilevel[b];
+  zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
+  zdc pot = mkz(0.0), g1 = mkz(0.0), g2 = mkz(0.0);
+  // L2T (zh2devalloc): one backward Miller sweep (jbessel2d) accumulating the
+  // unnormalised sums; the normalisation e^{-+iz}/psi is applied at the end.
+  // Derivative of the scaled Bessel function: fjder(n) = g_{n-1}/rs - (n/z) g_n,
+  // fjder(0) = -rs g_1 (equal to the reference's (g_{n-1}/rs - rs g_{n+1})/2).
+  if (lb >= 2) {
+    int p = A.T.p[lb];
+    double rs = A.T.rs[lb];
+    const zdc* L = expo(A, A.loc, b);
+    zdc a1 = x1 - A.zctarg[2 * b], a2 = x2 - A.zctarg[2 * b + 1];
+    zdc zr, ei;
+    polar(a1, a2, zr, ei);
+    zdc z = zr * A.zk;
+    if (zabs(z) >= 1e-200) {
+      int ntop = jbessel_top(p, z);
+      zdc zrr = rs * zinv(z), izz = zinv(z);
+      double sc2 = rs * rs;
+      zdc zmul = z.im < 0.0 ? mkz(0.0, 1.0) : mkz(0.0, -1.0);
+      zdc iei = zinv(ei);
+      zdc gp1 = mkz(0.0), g = mkz(1.0), psi = mkz(0.0);
+      zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
+      zdc eip = zpown(ei, p), eim = zpown(iei, p);
+      for (int n = ntop - 1; n >= 0; n--) {
+        zdc gm1 = n >= 1 ? ((2.0 * n) * zrr) * g - sc2 * gp1 : mkz(0.0);
+        if (n <= p) {
+          zdc cp = ldz(&L[n]) * eip;
+          zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&L[-n]) * eim);
+          zdc c = cp + cm;
+          sp += c * g;
+          if (GRAD) {
+            zdc fd = n >= 1 ? gm1 / rs - ((double)n * izz) * g : (-rs) * gp1;
+            srad += c * fd;
+            sang += ((double)n * zmul_i(cp - cm)) * g;
+          }
+          eip = eip * iei;
+          eim = eim * ei;
+        }
+        if (n >= 1) {
+          int rr = n & 3;
+          zdc zn = rr == 0 ? mkz(1.0) : (rr == 1 ? zmul : (rr == 2 ? mkz(-1.0) : -zmul));
+          psi = rs * psi + zn * g;
+          gp1 = g;
+          g = gm1;
+          if (zabs(g) > 1e200) {
+            g = 1e-200 * g; gp1 = 1e-200 * gp1; psi = 1e-200 * psi;
+            sp = 1e-200 * sp; srad = 1e-200 * srad; sang = 1e-200 * sang;
+          }
+        } else {
+          psi = 2.0 * rs * psi + g;
+        }
+      }
+      zdc sc = (z.im < 0.0 ? zexp_p(zmul_i(z)) : zexp_p(-zmul_i(z))) / psi;
+      pot += sp * sc;
+      if (GRAD) {
+        zdc rad = (srad * sc) * A.zk, ang = (sang * sc) / zr;
+        zdc vr1 = a1 / zr, vr2 = a2 / zr;
+        g1 += rad * vr1 - ang * vr2;
+        g2 += rad * vr2 + ang * vr1;
+      }
+    }
+  }
+  // M2T (zh2devalmp) over list3: streaming forward recurrence of H_n
+  int n3 = nl3[b];
+  for (int il = 0; il < n3; il++) {
+    int jb = l3[(size_t)b * m3 + il];
+    if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
+    int lj = A.ilevel[jb], p = A.T.p[lj];
+    double rs = A.T.rs[lj];
+    const zdc* M = expo(A, A.mp, jb);
+    zdc zr, ei;
+    zdc a1 = x1 - A.zcsrc[2 * jb], a2 = x2 - A.zcsrc[2 * jb + 1];
+    polar(a1, a2, zr, ei);
+    zdc z = zr * A.zk;
+    if (zabs(z) < 1e-200) continue;
+    zdc h0, h1;
+    hank01(z, h0, h1);
+    zdc iei = zinv(ei), zi = rs * zinv(z), zi1 = zinv(z);
+    double sc2 = rs * rs;
+    zdc hm1 = mkz(0.0), h = h0, hp = h1 * rs;  // scaled H_{n-1}, H_n, H_{n+1}
+    zdc eip = mkz(1.0), eim = mkz(1.0);
+    zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
+    for (int n = 0; n <= p; n++) {
+      zdc cp = ldz(&M[n]) * eip;
+      zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&M[-n]) * eim);
+      sp += (cp + cm) * h;
+      if (GRAD) {
+        zdc hd = n == 0 ? -hp / rs : rs * hm1 - ((double)n * zi1) * h;
+        srad += (cp + cm) * hd;
+        sang += ((double)n * zmul_i(cp - cm)) * h;
+      }
+      zdc hn = ((2.0 * (n + 1)) * zi) * hp - sc2 * h;
+      hm1 = h;
+      h = hp;
+      hp = hn;
+      eip = eip * ei;
+      eim = eim * iei;
+    }
+    pot += sp;
+    if (GRAD) {
+      zdc vr1 = a1 / zr, vr2 = a2 / zr;
+      zdc rad = srad * A.zk, ang = sang / zr;
+      g1 += rad * vr1 - ang * vr2;
+      g2 += rad * vr2 + ang * vr1;
+    }
+  }
+  potsort[ti] = pot;
+  if (GRAD) {
+    gradsort[2 * ti] = g1;
+    gradsort[2 * ti + 1] = g2;
+  }
+}
+
+// ---- step 3: P2P (list 1) per target leaf, added to L2T + M2T ----------------
+template <bool GRAD>
+__global__ void __launch_bounds__(32 * WPB, 3) k_hp2p(int nb, HelmArgs A, const int* nl1,
+                                                  const int* l1, int m1, zdc* potsort,
+                                                  zdc* gradsort) {
   int b = blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b >= nb) return;
   int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
   if (A.nchild[b] > 0 || t1 < t0) return;
   int ntb = t1 - t0 + 1;
-  int lb = A.ilevel[b];
-  // L2T and M2T: one lane per target
-  for (int base = 0; base < ntb; base += 32) {
-    int ti = t0 + base + lane;
-    if (base + lane < ntb) {
-      zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
-      zdc pot = mkz(0.0), g1 = mkz(0.0), g2 = mkz(0.0);
-      // L2T (zh2devalloc): one backward Miller sweep (jbessel2d) accumulating the
-      // unnormalised sums; the normalisation e^{-+iz}/psi is applied at the end.
-      // Derivative of the scaled Bessel function: fjder(n) = g_{n-1}/rs - (n/z) g_n,
-      // fjder(0) = -rs g_1 (equal to the reference's (g_{n-1}/rs - rs g_{n+1})/2).
-      if (lb >= 2) {
-        int p = A.T.p[lb];
-        double rs = A.T.rs[lb];
-        const zdc* L = expo(A, A.loc, b);
-        zdc a1 = x1 - A.zctarg[2 * b], a2 = x2 - A.zctarg[2 * b + 1];
-        zdc zr, ei;
-        polar(a1, a2, zr, ei);
-        zdc z = zr * A.zk;
-        if (zabs(z) >= 1e-200) {
-          int ntop = jbessel_top(p, z);
-          zdc zrr = rs * zinv(z), izz = zinv(z);
-          double sc2 = rs * rs;
-          zdc zmul = z.im < 0.0 ? mkz(0.0, 1.0) : mkz(0.0, -1.0);
-          zdc iei = zinv(ei);
-          zdc gp1 = mkz(0.0), g = mkz(1.0), psi = mkz(0.0);
-          zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
-          zdc eip = zpown(ei, p), eim = zpown(iei, p);
-          for (int n = ntop - 1; n >= 0; n--) {
-            zdc gm1 = n >= 1 ? ((2.0 * n) * zrr) * g - sc2 * gp1 : mkz(0.0);
-            if (n <= p) {
-              zdc cp = ldz(&L[n]) * eip;
-              zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&L[-n]) * eim);
-              zdc c = cp + cm;
-              sp += c * g;
-              if (GRAD) {
-                zdc fd = n >= 1 ? gm1 / rs - ((double)n * izz) * g : (-rs) * gp1;
-                srad += c * fd;
-                sang += ((double)n * zmul_i(cp - cm)) * g;
-              }
-              eip = eip * iei;
-              eim = eim * ei;
-            }
-            if (n >= 1) {
-              int rr = n & 3;
-              zdc zn = rr == 0 ? mkz(1.0) : (rr == 1 ? zmul : (rr == 2 ? mkz(-1.0) : -zmul));
-              psi = rs * psi + zn * g;
-              gp1 = g;
-              g = gm1;
-              if (zabs(g) > 1e200) {
-                g = 1e-200 * g; gp1 = 1e-200 * gp1; psi = 1e-200 * psi;
-                sp = 1e-200 * sp; srad = 1e-200 * srad; sang = 1e-200 * sang;
-              }
-            } else {
-              psi = 2.0 * rs * psi + g;
-            }
-          }
-          zdc sc = (z.im < 0.0 ? zexp_p(zmul_i(z)) : zexp_p(-zmul_i(z))) / psi;
-          pot += sp * sc;
-          if (GRAD) {
-            zdc rad = (srad * sc) * A.zk, ang = (sang * sc) / zr;
-            zdc vr1 = a1 / zr, vr2 = a2 / zr;
-            g1 += rad * vr1 - ang * vr2;
-            g2 += rad * vr2 + ang * vr1;
-          }
-        }
-      }
-      // M2T (zh2devalmp) over list3: streaming forward recurrence of H_n
-      int n3 = nl3[b];
-      for (int il = 0; il < n3; il++) {
-        int jb = l3[(size_t)b * m3 + il];
-        if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-        int lj = A.ilevel[jb], p = A.T.p[lj];
-        double rs = A.T.rs[lj];
-        const zdc* M = expo(A, A.mp, jb);
-        zdc zr, ei;
-        zdc a1 = x1 - A.zcsrc[2 * jb], a2 = x2 - A.zcsrc[2 * jb + 1];
-        polar(a1, a2, zr, ei);
-        zdc z = zr * A.zk;
-        if (zabs(z) < 1e-200) continue;
-        zdc h0, h1;
-        hank01(z, h0, h1);
-        zdc iei = zinv(ei), zi = rs * zinv(z), zi1 = zinv(z);
-        double sc2 = rs * rs;
-        zdc hm1 = mkz(0.0), h = h0, hp = h1 * rs;  // scaled H_{n-1}, H_n, H_{n+1}
-        zdc eip = mkz(1.0), eim = mkz(1.0);
-        zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
-        for (int n = 0; n <= p; n++) {
-          zdc cp = ldz(&M[n]) * eip;
-          zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&M[-n]) * eim);
-          sp += (cp + cm) * h;
-          if (GRAD) {
-            zdc hd = n == 0 ? -hp / rs : rs * hm1 - ((double)n * zi1) * h;
-            srad += (cp + cm) * hd;
-            sang += ((double)n * zmul_i(cp - cm)) * h;
-          }
-          zdc hn = ((2.0 * (n + 1)) * zi) * hp - sc2 * h;
-          hm1 = h;
-          h = hp;
-          hp = hn;
-          eip = eip * ei;
-          eim = eim * iei;
-        }
-        pot += sp;
-        if (GRAD) {
-          zdc vr1 = a1 / zr, vr2 = a2 / zr;
-          zdc rad = srad * A.zk, ang = sang / zr;
-          g1 += rad * vr1 - ang * vr2;
-          g2 += rad * vr2 + ang * vr1;
-        }
-      }
-      potsort[ti] = pot;
-      if (GRAD) {
-        gradsort[2 * ti] = g1;
-        gradsort[2 * ti + 1] = g2;
-      }
-    }
-  }
-  __syncwarp();
   // P2P (zh2devaldirect) over list1: group of G lanes per target, added on top
   int pw = 1;
   while (pw < ntb && pw < 32) pw <<= 1;
@@ -995,6 +1013,12 @@ struct Helm2DPrep {
   DevBuf<int> pairoff;
   DevBuf<double4> tab;
   DevBuf<double> pw;
+  // P2M / P2L column layout: leaf box of every source; per box the number of
+  // columns and the first column entry (P2M: own sources; P2L: list-4 sources)
+  DevBuf<int> srcleaf, tgtleaf;  // leaf box of every sorted source / target
+  DevBuf<long long> p2m_cnt, p2m_base, p2l_cnt, p2l_off, p2l_base;
+  long long p2m_total = 0, p2l_nq = 0, p2l_total = 0;
+  int ns = 0, nt = 0;
   long tot = 0;
   int pmax = 0;
 };
@@ -1009,6 +1033,21 @@ __global__ void k_pairoff_at(const int* pairoff, const int* idx, int n, int* out
 
 __global__ void k_last_plus(const int* off, const int* cnt, int nb, int* out) {
   *out = off[nb - 1] + cnt[nb - 1];
+}
+
+__global__ void k_totals3(const long long* a, const long long* wa, const long long* b,
+                          const long long* wb, const long long* c, const long long* wc, int nb,
+                          long long* out) {
+  out[0] = a[nb - 1] + wa[nb - 1];
+  out[1] = b[nb - 1] + wb[nb - 1];
+  out[2] = c[nb - 1] + wc[nb - 1];
+}
+
+void excl_scan_ll(const long long* in, long long* out, int n, cudaStream_t s) {
+  size_t bytes = 0;
+  ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
+  DevBuf<char> tmp(bytes, s);
+  ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s));
 }
 }  // namespace
 
@@ -1059,10 +1098,43 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
   ZF_CUDA(cudaMemcpyAsync(didx.get(), idx.data(), idx.size() * sizeof(int),
                           cudaMemcpyHostToDevice, s));
   klaunch(k_pairoff_at, 1, 64, 0, s, H->pairoff.get(), didx.get(), nlev + 2, dout.get());
-  std::vector<int> p0(nlev + 2);
-  ZF_CUDA(cudaMemcpyAsync(p0.data(), dout.get(), p0.size() * sizeof(int), cudaMemcpyDeviceToHost,
-                          s));
-  ZF_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> p0;
+  // P2M / P2L column layout
+  const int ns = (int)(S.zsrcsort.size() / 2);
+  H->ns = ns;
+  H->srcleaf.alloc(ns, s);
+  H->srcleaf.fill_bytes(0xff);
+  klaunch(k_src_leaf, div_up(nb, 128), 128, 0, s, nb, A, H->srcleaf.get());
+  const int ntg = (int)(S.ztargsort.size() / 2);
+  H->nt = ntg;
+  H->tgtleaf.alloc(ntg, s);
+  H->tgtleaf.fill_bytes(0xff);
+  klaunch(k_tgt_leaf, div_up(nb, 128), 128, 0, s, nb, A, H->tgtleaf.get());
+  H->p2m_cnt.alloc(nb, s);
+  H->p2l_cnt.alloc(nb, s);
+  H->p2m_base.alloc(nb, s);
+  H->p2l_off.alloc(nb, s);
+  H->p2l_base.alloc(nb, s);
+  {
+    DevBuf<long long> w2(nb, s), w4(nb, s), tot(3, s);
+    klaunch(k_form_counts, div_up(nb, 128), 128, 0, s, nb, A, L.n[3].get(), L.list[3].get(),
+            L.mn[3], H->p2m_cnt.get(), w2.get(), H->p2l_cnt.get(), w4.get());
+    excl_scan_ll(w2.get(), H->p2m_base.get(), nb, s);
+    excl_scan_ll(H->p2l_cnt.get(), H->p2l_off.get(), nb, s);
+    excl_scan_ll(w4.get(), H->p2l_base.get(), nb, s);
+    klaunch(k_totals3, 1, 1, 0, s, H->p2m_base.get(), w2.get(), H->p2l_off.get(),
+            H->p2l_cnt.get(), H->p2l_base.get(), w4.get(), nb, tot.get());
+    long long t3[3];
+    ZF_CUDA(cudaMemcpyAsync(t3, tot.get(), sizeof(t3), cudaMemcpyDeviceToHost, s));
+    std::vector<int> p0h(nlev + 2);
+    ZF_CUDA(cudaMemcpyAsync(p0h.data(), dout.get(), p0h.size() * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaStreamSynchronize(s));
+    H->p2m_total = t3[0];
+    H->p2l_nq = t3[1];
+    H->p2l_total = t3[2];
+    p0.swap(p0h);
+  }
   // table layout: M2L tables of levels 2..nlev, then the M2M / L2L tables of
   // the children of levels 2..nlev-1
   TabArgs& TA = H->TA;
@@ -1093,6 +1165,7 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
       double rp = A.T.rs[l], rc = A.T.rs[l + 1];  // parent, child scales
       for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rp * rc, (double)k));
       for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rc / rp, (double)k));
+      for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rp / rc, (double)k));
       TA.pw_l2l[l] = (long)pw.size();
       for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rc, 2.0 * k));
       for (int k = 0; k <= nt; k++) pw.push_back(std::pow(rc / rp, (double)k));
@@ -1154,34 +1227,35 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   auto slots = [](int ncoef) { return (ncoef + 31) / 32; };  // register slots per lane
   // a templated launch choosing R from {1, 2, 4, 8, 16} >= need
   auto pickR = [](int need) { return need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : need <= 8 ? 8 : 16; };
-  // sources per batch of the P2M / P2L kernels: FCH, fewer when the columns of
-  // order p would exceed the shared memory of a block
-  auto form_fch = [](int P2) {
-    int f = (int)((227 * 1024) / ((size_t)WPB * P2 * sizeof(zdc)));
-    return f < 1 ? 1 : (f > FCH ? FCH : f);
-  };
-  // P2M per level (leaves of levels >= 2)
-  for (int l = 2; l <= nlev; l++) {
-    int pl_ = A.T.p[l], P2 = 2 * pl_ + 1, fch = form_fch(P2);
-    size_t sm = (size_t)WPB * fch * P2 * sizeof(zdc);
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
-    auto go = [&](auto kern) {
-      ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, fch);
-    };
-    switch (pickR(slots(P2))) {
-      case 1: go(k_hp2m<1>); break;
-      case 2: go(k_hp2m<2>); break;
-      case 4: go(k_hp2m<4>); break;
-      case 8: go(k_hp2m<8>); break;
-      default: go(k_hp2m<16>); break;
+  // P2M: columns of every source of a leaf of level >= 2, then per level the
+  // sums over each leaf's columns
+  {
+    DevBuf<zdc> cols(H.p2m_total > 0 ? H.p2m_total : 1, s);
+    if (H.ns > 0)
+      klaunch(k_p2m_cols, div_up(H.ns, 128), 128, 0, s, H.ns, A, H.srcleaf.get(),
+              H.p2m_base.get(), cols.get());
+    for (int l = 2; l <= nlev; l++) {
+      int P2 = 2 * A.T.p[l] + 1;
+      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+      auto go = [&](auto kern) {
+        klaunch(kern, grid, 32 * WPB, 0, s, lo, hi, A, H.p2m_cnt.get(), H.p2m_base.get(),
+                (const zdc*)cols.get());
+      };
+      switch (pickR(slots(P2))) {
+        case 1: go(k_form_sum<1, false>); break;
+        case 2: go(k_form_sum<2, false>); break;
+        case 4: go(k_form_sum<4, false>); break;
+        case 8: go(k_form_sum<8, false>); break;
+        default: go(k_form_sum<16, false>); break;
+      }
     }
   }
   ZF_LAUNCH_CHECK();
   cmark(2);
   for (int l = nlev - 1; l >= 2; l--) {
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
-    int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l + 1]);
+    int ntt = A.T.p[l] + A.T.p[l + 1], nin = A.T.p[l + 1];
+    int stride = 3 * (2 * ntt + 1) + 2 * (2 * nin + 1);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     auto go = [&](auto kern) {
       ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -1200,7 +1274,7 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   // shared-memory stride and the register slots follow the level's order
   for (int l = 2; l <= nlev; l++) {
     int pl_ = A.T.p[l], n2 = 2 * pl_;
-    int stride = (2 * n2 + 1) + (n2 + 2) + 2 * (2 * pl_ + 1);
+    int stride = (2 * n2 + 1) + (n2 + 2) + (2 * pl_ + 1);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
     auto go = [&](auto kern) {
@@ -1216,24 +1290,29 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
     }
   }
   ZF_LAUNCH_CHECK();
-  if (L.mn[3] > 0)
+  // P2L: columns of every (target box, list-4 source), then per level the sums
+  // added to the local expansions
+  if (H.p2l_nq > 0) {
+    DevBuf<zdc> cols(H.p2l_total, s);
+    klaunch(k_p2l_cols, div_up(H.p2l_nq, 128), 128, 0, s, H.p2l_nq, 0, nb - 1, A,
+            H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_base.get(),
+            cols.get());
     for (int l = 2; l <= nlev; l++) {
-      int pl_ = A.T.p[l], P2 = 2 * pl_ + 1, fch = form_fch(P2);
-      size_t sm = (size_t)WPB * fch * P2 * sizeof(zdc);
+      int P2 = 2 * A.T.p[l] + 1;
       int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
       auto go = [&](auto kern) {
-        ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, L.n[3].get(), L.list[3].get(), L.mn[3],
-                fch);
+        klaunch(kern, grid, 32 * WPB, 0, s, lo, hi, A, H.p2l_cnt.get(), H.p2l_base.get(),
+                (const zdc*)cols.get());
       };
       switch (pickR(slots(P2))) {
-        case 1: go(k_hp2l<1>); break;
-        case 2: go(k_hp2l<2>); break;
-        case 4: go(k_hp2l<4>); break;
-        case 8: go(k_hp2l<8>); break;
-        default: go(k_hp2l<16>); break;
+        case 1: go(k_form_sum<1, true>); break;
+        case 2: go(k_form_sum<2, true>); break;
+        case 4: go(k_form_sum<4, true>); break;
+        case 8: go(k_form_sum<8, true>); break;
+        default: go(k_form_sum<16, true>); break;
       }
     }
+  }
   ZF_LAUNCH_CHECK();
   cmark(4);
   for (int l = 2; l <= nlev - 1; l++) {
@@ -1253,12 +1332,19 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   }
   ZF_LAUNCH_CHECK();
   cmark(5);
-  if (ifpgh > 1)
-    klaunch(k_heval<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-            L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort, gradsort);
-  else
-    klaunch(k_heval<false>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-            L.mn[0], L.n[2].get(), L.list[2].get(), L.mn[2], potsort, gradsort);
+  // L2T + M2T one thread per target (writes), then P2P per leaf (adds)
+  const int ntt = H.nt;
+  if (ifpgh > 1) {
+    klaunch(k_hl2t<true>, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
+            L.list[2].get(), L.mn[2], potsort, gradsort);
+    klaunch(k_hp2p<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
+            L.mn[0], potsort, gradsort);
+  } else {
+    klaunch(k_hl2t<false>, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
+            L.list[2].get(), L.mn[2], potsort, gradsort);
+    klaunch(k_hp2p<false>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
+            L.mn[0], potsort, gradsort);
+  }
   ZF_LAUNCH_CHECK();
   if (pl) *pl = std::vector<int>(A.T.p, A.T.p + nlev + 1);
   return H.pmax;
