@@ -46,6 +46,13 @@ WORKLOADS = {
                                cpu_n=200_000),
     "zhfmm2d_curve_2m_eps1e-6": dict(kind="helm2d", n=2_000_000, eps=1e-6, zk=40 + 0.5j, ifpgh=2,
                                      isep=1, cpu_n=200_000),
+    # zhfmm2d plan solve of 64 right-hand sides on the curve of the 2M case
+    # (500,000 points, zk = 40+0.5i, charges + dipoles, pot + grad): at eps
+    # 1e-6 the M2L runs on the tensor cores, at 1e-9 in FP64
+    "zhfmm2d_batched_500k_64_eps1e-6": dict(kind="helm2d", n=500_000, nrhs=64, eps=1e-6,
+                                            zk=40 + 0.5j, ifpgh=2, isep=1, cpu_n=50_000),
+    "zhfmm2d_batched_500k_64": dict(kind="helm2d", n=500_000, nrhs=64, eps=1e-9, zk=40 + 0.5j,
+                                    ifpgh=2, isep=1, cpu_n=50_000),
     "zhfmm2d_curve_2m_eps1e-12": dict(kind="helm2d", n=2_000_000, eps=1e-12, zk=40 + 0.5j,
                                       ifpgh=2, isep=1, cpu_n=200_000),
     # zlfmm3d single solve on the geometry of the batched configuration:
@@ -910,6 +917,187 @@ def run_ours_batched(args, wl, ws, rank, local, summary=False):
     print(json.dumps(line), flush=True)
 
 
+def run_ours_batched2d(args, wl, ws, rank, local):
+    """zhfmm2d plan solve of nd right-hand sides on the curve: one step = plan
+    (quadtree, lists, centres) + one solve of all right-hand sides, whose M2L
+    runs for groups of up to 64 right-hand sides on the tensor cores when
+    eps >= 1e-7 (TF32 three-term split) and in FP64 below."""
+    import ctypes
+
+    import torch
+
+    import zfmm_b200
+    from zfmm_b200 import _capi, shard
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _capi.lib()
+    n, nd_total = wl["n"], wl["nrhs"]
+    r0, r1 = shard.rhs_block(nd_total, rank, ws)
+    nd = r1 - r0
+    eps, isep, ifpgh = wl["eps"], wl["isep"], wl["ifpgh"]
+    zk = complex(wl["zk"])
+    zka = np.array([zk.real, zk.imag])
+    zkp = zka.ctypes.data_as(ctypes.c_void_p)
+    from zfmm_b200 import workloads as W
+    w = W.curve2d(n, seed=0)
+    rng = np.random.default_rng(4242)
+    cn = lambda *sh: rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    qh, dsh = cn(nd_total, n)[r0:r1], cn(nd_total, n)[r0:r1]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    zs = t(w["zsrc"].T)
+    q, ds, dv = t(qh.T), t(dsh.T), t(w["dipvec"].T)
+    pot = torch.empty((n, nd), dtype=torch.complex128, device=dev)
+    grad = torch.empty((n, 2, nd), dtype=torch.complex128, device=dev)
+    pot1 = torch.empty(n, dtype=torch.complex128, device=dev)
+    grad1 = torch.empty((n, 2), dtype=torch.complex128, device=dev)
+    q0, ds0 = t(qh[0]), t(dsh[0])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+
+    def solve():
+        h = ctypes.c_void_p()
+        _capi.check(L.zfmm_plan2d_create_dev(eps, n, P(zs), n, P(zs), isep, sp, ctypes.byref(h)))
+        _capi.check(L.zfmm_zhfmm2d_plan_dev(h, zkp, nd, 1, P(q), 1, P(ds), P(dv), ifpgh, P(pot),
+                                            P(grad), sp))
+        _capi.check(L.zfmm_plan2d_destroy(h))
+
+    def solve_plain():
+        _capi.check(L.zfmm_zhfmm2d_dev(eps, zkp, n, P(zs), 1, P(q0), 1, P(ds0), P(dv), P(pot1),
+                                       P(grad1), n, P(zs), ifpgh, isep, sp))
+
+    for _ in range(max(args.warmup, 3)):
+        solve()
+    # interaction counts of one right-hand side (not timed)
+    L.zfmm_set_step_timing(2)
+    solve_plain()
+    counts, _ = zfmm_b200.last_counts()
+    L.zfmm_set_step_timing(1)
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    parts = {"upward": 0.0, "m2l": 0.0, "downward": 0.0}
+    launches0 = L.zfmm_launch_count()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            ev0[k].record(stream)
+            solve()
+            ev1[k].record(stream)
+            st, _ = zfmm_b200.last_step_times()
+            parts["upward"] += st["p2m"]
+            parts["m2l"] += st["m2l_p2l"]
+            parts["downward"] += st["eval"]
+        torch.cuda.synchronize()
+    launches = L.zfmm_launch_count() - launches0
+    tot_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    if ws > 1:
+        tt = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    value = n * nd_total * args.steps / (tot_ms * 1e-3)
+    for _ in range(2):
+        solve_plain()
+    torch.cuda.synchronize()
+    pl = []
+    for k in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(k & 255)
+        e0.record(stream)
+        solve_plain()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pl.append(e0.elapsed_time(e1))
+    plain_ms = statistics.median(pl)
+    L.zfmm_set_step_timing(0)
+    # end to end through the host plan entry points
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hz, hq, hds, hdv = pin(w["zsrc"].T), pin(qh.T), pin(dsh.T), pin(w["dipvec"].T)
+    hpot = torch.empty((n, nd), dtype=torch.complex128).pin_memory().numpy()
+    hgrad = torch.empty((n, 2, nd), dtype=torch.complex128).pin_memory().numpy()
+    hp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def solve_host():
+        h = ctypes.c_void_p()
+        _capi.check(L.zfmm_plan2d_create(eps, n, hp(hz), n, hp(hz), isep, ctypes.byref(h)))
+        _capi.check(L.zfmm_zhfmm2d_plan(h, zkp, nd, 1, hp(hq), 1, hp(hds), hp(hdv), ifpgh,
+                                        hp(hpot), hp(hgrad)))
+        _capi.check(L.zfmm_plan2d_destroy(h))
+
+    solve_host()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        solve_host()
+    e2e_s = time.perf_counter() - t0
+    h2d = 2 * hz.nbytes + hq.nbytes + hds.nbytes + hdv.nbytes
+    d2h = hpot.nbytes + hgrad.nbytes
+    # accuracy: right-hand sides 0 and nd-1 against the FP64 direct sum, and
+    # against the single FP64 solve of right-hand side 0
+    pg = pot.cpu().numpy()
+    sub = np.sort(np.random.default_rng(1234).choice(n, size=min(n, 1024), replace=False))
+    errs = []
+    for r in (0, nd - 1):
+        pd, _ = zfmm_b200.zh2devaldirect(zk, len(sub), w["zsrc"][:, sub], n, w["zsrc"], qh[r],
+                                         dsh[r], w["dipvec"], 1, 1, 1)
+        errs.append(float(np.linalg.norm(pg[sub, r] - 0.25j * pd) / np.linalg.norm(0.25j * pd)))
+    p1 = pot1.cpu().numpy()
+    agree = float(np.linalg.norm(pg[:, 0] - p1) / np.linalg.norm(p1))
+    tc = eps >= 1e-7
+    avg = {k: v / args.steps for k, v in parts.items()}
+    flops_m2l = 8.0 * counts["m2l_pairs_P"] * nd
+    achieved = flops_m2l / (avg["m2l"] * 1e-3) / 1e12 if avg["m2l"] > 0 else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    if tc:
+        peak = peaks.get("bf16_tflops", 1590.0) / 2
+        psrc = ("dense TF32 = half the measured dense bf16 GEMM rate (MEASURED_PEAKS "
+                "bf16_tflops); the three-term split issues 3 TF32 products per useful one")
+    else:
+        peak = float(L.zfmm_probe_fp64_tflops(20000))
+        psrc = "measured FP64 FMA probe (zfmm_probe_fp64_tflops)"
+    if rank != 0:
+        return
+    line = {
+        "metric": "targets/sec at eps=%g" % eps, "value": value, "unit": "targets/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "nrhs": nd_total, "eps": eps,
+                   "zk": [zk.real, zk.imag], "ifpgh": ifpgh, "isep": isep, "charges": True,
+                   "dipoles": True,
+                   "m2l": ("tcgen05 TF32 three-term split, 64 right-hand sides per panel"
+                           if tc else "FP64, per right-hand side"),
+                   "step": "plan (quadtree, lists, centres) + one solve of all right-hand sides",
+                   "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": (f"right-hand sides sharded over {ws} ranks" if ws > 1
+                                   else "one GPU")},
+        "e2e": {"value": n * nd_total * args.steps / e2e_s, "unit": "targets/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "plain_single_rhs": {"ms_per_solve": plain_ms, "value": n / (plain_ms * 1e-3),
+                             "batched_per_rhs_speedup": (value / ws) / (n / (plain_ms * 1e-3))},
+        "rel_l2_err_vs_direct": max(errs),
+        "rel_l2_batched_vs_plain_rhs0": agree,
+        "step_ms": {k: round(v, 4) for k, v in avg.items()},
+        "roofline": {"bound": "tensor" if tc else "fp64", "kernel": "m2l (k_hm2l_tc)" if tc
+                     else "m2l (k_hm2l)", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if achieved else None,
+                     "peak_source": psrc, "traffic": None, "flops_per_step": flops_m2l,
+                     "flop_model": "8 P^2 real flops per (box pair, right-hand side)"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours_many(args, wl, ws, rank, local):
     """One step = all instances through the many-instance device entry point."""
     import ctypes
@@ -1284,6 +1472,8 @@ def main():
             run_ours_adjoint(args, wl, ws, rank, local)
         elif wl.get("instances"):
             run_ours_many(args, wl, ws, rank, local)
+        elif wl.get("nrhs", 1) > 1 and wl["kind"] == "helm2d":
+            run_ours_batched2d(args, wl, ws, rank, local)
         elif wl.get("nrhs", 1) > 1:
             run_ours_batched(args, wl, ws, rank, local)
         else:

@@ -240,6 +240,17 @@ int zfmm_zhfmm2d_plan_dev(zfmm_plan2d plan, const double *zk, int nd, int ifchar
                           const double *dipvec, int ifpgh, double *pot, double *grad,
                           void *stream);
 
+/* Plan files (no counterpart in the reference): the geometry of a plan
+ * (tree, point order and ranges, sorted points, complex centres, lists)
+ * written once and read back by a later process, which then solves without
+ * rebuilding the tree.  load creates the plan on the current device; a file
+ * of the other dimension, another format version, or a truncated file is
+ * refused with status 1. */
+int zfmm_plan2d_save(zfmm_plan2d plan, const char *path);
+int zfmm_plan2d_load(const char *path, zfmm_plan2d *plan);
+int zfmm_plan3d_save(zfmm_plan3d plan, const char *path);
+int zfmm_plan3d_load(const char *path, zfmm_plan3d *plan);
+
 /* Many independent 3D FMMs in one call (no counterpart in the reference,
  * where each instance is a separate zlfmm3d / zhfmm3d call): instance i has
  * ns[i] sources zsrc[i](3, ns[i]), strengths charge[i], dipstr[i],
@@ -293,6 +304,14 @@ int zfmm_zl2devaldirect_dev_noalloc(int nt, const double *ztarg, int ns, const d
                                     const double *dipvec, int ifcharge, double *pot, double *grad,
                                     int ifdipole, int ifpgh, void *stream);
 long zfmm_zl2devaldirect_noalloc_capacity(void);
+
+/* Self-test of the tensor-core building block of the batched translations
+ * (no reference counterpart): D = A B^T for A (128 x K), B (N x K), D (128 x N),
+ * row-major FP32 device arrays on `stream`, through tcgen05 TF32 MMAs with the
+ * three-term split (hi/lo parts, FP32 accumulation in tensor memory).
+ * 16 <= N <= 256, N % 16 == 0, 8 <= K <= 128, K % 8 == 0.  Status 4 if the
+ * tensor-core completion wait timed out. */
+int zfmm_tc_selftest(int N, int K, const float *A, const float *B, float *D, void *stream);
 
 /* Per-step device times (ms) of the last FMM call on this host thread:
  * [set-up, P2M, M2M, M2L+P2L, L2L, P2P+M2T+L2T, unsort], plus nboxes, nlevels

@@ -324,6 +324,32 @@ class _Plan:
             check(getattr(lib(), self._fn["create"])(self.eps, self.ns, _ptr(zs), self.nt,
                                                      _ptr(zt), int(isep), ctypes.byref(self._h)))
 
+    def save(self, path):
+        """Write the plan's geometry (tree, point order, centres, lists) to a
+        plan file that load() reads back in a later process."""
+        import os
+        check(getattr(lib(), self._fn["save"])(self._h, os.fsencode(str(path))))
+
+    @classmethod
+    def load(cls, path):
+        """A plan read from a file written by save(), on the current device."""
+        import os
+        self = cls.__new__(cls)
+        self._h = ctypes.c_void_p()
+        check(getattr(lib(), cls._fn["load"])(os.fsencode(str(path)), ctypes.byref(self._h)))
+        nb, nl, ns, nt = (ctypes.c_int() for _ in range(4))
+        check(getattr(lib(), cls._fn["info"])(self._h, ctypes.byref(nb), ctypes.byref(nl),
+                                              ctypes.byref(ns), ctypes.byref(nt)))
+        self.ns, self.nt, self.eps = ns.value, nt.value, None
+        self.device = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                self.device = torch.device("cuda", torch.cuda.current_device())
+        except ImportError:
+            pass
+        return self
+
     def info(self):
         """(nboxes, nlevels) of the plan's tree."""
         nb, nl, a, b = (ctypes.c_int() for _ in range(4))
@@ -402,6 +428,7 @@ class Plan3D(_Plan):
 
     D = 3
     _fn = dict(create="zfmm_plan3d_create", create_dev="zfmm_plan3d_create_dev",
+               save="zfmm_plan3d_save", load="zfmm_plan3d_load",
                info="zfmm_plan3d_info", destroy="zfmm_plan3d_destroy", lap="zfmm_zlfmm3d_plan",
                lap_dev="zfmm_zlfmm3d_plan_dev", helm="zfmm_zhfmm3d_plan",
                helm_dev="zfmm_zhfmm3d_plan_dev")
@@ -423,6 +450,7 @@ class Plan2D(_Plan):
 
     D = 2
     _fn = dict(create="zfmm_plan2d_create", create_dev="zfmm_plan2d_create_dev",
+               save="zfmm_plan2d_save", load="zfmm_plan2d_load",
                info="zfmm_plan2d_info", destroy="zfmm_plan2d_destroy", lap="zfmm_zlfmm2d_plan",
                lap_dev="zfmm_zlfmm2d_plan_dev", helm="zfmm_zhfmm2d_plan",
                helm_dev="zfmm_zhfmm2d_plan_dev")

@@ -34,6 +34,11 @@ SIGNATURES = {
                                                 c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                                 c_int, c_int, c_void_p]),
     "zfmm_zl2devaldirect_noalloc_capacity": (ctypes.c_long, []),
+    "zfmm_tc_selftest": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "zfmm_plan2d_save": (c_int, [c_void_p, ctypes.c_char_p]),
+    "zfmm_plan2d_load": (c_int, [ctypes.c_char_p, c_void_p]),
+    "zfmm_plan3d_save": (c_int, [c_void_p, ctypes.c_char_p]),
+    "zfmm_plan3d_load": (c_int, [ctypes.c_char_p, c_void_p]),
     "zhfmm2d_": (None, [c_void_p] * 16),
     "zh2devaldirect_": (None, [c_void_p] * 13),
     "zfmm_zhfmm2d": (c_int, [c_double, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int,

@@ -1401,3 +1401,56 @@ int zfmm_zhfmm2d_plan_dev(zfmm_plan2d plan, const double* zk, int nd, int ifchar
 }
 
 }  // extern "C"
+
+// ---- plan files ----------------------------------------------------------------
+extern "C" {
+
+int zfmm_plan2d_save(zfmm_plan2d plan, const char* path) {
+  return guarded([&] {
+    if (!plan || !path) throw zf_error(ZF_ERR_ARG, "plan or path is null");
+    if (plan->P.ns == 0 || plan->P.nt == 0) throw zf_error(ZF_ERR_ARG, "empty plan");
+    plan2d_save(plan->P, path, cudaStreamPerThread);
+  });
+}
+
+int zfmm_plan2d_load(const char* path, zfmm_plan2d* out) {
+  return guarded([&] {
+    if (!path || !out) throw zf_error(ZF_ERR_ARG, "path or plan output is null");
+    *out = nullptr;
+    check_device();
+    auto* pl = new zfmm_plan2d_s();
+    try {
+      plan2d_load(pl->P, path, cudaStreamPerThread);
+    } catch (...) {
+      delete pl;
+      throw;
+    }
+    *out = pl;
+  });
+}
+
+int zfmm_plan3d_save(zfmm_plan3d plan, const char* path) {
+  return guarded([&] {
+    if (!plan || !path) throw zf_error(ZF_ERR_ARG, "plan or path is null");
+    if (plan->P.ns == 0 || plan->P.nt == 0) throw zf_error(ZF_ERR_ARG, "empty plan");
+    plan3d_save(plan->P, path, cudaStreamPerThread);
+  });
+}
+
+int zfmm_plan3d_load(const char* path, zfmm_plan3d* out) {
+  return guarded([&] {
+    if (!path || !out) throw zf_error(ZF_ERR_ARG, "path or plan output is null");
+    *out = nullptr;
+    check_device();
+    auto* pl = new zfmm_plan3d_s();
+    try {
+      plan3d_load(pl->P, path, cudaStreamPerThread);
+    } catch (...) {
+      delete pl;
+      throw;
+    }
+    *out = pl;
+  });
+}
+
+}  // extern "C"

@@ -33,6 +33,7 @@
 #include "helm2d_pair.cuh"
 #include "hfmm2d.cuh"
 #include "lfmm2d.cuh"
+#include "tc100.cuh"
 
 namespace zf {
 namespace {
@@ -686,6 +687,177 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
   }
 }
 
+// ---- M2L of many right-hand sides on the tensor cores ------------------------
+// For nd right-hand sides sharing one tree, the M2L of a box pair is the same
+// complex matrix W (P2 x P2, W[m][n] = w(m, n) T[n - m] with the weights and
+// symbol of k_hm2l) applied to nd multipole vectors: a complex product
+// loc(P2 x nd) += W mp(P2 x nd), taken as the real product
+//   [Re loc; Im loc] += [Re W, -Im W; Im W, Re W] [Re mp; Im mp]
+// of a (2 P2) x (2 P2) matrix and (2 P2) x nd panel on the tcgen05 tensor
+// cores (TF32 three-term split, FP32 accumulation in tensor memory, tc100.cuh),
+// accumulated over all pairs of a target box before it is read back.  Used
+// for plan solves at eps >= 1e-7 (the split's ~1e-7 relative accuracy) on
+// levels with 2 P2 <= 128.  Right-hand side j of the expansions is
+// mp + j * stride; 64 right-hand sides per launch (columns of D).
+constexpr int TC_N = 64;
+
+// smem words of the operands: A and B, hi and lo parts
+__host__ __device__ inline size_t tc_m2l_smem(int p) {
+  int kp = ((2 * (2 * p + 1) + 7) / 8) * 8;
+  return (size_t)2 * (128 + TC_N) * kp * 4 + (size_t)(4 * p + 1) * 16 + (size_t)(2 * p + 1) * 8 +
+         64;
+}
+
+__global__ void __launch_bounds__(128) k_hm2l_tc(int lo, int hi, HelmArgs A, TabArgs TA,
+                                                 const int* pairoff, const int* nl2,
+                                                 const int* l2, int m2, int nrhs, long stride,
+                                                 int* err) {
+  extern __shared__ __align__(1024) uint32_t tsm[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t taddr_s;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int l = A.ilevel[lo], p = A.T.p[l], P2 = 2 * p + 1, n2 = 2 * p;
+  const int K2 = 2 * P2, Kp = ((K2 + 7) / 8) * 8;
+  uint32_t* ah = tsm;
+  uint32_t* al = ah + 128 * Kp;
+  uint32_t* bh = al + 128 * Kp;
+  uint32_t* bl = bh + TC_N * Kp;
+  zdc* T = reinterpret_cast<zdc*>(bl + TC_N * Kp);  // T[k], k = -2p..2p at T[n2 + k]
+  double* rp = reinterpret_cast<double*>(T + 2 * n2 + 1);
+  // padding rows / columns / right-hand sides stay zero
+  for (int i = tid; i < 128 * Kp; i += 128) ah[i] = al[i] = 0u;
+  for (int i = tid; i < TC_N * Kp; i += 128) bh[i] = bl[i] = 0u;
+  for (int k = tid; k <= n2; k += 128) rp[k] = TA.pw[TA.pw_m2l[l] + k];
+  if (warp == 0) tc::tmem_alloc(&taddr_s, TC_N);
+  if (tid == 0) tc::mbar_init(&mbar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t taddr = taddr_s;
+  const uint32_t idesc = tc::idesc_tf32(128, TC_N);
+  const uint32_t achunk = 128 / 8 * 256, bchunk = TC_N / 8 * 256;
+  uint32_t phase = 0;
+  bool ok = true, pending = false;
+  const double big = 3.0e37;  // beyond this an operand does not fit FP32
+  for (int b = lo + blockIdx.x; b <= hi && ok; b += gridDim.x) {
+    if (A.itargse[2 * b + 1] < A.itargse[2 * b]) continue;
+    int n2c = nl2[b];
+    if (n2c == 0) continue;
+    const double4* tl =
+        TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
+    int npairs = 0;
+    for (int il = 0; il < n2c && ok; il++) {
+      int jb = l2[(size_t)b * m2 + il];
+      if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
+      // operands of this pair (after the previous pair's MMAs have read theirs)
+      if (npairs > 0) {
+        ok = tc::mbar_wait(&mbar, phase, tc::kWaitLimit);
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+        phase ^= 1;
+        pending = false;
+      }
+      const double4* t = tl + (long)il * (n2 + 1);
+      for (int k = tid; k <= n2; k += 128) {
+        double4 v = t[k];
+        T[n2 + k] = mkz(v.x, v.y);
+        T[n2 - k] = mkz(v.z, v.w);
+      }
+      __syncthreads();
+      bool inrange = true;
+      for (int i = tid; i < P2 * P2; i += 128) {
+        int mi = i / P2, ni = i - mi * P2, m = mi - p, n = ni - p;
+        double w;
+        if (m >= 0) w = n < 0 ? 1.0 : rp[2 * min(n, m)];
+        else w = n > 0 ? 1.0 : rp[2 * min(-n, -m)];
+        zdc W = w * T[n2 + n - m];
+        inrange = inrange && fabs(W.re) < big && fabs(W.im) < big;
+        uint32_t rh, rl, ih, il_, nh, nl;
+        tc::split_tf32((float)W.re, rh, rl);
+        tc::split_tf32((float)W.im, ih, il_);
+        tc::split_tf32(-(float)W.im, nh, nl);
+        uint32_t o1 = tc::kmajor_off(mi, ni, 128) >> 2, o2 = tc::kmajor_off(mi, P2 + ni, 128) >> 2;
+        uint32_t o3 = tc::kmajor_off(P2 + mi, ni, 128) >> 2;
+        uint32_t o4 = tc::kmajor_off(P2 + mi, P2 + ni, 128) >> 2;
+        ah[o1] = rh; al[o1] = rl;    // Re W
+        ah[o2] = nh; al[o2] = nl;    // -Im W
+        ah[o3] = ih; al[o3] = il_;   // Im W
+        ah[o4] = rh; al[o4] = rl;    // Re W
+      }
+      const zdc* M0 = expo(A, A.mp, jb) - p;
+      for (int i = tid; i < nrhs * P2; i += 128) {
+        int j = i / P2, ni = i - j * P2;
+        zdc v = ldz(M0 + j * stride + ni);
+        inrange = inrange && fabs(v.re) < big && fabs(v.im) < big;
+        uint32_t h, lw;
+        tc::split_tf32((float)v.re, h, lw);
+        uint32_t o = tc::kmajor_off(j, ni, TC_N) >> 2;
+        bh[o] = h; bl[o] = lw;
+        tc::split_tf32((float)v.im, h, lw);
+        o = tc::kmajor_off(j, P2 + ni, TC_N) >> 2;
+        bh[o] = h; bl[o] = lw;
+      }
+      if (!inrange) atomicExch(err, 2);
+      tc::fence_smem_async();
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+      if (tid == 0) {
+        for (int c = 0; c < Kp / 8; c++) {
+          uint64_t dah = tc::make_desc(tc::smem_u32(ah) + c * achunk, 128, 256);
+          uint64_t dal = tc::make_desc(tc::smem_u32(al) + c * achunk, 128, 256);
+          uint64_t dbh = tc::make_desc(tc::smem_u32(bh) + c * bchunk, 128, 256);
+          uint64_t dbl = tc::make_desc(tc::smem_u32(bl) + c * bchunk, 128, 256);
+          tc::mma_tf32(taddr, dal, dbh, idesc, (npairs > 0 || c > 0) ? 1u : 0u);
+          tc::mma_tf32(taddr, dah, dbl, idesc, 1u);
+          tc::mma_tf32(taddr, dah, dbh, idesc, 1u);
+        }
+        tc::mma_commit(&mbar);
+      }
+      pending = true;
+      npairs++;
+    }
+    if (!ok) break;
+    // read the accumulated panel back: row r = 32 warp + lane of D
+    zdc* L0 = expo(A, A.loc, b) - p;
+    if (npairs > 0) {
+      ok = tc::mbar_wait(&mbar, phase, tc::kWaitLimit);
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
+      phase ^= 1;
+      pending = false;
+      tc::fence_after_sync();
+      int r = 32 * warp + lane;
+      for (int c0 = 0; c0 < TC_N; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(taddr, warp, c0, v);
+        if (r < K2) {
+          int mi = r < P2 ? r : r - P2;
+          double* dst = reinterpret_cast<double*>(L0 + mi) + (r < P2 ? 0 : 1);
+#pragma unroll
+          for (int i = 0; i < 16; i++)
+            if (c0 + i < nrhs) dst[2 * (c0 + i) * stride] = (double)v[i];
+        }
+      }
+      tc::fence_before_sync();
+      __syncthreads();  // TMEM read before the next box's first MMA overwrites it
+    } else {
+      // every list-2 source box was empty: the local expansion is zero
+      for (int i = tid; i < nrhs * P2; i += 128) {
+        int j = i / P2, ni = i - j * P2;
+        L0[j * stride + ni] = mkz(0.0);
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  // an MMA batch that did not report completion: wait once more (bounded)
+  // before the tensor memory it writes is released
+  if (pending) tc::mbar_wait(&mbar, phase, tc::kWaitLimit);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(taddr, TC_N);
+}
+
 // L2L (zh2dlocloc) into the children at level lev+1
 // L2L (zh2dlocloc): loc_child(m) += sum_n t(n-m) e^{i(n-m) theta} loc(n)
 //   rs1^|m| rs1^|n-m| / rs2^|n|   (rs1 child, rs2 parent scale, rs1 <= rs2)
@@ -1196,9 +1368,14 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
 // unscaled potentials / gradients into potsort / gradsort (zeroed by the
 // caller); ev (optional) gets the step boundaries 2..5; *pl (optional)
 // receives the order of every level
-int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc* ds,
-                  const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* potsort,
-                  zdc* gradsort, cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl) {
+namespace {
+enum Stage { ST_UP = 1, ST_M2L = 2, ST_DOWN = 4, ST_ALL = 7 };
+
+// the passes of one right-hand side on expansions mp / loc (zeroed by the
+// caller): ST_UP = P2M + M2M, ST_M2L = M2L, ST_DOWN = P2L, L2L, M2T, L2T and P2P
+void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc* ds,
+                   const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* mpp, zdc* locp,
+                   int stages, zdc* potsort, zdc* gradsort, cudaStream_t s, cudaEvent_t* ev) {
   auto cmark = [&](int i) {
     if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
   };
@@ -1206,14 +1383,11 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   int nb = t.nboxes, nlev = t.nlevels;
   HelmArgs A = H.A0;
   const TabArgs& TA = H.TA;
-  DevBuf<zdc> mp(H.tot, s), loc(H.tot, s);
-  mp.zero();
-  loc.zero();
   A.charge = q;
   A.dipstr = ds;
   A.dipvec = dv;
-  A.mp = mp.get();
-  A.loc = loc.get();
+  A.mp = mpp;
+  A.loc = locp;
   A.ifcharge = ifcharge;
   A.ifdipole = ifdipole;
   const DevLists& L = S.lists;
@@ -1229,7 +1403,7 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   auto pickR = [](int need) { return need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : need <= 8 ? 8 : 16; };
   // P2M: columns of every source of a leaf of level >= 2, then per level the
   // sums over each leaf's columns
-  {
+  if (stages & ST_UP) {
     DevBuf<zdc> cols(H.p2m_total > 0 ? H.p2m_total : 1, s);
     if (H.ns > 0)
       klaunch(k_p2m_cols, div_up(H.ns, 128), 128, 0, s, H.ns, A, H.srcleaf.get(),
@@ -1252,7 +1426,7 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   }
   ZF_LAUNCH_CHECK();
   cmark(2);
-  for (int l = nlev - 1; l >= 2; l--) {
+  for (int l = nlev - 1; l >= 2 && (stages & ST_UP); l--) {
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
     int ntt = A.T.p[l] + A.T.p[l + 1], nin = A.T.p[l + 1];
     int stride = 3 * (2 * ntt + 1) + 2 * (2 * nin + 1);
@@ -1272,7 +1446,7 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   cmark(3);
   // one launch per level (lists 2 and 4 are empty on levels 0 and 1): the
   // shared-memory stride and the register slots follow the level's order
-  for (int l = 2; l <= nlev; l++) {
+  for (int l = 2; l <= nlev && (stages & ST_M2L); l++) {
     int pl_ = A.T.p[l], n2 = 2 * pl_;
     int stride = (2 * n2 + 1) + (n2 + 2) + (2 * pl_ + 1);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
@@ -1292,7 +1466,7 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   ZF_LAUNCH_CHECK();
   // P2L: columns of every (target box, list-4 source), then per level the sums
   // added to the local expansions
-  if (H.p2l_nq > 0) {
+  if (H.p2l_nq > 0 && (stages & ST_DOWN)) {
     DevBuf<zdc> cols(H.p2l_total, s);
     klaunch(k_p2l_cols, div_up(H.p2l_nq, 128), 128, 0, s, H.p2l_nq, 0, nb - 1, A,
             H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_base.get(),
@@ -1315,7 +1489,7 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   }
   ZF_LAUNCH_CHECK();
   cmark(4);
-  for (int l = 2; l <= nlev - 1; l++) {
+  for (int l = 2; l <= nlev - 1 && (stages & ST_DOWN); l++) {
     int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1], grid = div_up(hi - lo + 1, WPB);
     int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
@@ -1334,7 +1508,8 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
   cmark(5);
   // L2T + M2T one thread per target (writes), then P2P per leaf (adds)
   const int ntt = H.nt;
-  if (ifpgh > 1) {
+  if (!(stages & ST_DOWN)) {
+  } else if (ifpgh > 1) {
     klaunch(k_hl2t<true>, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
             L.list[2].get(), L.mn[2], potsort, gradsort);
     klaunch(k_hp2p<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
@@ -1346,8 +1521,129 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
             L.mn[0], potsort, gradsort);
   }
   ZF_LAUNCH_CHECK();
-  if (pl) *pl = std::vector<int>(A.T.p, A.T.p + nlev + 1);
+}
+}  // namespace
+
+int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc* ds,
+                  const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* potsort,
+                  zdc* gradsort, cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl) {
+  DevBuf<zdc> mp(H.tot, s), loc(H.tot, s);
+  mp.zero();
+  loc.zero();
+  helm2d_stages(S, H, q, ds, dv, ifcharge, ifdipole, ifpgh, mp.get(), loc.get(), ST_ALL,
+                potsort, gradsort, s, ev);
+  if (pl) *pl = std::vector<int>(H.A0.T.p, H.A0.T.p + S.tree.nlevels + 1);
   return H.pmax;
+}
+
+// nd right-hand sides on one prepared tree (the plan solve): the upward and
+// downward passes run per right-hand side; the M2L of levels with
+// 2 (2p+1) <= 128 runs for 64 right-hand sides at a time on the tensor cores
+// when use_tc (eps >= 1e-7), every other level per right-hand side in FP64.
+// Expansions of a group of right-hand sides are kept side by side; charge,
+// dipstr (nd, ns), pot (nd, nt), grad (nd, 2, nt) as the plan solve's.
+void helm2d_passes_nd(const Setup2D& S, const Helm2DPrep& H, int nd, int ifcharge,
+                      const zdc* charge, int ifdipole, const zdc* dipstr, const zdc* dipvec,
+                      int ifpgh, bool use_tc, zdc* pot, zdc* grad, cudaStream_t s, float* ms3) {
+  const DevTree& t = S.tree;
+  const int nlev = t.nlevels, ns = H.ns, nt = H.nt;
+  const long tot = H.tot;
+  const DevLists& L = S.lists;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) ZF_CUDA(cudaEventCreate(&e));
+  float acc[3] = {0, 0, 0};
+  DevBuf<zdc> q(ns, s), ds(ns, s), dv(2 * (size_t)ns, s), potsort(nt, s),
+      gradsort(ifpgh > 1 ? 2 * (size_t)nt : 1, s);
+  DevBuf<int> err(1, s);
+  err.zero();
+  // right-hand sides per group: 64 (one tensor-core panel), fewer when the
+  // expansions of 64 would exceed 24 GB
+  const long budget = 24L << 30;
+  const int G = (int)std::max(1L, std::min((long)TC_N, budget / (2 * tot * (long)sizeof(zdc))));
+  DevBuf<zdc> mp((size_t)G * tot, s), loc((size_t)G * tot, s);
+  for (int r0 = 0; r0 < nd; r0 += G) {
+    const int nc = std::min(G, nd - r0);
+    mp.zero();
+    loc.zero();
+    ZF_CUDA(cudaEventRecord(ev[0], s));
+    for (int j = 0; j < nc; j++) {
+      gather2d_col(S, ns, nd, r0 + j, ifcharge ? charge : nullptr, ifdipole ? dipstr : nullptr,
+                   ifdipole ? dipvec : nullptr, q.get(), ds.get(), dv.get(), s);
+      helm2d_stages(S, H, q.get(), ds.get(), dv.get(), ifcharge, ifdipole, ifpgh,
+                    mp.get() + j * tot, loc.get() + j * tot, ST_UP, nullptr, nullptr, s,
+                    nullptr);
+    }
+    ZF_CUDA(cudaEventRecord(ev[1], s));
+    HelmArgs A = H.A0;
+    A.mp = mp.get();
+    A.loc = loc.get();
+    for (int l = 2; l <= nlev; l++) {
+      int p = A.T.p[l];
+      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+      if (hi < lo) continue;
+      if (use_tc && 2 * (2 * p + 1) <= 128) {
+        size_t sm = tc_m2l_smem(p);
+        ZF_CUDA(cudaFuncSetAttribute(k_hm2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+        int grid = std::min(hi - lo + 1, 148);
+        klaunch(k_hm2l_tc, grid, 128, sm, s, lo, hi, A, H.TA, H.pairoff.get(), L.n[1].get(),
+                L.list[1].get(), L.mn[1], nc, tot, err.get());
+      } else {
+        for (int j = 0; j < nc; j++) {
+          HelmArgs Aj = A;
+          Aj.mp = mp.get() + j * tot;
+          Aj.loc = loc.get() + j * tot;
+          int n2 = 2 * p, stride = (2 * n2 + 1) + (n2 + 2) + (2 * p + 1);
+          size_t sm = (size_t)WPB * stride * sizeof(zdc);
+          int grid = div_up(hi - lo + 1, WPB);
+          auto slots = (p + 1 + 31) / 32;
+          auto go = [&](auto kern) {
+            ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm));
+            klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, Aj, H.TA, H.pairoff.get(),
+                    L.n[1].get(), L.list[1].get(), L.mn[1], stride);
+          };
+          if (slots <= 1) go(k_hm2l<1>);
+          else if (slots <= 2) go(k_hm2l<2>);
+          else if (slots <= 4) go(k_hm2l<4>);
+          else go(k_hm2l<MAXR>);
+        }
+      }
+    }
+    ZF_LAUNCH_CHECK();
+    ZF_CUDA(cudaEventRecord(ev[2], s));
+    for (int j = 0; j < nc; j++) {
+      gather2d_col(S, ns, nd, r0 + j, ifcharge ? charge : nullptr, ifdipole ? dipstr : nullptr,
+                   ifdipole ? dipvec : nullptr, q.get(), ds.get(), dv.get(), s);
+      potsort.zero();
+      gradsort.zero();
+      helm2d_stages(S, H, q.get(), ds.get(), dv.get(), ifcharge, ifdipole, ifpgh,
+                    mp.get() + j * tot, loc.get() + j * tot, ST_DOWN, potsort.get(),
+                    gradsort.get(), s, nullptr);
+      unsort2d_col(nt, nd, r0 + j, S.itarg.get(), potsort.get(), gradsort.get(), mkz(0.0, 0.25),
+                   ifpgh, pot, grad, s);
+    }
+    ZF_CUDA(cudaEventRecord(ev[3], s));
+    ZF_CUDA(cudaEventSynchronize(ev[3]));
+    for (int k = 0; k < 3; k++) {
+      float ms;
+      ZF_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      acc[k] += ms;
+    }
+  }
+  int h = 0;
+  ZF_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  ZF_CUDA(cudaStreamSynchronize(s));
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (h == 1) throw zf_error(ZF_ERR_INTERNAL, "tensor-core M2L: completion wait timed out");
+  if (h == 2) {
+    // an operand outside the FP32 range: the whole solve again in FP64
+    helm2d_passes_nd(S, H, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh, false, pot,
+                     grad, s, ms3);
+    return;
+  }
+  if (ms3)
+    for (int k = 0; k < 3; k++) ms3[k] = acc[k];
 }
 
 int helm2d_core(const Setup2D& S, double eps, zdc zk, int isep, const zdc* q, const zdc* ds,

@@ -35,6 +35,16 @@ int helm2d_passes(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zdc
                   const zdc* dv, int ifcharge, int ifdipole, int ifpgh, zdc* potsort,
                   zdc* gradsort, cudaStream_t s, cudaEvent_t* ev, std::vector<int>* pl);
 
+// nd right-hand sides on one prepared tree: charge, dipstr (nd, ns) with the
+// right-hand side fastest, dipvec (2, ns) shared; pot (nd, nt), grad (nd, 2, nt)
+// overwritten with the i/4 scaling.  The M2L of levels with 2(2p+1) <= 128 runs
+// on the tcgen05 tensor cores (TF32 three-term split) when use_tc; ms3
+// (optional) receives the device times of the upward passes, the M2L and the
+// downward passes.
+void helm2d_passes_nd(const Setup2D& S, const Helm2DPrep& H, int nd, int ifcharge,
+                      const zdc* charge, int ifdipole, const zdc* dipstr, const zdc* dipvec,
+                      int ifpgh, bool use_tc, zdc* pot, zdc* grad, cudaStream_t s, float* ms3);
+
 // zh2devaldirect over all pairs: ADDS the unscaled sums (no i/4) into pot/grad
 void zh2ddirect_device(zdc zk, const Inputs2D& in, zdc* pot, zdc* grad, cudaStream_t s);
 

@@ -47,6 +47,27 @@ void fmm2d_plan_execute(const Plan2D& P, const zdc* zk, int nd, int ifcharge, co
   // only: built once for all right-hand sides
   Helm2DPrepPtr H;
   if (zk) H = helm2d_prepare(S, P.eps, *zk, P.isep, s);
+  if (zk && nd >= 2) {
+    // several right-hand sides: M2L of groups of right-hand sides at once, on
+    // the tensor cores when eps >= 1e-7 (TF32 three-term split, accurate to
+    // about 1e-7 relative), in FP64 otherwise
+    mark(0);
+    float ms3[3] = {0, 0, 0};
+    helm2d_passes_nd(S, *H, nd, ifcharge, charge, ifdipole, dipstr, dipvec, ifpgh,
+                     P.eps >= 1e-7, pot, grad, s, timing ? ms3 : nullptr);
+    if (timing) {
+      for (int k = 0; k < 7; k++) times->ms[k] = 0;
+      times->ms[1] = ms3[0];
+      times->ms[3] = ms3[1];
+      times->ms[5] = ms3[2];
+      times->nboxes = S.tree.nboxes;
+      times->nlevels = S.tree.nlevels;
+      times->nterms = 0;
+      for (auto& e : ev) cudaEventDestroy(e);
+      times->launches = launch_counter() - launches0;
+    }
+    return;
+  }
   for (int r = 0; r < nd; r++) {
     mark(0);
     gather2d_col(S, ns, nd, r, ifcharge ? charge : nullptr, ifdipole ? dipstr : nullptr,

@@ -20,6 +20,11 @@ struct Plan2D {
 void plan2d_build(Plan2D& P, double eps, int ns, const zdc* zsrc, int nt, const zdc* ztarg,
                   int isep, cudaStream_t s);
 
+// the plan's geometry to / from a plan file (plan_io.cu); load builds the
+// device arrays on the current device
+void plan2d_save(const Plan2D& P, const char* path, cudaStream_t s);
+void plan2d_load(Plan2D& P, const char* path, cudaStream_t s);
+
 // nd right-hand sides: charge(nd, ns), dipstr(nd, ns) (right-hand side fastest),
 // dipvec(2, ns) shared; pot(nd, nt), grad(nd, 2, nt) overwritten, scaled as
 // the reference (1/(2 pi) Laplace, i/4 Helmholtz).  zk == nullptr: Laplace.

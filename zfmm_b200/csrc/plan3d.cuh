@@ -30,6 +30,11 @@ struct StrengthsNd {
 void plan3d_build(Plan3D& P, double eps, int ns, const zdc* zsrc, int nt, const zdc* ztarg,
                   int isep, cudaStream_t s);
 
+// the plan's geometry to / from a plan file (plan_io.cu); load builds the
+// device arrays on the current device
+void plan3d_save(const Plan3D& P, const char* path, cudaStream_t s);
+void plan3d_load(Plan3D& P, const char* path, cudaStream_t s);
+
 // pot(nd, nt) and grad(nd, 3, nt) (device) are overwritten; scaling as zlfmm3d
 void zlfmm3d_plan_execute(const Plan3D& P, int nd, const StrengthsNd& in, int ifpgh, zdc* pot,
                           zdc* grad, cudaStream_t s, StepTimes* times);
