@@ -1144,7 +1144,7 @@ def run_ours_many(args, wl, ws, rank, local):
                                             A["v"], hp(ns), A["zs"], ifpgh, isep, A["p"],
                                             A["g"], nstreams, hp(done)))
 
-    nst = wl["nstreams"]
+    nst = args.nstreams or wl["nstreams"]
     for _ in range(max(1, min(args.warmup, 1))):
         solve(nst)
     torch.cuda.synchronize()
@@ -1460,6 +1460,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--nstreams", type=int, default=None,
+                    help="host workers / streams of the many-instance workload")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-right-hand-side key of the default line")
     args = ap.parse_args()

@@ -313,6 +313,19 @@ long zfmm_zl2devaldirect_noalloc_capacity(void);
  * tensor-core completion wait timed out. */
 int zfmm_tc_selftest(int N, int K, const float *A, const float *B, float *D, void *stream);
 
+/* Launch-shape autotuner (no reference counterpart).  Off by default (the
+ * fixed launch shapes); zfmm_set_autotune(1) or ZFMM_AUTOTUNE=1 in the
+ * environment turns it on: the first call of a tunable kernel (2D Helmholtz
+ * table, column, evaluation and P2P kernels) for a work-size bucket (log2 of
+ * its item count) on a device times each candidate block size and keeps the
+ * fastest for later calls.  Results do not change, only timings.  The table
+ * can be saved to and loaded from a text file ("<kernel> <bucket> <device>
+ * <block>" per line; load refuses a file with a malformed line, status 1). */
+void zfmm_set_autotune(int on);
+int zfmm_autotune_entries(void);
+int zfmm_autotune_save(const char *path);
+int zfmm_autotune_load(const char *path);
+
 /* Per-step device times (ms) of the last FMM call on this host thread:
  * [set-up, P2M, M2M, M2L+P2L, L2L, P2P+M2T+L2T, unsort], plus nboxes, nlevels
  * and the expansion order.  Recording adds CUDA events; enable with

@@ -35,6 +35,10 @@ SIGNATURES = {
                                                 c_int, c_int, c_void_p]),
     "zfmm_zl2devaldirect_noalloc_capacity": (ctypes.c_long, []),
     "zfmm_tc_selftest": (c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "zfmm_set_autotune": (None, [c_int]),
+    "zfmm_autotune_entries": (c_int, []),
+    "zfmm_autotune_save": (c_int, [ctypes.c_char_p]),
+    "zfmm_autotune_load": (c_int, [ctypes.c_char_p]),
     "zfmm_plan2d_save": (c_int, [c_void_p, ctypes.c_char_p]),
     "zfmm_plan2d_load": (c_int, [ctypes.c_char_p, c_void_p]),
     "zfmm_plan3d_save": (c_int, [c_void_p, ctypes.c_char_p]),

@@ -34,6 +34,7 @@
 #include "hfmm2d.cuh"
 #include "lfmm2d.cuh"
 #include "tc100.cuh"
+#include "tune.cuh"
 
 namespace zf {
 namespace {
@@ -1062,7 +1063,7 @@ template <bool GRAD>
 __global__ void __launch_bounds__(32 * WPB, 3) k_hp2p(int nb, HelmArgs A, const int* nl1,
                                                   const int* l1, int m1, zdc* potsort,
                                                   zdc* gradsort) {
-  int b = blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b >= nb) return;
   int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
   if (A.nchild[b] > 0 || t1 < t0) return;
@@ -1351,13 +1352,17 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
   if (nlev >= 2) {
     long q0 = p0[2], q1 = p0[nlev + 1];
     if (q1 > q0)
-      klaunch(k_tab_m2l, div_up(q1 - q0, 128), 128, 0, s, q0, q1, t.laddr[4], nb - 1, A, TA,
-              H->pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1]);
+      tuned_launch("k_tab_m2l", q1 - q0, 128, {32, 64, 128}, [&](int bs) {
+        klaunch(k_tab_m2l, div_up(q1 - q0, bs), bs, 0, s, q0, q1, t.laddr[4], nb - 1, A, TA,
+                H->pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1]);
+      }, s);
   }
   if (nlev >= 3) {
     int c0 = t.laddr[6], c1 = nb - 1;
-    klaunch(k_tab_m2m_l2l, div_up(c1 - c0 + 1, 128), 128, 0, s, c0, c1, A, TA, L.n[1].get(),
-            L.n[3].get());
+    tuned_launch("k_tab_m2m_l2l", c1 - c0 + 1, 128, {32, 64, 128}, [&](int bs) {
+      klaunch(k_tab_m2m_l2l, div_up(c1 - c0 + 1, bs), bs, 0, s, c0, c1, A, TA, L.n[1].get(),
+              L.n[3].get());
+    }, s);
   }
   ZF_LAUNCH_CHECK();
   return H;
@@ -1391,7 +1396,6 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   A.ifcharge = ifcharge;
   A.ifdipole = ifdipole;
   const DevLists& L = S.lists;
-  int grid_all = div_up(nb, WPB);
   // shared memory per warp (complex elements) of the M2M / L2L products: two
   // Toeplitz symbols of 2 nt + 1, two weighted input vectors and two real
   // power tables
@@ -1406,8 +1410,10 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   if (stages & ST_UP) {
     DevBuf<zdc> cols(H.p2m_total > 0 ? H.p2m_total : 1, s);
     if (H.ns > 0)
-      klaunch(k_p2m_cols, div_up(H.ns, 128), 128, 0, s, H.ns, A, H.srcleaf.get(),
-              H.p2m_base.get(), cols.get());
+      tuned_launch("k_p2m_cols", H.ns, 128, {32, 64, 128}, [&](int bs) {
+        klaunch(k_p2m_cols, div_up(H.ns, bs), bs, 0, s, H.ns, A, H.srcleaf.get(),
+                H.p2m_base.get(), cols.get());
+      }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
       int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
@@ -1468,9 +1474,11 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   // added to the local expansions
   if (H.p2l_nq > 0 && (stages & ST_DOWN)) {
     DevBuf<zdc> cols(H.p2l_total, s);
-    klaunch(k_p2l_cols, div_up(H.p2l_nq, 128), 128, 0, s, H.p2l_nq, 0, nb - 1, A,
-            H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_base.get(),
-            cols.get());
+    tuned_launch("k_p2l_cols", H.p2l_nq, 128, {32, 64, 128}, [&](int bs) {
+      klaunch(k_p2l_cols, div_up(H.p2l_nq, bs), bs, 0, s, H.p2l_nq, 0, nb - 1, A,
+              H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_base.get(),
+              cols.get());
+    }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
       int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
@@ -1509,16 +1517,38 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   // L2T + M2T one thread per target (writes), then P2P per leaf (adds)
   const int ntt = H.nt;
   if (!(stages & ST_DOWN)) {
-  } else if (ifpgh > 1) {
-    klaunch(k_hl2t<true>, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
-            L.list[2].get(), L.mn[2], potsort, gradsort);
-    klaunch(k_hp2p<true>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-            L.mn[0], potsort, gradsort);
   } else {
-    klaunch(k_hl2t<false>, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
-            L.list[2].get(), L.mn[2], potsort, gradsort);
-    klaunch(k_hp2p<false>, grid_all, 32 * WPB, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-            L.mn[0], potsort, gradsort);
+    auto eval = [&](auto l2t, auto p2p) {
+      tuned_launch(ifpgh > 1 ? "k_hl2t_g" : "k_hl2t", ntt, 128, {64, 128}, [&](int bs) {
+        klaunch(l2t, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
+                L.list[2].get(), L.mn[2], potsort, gradsort);
+      }, s);
+      // P2P adds to what L2T wrote: tuning restores that state before each trial
+      DevBuf<zdc> keep;
+      size_t ng = ifpgh > 1 ? 2 * (size_t)ntt : 0;
+      auto reset = [&] {
+        if (!keep.get()) {
+          keep.alloc(ntt + ng, s);
+          ZF_CUDA(cudaMemcpyAsync(keep.get(), potsort, ntt * sizeof(zdc),
+                                  cudaMemcpyDeviceToDevice, s));
+          if (ng)
+            ZF_CUDA(cudaMemcpyAsync(keep.get() + ntt, gradsort, ng * sizeof(zdc),
+                                    cudaMemcpyDeviceToDevice, s));
+        } else {
+          ZF_CUDA(cudaMemcpyAsync(potsort, keep.get(), ntt * sizeof(zdc),
+                                  cudaMemcpyDeviceToDevice, s));
+          if (ng)
+            ZF_CUDA(cudaMemcpyAsync(gradsort, keep.get() + ntt, ng * sizeof(zdc),
+                                    cudaMemcpyDeviceToDevice, s));
+        }
+      };
+      tuned_launch(ifpgh > 1 ? "k_hp2p_g" : "k_hp2p", nb, 32 * WPB, {64, 128}, [&](int bs) {
+        klaunch(p2p, div_up(nb, bs / 32), bs, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
+                L.mn[0], potsort, gradsort);
+      }, s, autotune_enabled() ? std::function<void()>(reset) : std::function<void()>());
+    };
+    if (ifpgh > 1) eval(k_hl2t<true>, k_hp2p<true>);
+    else eval(k_hl2t<false>, k_hp2p<false>);
   }
   ZF_LAUNCH_CHECK();
 }
@@ -1585,7 +1615,10 @@ void helm2d_passes_nd(const Setup2D& S, const Helm2DPrep& H, int nd, int ifcharg
         size_t sm = tc_m2l_smem(p);
         ZF_CUDA(cudaFuncSetAttribute(k_hm2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-        int grid = std::min(hi - lo + 1, 148);
+        // persistent CTAs: as many per SM as the shared memory holds (one CTA
+        // builds its next pair's operands while another's MMAs run)
+        int per_sm = std::max(1, (int)((227 * 1024) / (sm + 1024)));
+        int grid = std::min(hi - lo + 1, 148 * per_sm);
         klaunch(k_hm2l_tc, grid, 128, sm, s, lo, hi, A, H.TA, H.pairoff.get(), L.n[1].get(),
                 L.list[1].get(), L.mn[1], nc, tot, err.get());
       } else {

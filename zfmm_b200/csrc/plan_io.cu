@@ -100,7 +100,9 @@ void get_tree(File& F, DevTree& t, DevLists& L, cudaStream_t s) {
   t.mnbors = F.get_v<int32_t>(); t.nlevels = F.get_v<int32_t>(); t.nboxes = F.get_v<int32_t>();
   F.get_vec(t.laddr);
   F.get_vec(t.boxsize);
-  if (t.nboxes < 1 || t.nlevels < 0 || t.laddr.size() != 2 * (size_t)(t.nlevels + 1))
+  // the tree's arrays may be longer than nboxes / nlevels (capacity of the
+  // level-by-level build); they are stored and restored as they are
+  if (t.nboxes < 1 || t.nlevels < 0 || t.laddr.size() < 2 * (size_t)(t.nlevels + 1))
     throw zf_error(ZF_ERR_ARG, "plan file is corrupt");
   F.get_dev(t.ilevel, s); F.get_dev(t.iparent, s); F.get_dev(t.nchild, s);
   F.get_dev(t.ichild, s); F.get_dev(t.ncoll, s); F.get_dev(t.coll, s);
@@ -110,7 +112,8 @@ void get_tree(File& F, DevTree& t, DevLists& L, cudaStream_t s) {
     F.get_dev(L.n[k], s);
     F.get_dev(L.list[k], s);
   }
-  if (t.ilevel.size() != (size_t)t.nboxes) throw zf_error(ZF_ERR_ARG, "plan file is corrupt");
+  if (t.ilevel.size() < (size_t)t.nboxes || t.iparent.size() < (size_t)t.nboxes)
+    throw zf_error(ZF_ERR_ARG, "plan file is corrupt");
 }
 
 void header(File& F, uint32_t D) {
@@ -153,7 +156,7 @@ void plan2d_load(Plan2D& P, const char* path, cudaStream_t s) {
   F.get_dev(S.isrc, s); F.get_dev(S.isrcse, s); F.get_dev(S.itarg, s); F.get_dev(S.itargse, s);
   F.get_dev(S.zsrcsort, s); F.get_dev(S.ztargsort, s);
   F.get_dev(S.zcsrc, s); F.get_dev(S.zctarg, s);
-  if (S.isrc.size() != (size_t)P.ns || S.itarg.size() != (size_t)P.nt)
+  if (S.isrc.size() < (size_t)P.ns || S.itarg.size() < (size_t)P.nt)
     throw zf_error(ZF_ERR_ARG, "plan file is corrupt");
 }
 
@@ -184,7 +187,7 @@ void plan3d_load(Plan3D& P, const char* path, cudaStream_t s) {
   F.get_dev(S.zcsrc, s); F.get_dev(S.zctarg, s);
   S.b0 = F.get_v<double>();
   F.get_vec(S.bsz);
-  if (S.isrc.size() != (size_t)P.ns || S.itarg.size() != (size_t)P.nt)
+  if (S.isrc.size() < (size_t)P.ns || S.itarg.size() < (size_t)P.nt)
     throw zf_error(ZF_ERR_ARG, "plan file is corrupt");
 }
 
