@@ -550,7 +550,8 @@ def run_ours(args, wl, ws, rank, local):
         tt = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_tot = float(tt.item())
-    h2d = hz.nbytes * 2 + hq.nbytes + (hds.nbytes + hdv.nbytes if ifd else 0)  # zsrc, ztarg
+    # targets are the sources (one array): the coordinates are uploaded once
+    h2d = hz.nbytes + hq.nbytes + (hds.nbytes + hdv.nbytes if ifd else 0)
     d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
     # accuracy against the FP64 direct sum on a seeded subset of targets (device direct sum)
     pg = pot.cpu().numpy()
@@ -835,7 +836,7 @@ def run_ours_batched(args, wl, ws, rank, local, summary=False):
         tt = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_tot = float(tt.item())
-    h2d = 2 * hz.nbytes + hq.nbytes + (hds.nbytes + hdv.nbytes if ifd else 0)
+    h2d = hz.nbytes + hq.nbytes + (hds.nbytes + hdv.nbytes if ifd else 0)
     d2h = hpot.nbytes + (hgrad.nbytes if ifpgh > 1 else 0)
     # accuracy: right-hand sides 0 and nd-1 against the FP64 direct sum on a subset
     rng = np.random.default_rng(1234)
@@ -1033,7 +1034,7 @@ def run_ours_batched2d(args, wl, ws, rank, local):
     for k in range(args.steps):
         solve_host()
     e2e_s = time.perf_counter() - t0
-    h2d = 2 * hz.nbytes + hq.nbytes + hds.nbytes + hdv.nbytes
+    h2d = hz.nbytes + hq.nbytes + hds.nbytes + hdv.nbytes
     d2h = hpot.nbytes + hgrad.nbytes
     # accuracy: right-hand sides 0 and nd-1 against the FP64 direct sum, and
     # against the single FP64 solve of right-hand side 0
@@ -1194,7 +1195,7 @@ def run_ours_many(args, wl, ws, rank, local):
                                     H["v"], hp(ns), H["zs"], ifpgh, isep, H["p"], H["g"], nst,
                                     hp(done)))
     e2e_s = time.perf_counter() - t0
-    h2d = sum(a.nbytes for a in hz) * 2 + sum(a.nbytes for a in hq + hd + hv)
+    h2d = sum(a.nbytes for a in hz) + sum(a.nbytes for a in hq + hd + hv)  # targets = sources
     d2h = sum(a.nbytes for a in hpo + hgr)
     # accuracy: the largest instance against the FP64 direct sum on 1024 targets
     big = int(np.argmax(sizes))

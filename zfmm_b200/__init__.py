@@ -92,7 +92,7 @@ def _fmm2d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, zt
                             ztarg, ifpgh, isep)
     ns, nt = int(ns), int(nt)
     zs = _pts(zsrc, 2, ns, "zsrc")
-    zt = _pts(ztarg, 2, nt, "ztarg")
+    zt = zs if ztarg is zsrc and nt == ns else _pts(ztarg, 2, nt, "ztarg")
     q = _vec(charge, ns, "charge") if ifcharge == 1 else None
     ds = _vec(dipstr, ns, "dipstr") if ifdipole == 1 else None
     dv = _pts(dipvec, 2, ns, "dipvec") if ifdipole == 1 else None
@@ -137,7 +137,7 @@ def _fmm2d_torch(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, 
     import torch
     zs = _torch_pts(zsrc, 2, ns, "zsrc")
     dev = zs.device
-    zt = _torch_pts(ztarg, 2, nt, "ztarg", dev)
+    zt = zs if ztarg is zsrc and nt == ns else _torch_pts(ztarg, 2, nt, "ztarg", dev)
     q = _torch_vec(charge, ns, "charge", dev) if ifcharge == 1 else None
     ds = _torch_vec(dipstr, ns, "dipstr", dev) if ifdipole == 1 else None
     dv = _torch_pts(dipvec, 2, ns, "dipvec", dev) if ifdipole == 1 else None
@@ -193,7 +193,8 @@ def _fmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, zt
     if _is_torch(zsrc):
         import torch
         zs = _torch_pts(zsrc, 3, ns, "zsrc")
-        zt = _torch_pts(ztarg, 3, nt, "ztarg", zs.device)
+        zt = (zs if ztarg is zsrc and nt == ns
+              else _torch_pts(ztarg, 3, nt, "ztarg", zs.device))
         q = _torch_vec(charge, ns, "charge", zs.device) if ifcharge == 1 else None
         ds = _torch_vec(dipstr, ns, "dipstr", zs.device) if ifdipole == 1 else None
         dv = _torch_pts(dipvec, 3, ns, "dipvec", zs.device) if ifdipole == 1 else None
@@ -213,7 +214,7 @@ def _fmm3d(eps, zk, ns, zsrc, ifcharge, charge, ifdipole, dipstr, dipvec, nt, zt
         return pot, grad.t()
     ns, nt = int(ns), int(nt)
     zs = _pts(zsrc, 3, ns, "zsrc")
-    zt = _pts(ztarg, 3, nt, "ztarg")
+    zt = zs if ztarg is zsrc and nt == ns else _pts(ztarg, 3, nt, "ztarg")
     q = _vec(charge, ns, "charge") if ifcharge == 1 else None
     ds = _vec(dipstr, ns, "dipstr") if ifdipole == 1 else None
     dv = _pts(dipvec, 3, ns, "dipvec") if ifdipole == 1 else None
@@ -311,7 +312,8 @@ class _Plan:
         if _is_torch(zsrc):
             import torch
             zs = _torch_pts(zsrc, d, self.ns, "zsrc")
-            zt = _torch_pts(ztarg, d, self.nt, "ztarg", zs.device)
+            zt = (zs if ztarg is zsrc and self.nt == self.ns
+                  else _torch_pts(ztarg, d, self.nt, "ztarg", zs.device))
             self.device = zs.device
             stream = ctypes.c_void_p(torch.cuda.current_stream(zs.device).cuda_stream)
             check(getattr(lib(), self._fn["create_dev"])(
@@ -320,7 +322,7 @@ class _Plan:
         else:
             self.device = None
             zs = _pts(zsrc, d, self.ns, "zsrc")
-            zt = _pts(ztarg, d, self.nt, "ztarg")
+            zt = zs if ztarg is zsrc and self.nt == self.ns else _pts(ztarg, d, self.nt, "ztarg")
             check(getattr(lib(), self._fn["create"])(self.eps, self.ns, _ptr(zs), self.nt,
                                                      _ptr(zt), int(isep), ctypes.byref(self._h)))
 

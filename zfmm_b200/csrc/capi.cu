@@ -184,8 +184,10 @@ int fmm2d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
     check_device();
     cudaStream_t s = cudaStreamPerThread;
     HostIn h;
+    // targets passed as the source array itself: uploaded once
+    const bool same = ztarg == zsrc && nt == ns;
     upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
-    upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
+    if (!same) upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
     if (ifcharge == 1) upload(h.charge, charge, ns, s);
     if (ifdipole == 1) {
       upload(h.dipstr, dipstr, ns, s);
@@ -195,7 +197,7 @@ int fmm2d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
     Inputs2D in = make_inputs(ns, (const double*)h.zsrc.get(), ifcharge,
                               (const double*)h.charge.get(), ifdipole,
                               (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
-                              (const double*)h.ztarg.get(), ifpgh);
+                              (const double*)(same ? h.zsrc.get() : h.ztarg.get()), ifpgh);
     run_fmm2d(eps, zk, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
@@ -587,8 +589,10 @@ int fmm3d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
     check_device();
     cudaStream_t s = cudaStreamPerThread;
     HostIn h;
+    // targets passed as the source array itself: uploaded once
+    const bool same = ztarg == zsrc && nt == ns;
     upload(h.zsrc, zsrc, 3 * (size_t)ns, s);
-    upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
+    if (!same) upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
     if (ifcharge == 1) upload(h.charge, charge, ns, s);
     if (ifdipole == 1) {
       upload(h.dipstr, dipstr, ns, s);
@@ -598,7 +602,7 @@ int fmm3d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
     Inputs3D in = make_inputs3(ns, (const double*)h.zsrc.get(), ifcharge,
                                (const double*)h.charge.get(), ifdipole,
                                (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
-                               (const double*)h.ztarg.get(), ifpgh);
+                               (const double*)(same ? h.zsrc.get() : h.ztarg.get()), ifpgh);
     run_fmm3d(eps, zk, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
@@ -883,10 +887,12 @@ int plan3d_create_impl(double eps, int ns, const double* zsrc, int nt, const dou
       const zdc* zt = reinterpret_cast<const zdc*>(ztarg);
       if (!host) check_align16({zsrc, ztarg});
       if (host) {
+        // targets passed as the source array itself: uploaded once
+        const bool same = ztarg == zsrc && nt == ns;
         upload(h.zsrc, zsrc, 3 * (size_t)ns, s);
-        upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
+        if (!same) upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
         zs = h.zsrc.get();
-        zt = h.ztarg.get();
+        zt = same ? zs : h.ztarg.get();
       }
       if (ns > 0 && nt > 0) plan3d_build(pl->P, eps, ns, zs, nt, zt, isep, s);
       else {
@@ -1081,8 +1087,9 @@ void run_many(const ManyArgs& M, int nworkers, double* done_ms) {
         const int ns = M.ns[i], nt = M.nt[i];
         if (M.host) {
           HostIn h;
+          const bool same = M.ztarg[i] == M.zsrc[i] && nt == ns;  // uploaded once
           upload(h.zsrc, M.zsrc[i], 3 * (size_t)ns, s);
-          upload(h.ztarg, M.ztarg[i], 3 * (size_t)nt, s);
+          if (!same) upload(h.ztarg, M.ztarg[i], 3 * (size_t)nt, s);
           if (M.ifcharge == 1) upload(h.charge, M.charge[i], ns, s);
           if (M.ifdipole == 1) {
             upload(h.dipstr, M.dipstr[i], ns, s);
@@ -1092,7 +1099,8 @@ void run_many(const ManyArgs& M, int nworkers, double* done_ms) {
           Inputs3D in = make_inputs3(ns, (const double*)h.zsrc.get(), M.ifcharge,
                                      (const double*)h.charge.get(), M.ifdipole,
                                      (const double*)h.dipstr.get(), (const double*)h.dipvec.get(),
-                                     nt, (const double*)h.ztarg.get(), M.ifpgh);
+                                     nt, (const double*)(same ? h.zsrc.get() : h.ztarg.get()),
+                                     M.ifpgh);
           run_fmm3d(M.eps, M.zk, in, M.isep, dpot.get(), M.ifpgh > 1 ? dgrad.get() : nullptr, s);
           if (nt > 0) {
             ZF_CUDA(cudaMemcpyAsync(M.pot[i], dpot.get(), sizeof(zdc) * nt,
@@ -1240,10 +1248,12 @@ int plan2d_create_impl(double eps, int ns, const double* zsrc, int nt, const dou
       const zdc* zt = reinterpret_cast<const zdc*>(ztarg);
       if (!host) check_align16({zsrc, ztarg});
       if (host) {
+        // targets passed as the source array itself: uploaded once
+        const bool same = ztarg == zsrc && nt == ns;
         upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
-        upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
+        if (!same) upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
         zs = h.zsrc.get();
-        zt = h.ztarg.get();
+        zt = same ? zs : h.ztarg.get();
       }
       if (ns > 0 && nt > 0) plan2d_build(pl->P, eps, ns, zs, nt, zt, isep, s);
       else {

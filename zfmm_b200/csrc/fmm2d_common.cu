@@ -210,15 +210,33 @@ void count_interactions2d(const Setup2D& S, const int* p_per_level, unsigned lon
   ZF_CUDA(cudaStreamSynchronize(s));
 }
 
+// copy of a device buffer on stream s
+template <class T>
+void copy_buf(DevBuf<T>& dst, const DevBuf<T>& src, cudaStream_t s) {
+  dst.alloc(src.size(), s);
+  if (src.size())
+    ZF_CUDA(cudaMemcpyAsync(dst.get(), src.get(), src.size() * sizeof(T),
+                            cudaMemcpyDeviceToDevice, s));
+}
+
 void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t s) {
   int ns = in.ns, nt = in.nt;
-  DevBuf<double> srcR(2 * (size_t)ns, s), targR(2 * (size_t)nt, s);
+  // targets that are the sources (the same array) share the sources' tree
+  // assignment and order: computed once, copied
+  const bool same = in.ztarg == in.zsrc && nt == ns;
+  DevBuf<double> srcR(2 * (size_t)ns, s), targR(same ? 0 : 2 * (size_t)nt, s);
   klaunch(k_real_parts, div_up(2L * ns, TB), TB, 0, s, in.zsrc, 2L * ns, srcR.get());
-  klaunch(k_real_parts, div_up(2L * nt, TB), TB, 0, s, in.ztarg, 2L * nt, targR.get());
+  if (!same) klaunch(k_real_parts, div_up(2L * nt, TB), TB, 0, s, in.ztarg, 2L * nt, targR.get());
   ZF_LAUNCH_CHECK();
-  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
-  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  const double* tR = same ? srcR.get() : targR.get();
+  build_tree(srcR.get(), ns, tR, nt, tp, S.tree, s);
   sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  if (same) {
+    copy_buf(S.itarg, S.isrc, s);
+    copy_buf(S.itargse, S.isrcse, s);
+  } else {
+    sort_points(S.tree, tR, nt, S.itarg, S.itargse, s);
+  }
   S.zsrcsort.alloc(2 * (size_t)ns, s);
   S.chargesort.alloc(ns, s);
   S.dipstrsort.alloc(ns, s);
@@ -231,26 +249,35 @@ void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t 
   klaunch(k_gather_targ, div_up(nt, TB), TB, 0, s, nt, S.itarg.get(), in.ztarg, S.ztargsort.get());
   ZF_LAUNCH_CHECK();
   complex_centres(S.tree, S.isrcse, S.zsrcsort, S.zcsrc, s);
-  complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
+  if (same) copy_buf(S.zctarg, S.zcsrc, s);
+  else complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
   build_lists(S.tree, S.lists, s);
 }
 
 void setup2d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
                   Setup2D& S, cudaStream_t s) {
-  DevBuf<double> srcR(2 * (size_t)ns, s), targR(2 * (size_t)nt, s);
+  const bool same = ztarg == zsrc && nt == ns;
+  DevBuf<double> srcR(2 * (size_t)ns, s), targR(same ? 0 : 2 * (size_t)nt, s);
   klaunch(k_real_parts, div_up(2L * ns, TB), TB, 0, s, zsrc, 2L * ns, srcR.get());
-  klaunch(k_real_parts, div_up(2L * nt, TB), TB, 0, s, ztarg, 2L * nt, targR.get());
+  if (!same) klaunch(k_real_parts, div_up(2L * nt, TB), TB, 0, s, ztarg, 2L * nt, targR.get());
   ZF_LAUNCH_CHECK();
-  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
-  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  const double* tR = same ? srcR.get() : targR.get();
+  build_tree(srcR.get(), ns, tR, nt, tp, S.tree, s);
   sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  if (same) {
+    copy_buf(S.itarg, S.isrc, s);
+    copy_buf(S.itargse, S.isrcse, s);
+  } else {
+    sort_points(S.tree, tR, nt, S.itarg, S.itargse, s);
+  }
   S.zsrcsort.alloc(2 * (size_t)ns, s);
   S.ztargsort.alloc(2 * (size_t)nt, s);
   klaunch(k_gather_targ, div_up(ns, TB), TB, 0, s, ns, S.isrc.get(), zsrc, S.zsrcsort.get());
   klaunch(k_gather_targ, div_up(nt, TB), TB, 0, s, nt, S.itarg.get(), ztarg, S.ztargsort.get());
   ZF_LAUNCH_CHECK();
   complex_centres(S.tree, S.isrcse, S.zsrcsort, S.zcsrc, s);
-  complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
+  if (same) copy_buf(S.zctarg, S.zcsrc, s);
+  else complex_centres(S.tree, S.itargse, S.ztargsort, S.zctarg, s);
   build_lists(S.tree, S.lists, s);
 }
 

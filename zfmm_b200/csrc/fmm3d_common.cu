@@ -192,15 +192,33 @@ void unsort3d_col(int nt, int nd, int r, const int* itarg, const zdc* potsort,
   ZF_LAUNCH_CHECK();
 }
 
+// copy of a device buffer on stream s
+template <class T>
+static void copy_buf3(DevBuf<T>& dst, const DevBuf<T>& src, cudaStream_t s) {
+  dst.alloc(src.size(), s);
+  if (src.size())
+    ZF_CUDA(cudaMemcpyAsync(dst.get(), src.get(), src.size() * sizeof(T),
+                            cudaMemcpyDeviceToDevice, s));
+}
+
 void setup3d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeParams& tp,
                   Setup3D& S, cudaStream_t s) {
-  DevBuf<double> srcR(3 * (size_t)ns, s), targR(3 * (size_t)nt, s);
+  // targets that are the sources (the same array) share the sources' tree
+  // assignment, order and centres: computed once, copied
+  const bool same = ztarg == zsrc && nt == ns;
+  DevBuf<double> srcR(3 * (size_t)ns, s), targR(same ? 0 : 3 * (size_t)nt, s);
   klaunch(k_real3, div_up(3L * ns, TB), TB, 0, s, zsrc, 3L * ns, srcR.get());
-  klaunch(k_real3, div_up(3L * nt, TB), TB, 0, s, ztarg, 3L * nt, targR.get());
+  if (!same) klaunch(k_real3, div_up(3L * nt, TB), TB, 0, s, ztarg, 3L * nt, targR.get());
   ZF_LAUNCH_CHECK();
-  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
-  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  const double* tR = same ? srcR.get() : targR.get();
+  build_tree(srcR.get(), ns, tR, nt, tp, S.tree, s);
   sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  if (same) {
+    copy_buf3(S.itarg, S.isrc, s);
+    copy_buf3(S.itargse, S.isrcse, s);
+  } else {
+    sort_points(S.tree, tR, nt, S.itarg, S.itargse, s);
+  }
   S.b0 = S.tree.boxsize[0];
   const double* b0 = S.tree.bsz.get();
   S.zsrcsort.alloc(3 * (size_t)ns, s);
@@ -210,7 +228,8 @@ void setup3d_geom(int ns, const zdc* zsrc, int nt, const zdc* ztarg, const TreeP
           S.ztargsort.get());
   ZF_LAUNCH_CHECK();
   centres3(S.tree, S.isrcse, S.zsrcsort, b0, S.zcsrc, s);
-  centres3(S.tree, S.itargse, S.ztargsort, b0, S.zctarg, s);
+  if (same) copy_buf3(S.zctarg, S.zcsrc, s);
+  else centres3(S.tree, S.itargse, S.ztargsort, b0, S.zctarg, s);
   build_lists(S.tree, S.lists, s);
   S.bsz.resize(S.tree.nlevels + 1);
   for (int l = 0; l <= S.tree.nlevels; l++) S.bsz[l] = S.tree.boxsize[l] / S.b0;
@@ -237,13 +256,22 @@ void unsort3d_nd(int nt, int nd, const int* itarg, const zdc* potsort, const zdc
 void setup3d(const Inputs3D& in, const TreeParams& tp, Setup3D& S, bool rescale_charge,
              bool rescale_dipvec, cudaStream_t s) {
   int ns = in.ns, nt = in.nt;
-  DevBuf<double> srcR(3 * (size_t)ns, s), targR(3 * (size_t)nt, s);
+  // targets that are the sources (the same array) share the sources' tree
+  // assignment, order and centres: computed once, copied
+  const bool same = in.ztarg == in.zsrc && nt == ns;
+  DevBuf<double> srcR(3 * (size_t)ns, s), targR(same ? 0 : 3 * (size_t)nt, s);
   klaunch(k_real3, div_up(3L * ns, TB), TB, 0, s, in.zsrc, 3L * ns, srcR.get());
-  klaunch(k_real3, div_up(3L * nt, TB), TB, 0, s, in.ztarg, 3L * nt, targR.get());
+  if (!same) klaunch(k_real3, div_up(3L * nt, TB), TB, 0, s, in.ztarg, 3L * nt, targR.get());
   ZF_LAUNCH_CHECK();
-  build_tree(srcR.get(), ns, targR.get(), nt, tp, S.tree, s);
-  sort_points(S.tree, targR.get(), nt, S.itarg, S.itargse, s);
+  const double* tR = same ? srcR.get() : targR.get();
+  build_tree(srcR.get(), ns, tR, nt, tp, S.tree, s);
   sort_points(S.tree, srcR.get(), ns, S.isrc, S.isrcse, s);
+  if (same) {
+    copy_buf3(S.itarg, S.isrc, s);
+    copy_buf3(S.itargse, S.isrcse, s);
+  } else {
+    sort_points(S.tree, tR, nt, S.itarg, S.itargse, s);
+  }
   S.b0 = S.tree.boxsize[0];
   const double* b0 = S.tree.bsz.get();  // device copy of boxsize; entry 0 = b0
   S.zsrcsort.alloc(3 * (size_t)ns, s);
@@ -260,7 +288,8 @@ void setup3d(const Inputs3D& in, const TreeParams& tp, Setup3D& S, bool rescale_
           S.ztargsort.get());
   ZF_LAUNCH_CHECK();
   centres3(S.tree, S.isrcse, S.zsrcsort, b0, S.zcsrc, s);
-  centres3(S.tree, S.itargse, S.ztargsort, b0, S.zctarg, s);
+  if (same) copy_buf3(S.zctarg, S.zcsrc, s);
+  else centres3(S.tree, S.itargse, S.ztargsort, b0, S.zctarg, s);
   build_lists(S.tree, S.lists, s);
   S.bsz.resize(S.tree.nlevels + 1);
   for (int l = 0; l <= S.tree.nlevels; l++) S.bsz[l] = S.tree.boxsize[l] / S.b0;

@@ -639,7 +639,8 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
   ZF_LAUNCH_CHECK();
   std::vector<double> bsz(p.nlmax + 2, 0.0);
   ZF_CUDA(cudaMemcpyAsync(bsz.data(), d_bs0.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
-  DevBuf<int> pbs(ns, s), pbt(nt, s);
+  const bool same = d_targ == d_src && nt == ns;
+  DevBuf<int> pbs(ns, s), pbt(same ? 0 : nt, s);
   pbs.zero();
   pbt.zero();
   ZF_CUDA(cudaStreamSynchronize(s));
@@ -666,9 +667,12 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
         B.nsrc.get(), B.ntarg.get());
     klaunch(k_assign<D>, div_up(ns, TB), TB, 0, s, d_src, ns, pbs.get(), B.ilevel.get(), B.nchild.get(),
                                               B.ichild.get(), B.centers.get(), ilev, B.nsrc.get());
-    klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, d_targ, nt, pbt.get(), B.ilevel.get(),
-                                              B.nchild.get(), B.ichild.get(), B.centers.get(), ilev,
-                                              B.ntarg.get());
+    if (same)  // targets are the sources: the same children, the same counts
+      ZF_CUDA(cudaMemcpyAsync(B.ntarg.get() + n, B.nsrc.get() + n, sizeof(int) * nref * NC,
+                              cudaMemcpyDeviceToDevice, s));
+    else
+      klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, d_targ, nt, pbt.get(), B.ilevel.get(),
+              B.nchild.get(), B.ichild.get(), B.centers.get(), ilev, B.ntarg.get());
     ZF_LAUNCH_CHECK();
     laddr[2 * (ilev + 1)] = n;
     laddr[2 * (ilev + 1) + 1] = n + nref * NC - 1;
