@@ -17,6 +17,8 @@
 //   * new boxes are numbered by an exclusive scan of the refine flags of the
 //     level, i.e. children of the r-th refined box get ids nbctr + r*NC + c,
 //     which is the reference's cumsum numbering;
+//   * the per-level point-to-child assignment runs over a Z-ordered copy of
+//     the points (the counts it produces do not depend on the order);
 //   * the final point order of pts_tree_sort (a stable recursive partition) is
 //     the order of a stable sort of the points by the start offset of their
 //     leaf, with leaf offsets from a bottom-up count and a top-down prefix in
@@ -147,6 +149,23 @@ __global__ void k_gt0(const int* in, int n, int* out) {
   if (i < n) out[i] = in[i] > 0 ? 1 : 0;
 }
 
+// 0/1 flags of the concatenation of in[lo1, lo1+n1) and in[lo2, lo2+n2)
+__global__ void k_gt0_2(const int* in, int lo1, int n1, int lo2, int n2, int* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n1 + n2) return;
+  out[i] = in[i < n1 ? lo1 + i : lo2 + (i - n1)] > 0 ? 1 : 0;
+}
+
+// exclusive prefix of the flags at positions pos[0, np); a position equal to
+// the length n gives the total
+__global__ void k_pick(const int* flag, const int* rank, int n, const int* pos, int np,
+                       int* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= np) return;
+  int p = pos[k];
+  out[k] = p < n ? rank[p] : (n > 0 ? rank[n - 1] + flag[n - 1] : 0);
+}
+
 // children of every flagged box of [lo, lo+nb): ids first + rank*NC + c.
 // flagmode: children of iflag==1 parents become flag++ (3), of iflag==2 become 0
 // (tree_refine_boxes_flag); otherwise plain refinement.
@@ -203,6 +222,47 @@ __global__ void k_assign(const double* __restrict__ pts, int n, int* __restrict_
   // point, so the counters of the few coarse boxes are not serialised
   unsigned grp = __match_any_sync(__activemask(), j);
   if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&cnt[j], __popc(grp));
+}
+
+// ---- Z-order of the points for the assignment passes -------------------------
+// Key of a point: its coordinates relative to the root box, quantised to BITS
+// bits each and interleaved (Z order), so that the points of one box of any
+// level down to BITS are contiguous in key order, up to rounding at the box
+// faces.  The level-by-level assignment runs over the points in this order:
+// warps then read coalesced coordinates, look up one or two boxes and add to
+// one or two counters.  Box counts do not depend on the order, so the tree is
+// the same as in input order; the final point order (sort_points) is taken in
+// input order.
+template <int D>
+__global__ void k_zkey(const double* __restrict__ pts, int n, const double* __restrict__ centers,
+                       const double* __restrict__ bs0, unsigned long long* __restrict__ key,
+                       int* __restrict__ idx) {
+  constexpr int BITS = D == 2 ? 31 : 21;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double b = *bs0, top = (double)((1u << BITS) - 1);
+  const double sc = b > 0 ? ldexp(1.0, BITS) / b : 0.0;
+  unsigned long long k = 0;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    double u = (pts[(long)i * D + d] - (centers[d] - 0.5 * b)) * sc;
+    u = u < 0 ? 0.0 : (u > top ? top : u);
+    unsigned long long q = (unsigned long long)u;
+#pragma unroll
+    for (int bit = 0; bit < BITS; bit++) k |= ((q >> bit) & 1ull) << (bit * D + d);
+  }
+  key[i] = k;
+  idx[i] = i;
+}
+
+template <int D>
+__global__ void k_gather_pts(const double* __restrict__ pts, const int* __restrict__ idx, int n,
+                             double* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j = idx[i];
+#pragma unroll
+  for (int d = 0; d < D; d++) out[(long)i * D + d] = pts[(long)j * D + d];
 }
 
 // ---- colleagues --------------------------------------------------------------
@@ -516,6 +576,28 @@ struct Scanner {
     ZF_CUDA(cudaStreamSynchronize(s));
     return *h_total;
   }
+  // flags01/rank over the concatenation of src[lo1, lo1+n1) and
+  // src[lo2, lo2+n2) in one scan; returns the exclusive prefix at each of
+  // `pos` (a position n1+n2 gives the total), with one wait for the host
+  std::vector<int> scan_at(const int* src, int lo1, int n1, int lo2, int n2,
+                           const std::vector<int>& pos) {
+    const int n = n1 + n2, np = (int)pos.size();
+    std::vector<int> out(np, 0);
+    if (n <= 0 || np == 0) return out;
+    if ((int)flag01.size() < n) { flag01.alloc(n, s); rank.alloc(n, s); }
+    klaunch(k_gt0_2, div_up(n, TB), TB, 0, s, src, lo1, n1, lo2, n2, flag01.get());
+    size_t bytes = 0;
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag01.get(), rank.get(), n, s));
+    if (tmp.size() < bytes) tmp.alloc(bytes, s);
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, flag01.get(), rank.get(), n, s));
+    DevBuf<int> dpos(np, s), dout(np, s);
+    ZF_CUDA(cudaMemcpyAsync(dpos.get(), pos.data(), np * sizeof(int), cudaMemcpyHostToDevice, s));
+    klaunch(k_pick, div_up(np, TB), TB, 0, s, flag01.get(), rank.get(), n, dpos.get(), np,
+            dout.get());
+    ZF_CUDA(cudaMemcpyAsync(out.data(), dout.get(), np * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaStreamSynchronize(s));
+    return out;
+  }
 };
 
 struct BoxArrays {
@@ -555,21 +637,30 @@ void colleagues_all(BoxArrays& B, int nlevels, const std::vector<int>& laddr,
   ZF_LAUNCH_CHECK();
 }
 
-// subdivide the flagged boxes (iflag>0) of [lo,hi]; returns number of new boxes
+// subdivide the flagged boxes (iflag>0) of [lo,hi] and then of [tlo,thi] (the
+// children of the second range numbered after those of the first, as two
+// successive refinements would number them), with one scan; returns the
+// number of new boxes
 template <int D>
-int refine_flag_range(BoxArrays& B, Scanner& S, int& n, int lo, int hi, double bs, int ilev,
-                      DevBuf<int>& ncoll, DevBuf<int>& coll, int mnbors, cudaStream_t s) {
+int refine_flag_ranges(BoxArrays& B, Scanner& S, int& n, int lo, int hi, int tlo, int thi,
+                       double bs, int ilev, DevBuf<int>& ncoll, DevBuf<int>& coll, int mnbors,
+                       cudaStream_t s) {
   constexpr int NC = 1 << D;
-  if (hi < lo) return 0;
-  int nb = hi - lo + 1;
-  int nref = S.scan(B.iflag.get() + lo, nb);
+  const int nb1 = hi >= lo ? hi - lo + 1 : 0, nb2 = thi >= tlo ? thi - tlo + 1 : 0;
+  if (nb1 + nb2 == 0) return 0;
+  const int nref = S.scan_at(B.iflag.get(), lo, nb1, tlo, nb2, {nb1 + nb2})[0];
   if (nref == 0) return 0;
   B.reserve((size_t)n + (size_t)nref * NC, n);
   ncoll.grow(B.cap, n);
   coll.grow(B.cap * mnbors, (size_t)n * mnbors);
-  klaunch(k_make_children<D>, div_up(nb, TB), TB, 0, s, 
-      lo, nb, S.flag01.get(), S.rank.get(), n, bs, ilev + 1, 1, B.centers.get(), B.ilevel.get(),
-      B.iparent.get(), B.nchild.get(), B.ichild.get(), B.iflag.get(), nullptr, nullptr);
+  if (nb1 > 0)
+    klaunch(k_make_children<D>, div_up(nb1, TB), TB, 0, s, lo, nb1, S.flag01.get(),
+            S.rank.get(), n, bs, ilev + 1, 1, B.centers.get(), B.ilevel.get(), B.iparent.get(),
+            B.nchild.get(), B.ichild.get(), B.iflag.get(), nullptr, nullptr);
+  if (nb2 > 0)
+    klaunch(k_make_children<D>, div_up(nb2, TB), TB, 0, s, tlo, nb2, S.flag01.get() + nb1,
+            S.rank.get() + nb1, n, bs, ilev + 1, 1, B.centers.get(), B.ilevel.get(),
+            B.iparent.get(), B.nchild.get(), B.ichild.get(), B.iflag.get(), nullptr, nullptr);
   ZF_LAUNCH_CHECK();
   n += nref * NC;
   return nref * NC;
@@ -613,6 +704,25 @@ void reorg(BoxArrays& B, int n, int nlevels, std::vector<int>& laddr, const std:
   ZF_CUDA(cudaStreamSynchronize(s));  // d_info host vector lifetime
 }
 
+// copy of the n points of pts in Z order within the root box (k_zkey)
+template <int D>
+void zorder_copy(const double* pts, int n, const double* centers, const double* bs0,
+                 DevBuf<double>& out, cudaStream_t s) {
+  constexpr int BITS = D == 2 ? 31 : 21;
+  DevBuf<unsigned long long> key(n, s), key2(n, s);
+  DevBuf<int> idx(n, s), idx2(n, s);
+  klaunch(k_zkey<D>, div_up(n, TB), TB, 0, s, pts, n, centers, bs0, key.get(), idx.get());
+  size_t bytes = 0;
+  ZF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key.get(), key2.get(), idx.get(),
+                                          idx2.get(), n, 0, BITS * D, s));
+  DevBuf<char> tmp(bytes, s);
+  ZF_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, key.get(), key2.get(), idx.get(),
+                                          idx2.get(), n, 0, BITS * D, s));
+  out.alloc((size_t)n * D, s);
+  klaunch(k_gather_pts<D>, div_up(n, TB), TB, 0, s, pts, idx2.get(), n, out.get());
+  ZF_LAUNCH_CHECK();
+}
+
 template <int D>
 void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, const TreeParams& p,
                   DevTree& t, cudaStream_t s) {
@@ -648,6 +758,12 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
   // built (the reference would loop or divide by it), so the call is refused
   if (!std::isfinite(bsz[0]))
     throw zf_error(ZF_ERR_ARG, "coordinates must be finite (NaN or Inf in a real part)");
+  // the assignment passes run over Z-ordered copies of the points
+  DevBuf<double> zs_src, zs_targ;
+  zorder_copy<D>(d_src, ns, B.centers.get(), d_bs0.get(), zs_src, s);
+  if (!same) zorder_copy<D>(d_targ, nt, B.centers.get(), d_bs0.get(), zs_targ, s);
+  const double* a_src = zs_src.get();
+  const double* a_targ = same ? a_src : zs_targ.get();
 
   std::vector<int> laddr(2 * (p.nlmax + 1), 0);
   laddr[0] = 0;
@@ -665,13 +781,13 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
         lo, nb, S.flag01.get(), S.rank.get(), n, bsz[ilev + 1], ilev + 1, 0, B.centers.get(),
         B.ilevel.get(), B.iparent.get(), B.nchild.get(), B.ichild.get(), B.iflag.get(),
         B.nsrc.get(), B.ntarg.get());
-    klaunch(k_assign<D>, div_up(ns, TB), TB, 0, s, d_src, ns, pbs.get(), B.ilevel.get(), B.nchild.get(),
+    klaunch(k_assign<D>, div_up(ns, TB), TB, 0, s, a_src, ns, pbs.get(), B.ilevel.get(), B.nchild.get(),
                                               B.ichild.get(), B.centers.get(), ilev, B.nsrc.get());
     if (same)  // targets are the sources: the same children, the same counts
       ZF_CUDA(cudaMemcpyAsync(B.ntarg.get() + n, B.nsrc.get() + n, sizeof(int) * nref * NC,
                               cudaMemcpyDeviceToDevice, s));
     else
-      klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, d_targ, nt, pbt.get(), B.ilevel.get(),
+      klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, a_targ, nt, pbt.get(), B.ilevel.get(),
               B.nchild.get(), B.ichild.get(), B.centers.get(), ilev, B.ntarg.get());
     ZF_LAUNCH_CHECK();
     laddr[2 * (ilev + 1)] = n;
@@ -682,6 +798,8 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
   laddr.resize(2 * (nlevels + 1));
   pbs.release();
   pbt.release();
+  zs_src.release();
+  zs_targ.release();
 
   DevBuf<int> ncoll(B.cap, s), coll(B.cap * mnbors, s);
   colleagues_all<D>(B, nlevels, laddr, bsz, p.isep, mnbors, ncoll, coll, s);
@@ -710,11 +828,33 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
     ZF_LAUNCH_CHECK();
     std::vector<int> tail(2 * (nlevels + 1));
     for (int l = 0; l <= nlevels; l++) { tail[2 * l] = 0; tail[2 * l + 1] = -1; }
-    for (int l = 1; l <= nlevels - 2; l++) {
-      tail[2 * (l + 1)] = n;
-      refine_flag_range<D>(B, S, n, laddr[2 * l], laddr[2 * l + 1], bsz[l + 1], l, ncoll, coll,
-                           mnbors, s);
-      tail[2 * (l + 1) + 1] = n - 1;
+    // the flagged boxes of levels 1 .. nlevels-2 are refined independently of
+    // one another (the new boxes are not flagged here): one scan over those
+    // levels' boxes, which are contiguous, numbers all of their children
+    if (nlevels - 2 >= 1) {
+      const int L0 = laddr[2], L1 = laddr[2 * (nlevels - 2) + 1], nall = L1 - L0 + 1;
+      std::vector<int> pos;
+      for (int l = 1; l <= nlevels - 2; l++) pos.push_back(laddr[2 * l] - L0);
+      pos.push_back(nall);
+      std::vector<int> r = S.scan_at(B.iflag.get(), L0, nall, 0, 0, pos);
+      const int n0 = n, tot = r.back();
+      if (tot > 0) {
+        B.reserve((size_t)n0 + (size_t)tot * NC, n0);
+        ncoll.grow(B.cap, n0);
+        coll.grow(B.cap * mnbors, (size_t)n0 * mnbors);
+      }
+      for (int l = 1; l <= nlevels - 2; l++) {
+        const int k = l - 1, lo = laddr[2 * l], nb = laddr[2 * l + 1] - lo + 1;
+        if (r[k + 1] > r[k])
+          klaunch(k_make_children<D>, div_up(nb, TB), TB, 0, s, lo, nb,
+                  S.flag01.get() + (lo - L0), S.rank.get() + (lo - L0), n0, bsz[l + 1], l + 1, 1,
+                  B.centers.get(), B.ilevel.get(), B.iparent.get(), B.nchild.get(),
+                  B.ichild.get(), B.iflag.get(), nullptr, nullptr);
+        tail[2 * (l + 1)] = n0 + NC * r[k];
+        tail[2 * (l + 1) + 1] = n0 + NC * r[k + 1] - 1;
+      }
+      ZF_LAUNCH_CHECK();
+      n = n0 + NC * tot;
     }
     reorg<D>(B, n, nlevels, laddr, tail, s);
     ncoll.grow(B.cap, 0);
@@ -737,8 +877,9 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
             tlo, thi, distest, B.nchild.get(), B.ichild.get(), B.centers.get(), ncoll.get(),
             coll.get(), mnbors, B.iflag.get());
       tail[2 * (l + 1)] = n;
-      refine_flag_range<D>(B, S, n, lo, hi, bsz[l + 1], l, ncoll, coll, mnbors, s);
-      refine_flag_range<D>(B, S, n, tlo, thi, bsz[l + 1], l, ncoll, coll, mnbors, s);
+      // the level's boxes and its tail refined with one scan: the children of
+      // the tail's boxes are numbered after those of the level's boxes
+      refine_flag_ranges<D>(B, S, n, lo, hi, tlo, thi, bsz[l + 1], l, ncoll, coll, mnbors, s);
       tail[2 * (l + 1) + 1] = n - 1;
       int nlo = tail[2 * (l + 1)], nhi = tail[2 * (l + 1) + 1];
       if (nhi >= nlo) {
