@@ -616,7 +616,6 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
   int n2c = nl2[b];
   if (n2c == 0) return;
   int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
-  double rs = A.T.rs[l];
   zdc* T = sh + (threadIdx.x >> 5) * stride;  // [2*n2+1]
   double* rp = (double*)(T + 2 * n2 + 1);     // rs^k, k = 0..n2
   zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;    // b(n), n = -p..p
@@ -876,7 +875,6 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
   if (A.itargse[2 * b + 1] < A.itargse[2 * b] || (nl2[b] == 0 && nl4[b] == 0)) return;
   if (A.itargse[2 * jb + 1] < A.itargse[2 * jb]) return;
   int n1 = A.T.p[lev + 1], n2 = A.T.p[lev], nt = n1 + n2;
-  double rs1 = A.T.rs[lev + 1], rs2 = A.T.rs[lev];
   zdc* S1 = sh + (threadIdx.x >> 5) * stride + nt;  // S1[k] = t(k) e^{ik theta}, k = -nt..nt
   zdc* S3 = S1 + nt + 1 + nt;                       // S1[k] rs1^(2|k|)
   zdc* uu = S3 + nt + 1 + n2;                       // (rs1/rs2)^|n| loc_parent(n)
@@ -1058,58 +1056,42 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
   }
 }
 
-// ---- step 3: P2P (list 1) per target leaf, added to L2T + M2T ----------------
+// ---- step 3: P2P (list 1) one thread per target, added to L2T + M2T ----------
+// Consecutive threads take consecutive sorted targets, so a warp covers one to
+// a few neighbouring leaves with similar near fields, and no lane idles for
+// want of targets in its leaf.  Each thread sums its list-1 boxes in list
+// order and their sources in sorted order.
 template <bool GRAD>
-__global__ void __launch_bounds__(32 * WPB, 3) k_hp2p(int nb, HelmArgs A, const int* nl1,
-                                                  const int* l1, int m1, zdc* potsort,
-                                                  zdc* gradsort) {
-  int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b >= nb) return;
-  int t0 = A.itargse[2 * b], t1 = A.itargse[2 * b + 1];
-  if (A.nchild[b] > 0 || t1 < t0) return;
-  int ntb = t1 - t0 + 1;
-  // P2P (zh2devaldirect) over list1: group of G lanes per target, added on top
-  int pw = 1;
-  while (pw < ntb && pw < 32) pw <<= 1;
-  int G = 32 / pw, T = 32 / G, tl = lane / G, r = lane % G;
-  int n1 = nl1[b];
+__global__ void __launch_bounds__(128, 3) k_hp2p(int nt, HelmArgs A, const int* tgtleaf,
+                                                 const int* nl1, const int* l1, int m1,
+                                                 zdc* potsort, zdc* gradsort) {
+  int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= nt) return;
+  int b = tgtleaf[ti];
+  if (b < 0) return;
   const HelmK K = helm_k(A.zk);
-  for (int base = 0; base < ntb; base += T) {
-    int ti = t0 + base + tl;
-    bool valid = base + tl < ntb;
-    zdc pot = mkz(0.0), g1 = mkz(0.0), g2 = mkz(0.0);
-    if (valid) {
-      zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
-      for (int il = 0; il < n1; il++) {
-        int jb = l1[(size_t)b * m1 + il];
-        int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
-        for (int j = s0 + r; j <= s1; j += G) {
-          zdc q = A.ifcharge ? ldz(&A.charge[j]) : mkz(0.0);
-          zdc ds = mkz(0.0), d1 = mkz(0.0), d2 = mkz(0.0);
-          if (A.ifdipole) {
-            ds = ldz(&A.dipstr[j]);
-            d1 = ldz(&A.dipvec[2 * j]);
-            d2 = ldz(&A.dipvec[2 * j + 1]);
-          }
-          helm_pair<GRAD>(K, x1, x2, ldz(&A.zsrc[2 * j]), ldz(&A.zsrc[2 * j + 1]), q, ds, d1, d2,
-                          A.ifcharge, A.ifdipole, pot, g1, g2);
-        }
+  const zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
+  zdc pot = mkz(0.0), g1 = mkz(0.0), g2 = mkz(0.0);
+  const int n1 = nl1[b];
+  for (int il = 0; il < n1; il++) {
+    int jb = l1[(size_t)b * m1 + il];
+    int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
+    for (int j = s0; j <= s1; j++) {
+      zdc q = A.ifcharge ? ldz(&A.charge[j]) : mkz(0.0);
+      zdc ds = mkz(0.0), d1 = mkz(0.0), d2 = mkz(0.0);
+      if (A.ifdipole) {
+        ds = ldz(&A.dipstr[j]);
+        d1 = ldz(&A.dipvec[2 * j]);
+        d2 = ldz(&A.dipvec[2 * j + 1]);
       }
+      helm_pair<GRAD>(K, x1, x2, ldz(&A.zsrc[2 * j]), ldz(&A.zsrc[2 * j + 1]), q, ds, d1, d2,
+                      A.ifcharge, A.ifdipole, pot, g1, g2);
     }
-    for (int o = 1; o < G; o <<= 1) {
-      pot += shfl_xor_z(pot, o);
-      if (GRAD) {
-        g1 += shfl_xor_z(g1, o);
-        g2 += shfl_xor_z(g2, o);
-      }
-    }
-    if (valid && r == 0) {
-      potsort[ti] += pot;
-      if (GRAD) {
-        gradsort[2 * ti] += g1;
-        gradsort[2 * ti + 1] += g2;
-      }
-    }
+  }
+  potsort[ti] += pot;
+  if (GRAD) {
+    gradsort[2 * ti] += g1;
+    gradsort[2 * ti + 1] += g2;
   }
 }
 
@@ -1514,7 +1496,7 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   }
   ZF_LAUNCH_CHECK();
   cmark(5);
-  // L2T + M2T one thread per target (writes), then P2P per leaf (adds)
+  // L2T + M2T one thread per target (writes), then P2P one thread per target (adds)
   const int ntt = H.nt;
   if (!(stages & ST_DOWN)) {
   } else {
@@ -1542,9 +1524,9 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
                                     cudaMemcpyDeviceToDevice, s));
         }
       };
-      tuned_launch(ifpgh > 1 ? "k_hp2p_g" : "k_hp2p", nb, 32 * WPB, {64, 128}, [&](int bs) {
-        klaunch(p2p, div_up(nb, bs / 32), bs, 0, s, nb, A, L.n[0].get(), L.list[0].get(),
-                L.mn[0], potsort, gradsort);
+      tuned_launch(ifpgh > 1 ? "k_hp2p_g" : "k_hp2p", ntt, 128, {64, 128}, [&](int bs) {
+        klaunch(p2p, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), L.n[0].get(),
+                L.list[0].get(), L.mn[0], potsort, gradsort);
       }, s, autotune_enabled() ? std::function<void()>(reset) : std::function<void()>());
     };
     if (ifpgh > 1) eval(k_hl2t<true>, k_hp2p<true>);
