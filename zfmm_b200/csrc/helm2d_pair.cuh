@@ -42,20 +42,34 @@ ZF_HD HelmK helm_k(zdc zk) {
   return K;
 }
 
-// reciprocals of k^2, k (k+1) and k for the ascending series, k = 0..40
-struct SeriesRecip {
-  double k2[41], kk1[41], k1[42];
+// Coefficients of the ascending series as power series in x = -z^2/4:
+//   J0      = sum_k a_k x^k,  a_k = 1/(k!)^2
+//   2 J1/z  = sum_k b_k x^k,  b_k = 1/(k! (k+1)!)
+//   s0      = sum_k H_k a_k x^k                       (H_k = 1 + 1/2 + ... + 1/k)
+//   s1      = sum_k (2 H_k + 1/(k+1)) b_k x^k
+// (DLMF 10.8.1-2 with the harmonic sums of the regular parts), and
+// r4_k = 1/k^4 for the choice of the number of terms, k = 0..40.
+struct SeriesCoef {
+  double a[41], b[41], c[41], d[41], r4[41];
 };
-constexpr SeriesRecip make_series_recip() {
-  SeriesRecip r{};
-  for (int k = 1; k <= 40; k++) {
-    r.k2[k] = 1.0 / (double)(k * k);
-    r.kk1[k] = 1.0 / (double)(k * (k + 1));
+constexpr SeriesCoef make_series_coef() {
+  SeriesCoef r{};
+  double a = 1.0, b = 1.0, H = 0.0;
+  for (int k = 0; k <= 40; k++) {
+    if (k >= 1) {
+      a /= (double)k * (double)k;
+      b /= (double)k * (double)(k + 1);
+      H += 1.0 / (double)k;
+      r.r4[k] = 1.0 / ((double)k * k * k * k);
+    }
+    r.a[k] = a;
+    r.b[k] = b;
+    r.c[k] = H * a;
+    r.d[k] = (2.0 * H + 1.0 / (double)(k + 1)) * b;
   }
-  for (int k = 1; k <= 41; k++) r.k1[k] = 1.0 / (double)k;
   return r;
 }
-static __constant__ SeriesRecip c_series = make_series_recip();
+static __constant__ SeriesCoef c_series = make_series_coef();
 
 template <bool GRAD>
 __device__ __forceinline__ void helm_pair(const HelmK& K, zdc x1, zdc x2, zdc y1, zdc y2, zdc q,
@@ -68,23 +82,25 @@ __device__ __forceinline__ void helm_pair(const HelmK& K, zdc x1, zdc x2, zdc y1
   if (K.near_ok && az4 < 16.0) {
     const double thr = (double)1e-16f;  // REAL*4 literal of the exclusion test
     if (!(az4 > (thr * thr) * (thr * thr))) return;
-    // ascending series in q = z^2/4 (bessel01_series with the convergence
-    // test on squared moduli)
-    zdc mq = -(0.25 * (K.zk2 * w));
-    zdc t0 = mkz(1.0), t1 = mkz(1.0);
-    zdc sj0 = t0, sj1 = t1, s0 = mkz(0.0), s1 = t1;
-    double H = 0.0;
-    for (int k = 1; k < 40; k++) {
-      t0 = (mq * t0) * c_series.k2[k];
-      t1 = (mq * t1) * c_series.kk1[k];
-      H += c_series.k1[k];
-      sj0 += t0;
-      sj1 += t1;
-      s0 += H * t0;
-      s1 += (2.0 * H + c_series.k1[k + 1]) * t1;
-      double a0 = t0.re * t0.re + t0.im * t0.im, b0 = sj0.re * sj0.re + sj0.im * sj0.im;
-      double a1 = t1.re * t1.re + t1.im * t1.im, b1 = sj1.re * sj1.re + sj1.im * sj1.im;
-      if (a0 < 1e-36 * b0 && a1 < 1e-36 * b1) break;
+    // ascending series in x = -z^2/4 with the terms k = 0..nk, nk the last k
+    // with |x|^k / (k!)^2 >= 1e-20 (the terms fall monotonically for
+    // |x| < 4), |J0| > 0.2 and |2 J1/z| > 0.5 for |z| < 2, so the first term
+    // left out is below 1e-19 of the sums
+    const zdc x = -(0.25 * (K.zk2 * w));
+    const double ax2 = x.re * x.re + x.im * x.im;
+    int nk = 0;
+    for (double tt = 1.0; nk < 39;) {  // tt = (|x|^k / (k!)^2)^2 of k = nk + 1
+      tt *= ax2 * c_series.r4[nk + 1];
+      if (tt < 1e-40) break;
+      nk++;
+    }
+    zdc sj0 = mkz(1.0), sj1 = mkz(1.0), s0 = mkz(0.0), s1 = mkz(1.0), xp = x;
+    for (int k = 1; k <= nk; k++) {
+      sj0 += c_series.a[k] * xp;
+      sj1 += c_series.b[k] * xp;
+      s0 += c_series.c[k] * xp;
+      s1 += c_series.d[k] * xp;
+      xp = xp * x;
     }
     const double c = ZF_2_PI * (ZF_EULER - ZF_LN2);
     zdc L = ZF_2_PI * (K.lzk + 0.5 * zlog_p(w));

@@ -25,6 +25,7 @@
 //     child order.  cub's radix sort is stable.
 // This file is compiled with --fmad=false so that the distance tests see the
 // same roundings as the reference (no contracted multiply-adds).
+#include <algorithm>
 #include <cmath>
 #include <cub/cub.cuh>
 #include <vector>
@@ -549,6 +550,26 @@ __global__ void k_max4(int nb, const int* a, const int* b, const int* c, const i
 }
 
 // ---- host helpers -----------------------------------------------------------
+// Page-locked host words that receive the scan results, one block per host
+// thread, allocated on the thread's first tree build and freed when the
+// thread ends: page-locking and releasing memory on every build would cost
+// milliseconds (and the release waits for the device).
+constexpr int kPinnedWords = 1024;
+struct PinnedWords {
+  int* p = nullptr;
+  ~PinnedWords() {
+    if (p) cudaFreeHost(p);
+  }
+  int* get() {
+    if (!p) ZF_CUDA(cudaMallocHost((void**)&p, kPinnedWords * sizeof(int)));
+    return p;
+  }
+};
+int* pinned_words() {
+  thread_local PinnedWords w;
+  return w.get();
+}
+
 struct Scanner {
   DevBuf<char> tmp;
   DevBuf<int> total;
@@ -557,10 +578,7 @@ struct Scanner {
   cudaStream_t s;
   explicit Scanner(cudaStream_t st) : s(st) {
     total.alloc(1, s);
-    ZF_CUDA(cudaMallocHost((void**)&h_total, sizeof(int)));
-  }
-  ~Scanner() {
-    if (h_total) cudaFreeHost(h_total);
+    h_total = pinned_words();
   }
   // flags01/rank over `src` (values > 0 count as set) of length n; returns total
   int scan(const int* src, int n) {
@@ -594,8 +612,10 @@ struct Scanner {
     ZF_CUDA(cudaMemcpyAsync(dpos.get(), pos.data(), np * sizeof(int), cudaMemcpyHostToDevice, s));
     klaunch(k_pick, div_up(np, TB), TB, 0, s, flag01.get(), rank.get(), n, dpos.get(), np,
             dout.get());
-    ZF_CUDA(cudaMemcpyAsync(out.data(), dout.get(), np * sizeof(int), cudaMemcpyDeviceToHost, s));
+    int* h = np <= kPinnedWords ? h_total : out.data();  // a level count above 1024: pageable
+    ZF_CUDA(cudaMemcpyAsync(h, dout.get(), np * sizeof(int), cudaMemcpyDeviceToHost, s));
     ZF_CUDA(cudaStreamSynchronize(s));
+    if (h != out.data()) std::copy(h, h + np, out.begin());
     return out;
   }
 };
