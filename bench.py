@@ -245,6 +245,20 @@ def flop_model(kind, counts):
     return steps, per
 
 
+def read_traffic(workload, step):
+    """DRAM bytes (read + write) per solve of the kernels of `step`, from the
+    ncu summary profiles/<workload>_traffic.txt ("<step> <bytes>" lines, '#'
+    comments naming the capture), or None when there is none."""
+    path = os.path.join(ROOT, "profiles", f"{workload}_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split("#", 1)[0].split()
+        if len(f) == 2 and f[0] == step:
+            return float(f[1])
+    return None
+
+
 def make_inputs(wl, seed, n=None, nrhs=1):
     from zfmm_b200 import workloads as W
     n = wl["n"] if n is None else n
@@ -585,10 +599,7 @@ def run_ours(args, wl, ws, rank, local):
     top = max(flops, key=lambda k: avg[k])
     achieved = flops[top] / (avg[top] * 1e-3) / 1e12
     peak = float(L.zfmm_probe_fp64_tflops(20000))
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"{args.workload}_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(top)
+    traffic = read_traffic(args.workload, top)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         set_omp_threads()

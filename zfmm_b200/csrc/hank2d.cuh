@@ -53,7 +53,9 @@ ZF_HD void bessel01_series(zdc z, zdc& J0, zdc& J1, zdc& S0, zdc& S1) {
     sj1 += t1;
     s0 += H * t0;
     s1 += (2.0 * H + 1.0 / (k + 1)) * t1;
-    if (zabs(t0) < 1e-18 * zabs(sj0) && zabs(t1) < 1e-18 * zabs(sj1)) break;
+    double a0 = t0.re * t0.re + t0.im * t0.im, b0 = sj0.re * sj0.re + sj0.im * sj0.im;
+    double a1 = t1.re * t1.re + t1.im * t1.im, b1 = sj1.re * sj1.re + sj1.im * sj1.im;
+    if (a0 < 1e-36 * b0 && a1 < 1e-36 * b1) break;  // |t| < 1e-18 |s|, squared
   }
   zdc zh = 0.5 * z;
   J0 = sj0;
@@ -98,7 +100,7 @@ ZF_HD void bessel01_miller(zdc w, zdc& J0, zdc& J1, zdc& S0, zdc& S1) {
       zdc fm1 = ((double)n * iw2) * f - fp1;
       fp1 = f;
       f = fm1;
-      if (zabs(f) > 1e250) {
+      if (zbig(f, 1e250)) {
         const double sc = 1e-250;
         f = sc * f; fp1 = sc * fp1; norm = sc * norm; a0 = sc * a0; a1 = sc * a1; f1 = sc * f1;
       }
@@ -225,7 +227,7 @@ ZF_HD void jbessel2d(int nterms, zdc z, double rscale, zdc* fjs, int ifder, zdc*
   zdc zr = rscale * zi;
   for (int n = ntop - 1; n >= 1; n--) {
     tmp[n - 1] = ((2.0 * n) * zr) * tmp[n] - sc2 * tmp[n + 1];
-    if (zabs(tmp[n - 1]) > 1e200)
+    if (zbig(tmp[n - 1], 1e200))
       for (int k = n - 1; k <= ntop; k++) tmp[k] = 1e-200 * tmp[k];
   }
   // normalisation: psi = g_0 + 2 sum_n (zmul)^n rscale^n g_n

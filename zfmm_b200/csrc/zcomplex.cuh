@@ -36,7 +36,7 @@ ZF_HD zdc zmul_i(zdc a) { return zdc{-a.im, a.re}; }  // i*a
 ZF_HD double zabs(zdc a) { return hypot(a.re, a.im); }
 
 // a / b with Smith's scaling (avoids overflow of |b|^2)
-ZF_HD zdc operator/(zdc a, zdc b) {
+ZF_HD zdc zdiv_smith(zdc a, zdc b) {
   if (fabs(b.re) >= fabs(b.im)) {
     double r = b.im / b.re, d = b.re + b.im * r;
     return zdc{(a.re + a.im * r) / d, (a.im - a.re * r) / d};
@@ -45,8 +45,29 @@ ZF_HD zdc operator/(zdc a, zdc b) {
     return zdc{(a.re * r + a.im) / d, (a.im * r - a.re) / d};
   }
 }
-ZF_HD zdc zinv(zdc b) { return mkz(1.0) / b; }
-ZF_HD zdc operator/(double a, zdc b) { return mkz(a) / b; }
+// a / b = a conj(b) / |b|^2 with one real division where neither |b|^2 nor
+// the products can overflow or underflow (|b|^2 in [1e-290, 1e290], parts of
+// a below 1e150); Smith's form otherwise (and for NaN / Inf operands)
+ZF_HD zdc operator/(zdc a, zdc b) {
+  const double d = b.re * b.re + b.im * b.im;
+  if (d > 1e-290 && d < 1e290 && fabs(a.re) < 1e150 && fabs(a.im) < 1e150) {
+    const double r = 1.0 / d;
+    return zdc{(a.re * b.re + a.im * b.im) * r, (a.im * b.re - a.re * b.im) * r};
+  }
+  return zdiv_smith(a, b);
+}
+ZF_HD zdc zinv(zdc b) {
+  const double d = b.re * b.re + b.im * b.im;
+  if (d > 1e-290 && d < 1e290) {
+    const double r = 1.0 / d;
+    return zdc{b.re * r, -b.im * r};
+  }
+  return zdiv_smith(mkz(1.0), b);
+}
+ZF_HD zdc operator/(double a, zdc b) { return a * zinv(b); }
+// max(|Re a|, |Im a|) > t: the overflow guard of the recurrences (within a
+// factor sqrt(2) of |a| > t, without the square root)
+ZF_HD bool zbig(zdc a, double t) { return fabs(a.re) > t || fabs(a.im) > t; }
 
 ZF_HD zdc zsqrt_p(zdc z) {
   double x = z.re, y = z.im;
