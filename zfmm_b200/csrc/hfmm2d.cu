@@ -81,7 +81,7 @@ __device__ __forceinline__ double sgn(int n) { return (n & 1) ? -1.0 : 1.0; }
 __device__ __forceinline__ void polar(zdc a1, zdc a2, zdc& rz, zdc& ez) {
   // zcart2polar (toolbox.f:73-82)
   rz = zsqrt_p(a1 * a1 + a2 * a2);
-  ez = a1 / rz + zmul_i(a2 / rz);
+  ez = (a1 + zmul_i(a2)) * zinv(rz);
 }
 
 constexpr int MAXR = 8;  // M2M / M2L / L2L coefficient slots per lane: p <= 255
@@ -161,7 +161,7 @@ __device__ void bessel_table(zdc z, zdc e, double rs, int n, double4* out) {
       zdc gm1 = ((2.0 * k) * zr) * g - sc2 * gp1;
       gp1 = g;
       g = gm1;
-      if (zabs(g) > 1e200) {
+      if (zbig(g, 1e200)) {
         g = 1e-200 * g;
         gp1 = 1e-200 * gp1;
         psi = 1e-200 * psi;
@@ -335,7 +335,7 @@ __device__ void p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
       psi = rs * psi + zn * g;
       gp1 = g;
       g = gm1;
-      if (zabs(g) > 1e200) {
+      if (zbig(g, 1e200)) {
         g = 1e-200 * g;
         gp1 = 1e-200 * gp1;
         psi = 1e-200 * psi;
@@ -370,8 +370,9 @@ __device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
   double sc2 = rs * rs;
   zdc iez = zinv(ez), ep = mkz(1.0), em = mkz(1.0);
   zdc fm1 = mkz(0.0), f = h0, fp1 = h1 * rs;  // F_{m-1}, F_m, F_{m+1}
+  const double irs = 1.0 / rs;
   for (int m = 0; m <= p; m++) {
-    zdc fder = m == 0 ? -fp1 / rs : rs * fm1 - ((double)m * t.izk) * f;
+    zdc fder = m == 0 ? -(fp1 * irs) : rs * fm1 - ((double)m * t.izk) * f;
     zdc cp, cn;
     src_coeffs(A, t, m, f, fder, em, ep, cp, cn);
     col[p + m] = cp;
@@ -603,10 +604,30 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
   }
 }
 
-// M2L (zh2dmploc) over list 2; R coefficient slots per lane (p < 32 R).  The
-// local expansion is written here; P2L (k_hp2l) adds to it afterwards.
+// M2L (zh2dmploc) over list 2.  With T[k] = H_k e^{ik theta} (k = -2p..2p,
+// H_-k = (-1)^k H_k, scaled) the pair's Toeplitz symbol and b(n) the source
+// coefficients, the reference's weight rs^|m| rs^|n| / rs^|n-m| is 1 for n, m
+// of opposite signs and rs^(2 min(|m|,|n|)) otherwise, so for m >= 0
+//   loc(m)  = sum_{n<0} T[n-m] b(n)  + sum_{n>=0} s(n,m) T[n-m] b(n)
+//   loc(-m) = sum_{n<0} T[m-n] b(-n) + sum_{n>=0} s(n,m) T[m-n] b(-n)
+// (the second is the first with T and b mirrored), s(n,m) = rs^(2 min(n,m)).
+// Lane (h, k) of the warp computes the outputs m0 = 2k + 32r and m0 + 1 of the
+// sum with sign sigma = +1 (h = 0: loc(+m)) or -1 (h = 1: loc(-m)), walking n
+// upwards with a two-entry window of T: the entry T[sigma(n - m0 - 1)] used
+// for m0 + 1 is the entry used for m0 one step earlier, so each step reads one
+// entry of T and one of b for two multiply-adds.  T is kept split by parity
+// (the lanes of a step read entries of one parity, 2 apart), so that the 16
+// lanes of a half read 256 contiguous bytes.  R rounds of 32 outputs
+// (p < 32 R).  The local expansion is written here; P2L adds to it afterwards.
+__device__ __forceinline__ int tpos(int k, int n2) {  // position of T[k] in the split layout
+  return (k & 1) * (n2 + 3) + ((k + n2 + 2) >> 1);
+}
+// shared-memory entries per warp of k_hm2l at order p: T split by parity with
+// its two zero ends, rs^k (as doubles), b(n)
+inline int hm2l_stride(int p) { return 2 * (2 * p + 3) + (2 * p + 2) + (2 * p + 1); }
+
 template <int R>
-__global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A, TabArgs TA,
+__global__ void __launch_bounds__(32 * WPB, R == 1 ? 8 : 4) k_hm2l(int lo, int hi, HelmArgs A, TabArgs TA,
                                                       const int* pairoff, const int* nl2,
                                                       const int* l2, int m2, int stride) {
   extern __shared__ zdc sh[];
@@ -615,75 +636,71 @@ __global__ void __launch_bounds__(32 * WPB, 4) k_hm2l(int lo, int hi, HelmArgs A
   if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
   int n2c = nl2[b];
   if (n2c == 0) return;
-  int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
-  zdc* T = sh + (threadIdx.x >> 5) * stride;  // [2*n2+1]
-  double* rp = (double*)(T + 2 * n2 + 1);     // rs^k, k = 0..n2
-  zdc* bb = T + 2 * n2 + 1 + (n2 + 2) + p;    // b(n), n = -p..p
-  zdc accp[R], accm[R], acc0 = mkz(0.0);
-#pragma unroll
-  for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
+  const int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
+  zdc* Ts = sh + (threadIdx.x >> 5) * stride;  // T[k], k = -n2-1..n2+1, split by parity
+  double* rp = (double*)(Ts + 2 * (n2 + 3));    // rs^k, k = 0..n2
+  zdc* bb = Ts + 2 * (n2 + 3) + (n2 + 2) + p;   // b(n), n = -p..p
+  const int h = lane >> 4, kq = lane & 15, sg = h ? -1 : 1;
   for (int k = lane; k <= n2; k += 32) rp[k] = TA.pw[TA.pw_m2l[l] + k];
+  if (lane == 0) {  // the two ends, read only for outputs m > p (discarded)
+    Ts[tpos(-n2 - 1, n2)] = mkz(0.0);
+    Ts[tpos(n2 + 1, n2)] = mkz(0.0);
+  }
+  __syncwarp();
+  zdc acc0[R], acc1[R];
+  double rpm0[R], rpm1[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    acc0[r] = acc1[r] = mkz(0.0);
+    const int m0 = 2 * kq + 32 * r;
+    rpm0[r] = m0 <= p ? rp[2 * m0] : 0.0;
+    rpm1[r] = m0 + 1 <= p ? rp[2 * m0 + 2] : 0.0;
+  }
   const double4* tl = TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
   for (int il = 0; il < n2c; il++) {
     int jb = l2[(size_t)b * m2 + il];
     if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
     __syncwarp();
-    // Toeplitz symbol T[k] = H_k e^{ik theta} (k = -2p..2p, H_-k = (-1)^k H_k,
-    // scaled) from the pair's table and the source coefficients b(n): the
-    // reference's weight rs^|m| rs^|n| / rs^|n-m| is 1 for n, m of opposite
-    // signs and rs^(2 min(|m|,|n|)) otherwise, so
-    //   loc(m) = sum_{n<0} T[n-m] b(n) + sum_{n>=0} rs^(2 min(n,m)) T[n-m] b(n)
-    //   (m >= 0, mirrored for m < 0)
     const double4* t = tl + (long)il * (n2 + 1);
     for (int k = lane; k <= n2; k += 32) {
       double4 v = t[k];
-      T[n2 + k] = mkz(v.x, v.y);
-      T[n2 - k] = mkz(v.z, v.w);
+      Ts[tpos(k, n2)] = mkz(v.x, v.y);
+      Ts[tpos(-k, n2)] = mkz(v.z, v.w);
     }
     const zdc* M = expo(A, A.mp, jb);
     for (int n = lane - p; n <= p; n += 32) bb[n] = M[n];
     __syncwarp();
-    // per output the weight is rs^(2 min(|n|, |m|)) for n of the sign of m
-    // (n = 0 included) and 1 otherwise; it is applied to b(n) as the scale
-    // rp[2|n|] (|n| <= |m|) or rp[2|m|] (|n| > |m|), selected per lane, so
-    // the inner loops have no branches
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      int m = lane + 32 * r;
-      if (m > p) break;
-      const double rpm = rp[2 * m];
-      zdc a = mkz(0.0);
-      const zdc* Tm = T + n2 - m;  // Tm[n] = T[n - m]
-      for (int n = -p; n < 0; n++) a += Tm[n] * bb[n];
+      const int m0 = 2 * kq + 32 * r;
+      if (m0 > p) break;
+      zdc prev = Ts[tpos(sg * (-p - 1 - m0), n2)];  // T[sg (n - m0 - 1)] at n = -p
+      zdc s0 = mkz(0.0), s1 = mkz(0.0);
+      for (int n = -p; n < 0; n++) {
+        const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
+        s0 += cur * bn;
+        s1 += prev * bn;
+        prev = cur;
+      }
+      const int m1 = m0 + 1;
       for (int n = 0; n <= p; n++) {
-        double sc = n <= m ? rp[2 * n] : rpm;
-        a += Tm[n] * (sc * bb[n]);
+        const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
+        const double rn = rp[2 * n];
+        s0 += cur * ((n <= m0 ? rn : rpm0[r]) * bn);
+        s1 += prev * ((n <= m1 ? rn : rpm1[r]) * bn);
+        prev = cur;
       }
-      if (m == 0) {
-        acc0 += a;
-        continue;
-      }
-      zdc c = mkz(0.0);
-      const zdc* Tq = T + n2 + m;  // Tq[n] = T[n + m]
-      for (int n = 1; n <= p; n++) c += Tq[n] * bb[n];
-      for (int n = -p; n <= 0; n++) {
-        double sc = -n <= m ? rp[-2 * n] : rpm;
-        c += Tq[n] * (sc * bb[n]);
-      }
-      accp[r] += a;
-      accm[r] += c;
+      acc0[r] += s0;
+      acc1[r] += s1;
     }
   }
   zdc* L = expo(A, A.loc, b);
 #pragma unroll
   for (int r = 0; r < R; r++) {
-    int m = lane + 32 * r;
-    if (m > p) break;
-    if (m == 0) L[0] = acc0;
-    else {
-      L[m] = accp[r];
-      L[-m] = accm[r];
-    }
+    const int m0 = 2 * kq + 32 * r, m1 = m0 + 1;
+    if (m0 > p) break;
+    if (m0 > 0 || h == 0) L[sg * m0] = acc0[r];  // loc(0) once, from the + half
+    if (m1 <= p) L[sg * m1] = acc1[r];
   }
 }
 
@@ -959,8 +976,9 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
     zdc z = zr * A.zk;
     if (zabs(z) >= 1e-200) {
       int ntop = jbessel_top(p, z);
-      zdc zrr = rs * zinv(z), izz = zinv(z);
+      zdc izz = zinv(z), zrr = rs * izz;
       double sc2 = rs * rs;
+      const double irs = 1.0 / rs;
       zdc zmul = z.im < 0.0 ? mkz(0.0, 1.0) : mkz(0.0, -1.0);
       zdc iei = zinv(ei);
       zdc gp1 = mkz(0.0), g = mkz(1.0), psi = mkz(0.0);
@@ -974,7 +992,7 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
           zdc c = cp + cm;
           sp += c * g;
           if (GRAD) {
-            zdc fd = n >= 1 ? gm1 / rs - ((double)n * izz) * g : (-rs) * gp1;
+            zdc fd = n >= 1 ? gm1 * irs - ((double)n * izz) * g : (-rs) * gp1;
             srad += c * fd;
             sang += ((double)n * zmul_i(cp - cm)) * g;
           }
@@ -987,7 +1005,7 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
           psi = rs * psi + zn * g;
           gp1 = g;
           g = gm1;
-          if (zabs(g) > 1e200) {
+          if (zbig(g, 1e200)) {
             g = 1e-200 * g; gp1 = 1e-200 * gp1; psi = 1e-200 * psi;
             sp = 1e-200 * sp; srad = 1e-200 * srad; sang = 1e-200 * sang;
           }
@@ -1020,8 +1038,9 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
     if (zabs(z) < 1e-200) continue;
     zdc h0, h1;
     hank01(z, h0, h1);
-    zdc iei = zinv(ei), zi = rs * zinv(z), zi1 = zinv(z);
+    zdc iei = zinv(ei), zi1 = zinv(z), zi = rs * zi1;
     double sc2 = rs * rs;
+    const double irs = 1.0 / rs;
     zdc hm1 = mkz(0.0), h = h0, hp = h1 * rs;  // scaled H_{n-1}, H_n, H_{n+1}
     zdc eip = mkz(1.0), eim = mkz(1.0);
     zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
@@ -1030,7 +1049,7 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
       zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&M[-n]) * eim);
       sp += (cp + cm) * h;
       if (GRAD) {
-        zdc hd = n == 0 ? -hp / rs : rs * hm1 - ((double)n * zi1) * h;
+        zdc hd = n == 0 ? -(hp * irs) : rs * hm1 - ((double)n * zi1) * h;
         srad += (cp + cm) * hd;
         sang += ((double)n * zmul_i(cp - cm)) * h;
       }
@@ -1059,8 +1078,10 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
 // ---- step 3: P2P (list 1) one thread per target, added to L2T + M2T ----------
 // Consecutive threads take consecutive sorted targets, so a warp covers one to
 // a few neighbouring leaves with similar near fields, and no lane idles for
-// want of targets in its leaf.  Each thread sums its list-1 boxes in list
-// order and their sources in sorted order.
+// want of targets in its leaf.  Each thread walks the sources of its list-1
+// boxes (in list order, each box's sources in sorted order) as one flat loop,
+// so lanes of different leaves in one warp cost the larger of their source
+// counts rather than a sum over the boxes of the larger box.
 template <bool GRAD>
 __global__ void __launch_bounds__(128, 3) k_hp2p(int nt, HelmArgs A, const int* tgtleaf,
                                                  const int* nl1, const int* l1, int m1,
@@ -1073,20 +1094,25 @@ __global__ void __launch_bounds__(128, 3) k_hp2p(int nt, HelmArgs A, const int* 
   const zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
   zdc pot = mkz(0.0), g1 = mkz(0.0), g2 = mkz(0.0);
   const int n1 = nl1[b];
-  for (int il = 0; il < n1; il++) {
-    int jb = l1[(size_t)b * m1 + il];
-    int s0 = A.isrcse[2 * jb], s1 = A.isrcse[2 * jb + 1];
-    for (int j = s0; j <= s1; j++) {
-      zdc q = A.ifcharge ? ldz(&A.charge[j]) : mkz(0.0);
-      zdc ds = mkz(0.0), d1 = mkz(0.0), d2 = mkz(0.0);
-      if (A.ifdipole) {
-        ds = ldz(&A.dipstr[j]);
-        d1 = ldz(&A.dipvec[2 * j]);
-        d2 = ldz(&A.dipvec[2 * j + 1]);
-      }
-      helm_pair<GRAD>(K, x1, x2, ldz(&A.zsrc[2 * j]), ldz(&A.zsrc[2 * j + 1]), q, ds, d1, d2,
-                      A.ifcharge, A.ifdipole, pot, g1, g2);
+  const int* lb = l1 + (size_t)b * m1;
+  int il = 0, j = 0, s1 = -1;  // current source j of box lb[il], last source s1
+  while (true) {
+    while (j > s1 && il < n1) {  // next list-1 box with sources
+      const int jb = lb[il++];
+      j = A.isrcse[2 * jb];
+      s1 = A.isrcse[2 * jb + 1];
     }
+    if (j > s1) break;
+    zdc q = A.ifcharge ? ldz(&A.charge[j]) : mkz(0.0);
+    zdc ds = mkz(0.0), d1 = mkz(0.0), d2 = mkz(0.0);
+    if (A.ifdipole) {
+      ds = ldz(&A.dipstr[j]);
+      d1 = ldz(&A.dipvec[2 * j]);
+      d2 = ldz(&A.dipvec[2 * j + 1]);
+    }
+    helm_pair<GRAD>(K, x1, x2, ldz(&A.zsrc[2 * j]), ldz(&A.zsrc[2 * j + 1]), q, ds, d1, d2,
+                    A.ifcharge, A.ifdipole, pot, g1, g2);
+    j++;
   }
   potsort[ti] += pot;
   if (GRAD) {
@@ -1435,8 +1461,8 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   // one launch per level (lists 2 and 4 are empty on levels 0 and 1): the
   // shared-memory stride and the register slots follow the level's order
   for (int l = 2; l <= nlev && (stages & ST_M2L); l++) {
-    int pl_ = A.T.p[l], n2 = 2 * pl_;
-    int stride = (2 * n2 + 1) + (n2 + 2) + (2 * pl_ + 1);
+    int pl_ = A.T.p[l];
+    int stride = hm2l_stride(pl_);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
     auto go = [&](auto kern) {
@@ -1505,29 +1531,10 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
         klaunch(l2t, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
                 L.list[2].get(), L.mn[2], potsort, gradsort);
       }, s);
-      // P2P adds to what L2T wrote: tuning restores that state before each trial
-      DevBuf<zdc> keep;
-      size_t ng = ifpgh > 1 ? 2 * (size_t)ntt : 0;
-      auto reset = [&] {
-        if (!keep.get()) {
-          keep.alloc(ntt + ng, s);
-          ZF_CUDA(cudaMemcpyAsync(keep.get(), potsort, ntt * sizeof(zdc),
-                                  cudaMemcpyDeviceToDevice, s));
-          if (ng)
-            ZF_CUDA(cudaMemcpyAsync(keep.get() + ntt, gradsort, ng * sizeof(zdc),
-                                    cudaMemcpyDeviceToDevice, s));
-        } else {
-          ZF_CUDA(cudaMemcpyAsync(potsort, keep.get(), ntt * sizeof(zdc),
-                                  cudaMemcpyDeviceToDevice, s));
-          if (ng)
-            ZF_CUDA(cudaMemcpyAsync(gradsort, keep.get() + ntt, ng * sizeof(zdc),
-                                    cudaMemcpyDeviceToDevice, s));
-        }
-      };
-      tuned_launch(ifpgh > 1 ? "k_hp2p_g" : "k_hp2p", ntt, 128, {64, 128}, [&](int bs) {
-        klaunch(p2p, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), L.n[0].get(),
-                L.list[0].get(), L.mn[0], potsort, gradsort);
-      }, s, autotune_enabled() ? std::function<void()>(reset) : std::function<void()>());
+      // P2P adds to what L2T wrote (its block size is fixed: tuning would have
+      // to restore the L2T results before every trial)
+      klaunch(p2p, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[0].get(),
+              L.list[0].get(), L.mn[0], potsort, gradsort);
     };
     if (ifpgh > 1) eval(k_hl2t<true>, k_hp2p<true>);
     else eval(k_hl2t<false>, k_hp2p<false>);
@@ -1608,7 +1615,7 @@ void helm2d_passes_nd(const Setup2D& S, const Helm2DPrep& H, int nd, int ifcharg
           HelmArgs Aj = A;
           Aj.mp = mp.get() + j * tot;
           Aj.loc = loc.get() + j * tot;
-          int n2 = 2 * p, stride = (2 * n2 + 1) + (n2 + 2) + (2 * p + 1);
+          int stride = hm2l_stride(p);
           size_t sm = (size_t)WPB * stride * sizeof(zdc);
           int grid = div_up(hi - lo + 1, WPB);
           auto slots = (p + 1 + 31) / 32;
