@@ -186,31 +186,46 @@ struct TabArgs {
   const double* pw;
   long pw_m2l[MAXL], pw_m2m[MAXL], pw_l2l[MAXL];
   long m2l_base[MAXL];   // first entry of the level's M2L tables
-  long m2l_pair0[MAXL];  // first list-2 pair (index into pairoff order) of the level
+  long m2l_pair0[MAXL];  // first translated list-2 pair (pairoff order) of the level
   long ml_base[MAXL];    // first entry of the M2M / L2L tables of the children of level l
 };
 
-// first box of the level range [lo, hi] whose pair range contains pair q
-__device__ __forceinline__ int pair_box(const int* pairoff, int lo, int hi, long q) {
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (pairoff[mid] <= q) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
+// The list-2 pairs that are translated: target box with targets, source box
+// with sources (the conditions of zh2dmploc's call in the reference's step 3).
+// They are numbered box by box in list order (pairoff[b] = first pair of box
+// b), and the M2L tables are stored in that order, so the translation kernels
+// find the k-th translated pair of box b at pairoff[b] + k.
+__device__ __forceinline__ bool m2l_pair_used(const HelmArgs& A, int b, int jb) {
+  return A.itargse[2 * b + 1] >= A.itargse[2 * b] && A.isrcse[2 * jb + 1] >= A.isrcse[2 * jb];
 }
 
-// M2L tables of every list-2 pair of levels >= 2 (one thread per pair)
-__global__ void __launch_bounds__(128) k_tab_m2l(long q0, long q1, int b0, int b1, HelmArgs A,
-                                                 TabArgs TA, const int* pairoff, const int* nl2,
-                                                 const int* l2, int m2) {
+__global__ void k_m2l_pair_count(int nb, HelmArgs A, const int* nl2, const int* l2, int m2,
+                                 int* cnt) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int c = 0;
+  for (int il = 0; il < nl2[b]; il++) c += m2l_pair_used(A, b, l2[(size_t)b * m2 + il]) ? 1 : 0;
+  cnt[b] = c;
+}
+
+__global__ void k_m2l_pair_fill(int nb, HelmArgs A, const int* nl2, const int* l2, int m2,
+                                const int* pairoff, int2* pairs) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int k = pairoff[b];
+  for (int il = 0; il < nl2[b]; il++) {
+    int jb = l2[(size_t)b * m2 + il];
+    if (m2l_pair_used(A, b, jb)) pairs[k++] = make_int2(b, jb);
+  }
+}
+
+// M2L tables of the translated list-2 pairs q0 .. q1-1 (one thread per pair)
+__global__ void __launch_bounds__(128) k_tab_m2l(long q0, long q1, HelmArgs A, TabArgs TA,
+                                                 const int2* pairs) {
   long q = q0 + blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (q >= q1) return;
-  int b = pair_box(pairoff, b0, b1, q);
-  int il = (int)(q - pairoff[b]);
-  if (il >= nl2[b] || A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
-  int jb = l2[(size_t)b * m2 + il];
-  if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) return;
+  const int2 pr = pairs[q];
+  const int b = pr.x, jb = pr.y;
   int l = A.ilevel[b], p = A.T.p[l];
   zdc rz, e;
   polar(A.zctarg[2 * b] - A.zcsrc[2 * jb], A.zctarg[2 * b + 1] - A.zcsrc[2 * jb + 1], rz, e);
@@ -473,7 +488,7 @@ __global__ void __launch_bounds__(128) k_p2l_cols(long long nq, int b0, int b1, 
   p2l_column(A, j, A.zctarg[2 * b], A.zctarg[2 * b + 1], A.T.rs[l], p, col);
 }
 
-// sums of the columns of every box of one level: one warp per box, R register
+// sums of the columns of every box of one level: warps loop over the boxes, R register
 // slots per lane (2p+1 <= 32 R); P2M writes the multipole expansion, P2L adds
 // to the local expansion
 template <int R, bool LOCAL>
@@ -481,30 +496,31 @@ __global__ void __launch_bounds__(32 * WPB) k_form_sum(int lo, int hi, HelmArgs 
                                                        const long long* cnt,
                                                        const long long* colbase,
                                                        const zdc* cols) {
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int b = lo + blockIdx.x * WPB + w;
-  if (b > hi) return;
-  long long n = cnt[b];
-  if (n == 0) return;
-  int l = A.ilevel[b], p = A.T.p[l], P2 = 2 * p + 1;
-  const zdc* c = cols + colbase[b];
-  zdc acc[R];
+  const int lane = threadIdx.x & 31;
+  // every box of the launch is on one level; the warp loops over boxes
+  const int p = A.T.p[A.ilevel[lo]], P2 = 2 * p + 1;
+  for (int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5); b <= hi; b += gridDim.x * WPB) {
+    const long long n = cnt[b];
+    if (n == 0) continue;
+    const zdc* c = cols + colbase[b];
+    zdc acc[R];
 #pragma unroll
-  for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
-  for (long long k = 0; k < n; k++) {
+    for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
+    for (long long k = 0; k < n; k++) {
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        int i = lane + 32 * r;
+        if (i < P2) acc[r] += ldz(&c[k * P2 + i]);
+      }
+    }
+    zdc* E = expo(A, LOCAL ? A.loc : A.mp, b) - p;
 #pragma unroll
     for (int r = 0; r < R; r++) {
       int i = lane + 32 * r;
-      if (i < P2) acc[r] += ldz(&c[k * P2 + i]);
-    }
-  }
-  zdc* E = expo(A, LOCAL ? A.loc : A.mp, b) - p;
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    int i = lane + 32 * r;
-    if (i < P2) {
-      if (LOCAL) E[i] += acc[r];
-      else E[i] = acc[r];
+      if (i < P2) {
+        if (LOCAL) E[i] += acc[r];
+        else E[i] = acc[r];
+      }
     }
   }
 }
@@ -530,9 +546,8 @@ template <int R>
 __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, HelmArgs A,
                                                    TabArgs TA, int stride) {
   extern __shared__ zdc sh[];
-  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b > hi) return;
-  if (A.nchild[b] == 0 || A.isrcse[2 * b + 1] < A.isrcse[2 * b]) return;
+  const int lane = threadIdx.x & 31;
+  if (lo + blockIdx.x * WPB + (threadIdx.x >> 5) > hi) return;
   int n1 = A.T.p[lev], n2 = A.T.p[lev + 1], nt = n1 + n2;
   zdc* S1 = sh + (threadIdx.x >> 5) * stride + nt;  // S1[k], k = -nt..nt
   zdc* S3 = S1 + nt + 1 + nt;                       // S1[j] g(-j)
@@ -542,64 +557,68 @@ __global__ void __launch_bounds__(32 * WPB) k_hm2m(int lo, int hi, int lev, Helm
   const double* qa = TA.pw + TA.pw_m2m[lev];        // (rs1 rs2)^k, k = 0..nt
   const double* qb = qa + nt + 1;                   // (rs2/rs1)^k
   const double* qi = qb + nt + 1;                   // (rs1/rs2)^k
-  zdc accp[R], accm[R], acc0 = mkz(0.0);
-#pragma unroll
-  for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
-  const int lc = lev + 1;
-  for (int jc = 0; jc < 4; jc++) {
-    int jb = A.ichild[4 * b + jc];
-    if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-    const double4* t = TA.tab + TA.ml_base[lev] + (long)(jb - A.T.lo[lc]) * 2 * (nt + 2);
-    double4 nv = t[nt + 1];
-    zdc nrm = mkz(nv.x, nv.y);
-    __syncwarp();
-    for (int k = lane; k <= nt; k += 32) {
-      double4 v = t[k];
-      zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
-      S1[k] = vv;   // (-1)^k J_k e^{-ik theta}
-      S1[-k] = u;   // J_k e^{ik theta}
-      double gp = k > 0 ? qa[k] : 1.0, gm = qi[k];  // g(k), g(-k)
-      S3[k] = vv * gm;
-      S3[-k] = u * gp;
-      S4[k] = vv * gp;
-      S4[-k] = u * gm;
+  // the warp loops over the boxes of the level
+  for (int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5); b <= hi; b += gridDim.x * WPB) {
+    if (A.nchild[b] == 0 || A.isrcse[2 * b + 1] < A.isrcse[2 * b]) continue;
+    zdc accp[R], accm[R], acc0 = mkz(0.0);
+  #pragma unroll
+    for (int r = 0; r < R; r++) accp[r] = accm[r] = mkz(0.0);
+    const int lc = lev + 1;
+    for (int jc = 0; jc < 4; jc++) {
+      int jb = A.ichild[4 * b + jc];
+      if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
+      const double4* t = TA.tab + TA.ml_base[lev] + (long)(jb - A.T.lo[lc]) * 2 * (nt + 2);
+      double4 nv = t[nt + 1];
+      zdc nrm = mkz(nv.x, nv.y);
+      __syncwarp();
+      for (int k = lane; k <= nt; k += 32) {
+        double4 v = t[k];
+        zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
+        S1[k] = vv;   // (-1)^k J_k e^{-ik theta}
+        S1[-k] = u;   // J_k e^{ik theta}
+        double gp = k > 0 ? qa[k] : 1.0, gm = qi[k];  // g(k), g(-k)
+        S3[k] = vv * gm;
+        S3[-k] = u * gp;
+        S4[k] = vv * gp;
+        S4[-k] = u * gm;
+      }
+      const zdc* M2 = expo(A, A.mp, jb);
+      for (int n = lane - n2; n <= n2; n += 32) {
+        zdc v = M2[n];
+        mc[n] = v;
+        ww[n] = qa[abs(n)] * v;
+      }
+      __syncwarp();
+  #pragma unroll
+      for (int r = 0; r < R; r++) {
+        int m = lane + 32 * r;
+        if (m > n1) break;
+        zdc a1 = mkz(0.0), a2 = mkz(0.0);
+        for (int n = -n2; n <= 0; n++) a1 += S1[m - n] * ww[n];
+        for (int n = 1; n <= n2; n++) a2 += S3[m - n] * mc[n];
+        zdc sp = a1 + qb[m] * a2;
+        if (m == 0) {
+          acc0 += sp;
+          continue;
+        }
+        a1 = mkz(0.0);
+        a2 = mkz(0.0);
+        for (int n = 0; n <= n2; n++) a1 += S1[-m - n] * ww[n];
+        for (int n = -n2; n < 0; n++) a2 += S4[-m - n] * mc[n];
+        accp[r] += sp;
+        accm[r] += a1 + qb[m] * a2;
+      }
     }
-    const zdc* M2 = expo(A, A.mp, jb);
-    for (int n = lane - n2; n <= n2; n += 32) {
-      zdc v = M2[n];
-      mc[n] = v;
-      ww[n] = qa[abs(n)] * v;
-    }
-    __syncwarp();
-#pragma unroll
+    zdc* M = expo(A, A.mp, b);
+  #pragma unroll
     for (int r = 0; r < R; r++) {
       int m = lane + 32 * r;
       if (m > n1) break;
-      zdc a1 = mkz(0.0), a2 = mkz(0.0);
-      for (int n = -n2; n <= 0; n++) a1 += S1[m - n] * ww[n];
-      for (int n = 1; n <= n2; n++) a2 += S3[m - n] * mc[n];
-      zdc sp = a1 + qb[m] * a2;
-      if (m == 0) {
-        acc0 += sp;
-        continue;
+      if (m == 0) M[0] = acc0;
+      else {
+        M[m] = accp[r];
+        M[-m] = accm[r];
       }
-      a1 = mkz(0.0);
-      a2 = mkz(0.0);
-      for (int n = 0; n <= n2; n++) a1 += S1[-m - n] * ww[n];
-      for (int n = -n2; n < 0; n++) a2 += S4[-m - n] * mc[n];
-      accp[r] += sp;
-      accm[r] += a1 + qb[m] * a2;
-    }
-  }
-  zdc* M = expo(A, A.mp, b);
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    int m = lane + 32 * r;
-    if (m > n1) break;
-    if (m == 0) M[0] = acc0;
-    else {
-      M[m] = accp[r];
-      M[-m] = accm[r];
     }
   }
 }
@@ -626,17 +645,27 @@ __device__ __forceinline__ int tpos(int k, int n2) {  // position of T[k] in the
 // its two zero ends, rs^k (as doubles), b(n)
 inline int hm2l_stride(int p) { return 2 * (2 * p + 3) + (2 * p + 2) + (2 * p + 1); }
 
+// grid of a warp-per-box kernel whose warps loop over the boxes: as many CTAs
+// as the SMs hold at once, and no more than there are groups of WPB boxes
+// (a warp whose box has no work then moves on instead of holding its CTA)
+template <class K>
+int resident_grid(K kern, size_t smem, int nboxes) {
+  int dev = 0, nsm = 0, per = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  ZF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  ZF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * WPB, smem));
+  return std::max(1, std::min(div_up(nboxes, WPB), nsm * std::max(per, 1)));
+}
+
 template <int R>
-__global__ void __launch_bounds__(32 * WPB, R == 1 ? 8 : 4) k_hm2l(int lo, int hi, HelmArgs A, TabArgs TA,
-                                                      const int* pairoff, const int* nl2,
-                                                      const int* l2, int m2, int stride) {
+__global__ void __launch_bounds__(32 * WPB, R == 1 ? 8 : 4)
+    k_hm2l(int lo, int hi, HelmArgs A, TabArgs TA, const int* pairoff, const int* nl2,
+           const int* l2, int m2, int stride) {
   extern __shared__ zdc sh[];
-  int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b > hi) return;
-  if (A.itargse[2 * b + 1] < A.itargse[2 * b]) return;
-  int n2c = nl2[b];
-  if (n2c == 0) return;
-  const int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
+  const int lane = threadIdx.x & 31;
+  if (lo + blockIdx.x * WPB + (threadIdx.x >> 5) > hi) return;
+  // every box of the launch is on one level; the warp loops over boxes
+  const int l = A.ilevel[lo], p = A.T.p[l], n2 = 2 * p;
   zdc* Ts = sh + (threadIdx.x >> 5) * stride;  // T[k], k = -n2-1..n2+1, split by parity
   double* rp = (double*)(Ts + 2 * (n2 + 3));    // rs^k, k = 0..n2
   zdc* bb = Ts + 2 * (n2 + 3) + (n2 + 2) + p;   // b(n), n = -p..p
@@ -647,60 +676,67 @@ __global__ void __launch_bounds__(32 * WPB, R == 1 ? 8 : 4) k_hm2l(int lo, int h
     Ts[tpos(n2 + 1, n2)] = mkz(0.0);
   }
   __syncwarp();
-  zdc acc0[R], acc1[R];
   double rpm0[R], rpm1[R];
 #pragma unroll
   for (int r = 0; r < R; r++) {
-    acc0[r] = acc1[r] = mkz(0.0);
     const int m0 = 2 * kq + 32 * r;
     rpm0[r] = m0 <= p ? rp[2 * m0] : 0.0;
     rpm1[r] = m0 + 1 <= p ? rp[2 * m0 + 2] : 0.0;
   }
-  const double4* tl = TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
-  for (int il = 0; il < n2c; il++) {
-    int jb = l2[(size_t)b * m2 + il];
-    if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-    __syncwarp();
-    const double4* t = tl + (long)il * (n2 + 1);
-    for (int k = lane; k <= n2; k += 32) {
-      double4 v = t[k];
-      Ts[tpos(k, n2)] = mkz(v.x, v.y);
-      Ts[tpos(-k, n2)] = mkz(v.z, v.w);
+  for (int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5); b <= hi; b += gridDim.x * WPB) {
+    if (A.itargse[2 * b + 1] < A.itargse[2 * b]) continue;
+    const int n2c = nl2[b];
+    if (n2c == 0) continue;
+    zdc acc0[R], acc1[R];
+  #pragma unroll
+    for (int r = 0; r < R; r++) acc0[r] = acc1[r] = mkz(0.0);
+    const double4* tl = TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
+    int used = 0;  // translated pairs of the box so far
+    for (int il = 0; il < n2c; il++) {
+      int jb = l2[(size_t)b * m2 + il];
+      if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
+      __syncwarp();
+      const double4* t = tl + (long)(used++) * (n2 + 1);
+      for (int k = lane; k <= n2; k += 32) {
+        double4 v = t[k];
+        Ts[tpos(k, n2)] = mkz(v.x, v.y);
+        Ts[tpos(-k, n2)] = mkz(v.z, v.w);
+      }
+      const zdc* M = expo(A, A.mp, jb);
+      for (int n = lane - p; n <= p; n += 32) bb[n] = M[n];
+      __syncwarp();
+  #pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int m0 = 2 * kq + 32 * r;
+        if (m0 > p) break;
+        zdc prev = Ts[tpos(sg * (-p - 1 - m0), n2)];  // T[sg (n - m0 - 1)] at n = -p
+        zdc s0 = mkz(0.0), s1 = mkz(0.0);
+        for (int n = -p; n < 0; n++) {
+          const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
+          s0 += cur * bn;
+          s1 += prev * bn;
+          prev = cur;
+        }
+        const int m1 = m0 + 1;
+        for (int n = 0; n <= p; n++) {
+          const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
+          const double rn = rp[2 * n];
+          s0 += cur * ((n <= m0 ? rn : rpm0[r]) * bn);
+          s1 += prev * ((n <= m1 ? rn : rpm1[r]) * bn);
+          prev = cur;
+        }
+        acc0[r] += s0;
+        acc1[r] += s1;
+      }
     }
-    const zdc* M = expo(A, A.mp, jb);
-    for (int n = lane - p; n <= p; n += 32) bb[n] = M[n];
-    __syncwarp();
-#pragma unroll
+    zdc* L = expo(A, A.loc, b);
+  #pragma unroll
     for (int r = 0; r < R; r++) {
-      const int m0 = 2 * kq + 32 * r;
+      const int m0 = 2 * kq + 32 * r, m1 = m0 + 1;
       if (m0 > p) break;
-      zdc prev = Ts[tpos(sg * (-p - 1 - m0), n2)];  // T[sg (n - m0 - 1)] at n = -p
-      zdc s0 = mkz(0.0), s1 = mkz(0.0);
-      for (int n = -p; n < 0; n++) {
-        const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
-        s0 += cur * bn;
-        s1 += prev * bn;
-        prev = cur;
-      }
-      const int m1 = m0 + 1;
-      for (int n = 0; n <= p; n++) {
-        const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
-        const double rn = rp[2 * n];
-        s0 += cur * ((n <= m0 ? rn : rpm0[r]) * bn);
-        s1 += prev * ((n <= m1 ? rn : rpm1[r]) * bn);
-        prev = cur;
-      }
-      acc0[r] += s0;
-      acc1[r] += s1;
+      if (m0 > 0 || h == 0) L[sg * m0] = acc0[r];  // loc(0) once, from the + half
+      if (m1 <= p) L[sg * m1] = acc1[r];
     }
-  }
-  zdc* L = expo(A, A.loc, b);
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    const int m0 = 2 * kq + 32 * r, m1 = m0 + 1;
-    if (m0 > p) break;
-    if (m0 > 0 || h == 0) L[sg * m0] = acc0[r];  // loc(0) once, from the + half
-    if (m1 <= p) L[sg * m1] = acc1[r];
   }
 }
 
@@ -774,7 +810,7 @@ __global__ void __launch_bounds__(128) k_hm2l_tc(int lo, int hi, HelmArgs A, Tab
         phase ^= 1;
         pending = false;
       }
-      const double4* t = tl + (long)il * (n2 + 1);
+      const double4* t = tl + (long)npairs * (n2 + 1);
       for (int k = tid; k <= n2; k += 128) {
         double4 v = t[k];
         T[n2 + k] = mkz(v.x, v.y);
@@ -886,11 +922,8 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
                                                    TabArgs TA, const int* nl2, const int* nl4,
                                                    int stride) {
   extern __shared__ zdc sh[];
-  int jb = lo + blockIdx.x * WPB + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (jb > hi) return;
-  int b = A.iparent[jb];
-  if (A.itargse[2 * b + 1] < A.itargse[2 * b] || (nl2[b] == 0 && nl4[b] == 0)) return;
-  if (A.itargse[2 * jb + 1] < A.itargse[2 * jb]) return;
+  const int lane = threadIdx.x & 31;
+  if (lo + blockIdx.x * WPB + (threadIdx.x >> 5) > hi) return;
   int n1 = A.T.p[lev + 1], n2 = A.T.p[lev], nt = n1 + n2;
   zdc* S1 = sh + (threadIdx.x >> 5) * stride + nt;  // S1[k] = t(k) e^{ik theta}, k = -nt..nt
   zdc* S3 = S1 + nt + 1 + nt;                       // S1[k] rs1^(2|k|)
@@ -901,40 +934,46 @@ __global__ void __launch_bounds__(32 * WPB) k_hl2l(int lo, int hi, int lev, Helm
     qa[k] = TA.pw[TA.pw_l2l[lev] + k];
     qb[k] = TA.pw[TA.pw_l2l[lev] + nt + 1 + k];
   }
-  const double4* t =
-      TA.tab + TA.ml_base[lev] + (long)(jb - A.T.lo[lev + 1]) * 2 * (nt + 2) + (nt + 2);
-  double4 nv = t[nt + 1];
-  zdc nrm = mkz(nv.x, nv.y);
-  __syncwarp();
-  for (int k = lane; k <= nt; k += 32) {
-    double4 v = t[k];
-    zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
-    S1[k] = u;    // J_k e^{ik theta}
-    S1[-k] = vv;  // (-1)^k J_k e^{-ik theta}
-    S3[k] = u * qa[k];
-    S3[-k] = vv * qa[k];
-  }
-  const zdc* L2 = expo(A, A.loc, b);
-  for (int n = lane - n2; n <= n2; n += 32) uu[n] = qb[abs(n)] * L2[n];
-  __syncwarp();
-  zdc* L1 = expo(A, A.loc, jb);
-  // per output the terms with n of the other sign form a plain Toeplitz sum
-  // (times rs1^(2|m|)); for the others the symbol S1 or S3 is selected per
-  // lane, so the loops have no branches
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    int m = lane + 32 * r;
-    if (m > n1) break;
-    zdc a1 = mkz(0.0), a2 = mkz(0.0);
-    for (int n = -n2; n < 0; n++) a2 += S1[n - m] * uu[n];
-    for (int n = 0; n <= n2; n++) a1 += (n >= m ? S1[n - m] : S3[n - m]) * uu[n];
-    L1[m] += a1 + qa[m] * a2;
-    if (m == 0) continue;
-    a1 = mkz(0.0);
-    a2 = mkz(0.0);
-    for (int n = 1; n <= n2; n++) a2 += S1[n + m] * uu[n];
-    for (int n = -n2; n <= 0; n++) a1 += (n <= -m ? S1[n + m] : S3[n + m]) * uu[n];
-    L1[-m] += a1 + qa[m] * a2;
+  // the warp loops over the child boxes of the level
+  for (int jb = lo + blockIdx.x * WPB + (threadIdx.x >> 5); jb <= hi; jb += gridDim.x * WPB) {
+    const int b = A.iparent[jb];
+    if (A.itargse[2 * b + 1] < A.itargse[2 * b] || (nl2[b] == 0 && nl4[b] == 0)) continue;
+    if (A.itargse[2 * jb + 1] < A.itargse[2 * jb]) continue;
+    const double4* t =
+        TA.tab + TA.ml_base[lev] + (long)(jb - A.T.lo[lev + 1]) * 2 * (nt + 2) + (nt + 2);
+    double4 nv = t[nt + 1];
+    zdc nrm = mkz(nv.x, nv.y);
+    __syncwarp();
+    for (int k = lane; k <= nt; k += 32) {
+      double4 v = t[k];
+      zdc u = nrm * mkz(v.x, v.y), vv = nrm * mkz(v.z, v.w);
+      S1[k] = u;    // J_k e^{ik theta}
+      S1[-k] = vv;  // (-1)^k J_k e^{-ik theta}
+      S3[k] = u * qa[k];
+      S3[-k] = vv * qa[k];
+    }
+    const zdc* L2 = expo(A, A.loc, b);
+    for (int n = lane - n2; n <= n2; n += 32) uu[n] = qb[abs(n)] * L2[n];
+    __syncwarp();
+    zdc* L1 = expo(A, A.loc, jb);
+    // per output the terms with n of the other sign form a plain Toeplitz sum
+    // (times rs1^(2|m|)); for the others the symbol S1 or S3 is selected per
+    // lane, so the loops have no branches
+  #pragma unroll
+    for (int r = 0; r < R; r++) {
+      int m = lane + 32 * r;
+      if (m > n1) break;
+      zdc a1 = mkz(0.0), a2 = mkz(0.0);
+      for (int n = -n2; n < 0; n++) a2 += S1[n - m] * uu[n];
+      for (int n = 0; n <= n2; n++) a1 += (n >= m ? S1[n - m] : S3[n - m]) * uu[n];
+      L1[m] += a1 + qa[m] * a2;
+      if (m == 0) continue;
+      a1 = mkz(0.0);
+      a2 = mkz(0.0);
+      for (int n = 1; n <= n2; n++) a2 += S1[n + m] * uu[n];
+      for (int n = -n2; n <= 0; n++) a1 += (n <= -m ? S1[n + m] : S3[n + m]) * uu[n];
+      L1[-m] += a1 + qa[m] * a2;
+    }
   }
 }
 
@@ -1262,15 +1301,19 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
   A.zsrc = S.zsrcsort.get(); A.ztarg = S.ztargsort.get(); A.zcsrc = S.zcsrc.get();
   A.zctarg = S.zctarg.get();
   const DevLists& L = S.lists;
-  // list-2 pair offsets of every box, and the first pair of every level
+  // translated list-2 pairs: offsets of every box, the pairs themselves, and
+  // the first pair of every level
   H->pairoff.alloc(nb + 1, s);
+  DevBuf<int2> m2l_pairs;
   {
+    DevBuf<int> cnt(nb, s);
+    klaunch(k_m2l_pair_count, div_up(nb, 128), 128, 0, s, nb, A, L.n[1].get(), L.list[1].get(),
+            L.mn[1], cnt.get());
     size_t bytes = 0;
-    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, L.n[1].get(), H->pairoff.get(), nb, s));
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.get(), H->pairoff.get(), nb, s));
     DevBuf<char> tmp(bytes, s);
-    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, L.n[1].get(), H->pairoff.get(), nb,
-                                          s));
-    klaunch(k_last_plus, 1, 1, 0, s, H->pairoff.get(), L.n[1].get(), nb, H->pairoff.get() + nb);
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, cnt.get(), H->pairoff.get(), nb, s));
+    klaunch(k_last_plus, 1, 1, 0, s, H->pairoff.get(), cnt.get(), nb, H->pairoff.get() + nb);
   }
   std::vector<int> idx(nlev + 2);
   for (int l = 0; l <= nlev; l++) idx[l] = t.laddr[2 * l];
@@ -1359,10 +1402,12 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
   TA.pw = H->pw.get();
   if (nlev >= 2) {
     long q0 = p0[2], q1 = p0[nlev + 1];
+    m2l_pairs.alloc(std::max(1L, (long)p0[nlev + 1]), s);  // every translated pair
+    klaunch(k_m2l_pair_fill, div_up(nb, 128), 128, 0, s, nb, A, L.n[1].get(), L.list[1].get(),
+            L.mn[1], H->pairoff.get(), m2l_pairs.get());
     if (q1 > q0)
       tuned_launch("k_tab_m2l", q1 - q0, 128, {32, 64, 128}, [&](int bs) {
-        klaunch(k_tab_m2l, div_up(q1 - q0, bs), bs, 0, s, q0, q1, t.laddr[4], nb - 1, A, TA,
-                H->pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1]);
+        klaunch(k_tab_m2l, div_up(q1 - q0, bs), bs, 0, s, q0, q1, A, TA, m2l_pairs.get());
       }, s);
   }
   if (nlev >= 3) {
@@ -1424,10 +1469,11 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
       }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
-      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+      if (hi < lo) continue;
       auto go = [&](auto kern) {
-        klaunch(kern, grid, 32 * WPB, 0, s, lo, hi, A, H.p2m_cnt.get(), H.p2m_base.get(),
-                (const zdc*)cols.get());
+        klaunch(kern, resident_grid(kern, 0, hi - lo + 1), 32 * WPB, 0, s, lo, hi, A,
+                H.p2m_cnt.get(), H.p2m_base.get(), (const zdc*)cols.get());
       };
       switch (pickR(slots(P2))) {
         case 1: go(k_form_sum<1, false>); break;
@@ -1441,13 +1487,15 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   ZF_LAUNCH_CHECK();
   cmark(2);
   for (int l = nlev - 1; l >= 2 && (stages & ST_UP); l--) {
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    if (hi < lo) continue;
     int ntt = A.T.p[l] + A.T.p[l + 1], nin = A.T.p[l + 1];
     int stride = 3 * (2 * ntt + 1) + 2 * (2 * nin + 1);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     auto go = [&](auto kern) {
       ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, l, A, TA, stride);
+      klaunch(kern, resident_grid(kern, sm, hi - lo + 1), 32 * WPB, sm, s, lo, hi, l, A, TA,
+              stride);
     };
     switch (pickR(slots(A.T.p[l] + 1))) {
       case 1: go(k_hm2m<1>); break;
@@ -1464,11 +1512,14 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
     int pl_ = A.T.p[l];
     int stride = hm2l_stride(pl_);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+    if (hi < lo) continue;
     auto go = [&](auto kern) {
       ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, A, TA, H.pairoff.get(), L.n[1].get(),
-              L.list[1].get(), L.mn[1], stride);
+      // one warp per box: the boxes' pair counts vary too much for a fixed
+      // share of boxes per warp
+      klaunch(kern, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, A, TA, H.pairoff.get(),
+              L.n[1].get(), L.list[1].get(), L.mn[1], stride);
     };
     switch (pickR(slots(pl_ + 1))) {
       case 1: go(k_hm2l<1>); break;
@@ -1489,10 +1540,11 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
     }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
-      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1], grid = div_up(hi - lo + 1, WPB);
+      int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
+      if (hi < lo) continue;
       auto go = [&](auto kern) {
-        klaunch(kern, grid, 32 * WPB, 0, s, lo, hi, A, H.p2l_cnt.get(), H.p2l_base.get(),
-                (const zdc*)cols.get());
+        klaunch(kern, resident_grid(kern, 0, hi - lo + 1), 32 * WPB, 0, s, lo, hi, A,
+                H.p2l_cnt.get(), H.p2l_base.get(), (const zdc*)cols.get());
       };
       switch (pickR(slots(P2))) {
         case 1: go(k_form_sum<1, true>); break;
@@ -1506,12 +1558,14 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   ZF_LAUNCH_CHECK();
   cmark(4);
   for (int l = 2; l <= nlev - 1 && (stages & ST_DOWN); l++) {
-    int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1], grid = div_up(hi - lo + 1, WPB);
+    int lo = t.laddr[2 * (l + 1)], hi = t.laddr[2 * (l + 1) + 1];
+    if (hi < lo) continue;
     int stride = trans_stride(A.T.p[l] + A.T.p[l + 1], A.T.p[l]);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
     auto go = [&](auto kern) {
       ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, l, A, TA, L.n[1].get(), L.n[3].get(), stride);
+      klaunch(kern, resident_grid(kern, sm, hi - lo + 1), 32 * WPB, sm, s, lo, hi, l, A, TA,
+              L.n[1].get(), L.n[3].get(), stride);
     };
     switch (pickR(slots(A.T.p[l + 1] + 1))) {
       case 1: go(k_hl2l<1>); break;
@@ -1617,13 +1671,12 @@ void helm2d_passes_nd(const Setup2D& S, const Helm2DPrep& H, int nd, int ifcharg
           Aj.loc = loc.get() + j * tot;
           int stride = hm2l_stride(p);
           size_t sm = (size_t)WPB * stride * sizeof(zdc);
-          int grid = div_up(hi - lo + 1, WPB);
           auto slots = (p + 1 + 31) / 32;
           auto go = [&](auto kern) {
             ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm));
-            klaunch(kern, grid, 32 * WPB, sm, s, lo, hi, Aj, H.TA, H.pairoff.get(),
-                    L.n[1].get(), L.list[1].get(), L.mn[1], stride);
+            klaunch(kern, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, Aj, H.TA,
+                    H.pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1], stride);
           };
           if (slots <= 1) go(k_hm2l<1>);
           else if (slots <= 2) go(k_hm2l<2>);
