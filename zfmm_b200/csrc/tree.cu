@@ -291,6 +291,62 @@ __global__ void k_coll(int lo, int hi, double tol, const int* __restrict__ ipare
   ncoll[b] = cnt;
 }
 
+// The same lists with one lane per colleague of the parent: a group of G
+// lanes (G a power of two >= mnbors, within one warp) serves box b; lane i
+// tests the children of the parent's i-th colleague in child order, and an
+// exclusive prefix of the lanes' counts places them, so the list order is the
+// order of k_coll (parent colleague, then child).
+template <int D, int G>
+__global__ void k_coll_g(int lo, int hi, double tol, const int* __restrict__ iparent,
+                         const int* __restrict__ ichild, const double* __restrict__ centers,
+                         int mnbors, int* ncoll, int* coll) {
+  constexpr int NC = 1 << D;
+  const int sub = threadIdx.x & (G - 1);
+  const long gi = (blockIdx.x * (long)blockDim.x + threadIdx.x) / G;
+  const bool valid = gi <= (long)(hi - lo);
+  const int b = valid ? lo + (int)gi : lo;
+  const int dad = valid ? iparent[b] : 0;
+  const int nd = valid ? ncoll[dad] : 0;
+  int found[NC], cnt = 0;
+  if (sub < nd) {
+    const int jb = coll[(long)dad * mnbors + sub];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      const int kb = ichild[jb * NC + c];
+      if (kb >= 0 && within_tol<D>(centers + kb * D, centers + b * D, tol)) found[cnt++] = kb;
+    }
+  }
+  int x = cnt;  // inclusive prefix over the group
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o, G);
+    if (sub >= o) x += y;
+  }
+  const int total = __shfl_sync(0xffffffffu, x, G - 1, G);
+  if (!valid) return;
+  int* out = coll + (long)b * mnbors;
+  for (int k = 0; k < cnt; k++) out[x - cnt + k] = found[k];
+  for (int k = total + sub; k < mnbors; k += G) out[k] = -1;
+  if (sub == 0) ncoll[b] = total;
+}
+
+// colleagues of boxes lo..hi (their parents' lists complete)
+template <int D>
+void launch_coll(int lo, int hi, double tol, const int* iparent, const int* ichild,
+                 const double* centers, int mnbors, int* ncoll, int* coll, cudaStream_t s) {
+  if (hi < lo) return;
+  const long n = hi - lo + 1;
+  if (mnbors <= 16)
+    klaunch(k_coll_g<D, 16>, (int)div_up(n * 16, (long)TB), TB, 0, s, lo, hi, tol, iparent,
+            ichild, centers, mnbors, ncoll, coll);
+  else if (mnbors <= 32)
+    klaunch(k_coll_g<D, 32>, (int)div_up(n * 32, (long)TB), TB, 0, s, lo, hi, tol, iparent,
+            ichild, centers, mnbors, ncoll, coll);
+  else
+    klaunch(k_coll<D>, (int)div_up(n, (long)TB), TB, 0, s, lo, hi, tol, iparent, ichild,
+            centers, mnbors, ncoll, coll);
+}
+
 __global__ void k_coll_root(int* ncoll, int* coll, int mnbors) {
   ncoll[0] = 1;
   coll[0] = 0;
@@ -651,8 +707,8 @@ void colleagues_all(BoxArrays& B, int nlevels, const std::vector<int>& laddr,
     int lo = laddr[2 * l], hi = laddr[2 * l + 1];
     if (hi < lo) continue;
     double tol = (double)1.05f * bsz[l] * (double)isep;
-    klaunch(k_coll<D>, div_up(hi - lo + 1, TB), TB, 0, s, lo, hi, tol, B.iparent.get(), B.ichild.get(),
-                                                   B.centers.get(), mnbors, ncoll.get(), coll.get());
+    launch_coll<D>(lo, hi, tol, B.iparent.get(), B.ichild.get(), B.centers.get(), mnbors,
+                   ncoll.get(), coll.get(), s);
   }
   ZF_LAUNCH_CHECK();
 }
@@ -904,9 +960,8 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
       int nlo = tail[2 * (l + 1)], nhi = tail[2 * (l + 1) + 1];
       if (nhi >= nlo) {
         double tol = (double)((float)p.isep * 1.05f) * bsz[l + 1];
-        klaunch(k_coll<D>, div_up(nhi - nlo + 1, TB), TB, 0, s, nlo, nhi, tol, B.iparent.get(),
-                                                          B.ichild.get(), B.centers.get(), mnbors,
-                                                          ncoll.get(), coll.get());
+        launch_coll<D>(nlo, nhi, tol, B.iparent.get(), B.ichild.get(), B.centers.get(), mnbors,
+                       ncoll.get(), coll.get(), s);
       }
       ZF_LAUNCH_CHECK();
     }
