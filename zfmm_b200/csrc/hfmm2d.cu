@@ -219,6 +219,15 @@ __global__ void k_m2l_pair_fill(int nb, HelmArgs A, const int* nl2, const int* l
   }
 }
 
+__global__ void k_m2l_box_flag(int nb, const int* pairoff, int* flag) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb) flag[b] = pairoff[b + 1] > pairoff[b] ? 1 : 0;
+}
+__global__ void k_m2l_box_scatter(int nb, const int* flag, const int* rank, int* boxes) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb && flag[b]) boxes[rank[b]] = b;
+}
+
 // M2L tables of the translated list-2 pairs q0 .. q1-1 (one thread per pair)
 __global__ void __launch_bounds__(128) k_tab_m2l(long q0, long q1, HelmArgs A, TabArgs TA,
                                                  const int2* pairs) {
@@ -303,15 +312,15 @@ __device__ __forceinline__ void src_coeffs(const HelmArgs& A, const SrcTerm& t, 
 }
 
 // P2M column of source j about centre (c1, c2): Bessel functions by the
-// backward recurrence (coefficients emitted from m = p down to 0, scaled by
-// the normalisation at the end)
-__device__ void p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col) {
+// backward recurrence (coefficients emitted from m = p down to 0); returns
+// Miller's normalisation factor of the column, which the column sum applies
+// (a rescaling here would read and write the column a second time)
+__device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col) {
   zdc a1 = ldz(&A.zsrc[2 * j]) - c1, a2 = ldz(&A.zsrc[2 * j + 1]) - c2;
   zdc rzk, ez;
   polar(a1, a2, rzk, ez);
   SrcTerm t = src_term(A, j, a1, a2, rzk);
   zdc z = rzk * A.zk;
-  const int P2 = 2 * p + 1;
   if (zabs(z) < 1e-200) {  // jbessel2d's table for z = 0: J_0 = 1, the rest 0
     for (int m = 0; m <= p; m++) {
       zdc fm = m == 0 ? mkz(1.0) : mkz(0.0);
@@ -321,7 +330,7 @@ __device__ void p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
       col[p + m] = cp;
       if (m) col[p - m] = cn;
     }
-    return;
+    return mkz(1.0);
   }
   int ntop = jbessel_top(p, z);
   zdc zr = rs * zinv(z);
@@ -363,8 +372,7 @@ __device__ void p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
   }
   psi = 2.0 * rs * psi + g0;
   zdc ex = z.im < 0.0 ? zexp_p(zmul_i(z)) : zexp_p(-zmul_i(z));
-  zdc sc = ex / psi;
-  for (int i = 0; i < P2; i++) col[i] = col[i] * sc;
+  return ex / psi;
 }
 
 // P2L column of source j about centre (c1, c2): Hankel functions by the
@@ -442,14 +450,15 @@ __global__ void k_form_counts(int nb, HelmArgs A, const int* nl4, const int* l4,
 
 // P2M columns, one thread per source
 __global__ void __launch_bounds__(128) k_p2m_cols(int ns, HelmArgs A, const int* srcleaf,
-                                                  const long long* colbase, zdc* cols) {
+                                                  const long long* colbase, zdc* cols,
+                                                  zdc* colscale) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ns) return;
   int b = srcleaf[j];
   if (b < 0) return;
   int l = A.ilevel[b], p = A.T.p[l];
   zdc* col = cols + colbase[b] + (long long)(j - A.isrcse[2 * b]) * (2 * p + 1);
-  p2m_column(A, j, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, col);
+  colscale[j] = p2m_column(A, j, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, col);
 }
 
 // box of flattened index q: the last box in [lo, hi] with off[box] <= q
@@ -489,13 +498,14 @@ __global__ void __launch_bounds__(128) k_p2l_cols(long long nq, int b0, int b1, 
 }
 
 // sums of the columns of every box of one level: warps loop over the boxes, R register
-// slots per lane (2p+1 <= 32 R); P2M writes the multipole expansion, P2L adds
+// slots per lane (2p+1 <= 32 R); P2M writes the multipole expansion (its
+// columns times their sources' normalisation factors colscale[j]), P2L adds
 // to the local expansion
 template <int R, bool LOCAL>
 __global__ void __launch_bounds__(32 * WPB) k_form_sum(int lo, int hi, HelmArgs A,
                                                        const long long* cnt,
                                                        const long long* colbase,
-                                                       const zdc* cols) {
+                                                       const zdc* cols, const zdc* colscale) {
   const int lane = threadIdx.x & 31;
   // every box of the launch is on one level; the warp loops over boxes
   const int p = A.T.p[A.ilevel[lo]], P2 = 2 * p + 1;
@@ -507,10 +517,12 @@ __global__ void __launch_bounds__(32 * WPB) k_form_sum(int lo, int hi, HelmArgs 
 #pragma unroll
     for (int r = 0; r < R; r++) acc[r] = mkz(0.0);
     for (long long k = 0; k < n; k++) {
+      // P2M: the columns are the box's own sources in order
+      const zdc sc = LOCAL ? mkz(1.0) : ldz(&colscale[A.isrcse[2 * b] + k]);
 #pragma unroll
       for (int r = 0; r < R; r++) {
         int i = lane + 32 * r;
-        if (i < P2) acc[r] += ldz(&c[k * P2 + i]);
+        if (i < P2) acc[r] += LOCAL ? ldz(&c[k * P2 + i]) : ldz(&c[k * P2 + i]) * sc;
       }
     }
     zdc* E = expo(A, LOCAL ? A.loc : A.mp, b) - p;
@@ -659,13 +671,15 @@ int resident_grid(K kern, size_t smem, int nboxes) {
 
 template <int R>
 __global__ void __launch_bounds__(32 * WPB, R == 1 ? 8 : 4)
-    k_hm2l(int lo, int hi, HelmArgs A, TabArgs TA, const int* pairoff, const int* nl2,
-           const int* l2, int m2, int stride) {
+    k_hm2l(int nbx, const int* boxes, HelmArgs A, TabArgs TA, const int* pairoff,
+           const int* nl2, const int* l2, int m2, int stride) {
   extern __shared__ zdc sh[];
   const int lane = threadIdx.x & 31;
-  if (lo + blockIdx.x * WPB + (threadIdx.x >> 5) > hi) return;
-  // every box of the launch is on one level; the warp loops over boxes
-  const int l = A.ilevel[lo], p = A.T.p[l], n2 = 2 * p;
+  const int ib = blockIdx.x * WPB + (threadIdx.x >> 5);
+  if (ib >= nbx) return;
+  // boxes: the level's boxes with translated pairs, one warp each
+  const int b = boxes[ib];
+  const int l = A.ilevel[b], p = A.T.p[l], n2 = 2 * p;
   zdc* Ts = sh + (threadIdx.x >> 5) * stride;  // T[k], k = -n2-1..n2+1, split by parity
   double* rp = (double*)(Ts + 2 * (n2 + 3));    // rs^k, k = 0..n2
   zdc* bb = Ts + 2 * (n2 + 3) + (n2 + 2) + p;   // b(n), n = -p..p
@@ -683,60 +697,56 @@ __global__ void __launch_bounds__(32 * WPB, R == 1 ? 8 : 4)
     rpm0[r] = m0 <= p ? rp[2 * m0] : 0.0;
     rpm1[r] = m0 + 1 <= p ? rp[2 * m0 + 2] : 0.0;
   }
-  for (int b = lo + blockIdx.x * WPB + (threadIdx.x >> 5); b <= hi; b += gridDim.x * WPB) {
-    if (A.itargse[2 * b + 1] < A.itargse[2 * b]) continue;
-    const int n2c = nl2[b];
-    if (n2c == 0) continue;
-    zdc acc0[R], acc1[R];
-  #pragma unroll
-    for (int r = 0; r < R; r++) acc0[r] = acc1[r] = mkz(0.0);
-    const double4* tl = TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
-    int used = 0;  // translated pairs of the box so far
-    for (int il = 0; il < n2c; il++) {
-      int jb = l2[(size_t)b * m2 + il];
-      if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-      __syncwarp();
-      const double4* t = tl + (long)(used++) * (n2 + 1);
-      for (int k = lane; k <= n2; k += 32) {
-        double4 v = t[k];
-        Ts[tpos(k, n2)] = mkz(v.x, v.y);
-        Ts[tpos(-k, n2)] = mkz(v.z, v.w);
-      }
-      const zdc* M = expo(A, A.mp, jb);
-      for (int n = lane - p; n <= p; n += 32) bb[n] = M[n];
-      __syncwarp();
-  #pragma unroll
-      for (int r = 0; r < R; r++) {
-        const int m0 = 2 * kq + 32 * r;
-        if (m0 > p) break;
-        zdc prev = Ts[tpos(sg * (-p - 1 - m0), n2)];  // T[sg (n - m0 - 1)] at n = -p
-        zdc s0 = mkz(0.0), s1 = mkz(0.0);
-        for (int n = -p; n < 0; n++) {
-          const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
-          s0 += cur * bn;
-          s1 += prev * bn;
-          prev = cur;
-        }
-        const int m1 = m0 + 1;
-        for (int n = 0; n <= p; n++) {
-          const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
-          const double rn = rp[2 * n];
-          s0 += cur * ((n <= m0 ? rn : rpm0[r]) * bn);
-          s1 += prev * ((n <= m1 ? rn : rpm1[r]) * bn);
-          prev = cur;
-        }
-        acc0[r] += s0;
-        acc1[r] += s1;
-      }
+  const int n2c = nl2[b];
+  zdc acc0[R], acc1[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) acc0[r] = acc1[r] = mkz(0.0);
+  const double4* tl = TA.tab + TA.m2l_base[l] + (pairoff[b] - TA.m2l_pair0[l]) * (long)(n2 + 1);
+  int used = 0;  // translated pairs of the box so far
+  for (int il = 0; il < n2c; il++) {
+    int jb = l2[(size_t)b * m2 + il];
+    if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
+    __syncwarp();
+    const double4* t = tl + (long)(used++) * (n2 + 1);
+    for (int k = lane; k <= n2; k += 32) {
+      double4 v = t[k];
+      Ts[tpos(k, n2)] = mkz(v.x, v.y);
+      Ts[tpos(-k, n2)] = mkz(v.z, v.w);
     }
-    zdc* L = expo(A, A.loc, b);
-  #pragma unroll
+    const zdc* M = expo(A, A.mp, jb);
+    for (int n = lane - p; n <= p; n += 32) bb[n] = M[n];
+    __syncwarp();
+#pragma unroll
     for (int r = 0; r < R; r++) {
-      const int m0 = 2 * kq + 32 * r, m1 = m0 + 1;
+      const int m0 = 2 * kq + 32 * r;
       if (m0 > p) break;
-      if (m0 > 0 || h == 0) L[sg * m0] = acc0[r];  // loc(0) once, from the + half
-      if (m1 <= p) L[sg * m1] = acc1[r];
+      zdc prev = Ts[tpos(sg * (-p - 1 - m0), n2)];  // T[sg (n - m0 - 1)] at n = -p
+      zdc s0 = mkz(0.0), s1 = mkz(0.0);
+      for (int n = -p; n < 0; n++) {
+        const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
+        s0 += cur * bn;
+        s1 += prev * bn;
+        prev = cur;
+      }
+      const int m1 = m0 + 1;
+      for (int n = 0; n <= p; n++) {
+        const zdc bn = bb[sg * n], cur = Ts[tpos(sg * (n - m0), n2)];
+        const double rn = rp[2 * n];
+        s0 += cur * ((n <= m0 ? rn : rpm0[r]) * bn);
+        s1 += prev * ((n <= m1 ? rn : rpm1[r]) * bn);
+        prev = cur;
+      }
+      acc0[r] += s0;
+      acc1[r] += s1;
     }
+  }
+  zdc* L = expo(A, A.loc, b);
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int m0 = 2 * kq + 32 * r, m1 = m0 + 1;
+    if (m0 > p) break;
+    if (m0 > 0 || h == 0) L[sg * m0] = acc0[r];  // loc(0) once, from the + half
+    if (m1 <= p) L[sg * m1] = acc1[r];
   }
 }
 
@@ -1231,6 +1241,10 @@ struct Helm2DPrep {
   HelmArgs A0;  // level table and geometry pointers (strength pointers unset)
   TabArgs TA;
   DevBuf<int> pairoff;
+  // boxes with translated list-2 pairs in box order; those of level l are
+  // m2l_boxes[m2l_box0[l] .. m2l_box0[l+1])
+  DevBuf<int> m2l_boxes;
+  std::vector<int> m2l_box0;
   DevBuf<double4> tab;
   DevBuf<double> pw;
   // P2M / P2L column layout: leaf box of every source; per box the number of
@@ -1315,6 +1329,20 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
     ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, cnt.get(), H->pairoff.get(), nb, s));
     klaunch(k_last_plus, 1, 1, 0, s, H->pairoff.get(), cnt.get(), nb, H->pairoff.get() + nb);
   }
+  // the boxes with translated pairs (the M2L's work list)
+  DevBuf<int> boxrank(nb + 1, s);
+  H->m2l_boxes.alloc(nb, s);
+  {
+    DevBuf<int> fl(nb, s);
+    klaunch(k_m2l_box_flag, div_up(nb, 128), 128, 0, s, nb, H->pairoff.get(), fl.get());
+    size_t bytes = 0;
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, fl.get(), boxrank.get(), nb, s));
+    DevBuf<char> tmp(bytes, s);
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, fl.get(), boxrank.get(), nb, s));
+    klaunch(k_last_plus, 1, 1, 0, s, boxrank.get(), fl.get(), nb, boxrank.get() + nb);
+    klaunch(k_m2l_box_scatter, div_up(nb, 128), 128, 0, s, nb, fl.get(), boxrank.get(),
+            H->m2l_boxes.get());
+  }
   std::vector<int> idx(nlev + 2);
   for (int l = 0; l <= nlev; l++) idx[l] = t.laddr[2 * l];
   idx[nlev + 1] = nb;
@@ -1322,6 +1350,8 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
   ZF_CUDA(cudaMemcpyAsync(didx.get(), idx.data(), idx.size() * sizeof(int),
                           cudaMemcpyHostToDevice, s));
   klaunch(k_pairoff_at, 1, 64, 0, s, H->pairoff.get(), didx.get(), nlev + 2, dout.get());
+  DevBuf<int> dbox0(nlev + 2, s);
+  klaunch(k_pairoff_at, 1, 64, 0, s, boxrank.get(), didx.get(), nlev + 2, dbox0.get());
   std::vector<int> p0;
   // P2M / P2L column layout
   const int ns = (int)(S.zsrcsort.size() / 2);
@@ -1352,6 +1382,9 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
     ZF_CUDA(cudaMemcpyAsync(t3, tot.get(), sizeof(t3), cudaMemcpyDeviceToHost, s));
     std::vector<int> p0h(nlev + 2);
     ZF_CUDA(cudaMemcpyAsync(p0h.data(), dout.get(), p0h.size() * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+    H->m2l_box0.assign(nlev + 2, 0);
+    ZF_CUDA(cudaMemcpyAsync(H->m2l_box0.data(), dbox0.get(), (nlev + 2) * sizeof(int),
                             cudaMemcpyDeviceToHost, s));
     ZF_CUDA(cudaStreamSynchronize(s));
     H->p2m_total = t3[0];
@@ -1461,11 +1494,11 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   // P2M: columns of every source of a leaf of level >= 2, then per level the
   // sums over each leaf's columns
   if (stages & ST_UP) {
-    DevBuf<zdc> cols(H.p2m_total > 0 ? H.p2m_total : 1, s);
+    DevBuf<zdc> cols(H.p2m_total > 0 ? H.p2m_total : 1, s), colscale(H.ns > 0 ? H.ns : 1, s);
     if (H.ns > 0)
       tuned_launch("k_p2m_cols", H.ns, 128, {32, 64, 128}, [&](int bs) {
         klaunch(k_p2m_cols, div_up(H.ns, bs), bs, 0, s, H.ns, A, H.srcleaf.get(),
-                H.p2m_base.get(), cols.get());
+                H.p2m_base.get(), cols.get(), colscale.get());
       }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
@@ -1473,7 +1506,8 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
       if (hi < lo) continue;
       auto go = [&](auto kern) {
         klaunch(kern, resident_grid(kern, 0, hi - lo + 1), 32 * WPB, 0, s, lo, hi, A,
-                H.p2m_cnt.get(), H.p2m_base.get(), (const zdc*)cols.get());
+                H.p2m_cnt.get(), H.p2m_base.get(), (const zdc*)cols.get(),
+                (const zdc*)colscale.get());
       };
       switch (pickR(slots(P2))) {
         case 1: go(k_form_sum<1, false>); break;
@@ -1512,14 +1546,13 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
     int pl_ = A.T.p[l];
     int stride = hm2l_stride(pl_);
     size_t sm = (size_t)WPB * stride * sizeof(zdc);
-    int lo = t.laddr[2 * l], hi = t.laddr[2 * l + 1];
-    if (hi < lo) continue;
+    const int nbx = H.m2l_box0[l + 1] - H.m2l_box0[l];
+    if (nbx <= 0) continue;
     auto go = [&](auto kern) {
       ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      // one warp per box: the boxes' pair counts vary too much for a fixed
-      // share of boxes per warp
-      klaunch(kern, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, A, TA, H.pairoff.get(),
-              L.n[1].get(), L.list[1].get(), L.mn[1], stride);
+      // one warp per box with translated pairs
+      klaunch(kern, div_up(nbx, WPB), 32 * WPB, sm, s, nbx, H.m2l_boxes.get() + H.m2l_box0[l],
+              A, TA, H.pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1], stride);
     };
     switch (pickR(slots(pl_ + 1))) {
       case 1: go(k_hm2l<1>); break;
@@ -1544,7 +1577,7 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
       if (hi < lo) continue;
       auto go = [&](auto kern) {
         klaunch(kern, resident_grid(kern, 0, hi - lo + 1), 32 * WPB, 0, s, lo, hi, A,
-                H.p2l_cnt.get(), H.p2l_base.get(), (const zdc*)cols.get());
+                H.p2l_cnt.get(), H.p2l_base.get(), (const zdc*)cols.get(), (const zdc*)nullptr);
       };
       switch (pickR(slots(P2))) {
         case 1: go(k_form_sum<1, true>); break;
@@ -1675,8 +1708,11 @@ void helm2d_passes_nd(const Setup2D& S, const Helm2DPrep& H, int nd, int ifcharg
           auto go = [&](auto kern) {
             ZF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm));
-            klaunch(kern, div_up(hi - lo + 1, WPB), 32 * WPB, sm, s, lo, hi, Aj, H.TA,
-                    H.pairoff.get(), L.n[1].get(), L.list[1].get(), L.mn[1], stride);
+            const int nbx = H.m2l_box0[l + 1] - H.m2l_box0[l];
+            if (nbx > 0)
+              klaunch(kern, div_up(nbx, WPB), 32 * WPB, sm, s, nbx,
+                      H.m2l_boxes.get() + H.m2l_box0[l], Aj, H.TA, H.pairoff.get(),
+                      L.n[1].get(), L.list[1].get(), L.mn[1], stride);
           };
           if (slots <= 1) go(k_hm2l<1>);
           else if (slots <= 2) go(k_hm2l<2>);
