@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <initializer_list>
 #include <thread>
 #include <mutex>
@@ -110,6 +111,88 @@ void upload(DevBuf<zdc>& b, const double* h, size_t nz, cudaStream_t s) {
   if (nz) ZF_CUDA(cudaMemcpyAsync(b.get(), h, nz * sizeof(zdc), cudaMemcpyHostToDevice, s));
 }
 
+bool page_locked(const void* p) {
+  cudaPointerAttributes a{};
+  return p && cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeHost;
+}
+
+// The strengths (charges, dipole strengths, dipole vectors) of a host-array
+// FMM call, uploaded on a second stream while the solve's stream uploads the
+// points and builds the tree, which needs only the points.  Page-locked
+// arrays are copied asynchronously; pageable ones from a helper thread (a
+// pageable copy holds its calling thread until the data is staged).  The
+// device buffers are allocated on the solve's stream, which also frees them.
+// ready(s) makes the solve's stream wait for the copies (the set-up calls it
+// before it gathers the strengths); the destructor waits for them in any case.
+class StrengthUpload {
+ public:
+  StrengthUpload(HostIn& h, int ns, int dim, int ifcharge, const double* charge, int ifdipole,
+                 const double* dipstr, const double* dipvec, cudaStream_t s) {
+    ZF_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
+    ZF_CUDA(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
+    if (ifcharge == 1) h.charge.alloc(ns, s);
+    if (ifdipole == 1) {
+      h.dipstr.alloc(ns, s);
+      h.dipvec.alloc((size_t)dim * ns, s);
+    }
+    ZF_CUDA(cudaEventRecord(ev_, s));  // the buffers exist from here on
+    ZF_CUDA(cudaStreamWaitEvent(aux_, ev_, 0));
+    struct Copy {
+      void* d;
+      const void* h;
+      size_t bytes;
+    };
+    std::vector<Copy> copies;
+    if (ifcharge == 1) copies.push_back({h.charge.get(), charge, ns * sizeof(zdc)});
+    if (ifdipole == 1) {
+      copies.push_back({h.dipstr.get(), dipstr, ns * sizeof(zdc)});
+      copies.push_back({h.dipvec.get(), dipvec, (size_t)dim * ns * sizeof(zdc)});
+    }
+    bool pinned = true;
+    for (auto& c : copies) pinned = pinned && page_locked(c.h);
+    cudaStream_t aux = aux_;
+    cudaEvent_t ev = ev_;
+    auto run = [copies, aux, ev]() {
+      for (auto& c : copies)
+        if (c.bytes) ZF_CUDA(cudaMemcpyAsync(c.d, c.h, c.bytes, cudaMemcpyHostToDevice, aux));
+      ZF_CUDA(cudaEventRecord(ev, aux));
+    };
+    if (pinned) {
+      run();
+    } else {
+      int dev = 0;
+      ZF_CUDA(cudaGetDevice(&dev));
+      th_ = std::thread([this, run, dev]() {
+        try {
+          ZF_CUDA(cudaSetDevice(dev));
+          run();
+        } catch (...) {
+          err_ = std::current_exception();
+        }
+      });
+    }
+  }
+  void ready(cudaStream_t s) {
+    if (th_.joinable()) th_.join();
+    if (err_) std::rethrow_exception(err_);
+    ZF_CUDA(cudaStreamWaitEvent(s, ev_, 0));
+  }
+  ~StrengthUpload() {
+    if (th_.joinable()) th_.join();
+    cudaStreamSynchronize(aux_);
+    cudaEventDestroy(ev_);
+    cudaStreamDestroy(aux_);
+  }
+  StrengthUpload(const StrengthUpload&) = delete;
+  StrengthUpload& operator=(const StrengthUpload&) = delete;
+
+ private:
+  cudaStream_t aux_ = nullptr;
+  cudaEvent_t ev_ = nullptr;
+  std::thread th_;
+  std::exception_ptr err_;
+};
+
 Inputs2D make_inputs(int ns, const double* zsrc, int ifcharge, const double* charge,
                      int ifdipole, const double* dipstr, const double* dipvec, int nt,
                      const double* ztarg, int ifpgh) {
@@ -188,16 +271,13 @@ int fmm2d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
     const bool same = ztarg == zsrc && nt == ns;
     upload(h.zsrc, zsrc, 2 * (size_t)ns, s);
     if (!same) upload(h.ztarg, ztarg, 2 * (size_t)nt, s);
-    if (ifcharge == 1) upload(h.charge, charge, ns, s);
-    if (ifdipole == 1) {
-      upload(h.dipstr, dipstr, ns, s);
-      upload(h.dipvec, dipvec, 2 * (size_t)ns, s);
-    }
+    StrengthUpload su(h, ns, 2, ifcharge, charge, ifdipole, dipstr, dipvec, s);
     DevBuf<zdc> dpot(nt, s), dgrad(ifpgh > 1 ? 2 * (size_t)nt : 0, s);
     Inputs2D in = make_inputs(ns, (const double*)h.zsrc.get(), ifcharge,
                               (const double*)h.charge.get(), ifdipole,
                               (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
                               (const double*)(same ? h.zsrc.get() : h.ztarg.get()), ifpgh);
+    in.strengths_ready = [&su](cudaStream_t ss) { su.ready(ss); };
     run_fmm2d(eps, zk, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));
@@ -593,16 +673,13 @@ int fmm3d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
     const bool same = ztarg == zsrc && nt == ns;
     upload(h.zsrc, zsrc, 3 * (size_t)ns, s);
     if (!same) upload(h.ztarg, ztarg, 3 * (size_t)nt, s);
-    if (ifcharge == 1) upload(h.charge, charge, ns, s);
-    if (ifdipole == 1) {
-      upload(h.dipstr, dipstr, ns, s);
-      upload(h.dipvec, dipvec, 3 * (size_t)ns, s);
-    }
+    StrengthUpload su(h, ns, 3, ifcharge, charge, ifdipole, dipstr, dipvec, s);
     DevBuf<zdc> dpot(nt, s), dgrad(ifpgh > 1 ? 3 * (size_t)nt : 0, s);
     Inputs3D in = make_inputs3(ns, (const double*)h.zsrc.get(), ifcharge,
                                (const double*)h.charge.get(), ifdipole,
                                (const double*)h.dipstr.get(), (const double*)h.dipvec.get(), nt,
                                (const double*)(same ? h.zsrc.get() : h.ztarg.get()), ifpgh);
+    in.strengths_ready = [&su](cudaStream_t ss) { su.ready(ss); };
     run_fmm3d(eps, zk, in, isep, dpot.get(), ifpgh > 1 ? dgrad.get() : nullptr, s);
     if (nt > 0) {
       ZF_CUDA(cudaMemcpyAsync(pot, dpot.get(), sizeof(zdc) * nt, cudaMemcpyDeviceToHost, s));

@@ -237,6 +237,7 @@ void setup2d(const Inputs2D& in, const TreeParams& tp, Setup2D& S, cudaStream_t 
   } else {
     sort_points(S.tree, tR, nt, S.itarg, S.itargse, s);
   }
+  if (in.strengths_ready) in.strengths_ready(s);
   S.zsrcsort.alloc(2 * (size_t)ns, s);
   S.chargesort.alloc(ns, s);
   S.dipstrsort.alloc(ns, s);

@@ -6,6 +6,7 @@
 // real geometric centre plus i times the mean of the imaginary parts of the
 // box's sources (resp. targets), computed for every box.
 #pragma once
+#include <functional>
 #include <vector>
 #include "tree.cuh"
 #include "zcomplex.cuh"
@@ -22,6 +23,9 @@ struct Inputs2D {
   const zdc* dipvec = nullptr;
   const zdc* ztarg = nullptr;
   int ifcharge = 0, ifdipole = 0, ifpgh = 1;
+  // when set, called with the solve's stream before the strengths are first
+  // read (the host entry points upload them on a second stream meanwhile)
+  std::function<void(cudaStream_t)> strengths_ready;
 };
 
 struct Setup2D {

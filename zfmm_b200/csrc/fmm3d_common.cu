@@ -274,6 +274,7 @@ void setup3d(const Inputs3D& in, const TreeParams& tp, Setup3D& S, bool rescale_
   }
   S.b0 = S.tree.boxsize[0];
   const double* b0 = S.tree.bsz.get();  // device copy of boxsize; entry 0 = b0
+  if (in.strengths_ready) in.strengths_ready(s);
   S.zsrcsort.alloc(3 * (size_t)ns, s);
   S.chargesort.alloc(ns, s);
   S.dipstrsort.alloc(ns, s);

@@ -7,6 +7,7 @@
 // coordinate, centre and box size is multiplied by b0inv = 1/boxsize(0),
 // charges by b0inv and dipole vectors by b0inv^2 (zlfmm3d.f:187-200).
 #pragma once
+#include <functional>
 #include <vector>
 #include "tree.cuh"
 #include "zcomplex.cuh"
@@ -21,6 +22,9 @@ struct Inputs3D {
   const zdc* dipvec = nullptr;  // dipvec(3,ns)
   const zdc* ztarg = nullptr;   // ztarg(3,nt)
   int ifcharge = 0, ifdipole = 0, ifpgh = 1;
+  // when set, called with the solve's stream before the strengths are first
+  // read (the host entry points upload them on a second stream meanwhile)
+  std::function<void(cudaStream_t)> strengths_ready;
 };
 
 struct Setup3D {
