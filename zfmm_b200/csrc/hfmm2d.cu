@@ -1002,7 +1002,6 @@ __global__ void k_tgt_leaf(int nb, HelmArgs A, int* tgtleaf) {
 
 template <bool GRAD>
 __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgtleaf,
-                                              const int* nl3, const int* l3, int m3,
                                               zdc* potsort, zdc* gradsort) {
   int ti = blockIdx.x * blockDim.x + threadIdx.x;
   if (ti >= nt) return;
@@ -1072,8 +1071,34 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
       }
     }
   }
-  // M2T (zh2devalmp) over list3: streaming forward recurrence of H_n
+  potsort[ti] = pot;
+  if (GRAD) {
+    gradsort[2 * ti] = g1;
+    gradsort[2 * ti + 1] = g2;
+  }
+}
+
+// M2T (zh2devalmp) over list 3, one thread per target, added to what L2T
+// wrote (in the reference's order: L2T, then the list-3 boxes in list order);
+// a separate kernel so that the L2T sweep runs without the list-3 loop's
+// divergence and registers.
+template <bool GRAD>
+__global__ void __launch_bounds__(128) k_hm2t(int nt, HelmArgs A, const int* tgtleaf,
+                                              const int* nl3, const int* l3, int m3,
+                                              zdc* potsort, zdc* gradsort) {
+  int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= nt) return;
+  int b = tgtleaf[ti];
+  if (b < 0) return;
   int n3 = nl3[b];
+  if (n3 == 0) return;
+  zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
+  zdc pot = potsort[ti], g1 = mkz(0.0), g2 = mkz(0.0);
+  if (GRAD) {
+    g1 = gradsort[2 * ti];
+    g2 = gradsort[2 * ti + 1];
+  }
+  // streaming forward recurrence of H_n
   for (int il = 0; il < n3; il++) {
     int jb = l3[(size_t)b * m3 + il];
     if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
@@ -1609,22 +1634,23 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   }
   ZF_LAUNCH_CHECK();
   cmark(5);
-  // L2T + M2T one thread per target (writes), then P2P one thread per target (adds)
+  // L2T one thread per target (writes), then M2T and P2P one thread per target (add)
   const int ntt = H.nt;
   if (!(stages & ST_DOWN)) {
   } else {
-    auto eval = [&](auto l2t, auto p2p) {
+    auto eval = [&](auto l2t, auto m2t, auto p2p) {
       tuned_launch(ifpgh > 1 ? "k_hl2t_g" : "k_hl2t", ntt, 128, {64, 128}, [&](int bs) {
-        klaunch(l2t, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
-                L.list[2].get(), L.mn[2], potsort, gradsort);
+        klaunch(l2t, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), potsort, gradsort);
       }, s);
-      // P2P adds to what L2T wrote (its block size is fixed: tuning would have
-      // to restore the L2T results before every trial)
+      // M2T and P2P add to what L2T wrote (their block sizes are fixed: tuning
+      // would have to restore the L2T results before every trial)
+      klaunch(m2t, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
+              L.list[2].get(), L.mn[2], potsort, gradsort);
       klaunch(p2p, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[0].get(),
               L.list[0].get(), L.mn[0], potsort, gradsort);
     };
-    if (ifpgh > 1) eval(k_hl2t<true>, k_hp2p<true>);
-    else eval(k_hl2t<false>, k_hp2p<false>);
+    if (ifpgh > 1) eval(k_hl2t<true>, k_hm2t<true>, k_hp2p<true>);
+    else eval(k_hl2t<false>, k_hm2t<false>, k_hp2p<false>);
   }
   ZF_LAUNCH_CHECK();
 }
