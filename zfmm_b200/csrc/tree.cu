@@ -26,6 +26,7 @@
 // This file is compiled with --fmad=false so that the distance tests see the
 // same roundings as the reference (no contracted multiply-adds).
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cub/cub.cuh>
 #include <vector>
@@ -127,29 +128,6 @@ __global__ void k_root(const double* part, int nparts, double* centers, double* 
 }
 
 // ---- refinement --------------------------------------------------------------
-__global__ void k_level_flags(int lo, int nb, const int* nsrc, const int* ntarg, int idivflag,
-                              int ndiv, int force, int* flag) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb) return;
-  int b = lo + i;
-  int r = 1;
-  if (!force) {
-    int nss = nsrc[b], ntt = ntarg[b];
-    int nn = idivflag == 0 ? nss : (idivflag == 1 ? ntt : max(nss, ntt));
-    r = nn > ndiv;
-  }
-  flag[b] = r;
-}
-
-__global__ void k_scan_total(const int* flag, const int* rank, int n, int* out) {
-  *out = n > 0 ? rank[n - 1] + (flag[n - 1] > 0 ? 1 : 0) : 0;
-}
-
-__global__ void k_gt0(const int* in, int n, int* out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = in[i] > 0 ? 1 : 0;
-}
-
 // 0/1 flags of the concatenation of in[lo1, lo1+n1) and in[lo2, lo2+n2)
 __global__ void k_gt0_2(const int* in, int lo1, int n1, int lo2, int n2, int* out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,16 +148,13 @@ __global__ void k_pick(const int* flag, const int* rank, int n, const int* pos, 
 // children of every flagged box of [lo, lo+nb): ids first + rank*NC + c.
 // flagmode: children of iflag==1 parents become flag++ (3), of iflag==2 become 0
 // (tree_refine_boxes_flag); otherwise plain refinement.
+// the NC children of box b, ids base .. base+NC-1, on level lev
 template <int D>
-__global__ void k_make_children(int lo, int nb, const int* flag01, const int* rank, int first,
-                                double bs, int lev, int flagmode, double* centers, int* ilevel,
-                                int* iparent, int* nchild, int* ichild, int* iflag, int* nsrc,
-                                int* ntarg) {
+__device__ __forceinline__ void make_children_of(int b, int base, double bs, int lev,
+                                                 int flagmode, double* centers, int* ilevel,
+                                                 int* iparent, int* nchild, int* ichild,
+                                                 int* iflag, int* nsrc, int* ntarg) {
   constexpr int NC = 1 << D;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb || !flag01[i]) return;
-  int b = lo + i;
-  int base = first + rank[i] * NC;
   nchild[b] = NC;
   double cb[D];
 #pragma unroll
@@ -200,6 +175,76 @@ __global__ void k_make_children(int lo, int nb, const int* flag01, const int* ra
     iflag[j] = flagmode ? (pf == 1 ? 3 : 0) : 0;
     if (nsrc) { nsrc[j] = 0; ntarg[j] = 0; }
   }
+}
+
+template <int D>
+__global__ void k_make_children(int lo, int nb, const int* flag01, const int* rank, int first,
+                                double bs, int lev, int flagmode, double* centers, int* ilevel,
+                                int* iparent, int* nchild, int* ichild, int* iflag, int* nsrc,
+                                int* ntarg) {
+  constexpr int NC = 1 << D;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb || !flag01[i]) return;
+  make_children_of<D>(lo + i, first + rank[i] * NC, bs, lev, flagmode, centers, ilevel, iparent,
+                      nchild, ichild, iflag, nsrc, ntarg);
+}
+
+
+// ---- refinement loop driven from the device -----------------------------------
+// lev[2l], lev[2l+1]: first and last box of level l (empty when last < first);
+// *nbox: boxes so far; nref[l]: boxes refined on level l.  A level's kernels
+// are launched with grids sized by an upper bound ub on its box count and read
+// the level's range from lev, so the host does not wait for each level.
+
+// refinement flags of the boxes of level l (iflag, and fl[i] for the i-th box
+// of the level, 0 beyond the level's last box)
+__global__ void k_level_flags_d(const int* lev, int l, int ub, const int* nsrc, const int* ntarg,
+                                int idivflag, int ndiv, int force, int* iflag, int* fl) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ub) return;
+  const int lo = lev[2 * l], hi = lev[2 * l + 1];
+  int r = 0;
+  if (lo + i <= hi) {
+    const int b = lo + i;
+    r = 1;
+    if (!force) {
+      int nss = nsrc[b], ntt = ntarg[b];
+      int nn = idivflag == 0 ? nss : (idivflag == 1 ? ntt : max(nss, ntt));
+      r = nn > ndiv;
+    }
+    iflag[b] = r;
+  }
+  fl[i] = r;
+}
+
+// the range of level l+1 from the exclusive scan rank of fl (single thread)
+__global__ void k_level_advance(int* lev, int l, int ub, const int* fl, const int* rank, int NC,
+                                int* nbox, int* nref) {
+  const int tot = ub > 0 ? rank[ub - 1] + fl[ub - 1] : 0;
+  const int first = *nbox;
+  lev[2 * (l + 1)] = first;
+  lev[2 * (l + 1) + 1] = first + tot * NC - 1;
+  *nbox = first + tot * NC;
+  nref[l] = tot;
+}
+
+// children of the flagged boxes of level l, numbered from the first box of
+// level l+1 in scan order
+template <int D>
+__global__ void k_make_children_d(const int* lev, int l, int ub, const int* fl, const int* rank,
+                                  double bs, double* centers, int* ilevel, int* iparent,
+                                  int* nchild, int* ichild, int* iflag, int* nsrc, int* ntarg) {
+  constexpr int NC = 1 << D;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ub || !fl[i]) return;
+  make_children_of<D>(lev[2 * l] + i, lev[2 * (l + 1)] + rank[i] * NC, bs, l + 1, 0, centers,
+                      ilevel, iparent, nchild, ichild, iflag, nsrc, ntarg);
+}
+
+// dst = src over the boxes of level l (targets that are the sources)
+__global__ void k_copy_level(const int* lev, int l, int ub, const int* src, int* dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ub && lev[2 * l] + i <= lev[2 * l + 1]) dst[lev[2 * l] + i] = src[lev[2 * l] + i];
 }
 
 template <int D>
@@ -628,28 +673,10 @@ int* pinned_words() {
 
 struct Scanner {
   DevBuf<char> tmp;
-  DevBuf<int> total;
   DevBuf<int> flag01, rank;
-  int* h_total = nullptr;
+  int* h_words = nullptr;  // page-locked result words
   cudaStream_t s;
-  explicit Scanner(cudaStream_t st) : s(st) {
-    total.alloc(1, s);
-    h_total = pinned_words();
-  }
-  // flags01/rank over `src` (values > 0 count as set) of length n; returns total
-  int scan(const int* src, int n) {
-    if (n <= 0) return 0;
-    if ((int)flag01.size() < n) { flag01.alloc(n, s); rank.alloc(n, s); }
-    klaunch(k_gt0, div_up(n, TB), TB, 0, s, src, n, flag01.get());
-    size_t bytes = 0;
-    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag01.get(), rank.get(), n, s));
-    if (tmp.size() < bytes) tmp.alloc(bytes, s);
-    ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, flag01.get(), rank.get(), n, s));
-    klaunch(k_scan_total, 1, 1, 0, s, flag01.get(), rank.get(), n, total.get());
-    ZF_CUDA(cudaMemcpyAsync(h_total, total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    ZF_CUDA(cudaStreamSynchronize(s));
-    return *h_total;
-  }
+  explicit Scanner(cudaStream_t st) : s(st) { h_words = pinned_words(); }
   // flags01/rank over the concatenation of src[lo1, lo1+n1) and
   // src[lo2, lo2+n2) in one scan; returns the exclusive prefix at each of
   // `pos` (a position n1+n2 gives the total), with one wait for the host
@@ -668,7 +695,7 @@ struct Scanner {
     ZF_CUDA(cudaMemcpyAsync(dpos.get(), pos.data(), np * sizeof(int), cudaMemcpyHostToDevice, s));
     klaunch(k_pick, div_up(np, TB), TB, 0, s, flag01.get(), rank.get(), n, dpos.get(), np,
             dout.get());
-    int* h = np <= kPinnedWords ? h_total : out.data();  // a level count above 1024: pageable
+    int* h = np <= kPinnedWords ? h_words : out.data();  // above 1024 positions: pageable
     ZF_CUDA(cudaMemcpyAsync(h, dout.get(), np * sizeof(int), cudaMemcpyDeviceToHost, s));
     ZF_CUDA(cudaStreamSynchronize(s));
     if (h != out.data()) std::copy(h, h + np, out.begin());
@@ -841,37 +868,89 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
   const double* a_src = zs_src.get();
   const double* a_targ = same ? a_src : zs_targ.get();
 
-  std::vector<int> laddr(2 * (p.nlmax + 1), 0);
-  laddr[0] = 0;
-  laddr[1] = 0;
-  int n = 1, ilev;
-  for (ilev = 0; ilev < p.nlmax; ilev++) {
-    int lo = laddr[2 * ilev], hi = laddr[2 * ilev + 1], nb = hi - lo + 1;
-    klaunch(k_level_flags, div_up(nb, TB), TB, 0, s, lo, nb, B.nsrc.get(), B.ntarg.get(), p.idivflag,
-                                                 p.ndiv, ilev < p.nlmin, B.iflag.get());
-    int nref = S.scan(B.iflag.get() + lo, nb);
-    if (nref == 0) break;
-    bsz[ilev + 1] = bsz[ilev] / 2;
-    B.reserve((size_t)n + (size_t)nref * NC, n);
-    klaunch(k_make_children<D>, div_up(nb, TB), TB, 0, s, 
-        lo, nb, S.flag01.get(), S.rank.get(), n, bsz[ilev + 1], ilev + 1, 0, B.centers.get(),
-        B.ilevel.get(), B.iparent.get(), B.nchild.get(), B.ichild.get(), B.iflag.get(),
-        B.nsrc.get(), B.ntarg.get());
-    klaunch(k_assign<D>, div_up(ns, TB), TB, 0, s, a_src, ns, pbs.get(), B.ilevel.get(), B.nchild.get(),
-                                              B.ichild.get(), B.centers.get(), ilev, B.nsrc.get());
-    if (same)  // targets are the sources: the same children, the same counts
-      ZF_CUDA(cudaMemcpyAsync(B.ntarg.get() + n, B.nsrc.get() + n, sizeof(int) * nref * NC,
-                              cudaMemcpyDeviceToDevice, s));
-    else
-      klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, a_targ, nt, pbt.get(), B.ilevel.get(),
-              B.nchild.get(), B.ichild.get(), B.centers.get(), ilev, B.ntarg.get());
-    ZF_LAUNCH_CHECK();
-    laddr[2 * (ilev + 1)] = n;
-    laddr[2 * (ilev + 1) + 1] = n + nref * NC - 1;
-    n += nref * NC;
+  // Refinement, level by level as in the reference, with the level ranges on
+  // the device: a chunk of levels is launched with grids sized by upper
+  // bounds on the box counts (a box is refined only with more than ndiv
+  // points, so at most (ns + nt) / (ndiv + 1) + 1 boxes of a level are
+  // refined, all of them on forced levels), then the host reads the counts
+  // back once and stops at the first level that refines nothing.
+  const long rmax = ((long)ns + nt) / (p.ndiv + 1) + 1;
+  DevBuf<int> dlev(2 * (p.nlmax + 2), s), dnref(p.nlmax + 1, s), dnbox(1, s);
+  {
+    const int init[3] = {0, 0, 1};  // level 0 = the root; one box
+    ZF_CUDA(cudaMemcpyAsync(dlev.get(), init, 2 * sizeof(int), cudaMemcpyHostToDevice, s));
+    ZF_CUDA(cudaMemcpyAsync(dnbox.get(), init + 2, sizeof(int), cudaMemcpyHostToDevice, s));
   }
-  int nlevels = ilev;
-  laddr.resize(2 * (nlevels + 1));
+  DevBuf<int> fl, rank;
+  DevBuf<char> scan_tmp;
+  int* hw = pinned_words();
+  int n = 1, nb_cur = 1, l0 = 0, nlevels = -1;
+  while (nlevels < 0 && l0 < p.nlmax) {
+    // levels l0 .. l1-1 of this chunk, while the boxes they may add stay
+    // within max(2^20, 8 n)
+    std::vector<long> ub(1, nb_cur);
+    long add = 0;
+    int l1 = l0;
+    while (l1 < p.nlmax) {
+      const long u = ub.back(), refined = l1 < p.nlmin ? u : std::min(u, rmax);
+      const long next = refined * NC;
+      if (l1 > l0 && add + next > std::max(1L << 20, 8L * n)) break;
+      if ((long)n + add + next > (long)INT_MAX / 2)
+        throw zf_error(ZF_ERR_ARG, "tree too large");
+      add += next;
+      ub.push_back(next);
+      l1++;
+    }
+    B.reserve((size_t)n + (size_t)add, n);
+    long umax = 1;
+    for (long u : ub) umax = std::max(umax, u);
+    if ((long)fl.size() < umax) {
+      fl.alloc(umax, s);
+      rank.alloc(umax, s);
+    }
+    size_t bytes = 0;
+    ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, fl.get(), rank.get(), (int)umax, s));
+    if (scan_tmp.size() < bytes) scan_tmp.alloc(bytes, s);
+    for (int l = l0; l < l1; l++) {
+      const int u = (int)ub[l - l0], un = (int)ub[l - l0 + 1];
+      bsz[l + 1] = bsz[l] / 2;
+      klaunch(k_level_flags_d, div_up(u, TB), TB, 0, s, dlev.get(), l, u, B.nsrc.get(),
+              B.ntarg.get(), p.idivflag, p.ndiv, l < p.nlmin ? 1 : 0, B.iflag.get(), fl.get());
+      size_t tb = scan_tmp.size();
+      ZF_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.get(), tb, fl.get(), rank.get(), u, s));
+      klaunch(k_level_advance, 1, 1, 0, s, dlev.get(), l, u, fl.get(), rank.get(), NC,
+              dnbox.get(), dnref.get());
+      klaunch(k_make_children_d<D>, div_up(u, TB), TB, 0, s, dlev.get(), l, u, fl.get(),
+              rank.get(), bsz[l + 1], B.centers.get(), B.ilevel.get(), B.iparent.get(),
+              B.nchild.get(), B.ichild.get(), B.iflag.get(), B.nsrc.get(), B.ntarg.get());
+      klaunch(k_assign<D>, div_up(ns, TB), TB, 0, s, a_src, ns, pbs.get(), B.ilevel.get(),
+              B.nchild.get(), B.ichild.get(), B.centers.get(), l, B.nsrc.get());
+      if (same)  // targets are the sources: the same children, the same counts
+        klaunch(k_copy_level, div_up(std::max(un, 1), TB), TB, 0, s, dlev.get(), l + 1, un,
+                B.nsrc.get(), B.ntarg.get());
+      else
+        klaunch(k_assign<D>, div_up(nt, TB), TB, 0, s, a_targ, nt, pbt.get(), B.ilevel.get(),
+                B.nchild.get(), B.ichild.get(), B.centers.get(), l, B.ntarg.get());
+      ZF_LAUNCH_CHECK();
+    }
+    // counts of the chunk's levels, the ranges of levels l0+1 .. l1, the box count
+    const int nl = l1 - l0;
+    ZF_CUDA(cudaMemcpyAsync(hw, dnref.get() + l0, nl * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaMemcpyAsync(hw + nl, dlev.get() + 2 * (l0 + 1), 2 * nl * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaMemcpyAsync(hw + 3 * nl, dnbox.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ZF_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < nl && nlevels < 0; k++)
+      if (hw[k] == 0) nlevels = l0 + k;
+    n = hw[3 * nl];
+    nb_cur = hw[nl + 2 * nl - 1] - hw[nl + 2 * nl - 2] + 1;
+    l0 = l1;
+  }
+  if (nlevels < 0) nlevels = p.nlmax;
+  std::vector<int> laddr(2 * (nlevels + 1));
+  ZF_CUDA(cudaMemcpyAsync(laddr.data(), dlev.get(), laddr.size() * sizeof(int),
+                          cudaMemcpyDeviceToHost, s));
+  ZF_CUDA(cudaStreamSynchronize(s));
   pbs.release();
   pbt.release();
   zs_src.release();
