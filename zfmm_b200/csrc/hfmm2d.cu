@@ -1078,68 +1078,113 @@ __global__ void __launch_bounds__(128) k_hl2t(int nt, HelmArgs A, const int* tgt
   }
 }
 
-// M2T (zh2devalmp) over list 3, one thread per target, added to what L2T
-// wrote (in the reference's order: L2T, then the list-3 boxes in list order);
-// a separate kernel so that the L2T sweep runs without the list-3 loop's
-// divergence and registers.
-template <bool GRAD>
-__global__ void __launch_bounds__(128) k_hm2t(int nt, HelmArgs A, const int* tgtleaf,
-                                              const int* nl3, const int* l3, int m3,
-                                              zdc* potsort, zdc* gradsort) {
+// M2T (zh2devalmp) over list 3, added to what L2T wrote.  The (target,
+// list-3 box) pairs are numbered target by target in list order (boxes
+// without sources left out, as the reference skips them); one thread per pair
+// evaluates the box's multipole expansion at the target into scratch, then
+// one thread per target adds its pairs in order.  Lanes of a warp thus never
+// wait on a neighbour's longer list.
+__global__ void k_m2t_count(int nt, HelmArgs A, const int* tgtleaf, const int* nl3,
+                            const int* l3, int m3, int* cnt) {
   int ti = blockIdx.x * blockDim.x + threadIdx.x;
   if (ti >= nt) return;
-  int b = tgtleaf[ti];
+  int b = tgtleaf[ti], c = 0;
+  if (b >= 0)
+    for (int il = 0; il < nl3[b]; il++) {
+      int jb = l3[(size_t)b * m3 + il];
+      c += A.isrcse[2 * jb + 1] >= A.isrcse[2 * jb] ? 1 : 0;
+    }
+  cnt[ti] = c;
+}
+
+__global__ void k_m2t_fill(int nt, HelmArgs A, const int* tgtleaf, const int* nl3,
+                           const int* l3, int m3, const int* off, int2* pairs) {
+  int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= nt) return;
+  int b = tgtleaf[ti], k = off[ti];
   if (b < 0) return;
-  int n3 = nl3[b];
-  if (n3 == 0) return;
-  zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
+  for (int il = 0; il < nl3[b]; il++) {
+    int jb = l3[(size_t)b * m3 + il];
+    if (A.isrcse[2 * jb + 1] >= A.isrcse[2 * jb]) pairs[k++] = make_int2(ti, jb);
+  }
+}
+
+// one (target, box) pair: vals[q * W ...] = pot (and the two gradient parts),
+// used[q] = 0 when the pair contributes nothing (|zk R| below 1e-200)
+template <bool GRAD>
+__global__ void __launch_bounds__(128) k_m2t_pairs(long npairs, HelmArgs A, const int2* pairs,
+                                                   zdc* vals, int* used) {
+  constexpr int W = GRAD ? 3 : 1;
+  long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (q >= npairs) return;
+  const int ti = pairs[q].x, jb = pairs[q].y;
+  const zdc x1 = ldz(&A.ztarg[2 * ti]), x2 = ldz(&A.ztarg[2 * ti + 1]);
+  int lj = A.ilevel[jb], p = A.T.p[lj];
+  double rs = A.T.rs[lj];
+  const zdc* M = expo(A, A.mp, jb);
+  zdc zr, ei;
+  zdc a1 = x1 - A.zcsrc[2 * jb], a2 = x2 - A.zcsrc[2 * jb + 1];
+  polar(a1, a2, zr, ei);
+  zdc z = zr * A.zk;
+  if (zabs(z) < 1e-200) {
+    used[q] = 0;
+    return;
+  }
+  // streaming forward recurrence of H_n
+  zdc h0, h1;
+  hank01(z, h0, h1);
+  zdc iei = zinv(ei), zi1 = zinv(z), zi = rs * zi1;
+  double sc2 = rs * rs;
+  const double irs = 1.0 / rs;
+  zdc hm1 = mkz(0.0), h = h0, hp = h1 * rs;  // scaled H_{n-1}, H_n, H_{n+1}
+  zdc eip = mkz(1.0), eim = mkz(1.0);
+  zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
+  for (int n = 0; n <= p; n++) {
+    zdc cp = ldz(&M[n]) * eip;
+    zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&M[-n]) * eim);
+    sp += (cp + cm) * h;
+    if (GRAD) {
+      zdc hd = n == 0 ? -(hp * irs) : rs * hm1 - ((double)n * zi1) * h;
+      srad += (cp + cm) * hd;
+      sang += ((double)n * zmul_i(cp - cm)) * h;
+    }
+    zdc hn = ((2.0 * (n + 1)) * zi) * hp - sc2 * h;
+    hm1 = h;
+    h = hp;
+    hp = hn;
+    eip = eip * ei;
+    eim = eim * iei;
+  }
+  used[q] = 1;
+  vals[q * W] = sp;
+  if (GRAD) {
+    zdc vr1 = a1 / zr, vr2 = a2 / zr;
+    zdc rad = srad * A.zk, ang = sang / zr;
+    vals[q * W + 1] = rad * vr1 - ang * vr2;
+    vals[q * W + 2] = rad * vr2 + ang * vr1;
+  }
+}
+
+// the pairs of every target added to its entry, in list order
+template <bool GRAD>
+__global__ void k_m2t_sum(int nt, const int* off, const zdc* vals, const int* used,
+                          zdc* potsort, zdc* gradsort) {
+  constexpr int W = GRAD ? 3 : 1;
+  int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= nt) return;
+  const int q0 = off[ti], q1 = off[ti + 1];
+  if (q1 == q0) return;
   zdc pot = potsort[ti], g1 = mkz(0.0), g2 = mkz(0.0);
   if (GRAD) {
     g1 = gradsort[2 * ti];
     g2 = gradsort[2 * ti + 1];
   }
-  // streaming forward recurrence of H_n
-  for (int il = 0; il < n3; il++) {
-    int jb = l3[(size_t)b * m3 + il];
-    if (A.isrcse[2 * jb + 1] < A.isrcse[2 * jb]) continue;
-    int lj = A.ilevel[jb], p = A.T.p[lj];
-    double rs = A.T.rs[lj];
-    const zdc* M = expo(A, A.mp, jb);
-    zdc zr, ei;
-    zdc a1 = x1 - A.zcsrc[2 * jb], a2 = x2 - A.zcsrc[2 * jb + 1];
-    polar(a1, a2, zr, ei);
-    zdc z = zr * A.zk;
-    if (zabs(z) < 1e-200) continue;
-    zdc h0, h1;
-    hank01(z, h0, h1);
-    zdc iei = zinv(ei), zi1 = zinv(z), zi = rs * zi1;
-    double sc2 = rs * rs;
-    const double irs = 1.0 / rs;
-    zdc hm1 = mkz(0.0), h = h0, hp = h1 * rs;  // scaled H_{n-1}, H_n, H_{n+1}
-    zdc eip = mkz(1.0), eim = mkz(1.0);
-    zdc sp = mkz(0.0), srad = mkz(0.0), sang = mkz(0.0);
-    for (int n = 0; n <= p; n++) {
-      zdc cp = ldz(&M[n]) * eip;
-      zdc cm = n == 0 ? mkz(0.0) : sgn(n) * (ldz(&M[-n]) * eim);
-      sp += (cp + cm) * h;
-      if (GRAD) {
-        zdc hd = n == 0 ? -(hp * irs) : rs * hm1 - ((double)n * zi1) * h;
-        srad += (cp + cm) * hd;
-        sang += ((double)n * zmul_i(cp - cm)) * h;
-      }
-      zdc hn = ((2.0 * (n + 1)) * zi) * hp - sc2 * h;
-      hm1 = h;
-      h = hp;
-      hp = hn;
-      eip = eip * ei;
-      eim = eim * iei;
-    }
-    pot += sp;
+  for (int q = q0; q < q1; q++) {
+    if (!used[q]) continue;
+    pot += vals[(long)q * W];
     if (GRAD) {
-      zdc vr1 = a1 / zr, vr2 = a2 / zr;
-      zdc rad = srad * A.zk, ang = sang / zr;
-      g1 += rad * vr1 - ang * vr2;
-      g2 += rad * vr2 + ang * vr1;
+      g1 += vals[(long)q * W + 1];
+      g2 += vals[(long)q * W + 2];
     }
   }
   potsort[ti] = pot;
@@ -1275,6 +1320,11 @@ struct Helm2DPrep {
   // P2M / P2L column layout: leaf box of every source; per box the number of
   // columns and the first column entry (P2M: own sources; P2L: list-4 sources)
   DevBuf<int> srcleaf, tgtleaf;  // leaf box of every sorted source / target
+  // M2T pairs (target, list-3 box with sources): those of target t are
+  // m2t_pairs[m2t_off[t] .. m2t_off[t+1])
+  DevBuf<int> m2t_off;
+  DevBuf<int2> m2t_pairs;
+  long m2t_total = 0;
   DevBuf<long long> p2m_cnt, p2m_base, p2l_cnt, p2l_off, p2l_base;
   long long p2m_total = 0, p2l_nq = 0, p2l_total = 0;
   int ns = 0, nt = 0;
@@ -1389,6 +1439,22 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
   H->tgtleaf.alloc(ntg, s);
   H->tgtleaf.fill_bytes(0xff);
   klaunch(k_tgt_leaf, div_up(nb, 128), 128, 0, s, nb, A, H->tgtleaf.get());
+  H->m2t_off.alloc(ntg + 1, s);
+  {
+    DevBuf<int> cnt(std::max(ntg, 1), s);
+    if (ntg > 0) {
+      klaunch(k_m2t_count, div_up(ntg, 128), 128, 0, s, ntg, A, H->tgtleaf.get(), L.n[2].get(),
+              L.list[2].get(), L.mn[2], cnt.get());
+      size_t bytes = 0;
+      ZF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.get(), H->m2t_off.get(), ntg, s));
+      DevBuf<char> tmp(bytes, s);
+      ZF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, cnt.get(), H->m2t_off.get(), ntg,
+                                            s));
+      klaunch(k_last_plus, 1, 1, 0, s, H->m2t_off.get(), cnt.get(), ntg, H->m2t_off.get() + ntg);
+    } else {
+      H->m2t_off.zero();
+    }
+  }
   H->p2m_cnt.alloc(nb, s);
   H->p2l_cnt.alloc(nb, s);
   H->p2m_base.alloc(nb, s);
@@ -1408,6 +1474,9 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
     std::vector<int> p0h(nlev + 2);
     ZF_CUDA(cudaMemcpyAsync(p0h.data(), dout.get(), p0h.size() * sizeof(int),
                             cudaMemcpyDeviceToHost, s));
+    int m2t_n = 0;
+    ZF_CUDA(cudaMemcpyAsync(&m2t_n, H->m2t_off.get() + ntg, sizeof(int), cudaMemcpyDeviceToHost,
+                            s));
     H->m2l_box0.assign(nlev + 2, 0);
     ZF_CUDA(cudaMemcpyAsync(H->m2l_box0.data(), dbox0.get(), (nlev + 2) * sizeof(int),
                             cudaMemcpyDeviceToHost, s));
@@ -1416,6 +1485,11 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
     H->p2l_nq = t3[1];
     H->p2l_total = t3[2];
     p0.swap(p0h);
+    H->m2t_total = m2t_n;
+    H->m2t_pairs.alloc(std::max(1, m2t_n), s);
+    if (m2t_n > 0)
+      klaunch(k_m2t_fill, div_up(ntg, 128), 128, 0, s, ntg, A, H->tgtleaf.get(), L.n[2].get(),
+              L.list[2].get(), L.mn[2], H->m2t_off.get(), H->m2t_pairs.get());
   }
   // table layout: M2L tables of levels 2..nlev, then the M2M / L2L tables of
   // the children of levels 2..nlev-1
@@ -1638,19 +1712,26 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   const int ntt = H.nt;
   if (!(stages & ST_DOWN)) {
   } else {
-    auto eval = [&](auto l2t, auto m2t, auto p2p) {
+    auto eval = [&](auto l2t, auto m2t, auto msum, auto p2p) {
       tuned_launch(ifpgh > 1 ? "k_hl2t_g" : "k_hl2t", ntt, 128, {64, 128}, [&](int bs) {
         klaunch(l2t, div_up(ntt, bs), bs, 0, s, ntt, A, H.tgtleaf.get(), potsort, gradsort);
       }, s);
       // M2T and P2P add to what L2T wrote (their block sizes are fixed: tuning
       // would have to restore the L2T results before every trial)
-      klaunch(m2t, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[2].get(),
-              L.list[2].get(), L.mn[2], potsort, gradsort);
+      if (H.m2t_total > 0) {
+        const int W = ifpgh > 1 ? 3 : 1;
+        DevBuf<zdc> vals((size_t)H.m2t_total * W, s);
+        DevBuf<int> used(H.m2t_total, s);
+        klaunch(m2t, div_up(H.m2t_total, 128L), 128, 0, s, H.m2t_total, A, H.m2t_pairs.get(),
+                vals.get(), used.get());
+        klaunch(msum, div_up(ntt, 128), 128, 0, s, ntt, H.m2t_off.get(),
+                (const zdc*)vals.get(), (const int*)used.get(), potsort, gradsort);
+      }
       klaunch(p2p, div_up(ntt, 128), 128, 0, s, ntt, A, H.tgtleaf.get(), L.n[0].get(),
               L.list[0].get(), L.mn[0], potsort, gradsort);
     };
-    if (ifpgh > 1) eval(k_hl2t<true>, k_hm2t<true>, k_hp2p<true>);
-    else eval(k_hl2t<false>, k_hm2t<false>, k_hp2p<false>);
+    if (ifpgh > 1) eval(k_hl2t<true>, k_m2t_pairs<true>, k_m2t_sum<true>, k_hp2p<true>);
+    else eval(k_hl2t<false>, k_m2t_pairs<false>, k_m2t_sum<false>, k_hp2p<false>);
   }
   ZF_LAUNCH_CHECK();
 }

@@ -452,6 +452,12 @@ __global__ void k_updateflags(int lo, int hi, double distest, const int* nchild,
   iflag[b] = f;
 }
 
+// boxes per level whose flag is 3 (to be checked by the second pass)
+__global__ void k_count_flag3(int n, const int* ilevel, const int* iflag, int* cnt) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n && iflag[b] == 3) atomicAdd(&cnt[ilevel[b]], 1);
+}
+
 __global__ void k_reset_flags(int n, int* iflag) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < n && iflag[b] != 3) iflag[b] = 0;
@@ -1017,8 +1023,26 @@ void build_tree_t(const double* d_src, int ns, const double* d_targ, int nt, con
     colleagues_all<D>(B, nlevels, laddr, bsz, p.isep, mnbors, ncoll, coll, s);
 
     klaunch(k_reset_flags, div_up(n, TB), TB, 0, s, n, B.iflag.get());
+    // a level changes nothing unless some of its boxes have flag 3 or the
+    // level above added boxes to it (its tail): the others are skipped
+    // without a launch or a wait (flags of existing boxes change only when
+    // their own level is processed)
+    std::vector<int> nflag3(nlevels + 1, 0);
+    {
+      DevBuf<int> c3(nlevels + 1, s);
+      c3.zero();
+      klaunch(k_count_flag3, div_up(n, TB), TB, 0, s, n, B.ilevel.get(), B.iflag.get(), c3.get());
+      ZF_CUDA(cudaMemcpyAsync(nflag3.data(), c3.get(), (nlevels + 1) * sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+      ZF_CUDA(cudaStreamSynchronize(s));
+    }
     for (int l = 0; l <= nlevels; l++) { tail[2 * l] = 0; tail[2 * l + 1] = -1; }
     for (int l = 2; l <= nlevels - 2; l++) {
+      if (nflag3[l] == 0 && tail[2 * l + 1] < tail[2 * l]) {
+        tail[2 * (l + 1)] = n;
+        tail[2 * (l + 1) + 1] = n - 1;
+        continue;
+      }
       double distest = 1.05 * (bsz[l] + bsz[l + 1]) / 2.0;
       distest = distest * p.isep;
       int lo = laddr[2 * l], hi = laddr[2 * l + 1];
