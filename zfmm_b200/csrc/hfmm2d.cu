@@ -1202,7 +1202,7 @@ __global__ void k_m2t_sum(int nt, const int* off, const zdc* vals, const int* us
 // so lanes of different leaves in one warp cost the larger of their source
 // counts rather than a sum over the boxes of the larger box.
 template <bool GRAD>
-__global__ void __launch_bounds__(128, 3) k_hp2p(int nt, HelmArgs A, const int* tgtleaf,
+__global__ void __launch_bounds__(128, 4) k_hp2p(int nt, HelmArgs A, const int* tgtleaf,
                                                  const int* nl1, const int* l1, int m1,
                                                  zdc* potsort, zdc* gradsort) {
   int ti = blockIdx.x * blockDim.x + threadIdx.x;
