@@ -1112,7 +1112,7 @@ __global__ void k_m2t_fill(int nt, HelmArgs A, const int* tgtleaf, const int* nl
 // one (target, box) pair: vals[q * W ...] = pot (and the two gradient parts),
 // used[q] = 0 when the pair contributes nothing (|zk R| below 1e-200)
 template <bool GRAD>
-__global__ void __launch_bounds__(128) k_m2t_pairs(long npairs, HelmArgs A, const int2* pairs,
+__global__ void __launch_bounds__(128, 5) k_m2t_pairs(long npairs, HelmArgs A, const int2* pairs,
                                                    zdc* vals, int* used) {
   constexpr int W = GRAD ? 3 : 1;
   long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
