@@ -379,6 +379,13 @@ double zfmm_probe_dmma_tflops(int iters);
 
 /* Last error message of this host thread ("" when none). */
 const char *zfmm_last_error(void);
+
+/* Failure injection for tests (no reference counterpart): after
+ * zfmm_fail_alloc_after(n) the library's (n+1)-th following device
+ * allocation fails as an out-of-memory would (status 3, ZF_ERR_NOMEM, from
+ * the call that made it; the memory it had taken is returned), and the
+ * injection ends.  n < 0 switches it off. */
+void zfmm_fail_alloc_after(long n);
 /* Library version string. */
 const char *zfmm_version(void);
 

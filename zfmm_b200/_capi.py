@@ -135,6 +135,7 @@ SIGNATURES = {
     "zfmm_probe_fp64_tflops": (c_double, [c_int]),
     "zfmm_probe_dmma_tflops": (c_double, [c_int]),
     "zfmm_last_error": (ctypes.c_char_p, []),
+    "zfmm_fail_alloc_after": (None, [ctypes.c_long]),
     "zfmm_version": (ctypes.c_char_p, []),
 }
 

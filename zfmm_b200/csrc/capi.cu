@@ -42,6 +42,15 @@ std::mutex g_pool_mu;
 cudaMemPool_t g_pools[kMaxDev] = {};
 }  // namespace
 
+std::atomic<long> g_fail_after{-1};  // allocations left before the injected failure
+
+bool inject_alloc_failure() {
+  long v = g_fail_after.load(std::memory_order_relaxed);
+  while (v >= 0)  // count down; the allocation that finds 0 fails and ends it
+    if (g_fail_after.compare_exchange_weak(v, v == 0 ? -1 : v - 1)) return v == 0;
+  return false;
+}
+
 cudaMemPool_t pool() {
   int dev = 0;
   ZF_CUDA(cudaGetDevice(&dev));
@@ -128,12 +137,15 @@ class StrengthUpload {
  public:
   StrengthUpload(HostIn& h, int ns, int dim, int ifcharge, const double* charge, int ifdipole,
                  const double* dipstr, const double* dipvec, cudaStream_t s) {
-    ZF_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
-    ZF_CUDA(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
-    if (ifcharge == 1) h.charge.alloc(ns, s);
+    if (ifcharge == 1) h.charge.alloc(ns, s);  // may throw: nothing created yet
     if (ifdipole == 1) {
       h.dipstr.alloc(ns, s);
       h.dipvec.alloc((size_t)dim * ns, s);
+    }
+    ZF_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
+    if (cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming) != cudaSuccess) {
+      cudaStreamDestroy(aux_);
+      throw zf_error(ZF_ERR_CUDA, "cudaEventCreateWithFlags failed");
     }
     ZF_CUDA(cudaEventRecord(ev_, s));  // the buffers exist from here on
     ZF_CUDA(cudaStreamWaitEvent(aux_, ev_, 0));
@@ -297,6 +309,7 @@ int fmm2d_host(double eps, const zdc* zk, int ns, const double* zsrc, int ifchar
 extern "C" {
 
 const char* zfmm_last_error(void) { return g_err.c_str(); }
+void zfmm_fail_alloc_after(long n) { g_fail_after.store(n < 0 ? -1 : n); }
 const char* zfmm_version(void) { return "zfmm_b200 0.1 (sm_100a)"; }
 void zfmm_set_step_timing(int on) { g_timing = on; }
 

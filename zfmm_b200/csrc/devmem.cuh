@@ -30,6 +30,16 @@ enum Status {
 // the calling thread's current device's pool (created on first use)
 cudaMemPool_t pool();
 
+// Allocation-failure injection (zfmm_fail_alloc_after): true when this
+// allocation is the one chosen to fail, which then reports
+// cudaErrorMemoryAllocation without calling the allocator.
+bool inject_alloc_failure();
+
+inline cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  if (inject_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(p, bytes, pool(), s);
+}
+
 inline void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
     int code = (e == cudaErrorMemoryAllocation) ? ZF_ERR_NOMEM : ZF_ERR_CUDA;
@@ -56,13 +66,13 @@ class DevBuf {
     release();
     s_ = s;
     n_ = n;
-    if (n) ZF_CUDA(cudaMallocFromPoolAsync((void**)&p_, n * sizeof(T), pool(), s));
+    if (n) ZF_CUDA(pool_alloc((void**)&p_, n * sizeof(T), s));
   }
   // grow to at least n elements keeping the first `keep` elements
   void grow(size_t n, size_t keep) {
     if (n <= n_) return;
     T* q = nullptr;
-    ZF_CUDA(cudaMallocFromPoolAsync((void**)&q, n * sizeof(T), pool(), s_));
+    ZF_CUDA(pool_alloc((void**)&q, n * sizeof(T), s_));
     if (keep && p_) ZF_CUDA(cudaMemcpyAsync(q, p_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s_));
     if (p_) cudaFreeAsync(p_, s_);
     p_ = q;

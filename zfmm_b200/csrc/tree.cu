@@ -455,7 +455,13 @@ __global__ void k_updateflags(int lo, int hi, double distest, const int* nchild,
 // boxes per level whose flag is 3 (to be checked by the second pass)
 __global__ void k_count_flag3(int n, const int* ilevel, const int* iflag, int* cnt) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < n && iflag[b] == 3) atomicAdd(&cnt[ilevel[b]], 1);
+  const bool f = b < n && iflag[b] == 3;
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if (!f) return;
+  // consecutive boxes share a level: one atomic per level present in the warp
+  const int lv = ilevel[b];
+  const unsigned grp = __match_any_sync(m, lv);
+  if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&cnt[lv], __popc(grp));
 }
 
 __global__ void k_reset_flags(int n, int* iflag) {
