@@ -315,7 +315,8 @@ __device__ __forceinline__ void src_coeffs(const HelmArgs& A, const SrcTerm& t, 
 // backward recurrence (coefficients emitted from m = p down to 0); returns
 // Miller's normalisation factor of the column, which the column sum applies
 // (a rescaling here would read and write the column a second time)
-__device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col) {
+__device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col,
+                          long cs) {
   zdc a1 = ldz(&A.zsrc[2 * j]) - c1, a2 = ldz(&A.zsrc[2 * j + 1]) - c2;
   zdc rzk, ez;
   polar(a1, a2, rzk, ez);
@@ -327,8 +328,8 @@ __device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, i
       zdc fder = m == 1 ? mkz(0.5 / rs) : mkz(0.0);
       zdc cp, cn;
       src_coeffs(A, t, m, fm, fder, mkz(1.0), mkz(1.0), cp, cn);
-      col[p + m] = cp;
-      if (m) col[p - m] = cn;
+      col[(p + m) * cs] = cp;
+      if (m) col[(p - m) * cs] = cn;
     }
     return mkz(1.0);
   }
@@ -347,8 +348,8 @@ __device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, i
       zdc fder = n == 0 ? (-rs) * gp1 : (0.5 / rs) * gm1 - (0.5 * rs) * gp1;
       zdc cp, cn;
       src_coeffs(A, t, n, g, fder, em, ep, cp, cn);
-      col[p + n] = cp;
-      if (n) col[p - n] = cn;
+      col[(p + n) * cs] = cp;
+      if (n) col[(p - n) * cs] = cn;
       ep = ep * iez;
       em = em * ez;
     }
@@ -364,8 +365,8 @@ __device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, i
         gp1 = 1e-200 * gp1;
         psi = 1e-200 * psi;
         for (int m = n; m <= p; m++) {
-          col[p + m] = 1e-200 * col[p + m];
-          if (m) col[p - m] = 1e-200 * col[p - m];
+          col[(p + m) * cs] = 1e-200 * col[(p + m) * cs];
+          if (m) col[(p - m) * cs] = 1e-200 * col[(p - m) * cs];
         }
       }
     }
@@ -377,14 +378,15 @@ __device__ zdc p2m_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, i
 
 // P2L column of source j about centre (c1, c2): Hankel functions by the
 // forward recurrence (h2dall), coefficients emitted from m = 0 up to p
-__device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col) {
+__device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, int p, zdc* col,
+                           long cs) {
   zdc a1 = ldz(&A.zsrc[2 * j]) - c1, a2 = ldz(&A.zsrc[2 * j + 1]) - c2;
   zdc rzk, ez;
   polar(a1, a2, rzk, ez);
   SrcTerm t = src_term(A, j, a1, a2, rzk);
   zdc z = rzk * A.zk;
   if (zabs(z) < 1e-200) {  // h2dall's zero table
-    for (int i = 0; i <= 2 * p; i++) col[i] = mkz(0.0);
+    for (int i = 0; i <= 2 * p; i++) col[i * cs] = mkz(0.0);
     return;
   }
   zdc h0, h1;
@@ -398,8 +400,8 @@ __device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
     zdc fder = m == 0 ? -(fp1 * irs) : rs * fm1 - ((double)m * t.izk) * f;
     zdc cp, cn;
     src_coeffs(A, t, m, f, fder, em, ep, cp, cn);
-    col[p + m] = cp;
-    if (m) col[p - m] = cn;
+    col[(p + m) * cs] = cp;
+    if (m) col[(p - m) * cs] = cn;
     zdc fn = ((2.0 * (m + 1)) * zi) * fp1 - sc2 * f;
     fm1 = f;
     f = fp1;
@@ -410,8 +412,10 @@ __device__ void p2l_column(const HelmArgs& A, int j, zdc c1, zdc c2, double rs, 
 }
 
 // The columns of a pass live in global scratch: colbase[b] is the first
-// column entry of box b (P2M: the box's own sources; P2L: the sources of its
-// list-4 boxes in list order), (2p+1) entries per source.
+// entry of box b's block (P2M: the box's own sources; P2L: the sources of its
+// list-4 boxes in list order), stored coefficient-major: coefficient i of the
+// box's k-th column at colbase[b] + i n_b + k (n_b columns), so the threads of
+// neighbouring sources store to neighbouring addresses.
 
 // leaf box of every source of a leaf of level >= 2 (-1 otherwise): the P2M
 // centres, one thread per box
@@ -450,6 +454,7 @@ __global__ void k_form_counts(int nb, HelmArgs A, const int* nl4, const int* l4,
 
 // P2M columns, one thread per source
 __global__ void __launch_bounds__(128) k_p2m_cols(int ns, HelmArgs A, const int* srcleaf,
+                                                  const long long* colcnt,
                                                   const long long* colbase, zdc* cols,
                                                   zdc* colscale) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -457,8 +462,9 @@ __global__ void __launch_bounds__(128) k_p2m_cols(int ns, HelmArgs A, const int*
   int b = srcleaf[j];
   if (b < 0) return;
   int l = A.ilevel[b], p = A.T.p[l];
-  zdc* col = cols + colbase[b] + (long long)(j - A.isrcse[2 * b]) * (2 * p + 1);
-  colscale[j] = p2m_column(A, j, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, col);
+  zdc* col = cols + colbase[b] + (j - A.isrcse[2 * b]);
+  colscale[j] =
+      p2m_column(A, j, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, col, (long)colcnt[b]);
 }
 
 // box of flattened index q: the last box in [lo, hi] with off[box] <= q
@@ -474,7 +480,7 @@ __device__ __forceinline__ int search_box(const long long* off, int lo, int hi, 
 // P2L columns, one thread per (target box, list-4 source) in list order
 __global__ void __launch_bounds__(128) k_p2l_cols(long long nq, int b0, int b1, HelmArgs A,
                                                   const long long* off4, const int* nl4,
-                                                  const int* l4, int m4,
+                                                  const int* l4, int m4, const long long* colcnt,
                                                   const long long* colbase, zdc* cols) {
   long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (q >= nq) return;
@@ -493,8 +499,8 @@ __global__ void __launch_bounds__(128) k_p2l_cols(long long nq, int b0, int b1, 
   }
   if (j < 0) return;
   int l = A.ilevel[b], p = A.T.p[l];
-  zdc* col = cols + colbase[b] + (q - off4[b]) * (2 * p + 1);
-  p2l_column(A, j, A.zctarg[2 * b], A.zctarg[2 * b + 1], A.T.rs[l], p, col);
+  zdc* col = cols + colbase[b] + (q - off4[b]);
+  p2l_column(A, j, A.zctarg[2 * b], A.zctarg[2 * b + 1], A.T.rs[l], p, col, (long)colcnt[b]);
 }
 
 // sums of the columns of every box of one level: warps loop over the boxes, R register
@@ -522,7 +528,7 @@ __global__ void __launch_bounds__(32 * WPB) k_form_sum(int lo, int hi, HelmArgs 
 #pragma unroll
       for (int r = 0; r < R; r++) {
         int i = lane + 32 * r;
-        if (i < P2) acc[r] += LOCAL ? ldz(&c[k * P2 + i]) : ldz(&c[k * P2 + i]) * sc;
+        if (i < P2) acc[r] += LOCAL ? ldz(&c[i * n + k]) : ldz(&c[i * n + k]) * sc;
       }
     }
     zdc* E = expo(A, LOCAL ? A.loc : A.mp, b) - p;
@@ -1597,7 +1603,7 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
     if (H.ns > 0)
       tuned_launch("k_p2m_cols", H.ns, 128, {32, 64, 128}, [&](int bs) {
         klaunch(k_p2m_cols, div_up(H.ns, bs), bs, 0, s, H.ns, A, H.srcleaf.get(),
-                H.p2m_base.get(), cols.get(), colscale.get());
+                H.p2m_cnt.get(), H.p2m_base.get(), cols.get(), colscale.get());
       }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
@@ -1667,8 +1673,8 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
     DevBuf<zdc> cols(H.p2l_total, s);
     tuned_launch("k_p2l_cols", H.p2l_nq, 128, {32, 64, 128}, [&](int bs) {
       klaunch(k_p2l_cols, div_up(H.p2l_nq, bs), bs, 0, s, H.p2l_nq, 0, nb - 1, A,
-              H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_base.get(),
-              cols.get());
+              H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_cnt.get(),
+              H.p2l_base.get(), cols.get());
     }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
