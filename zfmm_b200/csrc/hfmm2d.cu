@@ -467,37 +467,26 @@ __global__ void __launch_bounds__(128) k_p2m_cols(int ns, HelmArgs A, const int*
       p2m_column(A, j, A.zcsrc[2 * b], A.zcsrc[2 * b + 1], A.T.rs[l], p, col, (long)colcnt[b]);
 }
 
-// box of flattened index q: the last box in [lo, hi] with off[box] <= q
-__device__ __forceinline__ int search_box(const long long* off, int lo, int hi, long long q) {
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (off[mid] <= q) lo = mid;
-    else hi = mid - 1;
+// the (target box, list-4 source) pairs of the P2L columns, box by box in
+// list order (pairs[off4[b] + k] = (b, source)), one thread per box
+__global__ void k_p2l_pair_fill(int nb, HelmArgs A, const long long* cnt4, const long long* off4,
+                                const int* nl4, const int* l4, int m4, int2* pairs) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb || cnt4[b] == 0) return;
+  long long k = off4[b];
+  for (int il = 0; il < nl4[b]; il++) {
+    int jb = l4[(size_t)b * m4 + il];
+    for (int j = A.isrcse[2 * jb]; j <= A.isrcse[2 * jb + 1]; j++) pairs[k++] = make_int2(b, j);
   }
-  return lo;
 }
 
-// P2L columns, one thread per (target box, list-4 source) in list order
-__global__ void __launch_bounds__(128) k_p2l_cols(long long nq, int b0, int b1, HelmArgs A,
-                                                  const long long* off4, const int* nl4,
-                                                  const int* l4, int m4, const long long* colcnt,
+// P2L columns, one thread per (target box, list-4 source) pair
+__global__ void __launch_bounds__(128) k_p2l_cols(long long nq, HelmArgs A, const int2* pairs,
+                                                  const long long* off4, const long long* colcnt,
                                                   const long long* colbase, zdc* cols) {
   long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (q >= nq) return;
-  int b = search_box(off4, b0, b1, q);
-  long long r = q - off4[b];
-  int j = -1;
-  for (int il = 0; il < nl4[b]; il++) {
-    int jb = l4[(size_t)b * m4 + il];
-    int s0 = A.isrcse[2 * jb], n = A.isrcse[2 * jb + 1] - s0 + 1;
-    if (n <= 0) continue;
-    if (r < n) {
-      j = s0 + (int)r;
-      break;
-    }
-    r -= n;
-  }
-  if (j < 0) return;
+  const int b = pairs[q].x, j = pairs[q].y;
   int l = A.ilevel[b], p = A.T.p[l];
   zdc* col = cols + colbase[b] + (q - off4[b]);
   p2l_column(A, j, A.zctarg[2 * b], A.zctarg[2 * b + 1], A.T.rs[l], p, col, (long)colcnt[b]);
@@ -1332,6 +1321,7 @@ struct Helm2DPrep {
   DevBuf<int2> m2t_pairs;
   long m2t_total = 0;
   DevBuf<long long> p2m_cnt, p2m_base, p2l_cnt, p2l_off, p2l_base;
+  DevBuf<int2> p2l_pairs;  // (target box, list-4 source) of every P2L column
   long long p2m_total = 0, p2l_nq = 0, p2l_total = 0;
   int ns = 0, nt = 0;
   long tot = 0;
@@ -1491,6 +1481,10 @@ Helm2DPrepPtr helm2d_prepare(const Setup2D& S, double eps, zdc zk, int isep, cud
     H->p2l_nq = t3[1];
     H->p2l_total = t3[2];
     p0.swap(p0h);
+    H->p2l_pairs.alloc(std::max(1LL, H->p2l_nq), s);
+    if (H->p2l_nq > 0)
+      klaunch(k_p2l_pair_fill, div_up(nb, 128), 128, 0, s, nb, A, H->p2l_cnt.get(),
+              H->p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H->p2l_pairs.get());
     H->m2t_total = m2t_n;
     H->m2t_pairs.alloc(std::max(1, m2t_n), s);
     if (m2t_n > 0)
@@ -1576,7 +1570,7 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
     if (ev) ZF_CUDA(cudaEventRecord(ev[i], s));
   };
   const DevTree& t = S.tree;
-  int nb = t.nboxes, nlev = t.nlevels;
+  const int nlev = t.nlevels;
   HelmArgs A = H.A0;
   const TabArgs& TA = H.TA;
   A.charge = q;
@@ -1672,9 +1666,8 @@ void helm2d_stages(const Setup2D& S, const Helm2DPrep& H, const zdc* q, const zd
   if (H.p2l_nq > 0 && (stages & ST_DOWN)) {
     DevBuf<zdc> cols(H.p2l_total, s);
     tuned_launch("k_p2l_cols", H.p2l_nq, 128, {32, 64, 128}, [&](int bs) {
-      klaunch(k_p2l_cols, div_up(H.p2l_nq, bs), bs, 0, s, H.p2l_nq, 0, nb - 1, A,
-              H.p2l_off.get(), L.n[3].get(), L.list[3].get(), L.mn[3], H.p2l_cnt.get(),
-              H.p2l_base.get(), cols.get());
+      klaunch(k_p2l_cols, div_up(H.p2l_nq, bs), bs, 0, s, H.p2l_nq, A, H.p2l_pairs.get(),
+              H.p2l_off.get(), H.p2l_cnt.get(), H.p2l_base.get(), cols.get());
     }, s);
     for (int l = 2; l <= nlev; l++) {
       int P2 = 2 * A.T.p[l] + 1;
